@@ -1,0 +1,360 @@
+"""Benchmark of the FMM cell-interaction kernels (one JSON line on rank 0).
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+                    [--workload uniform_level3|amr_polytrope] [--precision fp32_split|fp64|fp64_exact]
+
+A step is one gravity solve's interaction work list (every work item of the
+workload) through one batched launch. ``value`` = cell-interactions / s with the
+pool already resident in HBM (device time, CUDA events on the launch stream,
+L2 flushed between steps); ``e2e`` = the same through host buffers (pinned
+H2D of the pool and work list + launch + D2H of L and L_c inside the timed
+region). Under torchrun every rank solves its own copy of the workload
+(independent subgrid sets, no data-path collective: weak scaling); timing is
+the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+from octotiger_b200 import synthetic as syn  # noqa: E402
+from octotiger_b200.layout import DRHODT, RHO  # noqa: E402
+
+METRIC = "FMM cell-interactions/s, 1 B200: batched FP32-split vs plain FP64 at ≤1e-6 err"
+UNIT = "cell-interactions/s"
+
+# Nominal FLOPs per evaluated pair, counted on the reference's templates
+# (compute_kernel_templates.hpp / monopole_kernel_templates.hpp) with every
+# add, mul, div and sqrt counted as one.
+FLOPS_PER_PAIR = {("m2l", RHO): 406, ("m2l", DRHODT): 272, ("p2p", RHO): 12, ("p2p", DRHODT): 12,
+                  ("p2m", RHO): 317, ("p2m", DRHODT): 204}
+
+L2_FLUSH_BYTES = 256 << 20
+
+
+def make_workload(name: str):
+    if name == "uniform_level3":
+        return syn.uniform_level(3)
+    if name == "amr_polytrope":
+        from octotiger_b200 import amr
+        return amr.polytrope_batch()
+    raise SystemExit(f"unknown workload {name}")
+
+
+def pair_counts(batch) -> dict:
+    from oracle.pyoracle import Oracle
+    o = Oracle()
+    total, per_kind = o.count_pairs(batch.theta, batch.pool, batch.items)
+    return {"total": total, "m2l": int(per_kind[0] + per_kind[1]), "p2p": int(per_kind[2]), "p2m": int(per_kind[3])}
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.reader = threading.Thread(target=self._read, daemon=True)
+            self.reader.start()
+            time.sleep(0.3)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            time.sleep(0.2)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference_rate(batch, solve: int, seconds: float = 10.0, nthreads: int | None = None):
+    """The reference's own kernel arithmetic (oracle/_ref, SIMD lanes) on the
+    host cores, repeated over the workload for about ``seconds``."""
+    from oracle.pyoracle import Oracle, RefMath, ref_library_path
+    nthreads = nthreads or os.cpu_count() or 1
+    counts = pair_counts(batch)
+    if ref_library_path() is not None:
+        impl, kind = RefMath(), "reference"
+        run = lambda: impl.batch(batch.theta, batch.pool, batch.items, rho=(solve == RHO), nthreads=nthreads)
+        lanes = impl.simd_width()
+    else:
+        impl, kind = Oracle(), "port"
+        run = lambda: impl.batch(batch.theta, batch.pool, batch.items, rho=(solve == RHO), nthreads=nthreads)
+        lanes = 1
+    run()   # warm-up
+    reps, t0 = 0, time.perf_counter()
+    while True:
+        run()
+        reps += 1
+        el = time.perf_counter() - t0
+        if el >= seconds:
+            break
+    rate = counts["total"] * reps / el
+    sample = (f"{reps} full passes over the {batch.name} work list ({counts['total']} pairs each), "
+              f"{nthreads} host threads, {lanes}-lane SIMD")
+    return {"value": rate, "unit": UNIT, "cores": nthreads, "kind": kind, "sample": sample,
+            "seconds": round(el, 3)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def reference_arm(args) -> None:
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return
+    batch = make_workload(args.workload)
+    solve = RHO if args.gsolve == "rho" else DRHODT
+    from oracle.pyoracle import Oracle, RefMath, ref_library_path
+    nthreads = os.cpu_count() or 1
+    counts = pair_counts(batch)
+    if ref_library_path() is not None:
+        impl, kind, lanes = RefMath(), "reference", None
+        lanes = impl.simd_width()
+    else:
+        impl, kind, lanes = Oracle(), "port", 1
+    run = lambda: impl.batch(batch.theta, batch.pool, batch.items, rho=(solve == RHO), nthreads=nthreads)
+    for _ in range(args.warmup):
+        run()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        run()
+    el = time.perf_counter() - t0
+    value = counts["total"] * args.steps / el
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
+        "config": {"workload": batch.name, "n_subgrids": batch.pool.n, "n_items": int(len(batch.items)),
+                   "pairs_per_step": counts["total"], "theta": batch.theta, "gsolve": args.gsolve},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": nthreads, "kind": kind,
+                         "sample": f"the full work list per step, {nthreads} host threads, {lanes}-lane SIMD "
+                                   "(reference kernel templates, Kokkos host sweep order)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def gpu_arm(args) -> None:
+    import torch
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    from octotiger_b200.otfmm import BatchSolver, Context, DevicePool, measure_fma_peaks, order_work_list
+
+    batch = make_workload(args.workload)
+    solve = RHO if args.gsolve == "rho" else DRHODT
+    counts = pair_counts(batch)
+    ctx = Context(local, batch.theta)
+    solver = BatchSolver(ctx, batch.pool, batch.items)
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+
+    def timed_steps(precision: str, steps: int, warmup: int):
+        for _ in range(warmup):
+            solver.run(solve, precision)
+        torch.cuda.synchronize()
+        total_ms, per = 0.0, []
+        for _ in range(steps):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            solver.run(solve, precision)
+            e1.record(stream)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1)
+            per.append(ms)
+            total_ms += ms
+        solver.ctx.batch_status()
+        return total_ms, per
+
+    # device-resident timing of the headline precision, clocks sampled meanwhile
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        total_ms, per = timed_steps(args.precision, args.steps, args.warmup)
+    if pg:
+        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * counts["total"] * args.steps / (total_ms * 1e-3)
+
+    # the other precisions on the same workload (device-resident, same method)
+    others = {}
+    for prec in args.compare:
+        if prec == args.precision:
+            continue
+        ms, _ = timed_steps(prec, max(3, args.steps // 2), 3)
+        others[prec] = {"value": counts["total"] * max(3, args.steps // 2) / (ms * 1e-3),
+                        "ms_per_step": ms / max(3, args.steps // 2)}
+
+    # end to end: host pool + work list in pinned memory -> GPU -> L, L_c back
+    pin = {k: torch.from_numpy(getattr(batch.pool, k)).pin_memory() for k in ("M", "com", "mon", "is_leaf")}
+    items_h = order_work_list(batch.items)
+    items_pin = torch.from_numpy(items_h.view(np.uint8).reshape(-1).copy()).pin_memory()
+    L_pin = torch.empty(solver.L.shape, dtype=torch.float64).pin_memory()
+    Lc_pin = torch.empty(solver.Lc.shape, dtype=torch.float64).pin_memory()
+    dpool = DevicePool(M=torch.empty_like(solver.dev.M), com=torch.empty_like(solver.dev.com),
+                       mon=torch.empty_like(solver.dev.mon), is_leaf=torch.empty_like(solver.dev.is_leaf),
+                       n=batch.pool.n)
+    ditems = torch.empty_like(solver.items)
+    h2d = sum(t.numel() * t.element_size() for t in pin.values()) + items_pin.numel()
+    d2h = L_pin.numel() * 8 + Lc_pin.numel() * 8
+
+    def e2e_step():
+        dpool.M.copy_(pin["M"], non_blocking=True)
+        dpool.com.copy_(pin["com"], non_blocking=True)
+        dpool.mon.copy_(pin["mon"], non_blocking=True)
+        dpool.is_leaf.copy_(pin["is_leaf"], non_blocking=True)
+        ditems.copy_(items_pin, non_blocking=True)
+        ctx.batch(dpool, ditems, solver.n_items, solver.L, solver.Lc, solve, args.precision)
+        L_pin.copy_(solver.L, non_blocking=True)
+        Lc_pin.copy_(solver.Lc, non_blocking=True)
+
+    for _ in range(args.warmup):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_ms = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        e2e_step()
+        e1.record(stream)
+        e1.synchronize()
+        e2e_ms += e0.elapsed_time(e1)
+    ctx.batch_status()
+    if pg:
+        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * counts["total"] * args.steps / (e2e_ms * 1e-3)
+
+    # roofline: nominal reference FLOPs of one launch / its device time vs the
+    # FP64 FMA issue rate measured on this GPU in this run
+    flops = sum(counts[k] * FLOPS_PER_PAIR[(k, solve)] for k in ("m2l", "p2p", "p2m"))
+    ms_launch = total_ms / args.steps
+    achieved = flops / (ms_launch * 1e-3) / 1e12
+    fp64_peak, fp32_peak = measure_fma_peaks(local)
+    peak = fp32_peak if args.precision == "fp32_split" else fp64_peak
+    roof = {"bound": "fp64_fma" if args.precision != "fp32_split" else "fp32_fma", "achieved": achieved,
+            "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+            "flops_per_launch": flops,
+            "peak_source": "measured in this run: register-resident FMA loop (otfmm_measure_fma_peaks); "
+                           "MEASURED_PEAKS.json has no FP64/FP32 figure",
+            "fp64_peak_tflops": fp64_peak, "fp32_peak_tflops": fp32_peak}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if args.precision != "fp32_split" else "f32+f64",
+        "data": "synthetic (seeded generator)",
+        "config": {"workload": batch.name, "n_subgrids": batch.pool.n, "n_items": int(len(batch.items)),
+                   "pairs_per_step": counts["total"], "pairs_m2l": counts["m2l"], "pairs_p2p": counts["p2p"],
+                   "pairs_p2m": counts["p2m"],
+                   "theta": batch.theta, "gsolve": args.gsolve, "precision": args.precision,
+                   "l2": "flushed (256 MiB write) before every timed step",
+                   "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU"},
+        "precisions": others,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": args.steps,
+        "roofline": roof,
+        "clocks": clk.summary(),
+        "step_ms": [round(x, 4) for x in per],
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_reference_rate(batch, solve, seconds=args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    del solver
+    ctx.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="uniform_level3", choices=["uniform_level3", "amr_polytrope"])
+    ap.add_argument("--precision", default="fp64", choices=["fp32_split", "fp64", "fp64_exact"])
+    ap.add_argument("--compare", nargs="*", default=["fp64", "fp64_exact"])
+    ap.add_argument("--gsolve", default="rho", choices=["rho", "drhodt"])
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,162 @@
+/*
+ * otfmm.h — C ABI of the B200-native FMM cell-interaction kernels for
+ * Octo-Tiger (libotfmm.so).
+ *
+ * These entry points are what a new `interaction_device_kernel_type` backend
+ * inside Octo-Tiger binds. They replace, for one GPU:
+ *   - the multipole (M2L) launch path
+ *     octotiger::fmm::multipole_interactions::launch_interface
+ *     (octotiger/multipole_interactions/kernel/kokkos_kernel.hpp:768-863,
+ *      called from multipole_kernel at :944-983, itself behind
+ *      multipole_kernel_interface, src/multipole_interactions/multipole_kernel_interface.cpp:73-169);
+ *   - the monopole (P2P + P2M) launch path
+ *     octotiger::fmm::monopole_interactions::launch_interface_p2p_p2m / launch_interface_p2p
+ *     (octotiger/monopole_interactions/kernel/kokkos_kernel.hpp:1051-1165,
+ *      called from monopole_kernel at :1279-1354, behind monopole_kernel_interface,
+ *      src/monopole_interactions/monopole_kernel_interface.cpp:97-198);
+ *   - the stencil set-up those paths do on first use
+ *     (get_device_masks / get_device_constants, kokkos_kernel.hpp:58-82 and
+ *      monopole kokkos_kernel.hpp:78-114; calculate_stencil,
+ *      src/multipole_interactions/util/calculate_stencil.cpp:23-160).
+ * Beyond the reference, a batched entry point runs a whole gravity solve's
+ * work list (every refined and leaf subgrid of the octree) in one launch from
+ * subgrid data resident in GPU memory.
+ *
+ * Conventions
+ *   - All functions return an int status: OTFMM_OK (0) or a negative error
+ *     code; otfmm_last_error() gives a message for the calling thread. No C++
+ *     exception crosses this boundary. The reference aborts on misuse
+ *     (multipole_kernel_interface.cpp:107-158); here the caller decides.
+ *   - Thread-safe: a context may be used from several host threads; each call
+ *     is enqueued on the stream the caller passes (cudaStream_t as void*,
+ *     NULL = legacy default stream).
+ *   - Layouts: "SoA" is the reference's per-subgrid kernel layout
+ *     (mon[5832], M[20][5851], com[3][5851] over the 18^3 padded halo;
+ *     L[20][531], L_c[3][531]); "pool" is M[n][20][512], com[n][3][512],
+ *     mon[n][512] per subgrid. Cell order is x-major (x*64 + y*8 + z).
+ *   - Precision: OTFMM_FP64_EXACT reproduces the reference's arithmetic bit
+ *     for bit (IEEE operations in the reference's order, no contraction);
+ *     OTFMM_FP64 is the fast FP64 kernel (fused multiply-adds, reordered
+ *     constants; within 1e-12 of the reference); OTFMM_FP32_SPLIT builds the
+ *     derivative tensors and contracts them in FP32 with FP64 chunk sums,
+ *     and keeps centre-of-mass differences, the angular correction L_c and
+ *     the final accumulation in FP64.
+ */
+#ifndef OTFMM_H
+#define OTFMM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OTFMM_OK 0
+#define OTFMM_ERR_INVALID (-1)     /* bad argument (null pointer, size, kind, id) */
+#define OTFMM_ERR_THETA (-2)       /* theta below the compiled minimum 0.34 */
+#define OTFMM_ERR_CUDA (-3)        /* CUDA runtime error */
+#define OTFMM_ERR_DEVICE (-4)      /* kernel reported a bad work item on the device */
+#define OTFMM_ERR_UNSUPPORTED (-5) /* combination not built (e.g. precision for theta) */
+
+/* gsolve_type (octotiger/defs.hpp): RHO carries the angular correction L_c */
+#define OTFMM_RHO 0
+#define OTFMM_DRHODT 1
+
+#define OTFMM_FP64_EXACT 0
+#define OTFMM_FP64 1
+#define OTFMM_FP32_SPLIT 2
+
+/* Work-item kinds, as node_server::compute_fmm dispatches them (src/node_server.cpp:711-723). */
+#define OTFMM_KIND_M2L 0      /* refined node: multipole_kernel_interface, use_root_stencil = false */
+#define OTFMM_KIND_M2L_ROOT 1 /* level-0 node: multipole_kernel_interface, use_root_stencil = true */
+#define OTFMM_KIND_LEAF 2     /* leaf: monopole_kernel_interface (P2P, plus P2M per refined neighbour) */
+
+/* One work item (144 bytes). neighbors[d] is the pool index of the same-level
+ * neighbour in geo::direction flat order d = 0..25 (octotiger/geometry.hpp:91-197),
+ * or -1 for an empty direction (is_direction_empty). dx and xbase as passed to
+ * multipole_kernel_interface (xbase = centre of inner cell (0,0,0),
+ * src/node_server.cpp:712-715). */
+typedef struct otfmm_work_item {
+    int32_t subgrid;
+    int32_t kind;
+    int32_t neighbors[26];
+    double dx;
+    double xbase[3];
+} otfmm_work_item;
+
+typedef struct otfmm_context otfmm_context;
+
+/* Creates a context on `device` for opening angle theta (opts().theta,
+ * src/options_processing.cpp:119; must be >= 0.34, :234-236). Builds the
+ * multipole two-phase stencil and the monopole stencil with its constants and
+ * uploads them. Replaces calculate_stencil + get_device_masks. */
+int otfmm_create(int device, double theta, otfmm_context** out);
+int otfmm_destroy(otfmm_context* ctx);
+
+/* Stencil sizes of the context: counts[0] multipole offsets, [1] of which
+ * full multipole (phase one), [2] monopole offsets; masks may be NULL, else
+ * 1331 bytes each (11^3 box, x-major) like stencil_masks / inner_stencil_masks
+ * and the P2P mask. */
+int otfmm_stencil_info(const otfmm_context* ctx, int32_t counts[3], uint8_t* mpole_mask, uint8_t* mpole_phase,
+                       uint8_t* p2p_mask);
+
+/* Multipole interactions of one subgrid from the reference's SoA buffers
+ * (device pointers). Equivalent of launch_interface (kokkos_kernel.hpp:768-863)
+ * followed by its partial-sum reduction: writes L (20 x 531) and, for RHO,
+ * L_c (3 x 531). use_root_stencil selects the root kernel
+ * (multipole_kernel_root_*_impl); mon is not read then and may be NULL. */
+int otfmm_m2l_soa(otfmm_context* ctx, const double* mon, const double* M, const double* com, double* L,
+                  double* L_c, int gsolve_type, int use_root_stencil, int precision, void* stream);
+
+/* Same with host buffers: copies in, computes, copies out and waits, like the
+ * reference's launch_interface with host_buffer arguments and fut.get(). */
+int otfmm_m2l_soa_host(otfmm_context* ctx, const double* mon, const double* M, const double* com, double* L,
+                       double* L_c, int gsolve_type, int use_root_stencil, int precision);
+
+/* P2P of one leaf subgrid from its staged monopole buffer (mon[5832], device
+ * pointer), p2p_kernel_impl + sum_p2p_results (monopole kokkos_kernel.hpp:118-320):
+ * writes L4 (4 x 531). */
+int otfmm_p2p_soa(otfmm_context* ctx, const double* mon, double dx, double* L4, int precision, void* stream);
+
+/* P2M of one leaf subgrid against the refined neighbour in direction d
+ * (0..25): p2m_kernel_impl_rho / _non_rho (monopole kokkos_kernel.hpp:517-942).
+ * neighbor_M / neighbor_com hold the neighbour's slab in the layout of
+ * update_neighbor_input (20 / 3 components, stride = slab cells + 19),
+ * inner_com the leaf's centres of mass (3 x 531). Adds to L4 (4 x 531) and
+ * L_c (3 x 531); reset_lc zeroes L_c first (first P2M call of a subgrid). */
+int otfmm_p2m_soa(otfmm_context* ctx, int d, const double* neighbor_M, const double* neighbor_com,
+                  const double* inner_com, double* L4, double* L_c, int gsolve_type, int reset_lc, int precision,
+                  void* stream);
+
+/* Batched solve: every work item of `items` (device array of n_items) in one
+ * launch, reading the resident pool (device pointers, n_subgrids records) and
+ * writing per subgrid L[n][20][512] and L_c[n][3][512] (leaf items fill
+ * L[0..3], zero L[4..19]; L_c is zero for DRHODT and for leaves without a
+ * refined neighbour). Work items are validated on the device; a bad item makes
+ * the call return OTFMM_ERR_DEVICE (after the stream is synchronized) and
+ * leaves its outputs unwritten. */
+int otfmm_batch(otfmm_context* ctx, const double* pool_M, const double* pool_com, const double* pool_mon,
+                const uint8_t* pool_is_leaf, int32_t n_subgrids, const otfmm_work_item* items, int32_t n_items,
+                double* L, double* L_c, int gsolve_type, int precision, void* stream);
+
+/* Checks a device-side error flag written by the last otfmm_batch on `stream`
+ * without synchronizing the whole device: returns OTFMM_OK or OTFMM_ERR_DEVICE. */
+int otfmm_batch_status(otfmm_context* ctx, void* stream);
+
+/* Message for the last error on the calling thread ("" if none). */
+const char* otfmm_last_error(void);
+
+/* Library build information ("sm_100a ..."). */
+const char* otfmm_build_info(void);
+
+/* Measures the FP64 and FP32 FMA issue rates of the current device with a
+ * register-resident FMA loop (lanes x FMAs x 2 flops / time); results in
+ * TFLOP/s. Used as the roofline denominators. */
+int otfmm_measure_fma_peaks(int device, double* fp64_tflops, double* fp32_tflops);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OTFMM_H */

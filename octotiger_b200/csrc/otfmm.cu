@@ -1,0 +1,1048 @@
+// B200-native FMM cell-interaction kernels for Octo-Tiger (sm_100a).
+//
+// Hot path: the multipole (M2L) stencil sweep of refined subgrids and the
+// monopole (P2P + P2M) sweep of leaf subgrids, the work that
+// node_server::compute_fmm hands to multipole_kernel_interface /
+// monopole_kernel_interface (src/node_server.cpp:711-723).
+//
+// Design (one GPU):
+//  * A work unit ("tile") is half a subgrid: 4 x 8 x 8 target cells, one
+//    thread per cell, 256 threads per CTA, one CTA per SM.
+//  * For theta >= 0.5 a cell's partners lie in the 6^3 fine block of its
+//    parent's 3^3 coarse neighbourhood, so a tile needs the 8 x 12 x 12 cell
+//    region around it. The CTA gathers that region straight from the subgrid
+//    pool in HBM (own cells + 26 neighbours, on the device — no host staging)
+//    into shared memory: 23 doubles per cell (mass, 19 higher moments,
+//    centre of mass), 215 KB.
+//  * Shared memory is split by cell parity: the 8 parity classes of the
+//    region each form a 4 x 6 x 6 sub-lattice, stored as rows of
+//    [23 components x 6 z] padded to 140 doubles. A warp owns the 32 target
+//    cells of one parity class (2 x 4 x 4), so for every stencil offset the
+//    warp reads 32 partners of one class: per half-warp 4 rows x 4 z whose
+//    addresses are distinct modulo 16 double-words (140 = 12 mod 16) — no
+//    bank conflicts — and every lane walks the same offset list (warp-uniform
+//    control flow, offsets from a per-parity table).
+//  * Offsets are visited in the reference's stencil order (x, y, z
+//    lexicographic), so per-cell accumulation order equals the reference's
+//    and the exact form is bit-identical to it.
+//  * Leaf tiles gather the same region (masses of leaf cells, multipoles of
+//    refined neighbours) and run P2P then P2M; the level-0 node runs the
+//    root stencil over its 512 cells.
+//  * One launch runs a whole work list (ragged mix of kinds); the hardware
+//    block scheduler balances CTAs over the 148 SMs.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/otfmm.h"
+#include "pair_math.cuh"
+
+namespace otfmm {
+
+constexpr int INX = 8;
+constexpr int NCELL = 512;
+constexpr int SMAX = 5;
+constexpr int SINX = 11;
+constexpr int FULL = SINX * SINX * SINX;
+constexpr int PSTRIDE = 18;
+constexpr int ENTRIES = PSTRIDE * PSTRIDE * PSTRIDE;
+constexpr int CL = ENTRIES + 19;   // reference input component stride
+constexpr int CLU = NCELL + 19;    // reference output component stride
+constexpr int PAD_OFF = 3;
+constexpr double THETA_MIN = 0.34;
+
+// Tile geometry for coarse reach 1 (theta >= 0.5).
+constexpr int THREADS = 256;
+constexpr int TILE_X = 4;
+constexpr int REG_X = TILE_X + 4;          // region x extent, origin x0 - 2
+constexpr int REG_YZ = INX + 4;            // region y, z extent, origin -2
+constexpr int REG_CELLS = REG_X * REG_YZ * REG_YZ;   // 1152
+constexpr int SUB_YZ = REG_YZ / 2;         // 6
+constexpr int NCOMP = 23;                  // m0, M1..M19, com x/y/z
+constexpr int RB = NCOMP * SUB_YZ + 2;     // 140 doubles per (x', y') row
+constexpr int XS = SUB_YZ * RB;            // 840
+constexpr int CLS = (REG_X / 2) * XS;      // 3360 doubles per parity class
+constexpr int SMEM_DOUBLES = 8 * CLS;      // 26880 doubles = 215040 bytes
+constexpr int MAX_ENTRIES = 216;           // 6^3 - 1 partners per cell at most
+constexpr int ROOT_SMEM_DOUBLES = NCOMP * NCELL;
+static_assert(ROOT_SMEM_DOUBLES <= SMEM_DOUBLES, "root staging fits");
+static_assert(RB % 16 == 12 || RB % 16 == 4, "row stride must keep 4x4 lane blocks conflict-free");
+
+// Entry flags
+constexpr int F_FAR = 1;    // phase-one offset: full multipole partner
+constexpr int F_NEAR = 2;   // monopole-only offset
+
+struct Tables {
+    const int2* entries;     // [8][MAX_ENTRIES]: x = smem delta, y = packed offset/flags/stencil index
+    const int* count;        // [8]
+    const double* four;      // [FULL][4] monopole constants
+    const uint8_t* phase;    // [FULL] inner_stencil_masks (true outside the stencil)
+};
+
+__device__ __forceinline__ int entry_sx(int y) { return (y & 15) - 8; }
+__device__ __forceinline__ int entry_sy(int y) { return ((y >> 4) & 15) - 8; }
+__device__ __forceinline__ int entry_sz(int y) { return ((y >> 8) & 15) - 8; }
+__device__ __forceinline__ int entry_flags(int y) { return (y >> 12) & 3; }
+__device__ __forceinline__ int entry_sidx(int y) { return (y >> 16) & 2047; }
+
+// Raw direction (0..26, 13 = centre) of absolute cell coordinates a in [-8, 15].
+__device__ __forceinline__ int raw_dir(int ax, int ay, int az) {
+    return ((ax >> 3) + 1) + 3 * ((ay >> 3) + 1) + 9 * ((az >> 3) + 1);
+}
+
+enum : int { PREC_EXACT = OTFMM_FP64_EXACT, PREC_FAST = OTFMM_FP64 };
+
+// Scaling folded into staged moments by the fast form.
+template <int PREC>
+__device__ __forceinline__ double stage_scale(int q) {
+    if (PREC == PREC_FAST) {
+        if (q >= 4 && q < 10) return factor_of(q) / 2.0;
+        if (q >= 10 && q < 20) return factor_of(q) / 6.0;
+    }
+    return 1.0;
+}
+
+__device__ __forceinline__ int region_addr(int ax, int ay, int az, int x0) {
+    const int rx = ax - x0 + 2, ry = ay + 2, rz = az + 2;
+    const int cls = ((ax & 1) << 2) | ((ay & 1) << 1) | (az & 1);
+    return cls * CLS + (rx >> 1) * XS + (ry >> 1) * RB + (rz >> 1);
+}
+
+struct ItemInfo {
+    int subgrid, kind;
+    int nb[26];
+    double dx, xbase[3];
+};
+
+// ---------------------------------------------------------------- staging
+// Gathers the tile region from the subgrid pool
+// (restates multipole update_input, octotiger/multipole_interactions/legacy/
+// multipole_interaction_interface.hpp:88-281, for full-size neighbour payloads;
+// leaf tiles follow monopole update_input + update_neighbor_input,
+// octotiger/monopole_interactions/legacy/monopole_interaction_interface.hpp:64-143,
+// p2m_interaction_interface.hpp:102-160).
+template <int PREC>
+__device__ void stage_region_pool(double* sm, const ItemInfo& it, int x0, bool leaf_tile, const double* __restrict__ M,
+                                  const double* __restrict__ com, const double* __restrict__ mon,
+                                  const uint8_t* __restrict__ is_leaf) {
+    for (int r = threadIdx.x; r < REG_CELLS; r += blockDim.x) {
+        const int rx = r / (REG_YZ * REG_YZ), ry = (r / REG_YZ) % REG_YZ, rz = r % REG_YZ;
+        const int ax = x0 - 2 + rx, ay = ry - 2, az = rz - 2;
+        const int raw = raw_dir(ax, ay, az);
+        const bool centre = (raw == 13);
+        const int src = centre ? it.subgrid : it.nb[raw < 13 ? raw : raw - 1];
+        const int lx = ax & 7, ly = ay & 7, lz = az & 7;
+        const int u = lx * 64 + ly * 8 + lz;
+        const int base = region_addr(ax, ay, az, x0);
+        double v[NCOMP];
+        if (src < 0) {
+#pragma unroll
+            for (int q = 0; q < NCOMP; ++q) v[q] = 0.0;
+        } else {
+            const bool use_mon = centre ? leaf_tile : (is_leaf[src] != 0);
+            if (use_mon) {
+                v[0] = mon[(size_t)src * NCELL + u];
+#pragma unroll
+                for (int q = 1; q < 20; ++q) v[q] = 0.0;
+                if (centre) {
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) v[20 + a] = com[((size_t)src * 3 + a) * NCELL + u];
+                } else {
+                    // cell centre: i*dx + xbase - INX*dx with i the padded index (:221-234)
+                    const int ip[3] = {ax + INX, ay + INX, az + INX};
+#pragma unroll
+                    for (int a = 0; a < 3; ++a)
+                        v[20 + a] = __dsub_rn(__dadd_rn(__dmul_rn((double)ip[a], it.dx), it.xbase[a]),
+                                              __dmul_rn((double)INX, it.dx));
+                }
+            } else {
+#pragma unroll
+                for (int q = 0; q < 20; ++q) v[q] = M[((size_t)src * 20 + q) * NCELL + u] * stage_scale<PREC>(q);
+#pragma unroll
+                for (int a = 0; a < 3; ++a) v[20 + a] = com[((size_t)src * 3 + a) * NCELL + u];
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < NCOMP; ++q) sm[base + q * SUB_YZ] = v[q];
+    }
+}
+
+// Same region from the reference's 18^3 SoA buffers. m0 holds mon + M0, the
+// value phase-one offsets use (:270-283 of kokkos_kernel.hpp).
+template <int PREC>
+__device__ void stage_region_soa(double* sm, int x0, const double* __restrict__ mon, const double* __restrict__ M,
+                                 const double* __restrict__ com) {
+    for (int r = threadIdx.x; r < REG_CELLS; r += blockDim.x) {
+        const int rx = r / (REG_YZ * REG_YZ), ry = (r / REG_YZ) % REG_YZ, rz = r % REG_YZ;
+        const int ax = x0 - 2 + rx, ay = ry - 2, az = rz - 2;
+        const int f = (ax + INX - PAD_OFF) * PSTRIDE * PSTRIDE + (ay + INX - PAD_OFF) * PSTRIDE + (az + INX - PAD_OFF);
+        const int base = region_addr(ax, ay, az, x0);
+        sm[base] = __dadd_rn(mon[f], M[f]) * stage_scale<PREC>(0);
+#pragma unroll
+        for (int q = 1; q < 20; ++q) sm[base + q * SUB_YZ] = M[q * CL + f] * stage_scale<PREC>(q);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) sm[base + (20 + a) * SUB_YZ] = com[a * CL + f];
+    }
+}
+
+// ---------------------------------------------------------------- compute
+struct CellMap {
+    int p, i, j, k, cx, cy, cz, lane_off, own;
+};
+__device__ __forceinline__ CellMap cell_map(int x0) {
+    CellMap c;
+    const int lane = threadIdx.x & 31;
+    c.p = threadIdx.x >> 5;
+    c.i = lane >> 4;
+    c.j = (lane >> 2) & 3;
+    c.k = lane & 3;
+    c.cx = x0 + ((c.p >> 2) & 1) + 2 * c.i;
+    c.cy = ((c.p >> 1) & 1) + 2 * c.j;
+    c.cz = (c.p & 1) + 2 * c.k;
+    c.lane_off = c.i * XS + c.j * RB + c.k;
+    c.own = c.p * CLS + (c.i + 1) * XS + (c.j + 1) * RB + (c.k + 1);
+    return c;
+}
+
+struct OutPtr {
+    double* L;
+    double* Lc;
+    int stride;   // component stride
+    bool pool;    // pool outputs: L_c is written (zeros) for DRHODT too
+};
+
+template <bool RHO>
+__device__ __forceinline__ void write_lc(const OutPtr& out, int cf, const double corr[3]) {
+    if (RHO || out.pool) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) out.Lc[a * out.stride + cf] = RHO ? corr[a] : 0.0;
+    }
+}
+
+// M2L over the staged region. near_mon != nullptr: monopole-only offsets read
+// the partner mass from that 18^3 buffer (SoA path); else from the region for
+// leaf-neighbour partners (bit set in monomask, indexed by raw direction).
+template <int PREC, bool RHO>
+__device__ void m2l_tile(const double* sm, int x0, const Tables& t, uint32_t monomask, const double* near_mon,
+                         OutPtr out) {
+    const CellMap c = cell_map(x0);
+    double X[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) X[a] = sm[c.own + (20 + a) * SUB_YZ];
+    double acc[20], corr[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int q = 0; q < 20; ++q) acc[q] = 0.0;
+    const int n = t.count[c.p];
+    const int2* ent = t.entries + c.p * MAX_ENTRIES;
+    if (PREC == PREC_EXACT) {
+        double mc[20];
+#pragma unroll
+        for (int q = 0; q < 20; ++q) mc[q] = sm[c.own + q * SUB_YZ];
+        for (int e = 0; e < n; ++e) {
+            const int2 en = __ldg(ent + e);
+            const int pb = en.x + c.lane_off;
+            double Y[3], mp[20];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) Y[a] = sm[pb + (20 + a) * SUB_YZ];
+            if (entry_flags(en.y) & F_FAR) {
+#pragma unroll
+                for (int q = 0; q < 20; ++q) mp[q] = sm[pb + q * SUB_YZ];
+            } else {
+                const int ax = c.cx + entry_sx(en.y), ay = c.cy + entry_sy(en.y), az = c.cz + entry_sz(en.y);
+                double m0;
+                if (near_mon) {
+                    m0 = near_mon[(ax + INX - PAD_OFF) * PSTRIDE * PSTRIDE + (ay + INX - PAD_OFF) * PSTRIDE +
+                                  (az + INX - PAD_OFF)];
+                } else {
+                    if (!((monomask >> raw_dir(ax, ay, az)) & 1u)) continue;   // contributes exactly zero
+                    m0 = sm[pb];
+                }
+                mp[0] = m0;
+#pragma unroll
+                for (int q = 1; q < 20; ++q) mp[q] = 0.0;
+            }
+            exact_m2l_pair<RHO>(X, Y, mp, mc, acc, corr);
+        }
+    } else {
+        const double inv_m0 = 1.0 / sm[c.own];
+        double mc_oct[10];
+#pragma unroll
+        for (int o = 0; o < 10; ++o) mc_oct[o] = sm[c.own + (10 + o) * SUB_YZ];
+#pragma unroll 1
+        for (int e = 0; e < n; ++e) {
+            const int2 en = __ldg(ent + e);
+            const int pb = en.x + c.lane_off;
+            double Y[3];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) Y[a] = sm[pb + (20 + a) * SUB_YZ];
+            if (entry_flags(en.y) & F_FAR) {
+                double mp[20];
+#pragma unroll
+                for (int q = 0; q < 20; ++q) mp[q] = sm[pb + q * SUB_YZ];
+                fast_m2l_pair<RHO>(X, Y, mp, mc_oct, inv_m0, acc, corr);
+            } else {
+                const int ax = c.cx + entry_sx(en.y), ay = c.cy + entry_sy(en.y), az = c.cz + entry_sz(en.y);
+                double m0;
+                if (near_mon) {
+                    m0 = near_mon[(ax + INX - PAD_OFF) * PSTRIDE * PSTRIDE + (ay + INX - PAD_OFF) * PSTRIDE +
+                                  (az + INX - PAD_OFF)];
+                } else {
+                    if (!((monomask >> raw_dir(ax, ay, az)) & 1u)) continue;
+                    m0 = sm[pb];
+                }
+                fast_m2l_mass_pair<RHO>(X, Y, m0, mc_oct, inv_m0, acc, corr);
+            }
+        }
+    }
+    const int cf = c.cx * 64 + c.cy * 8 + c.cz;
+#pragma unroll
+    for (int q = 0; q < 20; ++q) out.L[q * out.stride + cf] = acc[q];
+    write_lc<RHO>(out, cf, corr);
+}
+
+// Leaf tile: P2P over own + leaf-neighbour masses, then P2M per refined
+// neighbour direction in direction order (monopole kokkos_kernel.hpp:1195-1273).
+template <int PREC, bool RHO>
+__device__ void leaf_tile(const double* sm, int x0, const Tables& t, uint32_t refmask, double dx, OutPtr out) {
+    const CellMap c = cell_map(x0);
+    double X[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) X[a] = sm[c.own + (20 + a) * SUB_YZ];
+    double acc[4] = {0.0, 0.0, 0.0, 0.0}, corr[3] = {0.0, 0.0, 0.0};
+    const int n = t.count[c.p];
+    const int2* ent = t.entries + c.p * MAX_ENTRIES;
+    const double dc0 = __ddiv_rn(1.0, dx), dc1 = __ddiv_rn(-1.0, dx);
+    // P2P (p2p_kernel_impl)
+    for (int e = 0; e < n; ++e) {
+        const int2 en = __ldg(ent + e);
+        const int ax = c.cx + entry_sx(en.y), ay = c.cy + entry_sy(en.y), az = c.cz + entry_sz(en.y);
+        if ((refmask >> raw_dir(ax, ay, az)) & 1u) continue;   // refined neighbour: no monopole
+        const double* four = t.four + 4 * entry_sidx(en.y);
+        const double m = sm[en.x + c.lane_off];
+        if (PREC == PREC_EXACT) {
+            const double ms = __dmul_rn(m, dc0);
+            acc[0] = __dadd_rn(acc[0], __dmul_rn(__ldg(four), ms));
+#pragma unroll
+            for (int a = 1; a < 4; ++a) acc[a] = __dadd_rn(acc[a], __dmul_rn(__dmul_rn(__ldg(four + a), ms), dc1));
+        } else {
+            const double ms = m * dc0;
+            const double ms1 = ms * dc1;
+            acc[0] = fma(__ldg(four), ms, acc[0]);
+#pragma unroll
+            for (int a = 1; a < 4; ++a) acc[a] = fma(__ldg(four + a), ms1, acc[a]);
+        }
+    }
+    // P2M, one refined direction after the other
+    if (refmask) {
+        for (int raw = 0; raw < 27; ++raw) {
+            if (!((refmask >> raw) & 1u)) continue;
+            for (int e = 0; e < n; ++e) {
+                const int2 en = __ldg(ent + e);
+                const int ax = c.cx + entry_sx(en.y), ay = c.cy + entry_sy(en.y), az = c.cz + entry_sz(en.y);
+                if (raw_dir(ax, ay, az) != raw) continue;
+                const int pb = en.x + c.lane_off;
+                double Y[3], mp[20];
+#pragma unroll
+                for (int a = 0; a < 3; ++a) Y[a] = sm[pb + (20 + a) * SUB_YZ];
+#pragma unroll
+                for (int q = 0; q < 20; ++q) mp[q] = sm[pb + q * SUB_YZ];
+                if (PREC == PREC_EXACT)
+                    exact_p2m_pair<RHO>(X, Y, mp, acc, corr);
+                else
+                    fast_p2m_pair<RHO>(X, Y, mp, acc, corr);
+            }
+        }
+    }
+    const int cf = c.cx * 64 + c.cy * 8 + c.cz;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) out.L[q * out.stride + cf] = acc[q];
+    if (out.pool) {   // pool output: L4..L19 are zero for leaves
+#pragma unroll
+        for (int q = 4; q < 20; ++q) out.L[q * out.stride + cf] = 0.0;
+    }
+    write_lc<RHO>(out, cf, corr);
+}
+
+// Root node: partners are all own cells except the monopole-only stencil
+// offsets and the cell itself (multipole_kernel_root_*_impl).
+// Staged layout: sm[q * 512 + cell].
+template <int PREC, bool RHO>
+__device__ void root_tile(const double* sm, int x0, const Tables& t, OutPtr out) {
+    const CellMap c = cell_map(x0);
+    const int cu = c.cx * 64 + c.cy * 8 + c.cz;
+    double X[3], acc[20], corr[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) X[a] = sm[(20 + a) * NCELL + cu];
+#pragma unroll
+    for (int q = 0; q < 20; ++q) acc[q] = 0.0;
+    double mc[20];
+#pragma unroll
+    for (int q = 0; q < 20; ++q) mc[q] = sm[q * NCELL + cu];
+    const double inv_m0 = 1.0 / mc[0];
+    for (int pu = 0; pu < NCELL; ++pu) {
+        const int sx = (pu >> 6) - c.cx, sy = ((pu >> 3) & 7) - c.cy, sz = (pu & 7) - c.cz;
+        if (abs(sx) <= SMAX && abs(sy) <= SMAX && abs(sz) <= SMAX) {
+            const int sidx = (sx + SMAX) * SINX * SINX + (sy + SMAX) * SINX + (sz + SMAX);
+            if (!__ldg(t.phase + sidx) || (sx == 0 && sy == 0 && sz == 0)) continue;
+        }
+        double Y[3], mp[20];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) Y[a] = sm[(20 + a) * NCELL + pu];
+#pragma unroll
+        for (int q = 0; q < 20; ++q) mp[q] = sm[q * NCELL + pu];
+        if (PREC == PREC_EXACT)
+            exact_m2l_pair<RHO>(X, Y, mp, mc, acc, corr);
+        else
+            fast_m2l_pair<RHO>(X, Y, mp, mc + 10, inv_m0, acc, corr);
+    }
+#pragma unroll
+    for (int q = 0; q < 20; ++q) out.L[q * out.stride + cu] = acc[q];
+    write_lc<RHO>(out, cu, corr);
+}
+
+// ---------------------------------------------------------------- kernels
+struct BatchArgs {
+    const double* M;
+    const double* com;
+    const double* mon;
+    const uint8_t* is_leaf;
+    int n_sub;
+    const otfmm_work_item* items;
+    int n_items;
+    double* L;
+    double* Lc;
+    Tables t;
+    int* err;
+};
+
+template <int PREC, bool RHO>
+__global__ void __launch_bounds__(THREADS, 1) batch_kernel(BatchArgs a) {
+    extern __shared__ double sm[];
+    __shared__ ItemInfo it;
+    __shared__ int bad;
+    const int item_idx = blockIdx.x >> 1;
+    const int half = blockIdx.x & 1;
+    if (threadIdx.x == 0) {
+        const otfmm_work_item& w = a.items[item_idx];
+        it.subgrid = w.subgrid;
+        it.kind = w.kind;
+        it.dx = w.dx;
+        for (int q = 0; q < 3; ++q) it.xbase[q] = w.xbase[q];
+        int b = (w.subgrid < 0 || w.subgrid >= a.n_sub || w.kind < 0 || w.kind > 2 || !(w.dx > 0.0));
+        for (int d = 0; d < 26; ++d) {
+            it.nb[d] = w.neighbors[d];
+            b |= (w.neighbors[d] < -1 || w.neighbors[d] >= a.n_sub);
+        }
+        if (!b && w.kind != OTFMM_KIND_M2L_ROOT) b |= (a.is_leaf[w.subgrid] != 0) != (w.kind == OTFMM_KIND_LEAF);
+        bad = b;
+        if (b) atomicOr(a.err, 1);
+    }
+    __syncthreads();
+    if (bad) return;
+    const int x0 = TILE_X * half;
+    const size_t sub = (size_t)it.subgrid;
+    OutPtr out{a.L + sub * 20 * NCELL, a.Lc + sub * 3 * NCELL, NCELL, true};
+    if (it.kind == OTFMM_KIND_M2L_ROOT) {
+        const int base_sub = it.subgrid;
+        for (int r = threadIdx.x; r < NCELL; r += blockDim.x)
+            for (int q = 0; q < NCOMP; ++q)
+                sm[q * NCELL + r] = (q < 20) ? a.M[((size_t)base_sub * 20 + q) * NCELL + r] * stage_scale<PREC>(q)
+                                             : a.com[((size_t)base_sub * 3 + (q - 20)) * NCELL + r];
+        __syncthreads();
+        root_tile<PREC, RHO>(sm, x0, a.t, out);
+        return;
+    }
+    const bool leaf = (it.kind == OTFMM_KIND_LEAF);
+    // direction masks indexed by raw direction: leaf neighbours (for M2L
+    // monopole-only offsets) or refined neighbours (leaf tiles)
+    uint32_t mask = 0;
+    for (int d = 0; d < 26; ++d) {
+        const int nb = it.nb[d];
+        if (nb < 0) continue;
+        const bool nb_leaf = a.is_leaf[nb] != 0;
+        if (leaf ? !nb_leaf : nb_leaf) mask |= 1u << (d < 13 ? d : d + 1);
+    }
+    stage_region_pool<PREC>(sm, it, x0, leaf, a.M, a.com, a.mon, a.is_leaf);
+    __syncthreads();
+    if (leaf) {
+        leaf_tile<PREC, RHO>(sm, x0, a.t, mask, it.dx, out);
+    } else {
+        m2l_tile<PREC, RHO>(sm, x0, a.t, mask, nullptr, out);
+    }
+}
+
+struct SoaArgs {
+    const double* mon;
+    const double* M;
+    const double* com;
+    double* L;
+    double* Lc;
+    Tables t;
+};
+
+template <int PREC, bool RHO, bool ROOT>
+__global__ void __launch_bounds__(THREADS, 1) soa_m2l_kernel(SoaArgs a) {
+    extern __shared__ double sm[];
+    const int x0 = TILE_X * blockIdx.x;
+    OutPtr out{a.L, a.Lc, CLU, false};
+    if (ROOT) {
+        for (int r = threadIdx.x; r < NCELL; r += blockDim.x) {
+            const int f = ((r >> 6) + INX - PAD_OFF) * PSTRIDE * PSTRIDE + (((r >> 3) & 7) + INX - PAD_OFF) * PSTRIDE +
+                          ((r & 7) + INX - PAD_OFF);
+            for (int q = 0; q < NCOMP; ++q)
+                sm[q * NCELL + r] = (q < 20) ? a.M[q * CL + f] * stage_scale<PREC>(q) : a.com[(q - 20) * CL + f];
+        }
+        __syncthreads();
+        root_tile<PREC, RHO>(sm, x0, a.t, out);
+    } else {
+        stage_region_soa<PREC>(sm, x0, a.mon, a.M, a.com);
+        __syncthreads();
+        m2l_tile<PREC, RHO>(sm, x0, a.t, 0u, a.mon, out);
+    }
+}
+
+// Per-subgrid P2P on the reference's staged mon[5832] (one thread per cell).
+template <int PREC>
+__global__ void soa_p2p_kernel(const double* __restrict__ mon, double dx, double* __restrict__ L4, Tables t) {
+    const int cu = blockIdx.x * blockDim.x + threadIdx.x;
+    if (cu >= NCELL) return;
+    const int cx = cu >> 6, cy = (cu >> 3) & 7, cz = cu & 7;
+    const int p = ((cx & 1) << 2) | ((cy & 1) << 1) | (cz & 1);
+    const int n = t.count[p];
+    const int2* ent = t.entries + p * MAX_ENTRIES;
+    const double dc0 = __ddiv_rn(1.0, dx), dc1 = __ddiv_rn(-1.0, dx);
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int e = 0; e < n; ++e) {
+        const int y = __ldg(&ent[e].y);
+        const int ax = cx + entry_sx(y), ay = cy + entry_sy(y), az = cz + entry_sz(y);
+        const double m = mon[(ax + INX - PAD_OFF) * PSTRIDE * PSTRIDE + (ay + INX - PAD_OFF) * PSTRIDE + (az + INX - PAD_OFF)];
+        const double* four = t.four + 4 * entry_sidx(y);
+        if (PREC == PREC_EXACT) {
+            const double ms = __dmul_rn(m, dc0);
+            acc[0] = __dadd_rn(acc[0], __dmul_rn(four[0], ms));
+            for (int q = 1; q < 4; ++q) acc[q] = __dadd_rn(acc[q], __dmul_rn(__dmul_rn(four[q], ms), dc1));
+        } else {
+            const double ms = m * dc0;
+            acc[0] = fma(four[0], ms, acc[0]);
+            for (int q = 1; q < 4; ++q) acc[q] = fma(four[q], ms * dc1, acc[q]);
+        }
+    }
+    for (int q = 0; q < 4; ++q) L4[q * CLU + cu] = acc[q];
+}
+
+// Per-subgrid P2M against one refined neighbour slab (update_neighbor_input layout).
+template <int PREC, bool RHO>
+__global__ void soa_p2m_kernel(int d, const double* __restrict__ nM, const double* __restrict__ ncom,
+                               const double* __restrict__ icom, double* L4, double* Lc, Tables t) {
+    const int cu = blockIdx.x * blockDim.x + threadIdx.x;
+    if (cu >= NCELL) return;
+    const int r = d < 13 ? d : d + 1;
+    const int o[3] = {r % 3 - 1, (r / 3) % 3 - 1, r / 9 - 1};
+    int s[3], e[3], sz[3];
+    for (int a = 0; a < 3; ++a) {
+        s[a] = (o[a] == -1) ? INX - SMAX : 0;
+        e[a] = (o[a] == 1) ? SMAX : INX;
+        sz[a] = e[a] - s[a];
+    }
+    const int stride = sz[0] * sz[1] * sz[2] + 19;
+    const int cx = cu >> 6, cy = (cu >> 3) & 7, cz = cu & 7;
+    const int p = ((cx & 1) << 2) | ((cy & 1) << 1) | (cz & 1);
+    const int n = t.count[p];
+    const int2* ent = t.entries + p * MAX_ENTRIES;
+    double X[3], acc[4], corr[3] = {0.0, 0.0, 0.0};
+    for (int a = 0; a < 3; ++a) X[a] = icom[a * CLU + cu];
+    for (int q = 0; q < 4; ++q) acc[q] = L4[q * CLU + cu];
+    if (RHO)
+        for (int a = 0; a < 3; ++a) corr[a] = Lc[a * CLU + cu];
+    bool any = false;
+    for (int en = 0; en < n; ++en) {
+        const int y = __ldg(&ent[en].y);
+        const int ax = cx + entry_sx(y), ay = cy + entry_sy(y), az = cz + entry_sz(y);
+        if (raw_dir(ax, ay, az) != r) continue;
+        const int lx = (ax & 7) - s[0], ly = (ay & 7) - s[1], lz = (az & 7) - s[2];
+        if (lx < 0 || ly < 0 || lz < 0 || lx >= sz[0] || ly >= sz[1] || lz >= sz[2]) continue;
+        const int f = lx * (sz[1] * sz[2]) + ly * sz[2] + lz;
+        double Y[3], mp[20];
+        for (int a = 0; a < 3; ++a) Y[a] = ncom[a * stride + f];
+        for (int q = 0; q < 20; ++q) mp[q] = nM[q * stride + f] * stage_scale<PREC>(q);
+        if (PREC == PREC_EXACT)
+            exact_p2m_pair<RHO>(X, Y, mp, acc, corr);
+        else
+            fast_p2m_pair<RHO>(X, Y, mp, acc, corr);
+        any = true;
+    }
+    (void)any;
+    for (int q = 0; q < 4; ++q) L4[q * CLU + cu] = acc[q];
+    if (RHO)
+        for (int a = 0; a < 3; ++a) Lc[a * CLU + cu] = corr[a];
+}
+
+__global__ void zero_kernel(double* p, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = 0.0;
+}
+
+// FMA issue-rate probes: 8 independent chains per thread.
+template <class T>
+__global__ void fma_probe_kernel(T* out, int iters, T x, T y) {
+    T a0 = threadIdx.x, a1 = a0 + 1, a2 = a0 + 2, a3 = a0 + 3, a4 = a0 + 4, a5 = a0 + 5, a6 = a0 + 6, a7 = a0 + 7;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+            a0 = fma(a0, x, y); a1 = fma(a1, x, y); a2 = fma(a2, x, y); a3 = fma(a3, x, y);
+            a4 = fma(a4, x, y); a5 = fma(a5, x, y); a6 = fma(a6, x, y); a7 = fma(a7, x, y);
+        }
+    }
+    const T s = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+    if (s == (T)-12345.0) out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+}   // namespace otfmm
+
+// ======================================================================== host
+using namespace otfmm;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+int cuda_fail(cudaError_t e, const char* what) {
+    return fail(OTFMM_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define OT_CUDA(call)                                     \
+    do {                                                  \
+        cudaError_t e_ = (call);                          \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+    } while (0)
+
+// Stencil generators, restating multipole_interactions::calculate_stencil +
+// calculate_stencil_masks (src/multipole_interactions/util/calculate_stencil.cpp:23-160)
+// and the monopole ones (src/monopole_interactions/util/calculate_stencil.cpp:19-178):
+// offsets j - i, over the 8 parity classes i, whose parents are not well
+// separated (theta_c > theta); phase one when the cells themselves are
+// (theta_f <= theta).
+double recip_dist(long a0, long a1, long a2, long b0, long b1, long b2) {
+    const double t = double((a0 - b0) * (a0 - b0) + (a1 - b1) * (a1 - b1) + (a2 - b2) * (a2 - b2));
+    return t > 0.0 ? 1.0 / std::sqrt(t) : 1.0e10;
+}
+
+struct HostStencil {
+    uint8_t mask[FULL];
+    uint8_t phase[FULL];
+    double four[FULL][4];
+    int n_mpole = 0, n_phase_one = 0;
+    int maxabs = 0;
+};
+
+void build_host_stencil(double theta, HostStencil& st) {
+    std::memset(st.mask, 0, sizeof st.mask);
+    std::memset(st.phase, 1, sizeof st.phase);
+    std::memset(st.four, 0, sizeof st.four);
+    struct E { int x, y, z; bool ph; };
+    std::vector<E> sup;
+    for (long i0 = 0; i0 < 2; ++i0)
+        for (long i1 = 0; i1 < 2; ++i1)
+            for (long i2 = 0; i2 < 2; ++i2)
+                for (long j0 = i0 - INX; j0 < i0 + INX; ++j0)
+                    for (long j1 = i1 - INX; j1 < i1 + INX; ++j1)
+                        for (long j2 = i2 - INX; j2 < i2 + INX; ++j2) {
+                            if (i0 == j0 && i1 == j1 && i2 == j2) continue;
+                            const double tf = recip_dist(i0, i1, i2, j0, j1, j2);
+                            const double tc = recip_dist((i0 + INX) / 2 - INX / 2, (i1 + INX) / 2 - INX / 2,
+                                                         (i2 + INX) / 2 - INX / 2, (j0 + INX) / 2 - INX / 2,
+                                                         (j1 + INX) / 2 - INX / 2, (j2 + INX) / 2 - INX / 2);
+                            if (!(tc > theta)) continue;
+                            const E e{int(j0 - i0), int(j1 - i1), int(j2 - i2), tf <= theta};
+                            bool found = false;
+                            for (const E& s : sup)
+                                if (s.x == e.x && s.y == e.y && s.z == e.z) { found = true; break; }
+                            if (!found) sup.push_back(e);
+                        }
+    for (const E& e : sup) st.maxabs = std::max({st.maxabs, std::abs(e.x), std::abs(e.y), std::abs(e.z)});
+    if (st.maxabs > SMAX) return;
+    for (const E& e : sup) {
+        const int idx = (e.x + SMAX) * SINX * SINX + (e.y + SMAX) * SINX + (e.z + SMAX);
+        st.mask[idx] = 1;
+        if (!e.ph) st.phase[idx] = 0;
+        ++st.n_mpole;
+        if (e.ph) ++st.n_phase_one;
+        const double x = e.x, y = e.y, z = e.z;
+        const double r = std::sqrt(x * x + y * y + z * z);
+        const double r3 = r * r * r;
+        st.four[idx][0] = -1.0 / r;
+        st.four[idx][1] = x / r3;
+        st.four[idx][2] = y / r3;
+        st.four[idx][3] = z / r3;
+    }
+}
+
+int coarse_of(int i) { return ((i + INX) >> 1) - INX / 2; }
+
+// Per parity class: the partner offsets in stencil (x, y, z) order that pass
+// the per-cell coarse criterion dist^2 < 1/theta^2
+// (kokkos_kernel.hpp:241-256), packed with their shared-memory delta. False
+// when the stencil reaches further than one coarse cell (theta < 0.5).
+bool build_entries(const HostStencil& st, double theta, std::vector<int2>& entries, int counts[8], int& reach) {
+    const double trs = (1.0 / theta) * (1.0 / theta);
+    entries.assign(8 * MAX_ENTRIES, int2{0, 0});
+    reach = 0;
+    for (int p = 0; p < 8; ++p) {
+        const int px = (p >> 2) & 1, py = (p >> 1) & 1, pz = p & 1;
+        int n = 0;
+        for (int sx = -SMAX; sx <= SMAX; ++sx)
+            for (int sy = -SMAX; sy <= SMAX; ++sy)
+                for (int sz = -SMAX; sz <= SMAX; ++sz) {
+                    const int idx = (sx + SMAX) * SINX * SINX + (sy + SMAX) * SINX + (sz + SMAX);
+                    if (!st.mask[idx]) continue;
+                    const int a = coarse_of(px + INX) - coarse_of(px + INX + sx);
+                    const int b = coarse_of(py + INX) - coarse_of(py + INX + sy);
+                    const int c = coarse_of(pz + INX) - coarse_of(pz + INX + sz);
+                    if (!(double(a * a + b * b + c * c) < trs)) continue;
+                    reach = std::max({reach, std::abs(a), std::abs(b), std::abs(c)});
+                    if (reach > 1 || n >= MAX_ENTRIES) return false;
+                    const int qx = px + 2 + sx, qy = py + 2 + sy, qz = pz + 2 + sz;   // >= 0 for reach 1
+                    const int cls = (((px + sx) & 1) << 2) | (((py + sy) & 1) << 1) | ((pz + sz) & 1);
+                    const int delta = cls * CLS + (qx >> 1) * XS + (qy >> 1) * RB + (qz >> 1);
+                    const int flags = st.phase[idx] ? F_FAR : F_NEAR;
+                    const int packed = (sx + 8) | ((sy + 8) << 4) | ((sz + 8) << 8) | (flags << 12) | (idx << 16);
+                    entries[p * MAX_ENTRIES + n] = int2{delta, packed};
+                    ++n;
+                }
+        counts[p] = n;
+    }
+    return true;
+}
+
+}   // namespace
+
+struct otfmm_context {
+    int device = 0;
+    double theta = 0.5;
+    int reach = 1;     // coarse reach of the stencil (1 for theta >= 0.5)
+    HostStencil st;
+    int counts[8] = {};
+    int2* d_entries = nullptr;
+    int* d_count = nullptr;
+    double* d_four = nullptr;
+    uint8_t* d_phase = nullptr;
+    int* d_err = nullptr;
+    double* d_soa_scratch = nullptr;   // host-buffer path staging
+    std::mutex mu;
+    Tables tables() const { return Tables{d_entries, d_count, d_four, d_phase}; }
+};
+
+namespace {
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+bool g_attr_set[8] = {};
+std::mutex g_attr_mu;
+
+template <class K>
+int set_smem(K kernel, int bytes) {
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+    return OTFMM_OK;
+}
+
+int ensure_attributes(int device) {
+    std::lock_guard<std::mutex> lock(g_attr_mu);
+    if (device < 0 || device >= 8) return OTFMM_OK;
+    if (g_attr_set[device]) return OTFMM_OK;
+    const int bytes = SMEM_DOUBLES * (int)sizeof(double);
+    int rc = OTFMM_OK;
+    rc = rc ? rc : set_smem(batch_kernel<PREC_EXACT, true>, bytes);
+    rc = rc ? rc : set_smem(batch_kernel<PREC_EXACT, false>, bytes);
+    rc = rc ? rc : set_smem(batch_kernel<PREC_FAST, true>, bytes);
+    rc = rc ? rc : set_smem(batch_kernel<PREC_FAST, false>, bytes);
+    rc = rc ? rc : set_smem(soa_m2l_kernel<PREC_EXACT, true, false>, bytes);
+    rc = rc ? rc : set_smem(soa_m2l_kernel<PREC_EXACT, false, false>, bytes);
+    rc = rc ? rc : set_smem(soa_m2l_kernel<PREC_FAST, true, false>, bytes);
+    rc = rc ? rc : set_smem(soa_m2l_kernel<PREC_FAST, false, false>, bytes);
+    rc = rc ? rc : set_smem(soa_m2l_kernel<PREC_EXACT, true, true>, bytes);
+    rc = rc ? rc : set_smem(soa_m2l_kernel<PREC_EXACT, false, true>, bytes);
+    rc = rc ? rc : set_smem(soa_m2l_kernel<PREC_FAST, true, true>, bytes);
+    rc = rc ? rc : set_smem(soa_m2l_kernel<PREC_FAST, false, true>, bytes);
+    if (rc == OTFMM_OK) g_attr_set[device] = true;
+    return rc;
+}
+
+int check_precision(int precision) {
+    if (precision != OTFMM_FP64_EXACT && precision != OTFMM_FP64)
+        return fail(OTFMM_ERR_UNSUPPORTED, "precision not available in this build");
+    return OTFMM_OK;
+}
+
+}   // namespace
+
+extern "C" {
+
+const char* otfmm_last_error(void) { return g_last_error.c_str(); }
+
+const char* otfmm_build_info(void) {
+    return "otfmm sm_100a; tiles of 4x8x8 cells, 256 threads, 215040 B shared memory; theta >= 0.5";
+}
+
+int otfmm_create(int device, double theta, otfmm_context** out) {
+    if (!out) return fail(OTFMM_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    if (!(theta >= THETA_MIN)) return fail(OTFMM_ERR_THETA, "theta below the compiled minimum 0.34");
+    int ndev = 0;
+    OT_CUDA(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) return fail(OTFMM_ERR_INVALID, "device index out of range");
+    auto* ctx = new otfmm_context();
+    ctx->device = device;
+    ctx->theta = theta;
+    build_host_stencil(theta, ctx->st);
+    if (ctx->st.maxabs > SMAX) {
+        delete ctx;
+        return fail(OTFMM_ERR_THETA, "stencil exceeds the compiled maximum width");
+    }
+    // Per-parity offset lists in stencil order, filtered by the coarse criterion.
+    std::vector<int2> entries;
+    int reach = 0;
+    if (!build_entries(ctx->st, theta, entries, ctx->counts, reach)) {
+        delete ctx;
+        return fail(OTFMM_ERR_UNSUPPORTED, "theta < 0.5 (coarse reach 2) is not built into this library");
+    }
+    ctx->reach = reach;
+    DeviceGuard g(device);
+    cudaError_t e;
+    if ((e = cudaMalloc(&ctx->d_entries, sizeof(int2) * entries.size())) != cudaSuccess ||
+        (e = cudaMalloc(&ctx->d_count, sizeof(int) * 8)) != cudaSuccess ||
+        (e = cudaMalloc(&ctx->d_four, sizeof(double) * 4 * FULL)) != cudaSuccess ||
+        (e = cudaMalloc(&ctx->d_phase, FULL)) != cudaSuccess ||
+        (e = cudaMalloc(&ctx->d_err, sizeof(int))) != cudaSuccess ||
+        (e = cudaMemcpy(ctx->d_entries, entries.data(), sizeof(int2) * entries.size(), cudaMemcpyHostToDevice)) !=
+            cudaSuccess ||
+        (e = cudaMemcpy(ctx->d_count, ctx->counts, sizeof(int) * 8, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(ctx->d_four, ctx->st.four, sizeof(double) * 4 * FULL, cudaMemcpyHostToDevice)) !=
+            cudaSuccess ||
+        (e = cudaMemcpy(ctx->d_phase, ctx->st.phase, FULL, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemset(ctx->d_err, 0, sizeof(int))) != cudaSuccess) {
+        otfmm_destroy(ctx);
+        return cuda_fail(e, "otfmm_create");
+    }
+    const int rc = ensure_attributes(device);
+    if (rc != OTFMM_OK) {
+        otfmm_destroy(ctx);
+        return rc;
+    }
+    *out = ctx;
+    return OTFMM_OK;
+}
+
+int otfmm_destroy(otfmm_context* ctx) {
+    if (!ctx) return OTFMM_OK;
+    DeviceGuard g(ctx->device);
+    cudaFree(ctx->d_entries);
+    cudaFree(ctx->d_count);
+    cudaFree(ctx->d_four);
+    cudaFree(ctx->d_phase);
+    cudaFree(ctx->d_err);
+    cudaFree(ctx->d_soa_scratch);
+    delete ctx;
+    return OTFMM_OK;
+}
+
+int otfmm_stencil_info(const otfmm_context* ctx, int32_t counts[3], uint8_t* mpole_mask, uint8_t* mpole_phase,
+                       uint8_t* p2p_mask) {
+    if (!ctx || !counts) return fail(OTFMM_ERR_INVALID, "NULL argument");
+    counts[0] = ctx->st.n_mpole;
+    counts[1] = ctx->st.n_phase_one;
+    counts[2] = ctx->st.n_mpole;   // the monopole stencil is the same offset set
+    if (mpole_mask) std::memcpy(mpole_mask, ctx->st.mask, FULL);
+    if (mpole_phase) std::memcpy(mpole_phase, ctx->st.phase, FULL);
+    if (p2p_mask) std::memcpy(p2p_mask, ctx->st.mask, FULL);
+    return OTFMM_OK;
+}
+
+int otfmm_m2l_soa(otfmm_context* ctx, const double* mon, const double* M, const double* com, double* L, double* L_c,
+                  int gsolve_type, int use_root_stencil, int precision, void* stream) {
+    if (!ctx || !M || !com || !L) return fail(OTFMM_ERR_INVALID, "NULL argument");
+    const bool rho = (gsolve_type == OTFMM_RHO);
+    if (gsolve_type != OTFMM_RHO && gsolve_type != OTFMM_DRHODT) return fail(OTFMM_ERR_INVALID, "bad gsolve_type");
+    if (rho && !L_c) return fail(OTFMM_ERR_INVALID, "L_c is NULL for RHO");
+    if (!use_root_stencil && !mon) return fail(OTFMM_ERR_INVALID, "mon is NULL");
+    int rc = check_precision(precision);
+    if (rc) return rc;
+    DeviceGuard g(ctx->device);
+    SoaArgs a{mon, M, com, L, L_c, ctx->tables()};
+    const size_t bytes = SMEM_DOUBLES * sizeof(double);
+    cudaStream_t s = (cudaStream_t)stream;
+#define OT_SOA(P, R, T) soa_m2l_kernel<P, R, T><<<2, THREADS, bytes, s>>>(a)
+    if (precision == OTFMM_FP64_EXACT) {
+        if (use_root_stencil) { if (rho) OT_SOA(PREC_EXACT, true, true); else OT_SOA(PREC_EXACT, false, true); }
+        else { if (rho) OT_SOA(PREC_EXACT, true, false); else OT_SOA(PREC_EXACT, false, false); }
+    } else {
+        if (use_root_stencil) { if (rho) OT_SOA(PREC_FAST, true, true); else OT_SOA(PREC_FAST, false, true); }
+        else { if (rho) OT_SOA(PREC_FAST, true, false); else OT_SOA(PREC_FAST, false, false); }
+    }
+#undef OT_SOA
+    OT_CUDA(cudaGetLastError());
+    return OTFMM_OK;
+}
+
+int otfmm_m2l_soa_host(otfmm_context* ctx, const double* mon, const double* M, const double* com, double* L,
+                       double* L_c, int gsolve_type, int use_root_stencil, int precision) {
+    if (!ctx || !M || !com || !L) return fail(OTFMM_ERR_INVALID, "NULL argument");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    DeviceGuard g(ctx->device);
+    const size_t n_in = ENTRIES + 20 * (size_t)CL + 3 * (size_t)CL, n_out = 23 * (size_t)CLU;
+    if (!ctx->d_soa_scratch) OT_CUDA(cudaMalloc(&ctx->d_soa_scratch, sizeof(double) * (n_in + n_out)));
+    double* d_mon = ctx->d_soa_scratch;
+    double* d_M = d_mon + ENTRIES;
+    double* d_com = d_M + 20 * CL;
+    double* d_L = d_com + 3 * CL;
+    double* d_Lc = d_L + 20 * CLU;
+    if (mon) OT_CUDA(cudaMemcpy(d_mon, mon, sizeof(double) * ENTRIES, cudaMemcpyHostToDevice));
+    OT_CUDA(cudaMemcpy(d_M, M, sizeof(double) * 20 * CL, cudaMemcpyHostToDevice));
+    OT_CUDA(cudaMemcpy(d_com, com, sizeof(double) * 3 * CL, cudaMemcpyHostToDevice));
+    int rc = otfmm_m2l_soa(ctx, mon ? d_mon : nullptr, d_M, d_com, d_L, d_Lc, gsolve_type, use_root_stencil,
+                           precision, nullptr);
+    if (rc) return rc;
+    OT_CUDA(cudaMemcpy(L, d_L, sizeof(double) * 20 * CLU, cudaMemcpyDeviceToHost));
+    if (gsolve_type == OTFMM_RHO && L_c) OT_CUDA(cudaMemcpy(L_c, d_Lc, sizeof(double) * 3 * CLU, cudaMemcpyDeviceToHost));
+    return OTFMM_OK;
+}
+
+int otfmm_p2p_soa(otfmm_context* ctx, const double* mon, double dx, double* L4, int precision, void* stream) {
+    if (!ctx || !mon || !L4) return fail(OTFMM_ERR_INVALID, "NULL argument");
+    if (!(dx > 0.0)) return fail(OTFMM_ERR_INVALID, "dx must be positive");
+    int rc = check_precision(precision);
+    if (rc) return rc;
+    DeviceGuard g(ctx->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (precision == OTFMM_FP64_EXACT)
+        soa_p2p_kernel<PREC_EXACT><<<4, 128, 0, s>>>(mon, dx, L4, ctx->tables());
+    else
+        soa_p2p_kernel<PREC_FAST><<<4, 128, 0, s>>>(mon, dx, L4, ctx->tables());
+    OT_CUDA(cudaGetLastError());
+    return OTFMM_OK;
+}
+
+int otfmm_p2m_soa(otfmm_context* ctx, int d, const double* neighbor_M, const double* neighbor_com,
+                  const double* inner_com, double* L4, double* L_c, int gsolve_type, int reset_lc, int precision,
+                  void* stream) {
+    if (!ctx || !neighbor_M || !neighbor_com || !inner_com || !L4) return fail(OTFMM_ERR_INVALID, "NULL argument");
+    if (d < 0 || d >= 26) return fail(OTFMM_ERR_INVALID, "direction out of range");
+    const bool rho = (gsolve_type == OTFMM_RHO);
+    if (rho && !L_c) return fail(OTFMM_ERR_INVALID, "L_c is NULL for RHO");
+    int rc = check_precision(precision);
+    if (rc) return rc;
+    DeviceGuard g(ctx->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (rho && reset_lc) {
+        zero_kernel<<<(3 * CLU + 255) / 256, 256, 0, s>>>(L_c, 3 * CLU);
+    }
+    const Tables t = ctx->tables();
+    if (precision == OTFMM_FP64_EXACT) {
+        if (rho) soa_p2m_kernel<PREC_EXACT, true><<<4, 128, 0, s>>>(d, neighbor_M, neighbor_com, inner_com, L4, L_c, t);
+        else soa_p2m_kernel<PREC_EXACT, false><<<4, 128, 0, s>>>(d, neighbor_M, neighbor_com, inner_com, L4, L_c, t);
+    } else {
+        if (rho) soa_p2m_kernel<PREC_FAST, true><<<4, 128, 0, s>>>(d, neighbor_M, neighbor_com, inner_com, L4, L_c, t);
+        else soa_p2m_kernel<PREC_FAST, false><<<4, 128, 0, s>>>(d, neighbor_M, neighbor_com, inner_com, L4, L_c, t);
+    }
+    OT_CUDA(cudaGetLastError());
+    return OTFMM_OK;
+}
+
+int otfmm_batch(otfmm_context* ctx, const double* pool_M, const double* pool_com, const double* pool_mon,
+                const uint8_t* pool_is_leaf, int32_t n_subgrids, const otfmm_work_item* items, int32_t n_items,
+                double* L, double* L_c, int gsolve_type, int precision, void* stream) {
+    if (!ctx || !pool_M || !pool_com || !pool_mon || !pool_is_leaf || !items || !L || !L_c)
+        return fail(OTFMM_ERR_INVALID, "NULL argument");
+    if (n_subgrids <= 0 || n_items < 0 || n_items > (1 << 29)) return fail(OTFMM_ERR_INVALID, "bad sizes");
+    if (gsolve_type != OTFMM_RHO && gsolve_type != OTFMM_DRHODT) return fail(OTFMM_ERR_INVALID, "bad gsolve_type");
+    int rc = check_precision(precision);
+    if (rc) return rc;
+    if (n_items == 0) return OTFMM_OK;
+    DeviceGuard g(ctx->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    OT_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), s));
+    BatchArgs a{pool_M, pool_com, pool_mon, pool_is_leaf, n_subgrids, items, n_items, L, L_c, ctx->tables(),
+                ctx->d_err};
+    const size_t bytes = SMEM_DOUBLES * sizeof(double);
+    const dim3 grid(2 * n_items);
+    const bool rho = (gsolve_type == OTFMM_RHO);
+    if (precision == OTFMM_FP64_EXACT) {
+        if (rho) batch_kernel<PREC_EXACT, true><<<grid, THREADS, bytes, s>>>(a);
+        else batch_kernel<PREC_EXACT, false><<<grid, THREADS, bytes, s>>>(a);
+    } else {
+        if (rho) batch_kernel<PREC_FAST, true><<<grid, THREADS, bytes, s>>>(a);
+        else batch_kernel<PREC_FAST, false><<<grid, THREADS, bytes, s>>>(a);
+    }
+    OT_CUDA(cudaGetLastError());
+    return OTFMM_OK;
+}
+
+int otfmm_batch_status(otfmm_context* ctx, void* stream) {
+    if (!ctx) return fail(OTFMM_ERR_INVALID, "NULL context");
+    DeviceGuard g(ctx->device);
+    int h = 0;
+    OT_CUDA(cudaMemcpyAsync(&h, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    OT_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    if (h) return fail(OTFMM_ERR_DEVICE, "a work item failed validation on the device");
+    return OTFMM_OK;
+}
+
+int otfmm_measure_fma_peaks(int device, double* fp64_tflops, double* fp32_tflops) {
+    if (!fp64_tflops || !fp32_tflops) return fail(OTFMM_ERR_INVALID, "NULL argument");
+    DeviceGuard g(device);
+    int sms = 0;
+    OT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    const int blocks = sms * 8, threads = 256, iters = 4096;
+    void* out = nullptr;
+    OT_CUDA(cudaMalloc(&out, sizeof(double) * blocks * threads));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const double fmas = double(blocks) * threads * iters * 16 * 8;
+    float best64 = 1e30f, best32 = 1e30f;
+    for (int rep = 0; rep < 4; ++rep) {
+        float ms = 0;
+        cudaEventRecord(e0);
+        fma_probe_kernel<double><<<blocks, threads>>>((double*)out, iters, 0.999999, 1e-7);
+        cudaEventRecord(e1);
+        cudaEventSynchronize(e1);
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (rep > 0) best64 = std::min(best64, ms);
+        cudaEventRecord(e0);
+        fma_probe_kernel<float><<<blocks, threads>>>((float*)out, iters, 0.999999f, 1e-7f);
+        cudaEventRecord(e1);
+        cudaEventSynchronize(e1);
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (rep > 0) best32 = std::min(best32, ms);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(out);
+    OT_CUDA(cudaGetLastError());
+    *fp64_tflops = 2.0 * fmas / (best64 * 1e-3) / 1e12;
+    *fp32_tflops = 2.0 * fmas / (best32 * 1e-3) / 1e12;
+    return OTFMM_OK;
+}
+
+}   // extern "C"

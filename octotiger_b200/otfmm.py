@@ -1,0 +1,227 @@
+"""Host binding of libotfmm.so (the C ABI in include/otfmm.h).
+
+Device memory and streams come from PyTorch; the kernels are the library's.
+There is no CPU fallback: without the built library or a CUDA device every
+entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+from .layout import (COMPONENT_LENGTH, COMPONENT_LENGTH_UNPADDED, ENTRIES, NCELL, RHO, WORK_ITEM_DTYPE,
+                     SubgridPool, validate_work_list)
+
+LIB_PATH = Path(__file__).resolve().parent / "libotfmm.so"
+
+OTFMM_OK = 0
+ERRORS = {-1: "invalid argument", -2: "theta below minimum", -3: "CUDA error", -4: "device-side work item error",
+          -5: "unsupported"}
+FP64_EXACT, FP64, FP32_SPLIT = 0, 1, 2
+PRECISIONS = {"fp64_exact": FP64_EXACT, "fp64": FP64, "fp32_split": FP32_SPLIT}
+
+EXPORTED = ["otfmm_create", "otfmm_destroy", "otfmm_stencil_info", "otfmm_m2l_soa", "otfmm_m2l_soa_host",
+            "otfmm_p2p_soa", "otfmm_p2m_soa", "otfmm_batch", "otfmm_batch_status", "otfmm_last_error",
+            "otfmm_build_info", "otfmm_measure_fma_peaks"]
+
+_lib = None
+
+
+class OtfmmError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"otfmm error {code} ({ERRORS.get(code, '?')}): {msg}")
+        self.code = code
+
+
+def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
+    """Loads libotfmm.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not Path(path).exists():
+            raise FileNotFoundError(f"{path} not built: run `python -m octotiger_b200.build`")
+        lib = ctypes.CDLL(str(path))
+        vp, dp, i = ctypes.c_void_p, ctypes.c_double, ctypes.c_int
+        lib.otfmm_create.argtypes = [i, dp, ctypes.POINTER(vp)]
+        lib.otfmm_destroy.argtypes = [vp]
+        lib.otfmm_stencil_info.argtypes = [vp, vp, vp, vp, vp]
+        lib.otfmm_m2l_soa.argtypes = [vp, vp, vp, vp, vp, vp, i, i, i, vp]
+        lib.otfmm_m2l_soa_host.argtypes = [vp, vp, vp, vp, vp, vp, i, i, i]
+        lib.otfmm_p2p_soa.argtypes = [vp, vp, dp, vp, i, vp]
+        lib.otfmm_p2m_soa.argtypes = [vp, i, vp, vp, vp, vp, vp, i, i, i, vp]
+        lib.otfmm_batch.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int32, vp, ctypes.c_int32, vp, vp, i, i, vp]
+        lib.otfmm_batch_status.argtypes = [vp, vp]
+        lib.otfmm_last_error.restype = ctypes.c_char_p
+        lib.otfmm_build_info.restype = ctypes.c_char_p
+        lib.otfmm_measure_fma_peaks.argtypes = [i, ctypes.POINTER(dp), ctypes.POINTER(dp)]
+        _lib = lib
+    return _lib
+
+
+def _check(rc: int) -> None:
+    if rc != OTFMM_OK:
+        raise OtfmmError(rc, load_library().otfmm_last_error().decode())
+
+
+def _require_cuda():
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError("octotiger_b200 kernels need a CUDA device; there is no CPU fallback")
+    return torch
+
+
+def _ptr(t) -> ctypes.c_void_p:
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else ctypes.c_void_p(0)
+
+
+def _stream(stream) -> ctypes.c_void_p:
+    if stream is None:
+        import torch
+        stream = torch.cuda.current_stream()
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+def precision_code(precision) -> int:
+    return PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+
+
+class Context:
+    """A library context: device, opening angle and its stencil tables."""
+
+    def __init__(self, device: int = 0, theta: float = 0.5):
+        _require_cuda()
+        lib = load_library()
+        h = ctypes.c_void_p()
+        _check(lib.otfmm_create(int(device), float(theta), ctypes.byref(h)))
+        self.handle = h
+        self.device = device
+        self.theta = theta
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            load_library().otfmm_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def stencil_info(self) -> dict:
+        counts = np.zeros(3, np.int32)
+        mm = np.zeros(1331, np.uint8)
+        ph = np.zeros(1331, np.uint8)
+        pm = np.zeros(1331, np.uint8)
+        _check(load_library().otfmm_stencil_info(self.handle, counts.ctypes.data, mm.ctypes.data, ph.ctypes.data,
+                                                 pm.ctypes.data))
+        return dict(n_mpole=int(counts[0]), n_phase_one=int(counts[1]), n_p2p=int(counts[2]), mpole_mask=mm,
+                    mpole_phase=ph, p2p_mask=pm)
+
+    # ---------------------------------------------------------------- per subgrid (reference SoA layout)
+    def m2l_soa(self, mon, M, com, L, Lc, gsolve_type=RHO, use_root_stencil=False, precision=FP64, stream=None):
+        """Device tensors in the reference's SoA layout (see include/otfmm.h)."""
+        _check(load_library().otfmm_m2l_soa(self.handle, _ptr(mon), _ptr(M), _ptr(com), _ptr(L), _ptr(Lc),
+                                            int(gsolve_type), int(bool(use_root_stencil)),
+                                            precision_code(precision), _stream(stream)))
+
+    def m2l_soa_host(self, mon: np.ndarray, M: np.ndarray, com: np.ndarray, gsolve_type=RHO,
+                     use_root_stencil=False, precision=FP64):
+        """Host buffers in, host buffers out (the reference's launch_interface)."""
+        L = np.zeros(20 * COMPONENT_LENGTH_UNPADDED)
+        Lc = np.zeros(3 * COMPONENT_LENGTH_UNPADDED)
+        for a, n in ((mon, ENTRIES), (M, 20 * COMPONENT_LENGTH), (com, 3 * COMPONENT_LENGTH)):
+            if a is not None and (a.dtype != np.float64 or a.size < n or not a.flags.c_contiguous):
+                raise ValueError("SoA buffers must be contiguous float64 of the reference sizes")
+        _check(load_library().otfmm_m2l_soa_host(
+            self.handle, None if mon is None else mon.ctypes.data, M.ctypes.data, com.ctypes.data, L.ctypes.data,
+            Lc.ctypes.data, int(gsolve_type), int(bool(use_root_stencil)), precision_code(precision)))
+        return L, Lc
+
+    def p2p_soa(self, mon, dx, L4, precision=FP64, stream=None):
+        _check(load_library().otfmm_p2p_soa(self.handle, _ptr(mon), float(dx), _ptr(L4), precision_code(precision),
+                                            _stream(stream)))
+
+    def p2m_soa(self, d, nM, ncom, icom, L4, Lc, gsolve_type=RHO, reset_lc=True, precision=FP64, stream=None):
+        _check(load_library().otfmm_p2m_soa(self.handle, int(d), _ptr(nM), _ptr(ncom), _ptr(icom), _ptr(L4),
+                                            _ptr(Lc), int(gsolve_type), int(bool(reset_lc)),
+                                            precision_code(precision), _stream(stream)))
+
+    # ---------------------------------------------------------------- batched
+    def batch(self, dev: "DevicePool", items_dev, n_items: int, L, Lc, gsolve_type=RHO, precision=FP64,
+              stream=None):
+        _check(load_library().otfmm_batch(self.handle, _ptr(dev.M), _ptr(dev.com), _ptr(dev.mon), _ptr(dev.is_leaf),
+                                          ctypes.c_int32(dev.n), _ptr(items_dev), ctypes.c_int32(n_items), _ptr(L),
+                                          _ptr(Lc), int(gsolve_type), precision_code(precision), _stream(stream)))
+
+    def batch_status(self, stream=None) -> None:
+        _check(load_library().otfmm_batch_status(self.handle, _stream(stream)))
+
+
+@dataclass
+class DevicePool:
+    """A subgrid pool resident on the GPU (torch tensors)."""
+
+    M: object
+    com: object
+    mon: object
+    is_leaf: object
+    n: int
+
+    @classmethod
+    def upload(cls, pool: SubgridPool, device: int = 0, non_blocking: bool = False) -> "DevicePool":
+        torch = _require_cuda()
+        pool.validate()
+        dev = torch.device("cuda", device)
+        t = {k: torch.from_numpy(getattr(pool, k)).to(dev, non_blocking=non_blocking)
+             for k in ("M", "com", "mon", "is_leaf")}
+        return cls(n=pool.n, **t)
+
+
+def order_work_list(items: np.ndarray) -> np.ndarray:
+    """Multipole (heaviest) items first: the block scheduler then fills the
+    GPU with the long tiles and ends with the short leaf tiles."""
+    key = np.where(items["kind"] == 2, 1, 0)
+    return np.ascontiguousarray(items[np.argsort(key, kind="stable")])
+
+
+def upload_work_list(items: np.ndarray, n_subgrids: int, device: int = 0):
+    torch = _require_cuda()
+    validate_work_list(items, n_subgrids)
+    raw = np.ascontiguousarray(items).view(np.uint8).reshape(-1)
+    return torch.from_numpy(raw.copy()).to(torch.device("cuda", device))
+
+
+class BatchSolver:
+    """Runs one gravity solve's work list on the GPU from a resident pool."""
+
+    def __init__(self, ctx: Context, pool: SubgridPool, items: np.ndarray):
+        torch = _require_cuda()
+        self.ctx = ctx
+        self.dev = DevicePool.upload(pool, ctx.device)
+        self.items_host = order_work_list(items)
+        self.items = upload_work_list(self.items_host, pool.n, ctx.device)
+        self.n_items = len(items)
+        d = torch.device("cuda", ctx.device)
+        self.L = torch.zeros((pool.n, 20, NCELL), dtype=torch.float64, device=d)
+        self.Lc = torch.zeros((pool.n, 3, NCELL), dtype=torch.float64, device=d)
+
+    def run(self, gsolve_type=RHO, precision=FP64, stream=None) -> None:
+        self.ctx.batch(self.dev, self.items, self.n_items, self.L, self.Lc, gsolve_type, precision, stream)
+
+    def results(self):
+        self.ctx.batch_status()
+        return self.L.cpu().numpy(), self.Lc.cpu().numpy()
+
+
+def build_info() -> str:
+    return load_library().otfmm_build_info().decode()
+
+
+def measure_fma_peaks(device: int = 0) -> tuple[float, float]:
+    _require_cuda()
+    a, b = ctypes.c_double(), ctypes.c_double()
+    _check(load_library().otfmm_measure_fma_peaks(int(device), ctypes.byref(a), ctypes.byref(b)))
+    return a.value, b.value

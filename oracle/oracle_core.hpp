@@ -317,9 +317,11 @@ inline void p2m_cells(const int o[3], int cs[3], int ce[3]) {
 // ---------------------------------------------------------------- counting
 // Cell-interactions the reference evaluates for one work item: (cell,
 // partner) pairs that pass the stencil and coarse-distance masks.
-inline long long count_pairs(const Stencil& st, const Pool& pool, const WorkItem& it) {
+// n[0] M2L, n[1] root M2L, n[2] P2P, n[3] P2M pairs.
+inline void count_pairs(const Stencil& st, const Pool& pool, const WorkItem& it, long long n4[4]) {
     const double trs = (1.0 / st.theta) * (1.0 / st.theta);
     long long n = 0;
+    n4[0] = n4[1] = n4[2] = n4[3] = 0;
     if (it.kind == KIND_M2L_ROOT) {
         for (int c = 0; c < NCELL; ++c)
             for (int p = 0; p < NCELL; ++p) {
@@ -329,7 +331,8 @@ inline long long count_pairs(const Stencil& st, const Pool& pool, const WorkItem
                     continue;
                 ++n;
             }
-        return n;
+        n4[1] = n;
+        return;
     }
     const uint8_t* mask = (it.kind == KIND_M2L) ? st.mpole_mask : st.p2p_mask;
     for (int x = 0; x < INX; ++x)
@@ -344,6 +347,8 @@ inline long long count_pairs(const Stencil& st, const Pool& pool, const WorkItem
                             const int dzc = coarse(z + INX) - coarse(z + INX + sz);
                             if (double(dxc * dxc + dyc * dyc + dzc * dzc) < trs) ++n;
                         }
+    n4[it.kind == KIND_LEAF ? 2 : 0] = n;
+    n = 0;
     if (it.kind == KIND_LEAF) {
         // P2M pairs with refined neighbours
         for (int d = 0; d < 26; ++d) {
@@ -369,8 +374,8 @@ inline long long count_pairs(const Stencil& st, const Pool& pool, const WorkItem
                                     if (double(a * a + b * b + c * c) < trs) ++n;
                                 }
         }
+        n4[3] = n;
     }
-    return n;
 }
 
 // ---------------------------------------------------------------- batch driver

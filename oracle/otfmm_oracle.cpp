@@ -400,16 +400,19 @@ int oracle_batch(double theta, const double* M, const double* com, const double*
 }
 
 long long oracle_count_pairs(double theta, const uint8_t* is_leaf, int n_sub, const ora::WorkItem* items,
-                             int n_items, long long* per_kind /*3*/) {
+                             int n_items, long long* per_class /*4: m2l, root, p2p, p2m*/) {
     const ora::Stencil& st = ora::stencil_for(theta);
     if (!st.ok) return -1;
     ora::Pool pool{nullptr, nullptr, nullptr, is_leaf, n_sub};
     long long total = 0;
-    if (per_kind) per_kind[0] = per_kind[1] = per_kind[2] = 0;
+    if (per_class) per_class[0] = per_class[1] = per_class[2] = per_class[3] = 0;
     for (int i = 0; i < n_items; ++i) {
-        const long long n = ora::count_pairs(st, pool, items[i]);
-        total += n;
-        if (per_kind) per_kind[items[i].kind] += n;
+        long long n4[4];
+        ora::count_pairs(st, pool, items[i], n4);
+        for (int c = 0; c < 4; ++c) {
+            total += n4[c];
+            if (per_class) per_class[c] += n4[c];
+        }
     }
     return total;
 }

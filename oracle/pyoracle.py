@@ -116,7 +116,8 @@ class Oracle(_Common):
         return L, Lc
 
     def count_pairs(self, theta, pool: SubgridPool, items: np.ndarray):
-        per = np.zeros(3, np.int64)
+        """Total evaluated pairs and the split [M2L, root M2L, P2P, P2M]."""
+        per = np.zeros(4, np.int64)
         self.lib.oracle_count_pairs.restype = ctypes.c_longlong
         tot = self.lib.oracle_count_pairs(ctypes.c_double(theta), _ptr(pool.is_leaf, _u8p), ctypes.c_int(pool.n),
                                           items.ctypes.data_as(ctypes.c_void_p), ctypes.c_int(len(items)),

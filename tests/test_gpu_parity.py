@@ -1,0 +1,199 @@
+"""GPU kernels (through the C ABI) against the oracle on the same seeded inputs.
+
+* OTFMM_FP64_EXACT: bit-for-bit equal to the oracle (which is bit-for-bit the
+  reference's own kernel arithmetic, tests/test_oracle.py);
+* OTFMM_FP64: within 1e-12 of the oracle, per output component relative to that
+  component's largest magnitude over the batch (L components cross zero).
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from octotiger_b200 import synthetic as syn
+from octotiger_b200.layout import COMPONENT_LENGTH_UNPADDED, DRHODT, NCELL, RHO
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-12
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    from octotiger_b200.otfmm import Context
+    c = Context(0, 0.5)
+    yield c
+    c.close()
+
+
+def scaled_err(a, ref):
+    """max |a - ref| / max |ref| per leading component axis."""
+    a = np.asarray(a)
+    ref = np.asarray(ref)
+    axes = tuple(i for i in range(ref.ndim) if i != ref.ndim - 2) if ref.ndim >= 2 else None
+    num = np.abs(a - ref).max(axis=axes)
+    den = np.abs(ref).max(axis=axes)
+    return np.where(den > 0, num / np.where(den > 0, den, 1), num)
+
+
+def run_batch(ctx, b, solve, precision):
+    from octotiger_b200.otfmm import BatchSolver
+    s = BatchSolver(ctx, b.pool, b.items)
+    s.run(solve, precision)
+    return s.results()
+
+
+CASES = {
+    "single": lambda: syn.single_subgrid(seed=21),
+    "root": lambda: syn.root_subgrid(seed=22),
+    "mixed": lambda: syn.single_subgrid(seed=23, leaf_dirs=(0, 4, 12, 13, 25), empty_dirs=(1, 7, 20)),
+    "leaf": lambda: syn.single_subgrid(seed=24, leaf_centre=True, leaf_dirs=tuple(range(0, 26, 2)),
+                                       empty_dirs=(5,)),
+    "leaf_all_refined": lambda: syn.single_subgrid(seed=25, leaf_centre=True),
+    "leaf_only_leaves": lambda: syn.single_subgrid(seed=26, leaf_centre=True, leaf_dirs=tuple(range(26))),
+    "uniform_level2": lambda: syn.uniform_level(2, seed=27),
+}
+
+
+@pytest.mark.parametrize("solve", [RHO, DRHODT])
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_batch_exact_is_bit_identical(ctx, oracle, name, solve):
+    b = CASES[name]()
+    L, Lc = run_batch(ctx, b, solve, "fp64_exact")
+    Lo, Lco = oracle.batch(0.5, b.pool, b.items, rho=(solve == RHO))
+    sel = b.items["subgrid"]
+    np.testing.assert_array_equal(L[sel], Lo[sel])
+    np.testing.assert_array_equal(Lc[sel], Lco[sel])
+
+
+@pytest.mark.parametrize("solve", [RHO, DRHODT])
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_batch_fast_fp64_within_1e12(ctx, oracle, name, solve):
+    b = CASES[name]()
+    L, Lc = run_batch(ctx, b, solve, "fp64")
+    Lo, Lco = oracle.batch(0.5, b.pool, b.items, rho=(solve == RHO))
+    sel = b.items["subgrid"]
+    assert scaled_err(L[sel], Lo[sel]).max() <= FP64_TOL
+    if solve == RHO:
+        assert scaled_err(Lc[sel], Lco[sel]).max() <= FP64_TOL
+    else:
+        assert not Lc[sel].any()
+
+
+def test_uniform_level3_full_size_fast(ctx, oracle):
+    """The 512-subgrid batch (64^3 cells) at full size."""
+    b = syn.uniform_level(3)
+    L, Lc = run_batch(ctx, b, RHO, "fp64")
+    Lo, Lco = oracle.batch(0.5, b.pool, b.items, rho=True)
+    assert scaled_err(L, Lo).max() <= FP64_TOL
+    assert scaled_err(Lc, Lco).max() <= FP64_TOL
+
+
+@pytest.mark.parametrize("precision", ["fp64_exact", "fp64"])
+@pytest.mark.parametrize("root", [False, True])
+@pytest.mark.parametrize("solve", [RHO, DRHODT])
+def test_soa_entry_points(ctx, oracle, precision, root, solve):
+    import torch
+    b = syn.root_subgrid(seed=31) if root else syn.single_subgrid(seed=31, leaf_dirs=(2, 17), empty_dirs=(9,))
+    mon, M, com = oracle.stage_m2l(b.pool, b.items[0])
+    Lo, Lco = oracle.m2l_soa(0.5, mon, M, com, rho=(solve == RHO), root=root)
+    d = torch.device("cuda", 0)
+    tm, tM, tc = (torch.from_numpy(x).to(d) for x in (mon, M, com))
+    L = torch.zeros(20 * COMPONENT_LENGTH_UNPADDED, dtype=torch.float64, device=d)
+    Lc = torch.zeros(3 * COMPONENT_LENGTH_UNPADDED, dtype=torch.float64, device=d)
+    ctx.m2l_soa(tm, tM, tc, L, Lc, solve, root, precision)
+    torch.cuda.synchronize()
+    Lh = L.cpu().numpy().reshape(20, -1)[:, :NCELL]
+    Lch = Lc.cpu().numpy().reshape(3, -1)[:, :NCELL]
+    Lo = Lo.reshape(20, -1)[:, :NCELL]
+    Lco = Lco.reshape(3, -1)[:, :NCELL]
+    if precision == "fp64_exact":
+        np.testing.assert_array_equal(Lh, Lo)
+        if solve == RHO:
+            np.testing.assert_array_equal(Lch, Lco)
+    else:
+        assert scaled_err(Lh, Lo).max() <= FP64_TOL
+        if solve == RHO:
+            assert scaled_err(Lch, Lco).max() <= FP64_TOL
+    # host-buffer variant of the same call
+    Lh2, Lch2 = ctx.m2l_soa_host(None if root else mon, M, com, solve, root, precision)
+    np.testing.assert_array_equal(Lh2.reshape(20, -1)[:, :NCELL], Lh)
+    if solve == RHO:
+        np.testing.assert_array_equal(Lch2.reshape(3, -1)[:, :NCELL], Lch)
+
+
+@pytest.mark.parametrize("precision", ["fp64_exact", "fp64"])
+@pytest.mark.parametrize("solve", [RHO, DRHODT])
+def test_p2p_p2m_soa_entry_points(ctx, oracle, precision, solve):
+    import torch
+    b = syn.single_subgrid(seed=41, leaf_centre=True, leaf_dirs=(0, 1, 2, 13, 24))
+    mon = oracle.stage_p2p(b.pool, b.items[0])
+    dx = float(b.items[0]["dx"])
+    L4o = oracle.p2p_soa(0.5, mon, dx)
+    d = torch.device("cuda", 0)
+    L4 = torch.zeros(4 * COMPONENT_LENGTH_UNPADDED, dtype=torch.float64, device=d)
+    ctx.p2p_soa(torch.from_numpy(mon).to(d), dx, L4, precision)
+    torch.cuda.synchronize()
+    got = L4.cpu().numpy().reshape(4, -1)[:, :NCELL]
+    exp = L4o.reshape(4, -1)[:, :NCELL]
+    if precision == "fp64_exact":
+        np.testing.assert_array_equal(got, exp)
+    else:
+        assert scaled_err(got, exp).max() <= FP64_TOL
+    icom = np.zeros(3 * COMPONENT_LENGTH_UNPADDED)
+    icom.reshape(3, -1)[:, :NCELL] = b.pool.com[0]
+    Lco = np.zeros(3 * COMPONENT_LENGTH_UNPADDED)
+    Lc = torch.zeros(3 * COMPONENT_LENGTH_UNPADDED, dtype=torch.float64, device=d)
+    ticom = torch.from_numpy(icom).to(d)
+    first = True
+    for dd in range(26):
+        nb = int(b.items[0]["neighbors"][dd])
+        if nb < 0 or b.pool.is_leaf[nb]:
+            continue
+        nM, ncom, stride = oracle.stage_p2m(b.pool, nb, dd)
+        oracle.p2m_dir(0.5, dd, nM, ncom, stride, icom, L4o, Lco, rho=(solve == RHO), reset=first)
+        ctx.p2m_soa(dd, torch.from_numpy(nM).to(d), torch.from_numpy(ncom).to(d), ticom, L4, Lc, solve, first,
+                    precision)
+        first = False
+    torch.cuda.synchronize()
+    got = L4.cpu().numpy().reshape(4, -1)[:, :NCELL]
+    exp = L4o.reshape(4, -1)[:, :NCELL]
+    gotc = Lc.cpu().numpy().reshape(3, -1)[:, :NCELL]
+    expc = Lco.reshape(3, -1)[:, :NCELL]
+    if precision == "fp64_exact":
+        np.testing.assert_array_equal(got, exp)
+        if solve == RHO:
+            np.testing.assert_array_equal(gotc, expc)
+    else:
+        assert scaled_err(got, exp).max() <= FP64_TOL
+        if solve == RHO:
+            assert scaled_err(gotc, expc).max() <= FP64_TOL
+
+
+def test_device_rejects_bad_work_item(ctx):
+    """A neighbour id outside the pool is caught by the kernel's own checks
+    (no access is made with it) and reported as OTFMM_ERR_DEVICE."""
+    import torch
+    from octotiger_b200.otfmm import DevicePool, OtfmmError
+    b = syn.single_subgrid(seed=51)
+    dev = DevicePool.upload(b.pool)
+    items = b.items.copy()
+    items[0]["neighbors"][3] = b.pool.n + 100
+    raw = torch.from_numpy(items.view(np.uint8).reshape(-1).copy()).cuda()
+    L = torch.full((b.pool.n, 20, NCELL), 7.0, dtype=torch.float64, device="cuda")
+    Lc = torch.zeros((b.pool.n, 3, NCELL), dtype=torch.float64, device="cuda")
+    ctx.batch(dev, raw, 1, L, Lc, RHO, "fp64")
+    with pytest.raises(OtfmmError) as e:
+        ctx.batch_status()
+    assert e.value.code == -4
+    assert bool((L == 7.0).all())   # outputs of the rejected item untouched
+    # the context stays usable
+    good = torch.from_numpy(b.items.view(np.uint8).reshape(-1).copy()).cuda()
+    ctx.batch(dev, good, 1, L, Lc, RHO, "fp64")
+    ctx.batch_status()
+
+
+def test_fma_peaks_measurable():
+    from octotiger_b200.otfmm import measure_fma_peaks
+    f64, f32 = measure_fma_peaks(0)
+    assert 5.0 < f64 < 200.0 and 10.0 < f32 < 400.0

@@ -36,6 +36,7 @@ def test_stencil_sizes(oracle):
 def test_pairs_per_subgrid(oracle):
     b = syn.single_subgrid()
     total, per = oracle.count_pairs(0.5, b.pool, b.items)
+    assert per[0] == total
     assert total == 110080 == 215 * NCELL
     b34 = syn.single_subgrid(theta=0.34)
     assert oracle.count_pairs(0.34, b34.pool, b34.items)[0] == 743 * NCELL
