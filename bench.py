@@ -145,6 +145,26 @@ def cpu_reference_rate(batch, solve: int, seconds: float = 10.0, nthreads: int |
             "seconds": round(el, 3)}
 
 
+def accuracy_report(L, Lc, Lref, Lcref) -> dict:
+    """Relative errors per output group against the exact FP64 result:
+    max |err| / max |ref| per component (worst component of the group) and the
+    relative L2 norm of the group."""
+    groups = {"potential_L0": (0, 1), "force_L1_3": (1, 4), "higher_L4_19": (4, 20)}
+    out = {}
+    for name, (a, b) in groups.items():
+        d = (L[:, a:b] - Lref[:, a:b]).double()
+        r = Lref[:, a:b].double()
+        mx = (d.abs().amax(dim=(0, 2)) / r.abs().amax(dim=(0, 2)).clamp_min(1e-300)).max().item()
+        l2 = (d.norm() / r.norm().clamp_min(1e-300)).item()
+        out[name] = {"max_rel": mx, "l2_rel": l2}
+    d = (Lc - Lcref).double()
+    r = Lcref.double()
+    if r.abs().max().item() > 0:
+        out["L_c"] = {"max_rel": (d.abs().amax(dim=(0, 2)) / r.abs().amax(dim=(0, 2)).clamp_min(1e-300)).max().item(),
+                      "l2_rel": (d.norm() / r.norm()).item()}
+    return out
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -249,6 +269,16 @@ def gpu_arm(args) -> None:
         others[prec] = {"value": counts["total"] * max(3, args.steps // 2) / (ms * 1e-3),
                         "ms_per_step": ms / max(3, args.steps // 2)}
 
+    # accuracy of the headline form against the exact FP64 form (bit-identical
+    # to the reference arithmetic) on this workload
+    accuracy = None
+    if args.precision != "fp64_exact":
+        solver.run(solve, "fp64_exact")
+        Le, Lce = solver.L.clone(), solver.Lc.clone()
+        solver.run(solve, args.precision)
+        torch.cuda.synchronize()
+        accuracy = accuracy_report(solver.L, solver.Lc, Le, Lce)
+
     # end to end: host pool + work list in pinned memory -> GPU -> L, L_c back
     pin = {k: torch.from_numpy(getattr(batch.pool, k)).pin_memory() for k in ("M", "com", "mon", "is_leaf")}
     items_h = order_work_list(batch.items)
@@ -318,6 +348,7 @@ def gpu_arm(args) -> None:
                    "l2": "flushed (256 MiB write) before every timed step",
                    "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU"},
         "precisions": others,
+        "accuracy_vs_fp64_exact": accuracy,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": args.steps,
         "roofline": roof,
@@ -342,7 +373,7 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="uniform_level3", choices=["uniform_level3", "amr_polytrope"])
-    ap.add_argument("--precision", default="fp64", choices=["fp32_split", "fp64", "fp64_exact"])
+    ap.add_argument("--precision", default="fp32_split", choices=["fp32_split", "fp64", "fp64_exact"])
     ap.add_argument("--compare", nargs="*", default=["fp64", "fp64_exact"])
     ap.add_argument("--gsolve", default="rho", choices=["rho", "drhodt"])
     ap.add_argument("--cpu-seconds", type=float, default=10.0)

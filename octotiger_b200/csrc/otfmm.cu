@@ -74,6 +74,25 @@ constexpr int ROOT_SMEM_DOUBLES = NCOMP * NCELL;
 static_assert(ROOT_SMEM_DOUBLES <= SMEM_DOUBLES, "root staging fits");
 static_assert(RB % 16 == 12 || RB % 16 == 4, "row stride must keep 4x4 lane blocks conflict-free");
 
+// FP32-split layout: per cell 14 FP64 components (centre of mass / dx, mass,
+// scaled octupoles for L_c) and 20 FP32 components (scaled moments). Rows of
+// 6 cells: 84 doubles then 120 floats, padded to 148 doubles (= 4 mod 16:
+// conflict-free 8-byte loads per half-warp); the x stride of 890 doubles
+// makes the 32 lanes' 4-byte loads hit 32 distinct banks.
+constexpr int S_DCOMP = 14;
+constexpr int S_FCOMP = 20;
+constexpr int S_RB = 148;
+constexpr int S_FOFF = 2 * S_DCOMP * SUB_YZ;   // float offset of the FP32 part within a row
+constexpr int S_XS = 890;
+constexpr int S_CLS = (REG_X / 2) * S_XS;
+constexpr int S_SMEM_DOUBLES = 8 * S_CLS;      // 28480 doubles = 227840 bytes
+constexpr int SPLIT_CHUNK = 16;                // FP32 partial sums promoted to FP64 every 16 partners
+static_assert(S_RB >= S_DCOMP * SUB_YZ + S_FCOMP * SUB_YZ / 2, "split row fits");
+static_assert(S_RB % 16 == 4 || S_RB % 16 == 12, "split rows conflict-free for 8-byte loads");
+static_assert(S_XS >= SUB_YZ * S_RB && (S_XS % 16 == 2 || S_XS % 16 == 6 || S_XS % 16 == 10 || S_XS % 16 == 14),
+              "split x stride");
+static_assert(S_SMEM_DOUBLES * 8 <= 232448, "split layout fits the 227 KB shared-memory limit");
+
 // Entry flags
 constexpr int F_FAR = 1;    // phase-one offset: full multipole partner
 constexpr int F_NEAR = 2;   // monopole-only offset
@@ -81,6 +100,9 @@ constexpr int F_NEAR = 2;   // monopole-only offset
 struct Tables {
     const int2* entries;     // [8][MAX_ENTRIES]: x = smem delta, y = packed offset/flags/stencil index
     const int* count;        // [8]
+    const int2* entries_fast;   // same entries, full-multipole (far) offsets first
+    const int* count_far;       // [8] number of far offsets
+    const int4* entries_split;  // far-first entries for the split layout: x = double delta, y = packed, z = float delta
     const double* four;      // [FULL][4] monopole constants
     const uint8_t* phase;    // [FULL] inner_stencil_masks (true outside the stencil)
 };
@@ -96,7 +118,7 @@ __device__ __forceinline__ int raw_dir(int ax, int ay, int az) {
     return ((ax >> 3) + 1) + 3 * ((ay >> 3) + 1) + 9 * ((az >> 3) + 1);
 }
 
-enum : int { PREC_EXACT = OTFMM_FP64_EXACT, PREC_FAST = OTFMM_FP64 };
+enum : int { PREC_EXACT = OTFMM_FP64_EXACT, PREC_FAST = OTFMM_FP64, PREC_SPLIT = OTFMM_FP32_SPLIT };
 
 // Scaling folded into staged moments by the fast form.
 template <int PREC>
@@ -274,35 +296,170 @@ __device__ void m2l_tile(const double* sm, int x0, const Tables& t, uint32_t mon
         double mc_oct[10];
 #pragma unroll
         for (int o = 0; o < 10; ++o) mc_oct[o] = sm[c.own + (10 + o) * SUB_YZ];
+        const int nfar = t.count_far[c.p];
+        const int2* entf = t.entries_fast + c.p * MAX_ENTRIES;
+        // full-multipole partners: branch-free, two pairs in flight
+#pragma unroll 2
+        for (int e = 0; e < nfar; ++e) {
+            const int pb = __ldg(&entf[e].x) + c.lane_off;
+            double Y[3], mp[20];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) Y[a] = sm[pb + (20 + a) * SUB_YZ];
+#pragma unroll
+            for (int q = 0; q < 20; ++q) mp[q] = sm[pb + q * SUB_YZ];
+            fast_m2l_pair<RHO>(X, Y, mp, mc_oct, inv_m0, acc, corr);
+        }
+        // monopole-only offsets: only leaf-neighbour partners contribute
 #pragma unroll 1
-        for (int e = 0; e < n; ++e) {
-            const int2 en = __ldg(ent + e);
+        for (int e = nfar; e < n; ++e) {
+            const int2 en = __ldg(entf + e);
             const int pb = en.x + c.lane_off;
+            const int ax = c.cx + entry_sx(en.y), ay = c.cy + entry_sy(en.y), az = c.cz + entry_sz(en.y);
+            double m0;
+            if (near_mon) {
+                m0 = near_mon[(ax + INX - PAD_OFF) * PSTRIDE * PSTRIDE + (ay + INX - PAD_OFF) * PSTRIDE +
+                              (az + INX - PAD_OFF)];
+            } else {
+                if (!((monomask >> raw_dir(ax, ay, az)) & 1u)) continue;
+                m0 = sm[pb];
+            }
             double Y[3];
 #pragma unroll
             for (int a = 0; a < 3; ++a) Y[a] = sm[pb + (20 + a) * SUB_YZ];
-            if (entry_flags(en.y) & F_FAR) {
-                double mp[20];
-#pragma unroll
-                for (int q = 0; q < 20; ++q) mp[q] = sm[pb + q * SUB_YZ];
-                fast_m2l_pair<RHO>(X, Y, mp, mc_oct, inv_m0, acc, corr);
-            } else {
-                const int ax = c.cx + entry_sx(en.y), ay = c.cy + entry_sy(en.y), az = c.cz + entry_sz(en.y);
-                double m0;
-                if (near_mon) {
-                    m0 = near_mon[(ax + INX - PAD_OFF) * PSTRIDE * PSTRIDE + (ay + INX - PAD_OFF) * PSTRIDE +
-                                  (az + INX - PAD_OFF)];
-                } else {
-                    if (!((monomask >> raw_dir(ax, ay, az)) & 1u)) continue;
-                    m0 = sm[pb];
-                }
-                fast_m2l_mass_pair<RHO>(X, Y, m0, mc_oct, inv_m0, acc, corr);
-            }
+            fast_m2l_mass_pair<RHO>(X, Y, m0, mc_oct, inv_m0, acc, corr);
         }
     }
     const int cf = c.cx * 64 + c.cy * 8 + c.cz;
 #pragma unroll
     for (int q = 0; q < 20; ++q) out.L[q * out.stride + cf] = acc[q];
+    write_lc<RHO>(out, cf, corr);
+}
+
+// Split staging from the pool: same sources as stage_region_pool, values in
+// units of dx (inv_dx = 1/dx), multinomial factors folded in.
+__device__ void stage_region_split(double* sm, const ItemInfo& it, int x0, double inv_dx, const double* __restrict__ M,
+                                   const double* __restrict__ com, const double* __restrict__ mon,
+                                   const uint8_t* __restrict__ is_leaf) {
+    float* smf = reinterpret_cast<float*>(sm);
+    const double inv2 = inv_dx * inv_dx, inv3 = inv2 * inv_dx;
+    for (int r = threadIdx.x; r < REG_CELLS; r += blockDim.x) {
+        const int rx = r / (REG_YZ * REG_YZ), ry = (r / REG_YZ) % REG_YZ, rz = r % REG_YZ;
+        const int ax = x0 - 2 + rx, ay = ry - 2, az = rz - 2;
+        const int raw = raw_dir(ax, ay, az);
+        const bool centre = (raw == 13);
+        const int src = centre ? it.subgrid : it.nb[raw < 13 ? raw : raw - 1];
+        const int u = (ax & 7) * 64 + (ay & 7) * 8 + (az & 7);
+        const int cls = ((ax & 1) << 2) | ((ay & 1) << 1) | (az & 1);
+        const int row = cls * S_CLS + (rx >> 1) * S_XS + (ry >> 1) * S_RB;
+        const int zp = rz >> 1;
+        double m[20], c[3];
+        if (src < 0) {
+#pragma unroll
+            for (int q = 0; q < 20; ++q) m[q] = 0.0;
+#pragma unroll
+            for (int a = 0; a < 3; ++a) c[a] = 0.0;
+        } else if (!centre && is_leaf[src]) {
+            m[0] = mon[(size_t)src * NCELL + u];
+#pragma unroll
+            for (int q = 1; q < 20; ++q) m[q] = 0.0;
+            const int ip[3] = {ax + INX, ay + INX, az + INX};
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+                c[a] = __dsub_rn(__dadd_rn(__dmul_rn((double)ip[a], it.dx), it.xbase[a]), __dmul_rn((double)INX, it.dx));
+        } else {
+#pragma unroll
+            for (int q = 0; q < 20; ++q) m[q] = M[((size_t)src * 20 + q) * NCELL + u];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) c[a] = com[((size_t)src * 3 + a) * NCELL + u];
+        }
+#pragma unroll
+        for (int q = 1; q < 4; ++q) m[q] *= inv_dx;
+#pragma unroll
+        for (int q = 4; q < 10; ++q) m[q] *= (factor_of(q) / 2.0) * inv2;
+#pragma unroll
+        for (int q = 10; q < 20; ++q) m[q] *= (factor_of(q) / 6.0) * inv3;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) sm[row + a * SUB_YZ + zp] = c[a] * inv_dx;
+        sm[row + 3 * SUB_YZ + zp] = m[0];
+#pragma unroll
+        for (int o = 0; o < 10; ++o) sm[row + (4 + o) * SUB_YZ + zp] = m[10 + o];
+#pragma unroll
+        for (int q = 0; q < 20; ++q) smf[2 * row + S_FOFF + q * SUB_YZ + zp] = (float)m[q];
+    }
+}
+
+// M2L over the split-staged region: FP32 tensor and contraction with FP64
+// chunk sums, FP64 centre-of-mass differences, derivative factors and L_c.
+template <bool RHO>
+__device__ void m2l_tile_split(const double* sm, int x0, const Tables& t, uint32_t monomask, double inv_dx,
+                               OutPtr out) {
+    const float* smf = reinterpret_cast<const float*>(sm);
+    const CellMap c = cell_map(x0);
+    const int lane_d = c.i * S_XS + c.j * S_RB + c.k;
+    const int lane_f = 2 * (c.i * S_XS + c.j * S_RB) + c.k;
+    const int own = c.p * S_CLS + (c.i + 1) * S_XS + (c.j + 1) * S_RB + (c.k + 1);
+    double X[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) X[a] = sm[own + a * SUB_YZ];
+    const double inv_m0 = 1.0 / sm[own + 3 * SUB_YZ];
+    double mc_oct[10];
+#pragma unroll
+    for (int o = 0; o < 10; ++o) mc_oct[o] = sm[own + (4 + o) * SUB_YZ];
+    double acc[20], corr[3] = {0.0, 0.0, 0.0};
+    float accf[20];
+#pragma unroll
+    for (int q = 0; q < 20; ++q) {
+        acc[q] = 0.0;
+        accf[q] = 0.0f;
+    }
+    const int n = t.count[c.p];
+    const int nfar = t.count_far[c.p];
+    const int4* ent = t.entries_split + c.p * MAX_ENTRIES;
+#pragma unroll 1
+    for (int e0 = 0; e0 < nfar; e0 += SPLIT_CHUNK) {
+        const int e1 = min(e0 + SPLIT_CHUNK, nfar);
+#pragma unroll 2
+        for (int e = e0; e < e1; ++e) {
+            const int4 en = __ldg(ent + e);
+            const int pd = en.x + lane_d, pf = en.z + lane_f;
+            double Y[3], mp_oct[10];
+            float mpf[20];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) Y[a] = sm[pd + a * SUB_YZ];
+            const double m0 = sm[pd + 3 * SUB_YZ];
+            if (RHO) {
+#pragma unroll
+                for (int o = 0; o < 10; ++o) mp_oct[o] = sm[pd + (4 + o) * SUB_YZ];
+            }
+#pragma unroll
+            for (int q = 0; q < 20; ++q) mpf[q] = smf[pf + q * SUB_YZ];
+            split_m2l_pair<RHO>(X, Y, mpf, m0, mp_oct, mc_oct, inv_m0, accf, corr);
+        }
+#pragma unroll
+        for (int q = 0; q < 20; ++q) {
+            acc[q] += (double)accf[q];
+            accf[q] = 0.0f;
+        }
+    }
+    // monopole-only offsets (leaf-neighbour partners), FP64 in dx units
+#pragma unroll 1
+    for (int e = nfar; e < n; ++e) {
+        const int4 en = __ldg(ent + e);
+        const int ax = c.cx + entry_sx(en.y), ay = c.cy + entry_sy(en.y), az = c.cz + entry_sz(en.y);
+        if (!((monomask >> raw_dir(ax, ay, az)) & 1u)) continue;
+        const int pd = en.x + lane_d;
+        double Y[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) Y[a] = sm[pd + a * SUB_YZ];
+        fast_m2l_mass_pair<RHO>(X, Y, sm[pd + 3 * SUB_YZ], mc_oct, inv_m0, acc, corr);
+    }
+    // back to physical units: L_(n) = L'_(n) dx^-(n+1), L_c = L_c' dx^-2
+    const double s1 = inv_dx, s2 = s1 * inv_dx, s3 = s2 * inv_dx, s4 = s3 * inv_dx;
+    const int cf = c.cx * 64 + c.cy * 8 + c.cz;
+#pragma unroll
+    for (int q = 0; q < 20; ++q) out.L[q * out.stride + cf] = acc[q] * (q == 0 ? s1 : q < 4 ? s2 : q < 10 ? s3 : s4);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) corr[a] *= s2;
     write_lc<RHO>(out, cf, corr);
 }
 
@@ -448,14 +605,16 @@ __global__ void __launch_bounds__(THREADS, 1) batch_kernel(BatchArgs a) {
     const int x0 = TILE_X * half;
     const size_t sub = (size_t)it.subgrid;
     OutPtr out{a.L + sub * 20 * NCELL, a.Lc + sub * 3 * NCELL, NCELL, true};
+    // the split form covers multipole tiles; leaf and root tiles use fast FP64
+    constexpr int P64 = (PREC == PREC_SPLIT) ? PREC_FAST : PREC;
     if (it.kind == OTFMM_KIND_M2L_ROOT) {
         const int base_sub = it.subgrid;
         for (int r = threadIdx.x; r < NCELL; r += blockDim.x)
             for (int q = 0; q < NCOMP; ++q)
-                sm[q * NCELL + r] = (q < 20) ? a.M[((size_t)base_sub * 20 + q) * NCELL + r] * stage_scale<PREC>(q)
+                sm[q * NCELL + r] = (q < 20) ? a.M[((size_t)base_sub * 20 + q) * NCELL + r] * stage_scale<P64>(q)
                                              : a.com[((size_t)base_sub * 3 + (q - 20)) * NCELL + r];
         __syncthreads();
-        root_tile<PREC, RHO>(sm, x0, a.t, out);
+        root_tile<P64, RHO>(sm, x0, a.t, out);
         return;
     }
     const bool leaf = (it.kind == OTFMM_KIND_LEAF);
@@ -468,12 +627,19 @@ __global__ void __launch_bounds__(THREADS, 1) batch_kernel(BatchArgs a) {
         const bool nb_leaf = a.is_leaf[nb] != 0;
         if (leaf ? !nb_leaf : nb_leaf) mask |= 1u << (d < 13 ? d : d + 1);
     }
-    stage_region_pool<PREC>(sm, it, x0, leaf, a.M, a.com, a.mon, a.is_leaf);
+    if (PREC == PREC_SPLIT && !leaf) {
+        const double inv_dx = 1.0 / it.dx;
+        stage_region_split(sm, it, x0, inv_dx, a.M, a.com, a.mon, a.is_leaf);
+        __syncthreads();
+        m2l_tile_split<RHO>(sm, x0, a.t, mask, inv_dx, out);
+        return;
+    }
+    stage_region_pool<P64>(sm, it, x0, leaf, a.M, a.com, a.mon, a.is_leaf);
     __syncthreads();
     if (leaf) {
-        leaf_tile<PREC, RHO>(sm, x0, a.t, mask, it.dx, out);
+        leaf_tile<P64, RHO>(sm, x0, a.t, mask, it.dx, out);
     } else {
-        m2l_tile<PREC, RHO>(sm, x0, a.t, mask, nullptr, out);
+        m2l_tile<P64, RHO>(sm, x0, a.t, mask, nullptr, out);
     }
 }
 
@@ -734,12 +900,16 @@ struct otfmm_context {
     int counts[8] = {};
     int2* d_entries = nullptr;
     int* d_count = nullptr;
+    int2* d_entries_fast = nullptr;
+    int* d_count_far = nullptr;
+    int4* d_entries_split = nullptr;
+    int counts_far[8] = {};
     double* d_four = nullptr;
     uint8_t* d_phase = nullptr;
     int* d_err = nullptr;
     double* d_soa_scratch = nullptr;   // host-buffer path staging
     std::mutex mu;
-    Tables tables() const { return Tables{d_entries, d_count, d_four, d_phase}; }
+    Tables tables() const { return Tables{d_entries, d_count, d_entries_fast, d_count_far, d_entries_split, d_four, d_phase}; }
 };
 
 namespace {
@@ -777,6 +947,8 @@ int ensure_attributes(int device) {
     rc = rc ? rc : set_smem(batch_kernel<PREC_EXACT, false>, bytes);
     rc = rc ? rc : set_smem(batch_kernel<PREC_FAST, true>, bytes);
     rc = rc ? rc : set_smem(batch_kernel<PREC_FAST, false>, bytes);
+    rc = rc ? rc : set_smem(batch_kernel<PREC_SPLIT, true>, S_SMEM_DOUBLES * (int)sizeof(double));
+    rc = rc ? rc : set_smem(batch_kernel<PREC_SPLIT, false>, S_SMEM_DOUBLES * (int)sizeof(double));
     rc = rc ? rc : set_smem(soa_m2l_kernel<PREC_EXACT, true, false>, bytes);
     rc = rc ? rc : set_smem(soa_m2l_kernel<PREC_EXACT, false, false>, bytes);
     rc = rc ? rc : set_smem(soa_m2l_kernel<PREC_FAST, true, false>, bytes);
@@ -789,10 +961,10 @@ int ensure_attributes(int device) {
     return rc;
 }
 
-int check_precision(int precision) {
-    if (precision != OTFMM_FP64_EXACT && precision != OTFMM_FP64)
-        return fail(OTFMM_ERR_UNSUPPORTED, "precision not available in this build");
-    return OTFMM_OK;
+int check_precision(int precision, bool batched = false) {
+    if (precision == OTFMM_FP64_EXACT || precision == OTFMM_FP64) return OTFMM_OK;
+    if (precision == OTFMM_FP32_SPLIT && batched) return OTFMM_OK;
+    return fail(OTFMM_ERR_UNSUPPORTED, "precision not available for this entry point (FP32 split is batched only)");
 }
 
 }   // namespace
@@ -802,7 +974,7 @@ extern "C" {
 const char* otfmm_last_error(void) { return g_last_error.c_str(); }
 
 const char* otfmm_build_info(void) {
-    return "otfmm sm_100a; tiles of 4x8x8 cells, 256 threads, 215040 B shared memory; theta >= 0.5";
+    return "otfmm sm_100a; tiles of 4x8x8 cells, 256 threads, 215040 B (FP64) / 227840 B (FP32 split) shared memory; theta >= 0.5";
 }
 
 int otfmm_create(int device, double theta, otfmm_context** out) {
@@ -828,6 +1000,28 @@ int otfmm_create(int device, double theta, otfmm_context** out) {
         return fail(OTFMM_ERR_UNSUPPORTED, "theta < 0.5 (coarse reach 2) is not built into this library");
     }
     ctx->reach = reach;
+    // split-layout table (far first, like the fast one)
+    std::vector<int4> entries_split(8 * MAX_ENTRIES, int4{0, 0, 0, 0});
+    // fast-form table: far offsets first (accumulation order is free there)
+    std::vector<int2> entries_fast(entries.size(), int2{0, 0});
+    for (int p = 0; p < 8; ++p) {
+        int k = 0;
+        for (int pass = 0; pass < 2; ++pass)
+            for (int e = 0; e < ctx->counts[p]; ++e) {
+                const int2 en = entries[p * MAX_ENTRIES + e];
+                const bool far = ((en.y >> 12) & 3) == F_FAR;
+                if (far == (pass == 0)) {
+                    const int sx = (en.y & 15) - 8, sy = ((en.y >> 4) & 15) - 8, sz = ((en.y >> 8) & 15) - 8;
+                    const int px = (p >> 2) & 1, py = (p >> 1) & 1, pz = p & 1;
+                    const int qx = px + 2 + sx, qy = py + 2 + sy, qz = pz + 2 + sz;
+                    const int cls = (((px + sx) & 1) << 2) | (((py + sy) & 1) << 1) | ((pz + sz) & 1);
+                    const int row = cls * S_CLS + (qx >> 1) * S_XS + (qy >> 1) * S_RB;
+                    entries_split[p * MAX_ENTRIES + k] = int4{row + (qz >> 1), en.y, 2 * row + S_FOFF + (qz >> 1), 0};
+                    entries_fast[p * MAX_ENTRIES + k++] = en;
+                }
+                if (pass == 0 && far) ++ctx->counts_far[p];
+            }
+    }
     DeviceGuard g(device);
     cudaError_t e;
     if ((e = cudaMalloc(&ctx->d_entries, sizeof(int2) * entries.size())) != cudaSuccess ||
@@ -835,6 +1029,14 @@ int otfmm_create(int device, double theta, otfmm_context** out) {
         (e = cudaMalloc(&ctx->d_four, sizeof(double) * 4 * FULL)) != cudaSuccess ||
         (e = cudaMalloc(&ctx->d_phase, FULL)) != cudaSuccess ||
         (e = cudaMalloc(&ctx->d_err, sizeof(int))) != cudaSuccess ||
+        (e = cudaMalloc(&ctx->d_entries_fast, sizeof(int2) * entries_fast.size())) != cudaSuccess ||
+        (e = cudaMalloc(&ctx->d_count_far, sizeof(int) * 8)) != cudaSuccess ||
+        (e = cudaMemcpy(ctx->d_entries_fast, entries_fast.data(), sizeof(int2) * entries_fast.size(),
+                        cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(ctx->d_count_far, ctx->counts_far, sizeof(int) * 8, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMalloc(&ctx->d_entries_split, sizeof(int4) * entries_split.size())) != cudaSuccess ||
+        (e = cudaMemcpy(ctx->d_entries_split, entries_split.data(), sizeof(int4) * entries_split.size(),
+                        cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemcpy(ctx->d_entries, entries.data(), sizeof(int2) * entries.size(), cudaMemcpyHostToDevice)) !=
             cudaSuccess ||
         (e = cudaMemcpy(ctx->d_count, ctx->counts, sizeof(int) * 8, cudaMemcpyHostToDevice)) != cudaSuccess ||
@@ -859,6 +1061,9 @@ int otfmm_destroy(otfmm_context* ctx) {
     DeviceGuard g(ctx->device);
     cudaFree(ctx->d_entries);
     cudaFree(ctx->d_count);
+    cudaFree(ctx->d_entries_fast);
+    cudaFree(ctx->d_entries_split);
+    cudaFree(ctx->d_count_far);
     cudaFree(ctx->d_four);
     cudaFree(ctx->d_phase);
     cudaFree(ctx->d_err);
@@ -976,7 +1181,7 @@ int otfmm_batch(otfmm_context* ctx, const double* pool_M, const double* pool_com
         return fail(OTFMM_ERR_INVALID, "NULL argument");
     if (n_subgrids <= 0 || n_items < 0 || n_items > (1 << 29)) return fail(OTFMM_ERR_INVALID, "bad sizes");
     if (gsolve_type != OTFMM_RHO && gsolve_type != OTFMM_DRHODT) return fail(OTFMM_ERR_INVALID, "bad gsolve_type");
-    int rc = check_precision(precision);
+    int rc = check_precision(precision, true);
     if (rc) return rc;
     if (n_items == 0) return OTFMM_OK;
     DeviceGuard g(ctx->device);
@@ -990,6 +1195,10 @@ int otfmm_batch(otfmm_context* ctx, const double* pool_M, const double* pool_com
     if (precision == OTFMM_FP64_EXACT) {
         if (rho) batch_kernel<PREC_EXACT, true><<<grid, THREADS, bytes, s>>>(a);
         else batch_kernel<PREC_EXACT, false><<<grid, THREADS, bytes, s>>>(a);
+    } else if (precision == OTFMM_FP32_SPLIT) {
+        const size_t sbytes = S_SMEM_DOUBLES * sizeof(double);
+        if (rho) batch_kernel<PREC_SPLIT, true><<<grid, THREADS, sbytes, s>>>(a);
+        else batch_kernel<PREC_SPLIT, false><<<grid, THREADS, sbytes, s>>>(a);
     } else {
         if (rho) batch_kernel<PREC_FAST, true><<<grid, THREADS, bytes, s>>>(a);
         else batch_kernel<PREC_FAST, false><<<grid, THREADS, bytes, s>>>(a);

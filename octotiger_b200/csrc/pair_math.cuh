@@ -19,6 +19,10 @@
 
 namespace otfmm {
 
+// Fused multiply-add with the precision of its operands (no promotion).
+__device__ __forceinline__ float fmat(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fmat(double a, double b, double c) { return __fma_rn(a, b, c); }
+
 // factor[] of compute_kernel_templates.hpp:37-39 (multinomial multiplicities).
 __host__ __device__ constexpr double factor_of(int k) {
     return (k == 5 || k == 6 || k == 8) ? 2.0
@@ -254,39 +258,93 @@ __device__ __forceinline__ void fast_d_factors(const double dX[3], FastDerivs& f
     D[19] = dX[2] * b2;
 }
 
-// Contraction shared by M2L and P2M for L0..L3 (quadrupole/octupole partner
-// moments; Scaled moments carry the factors).
-__device__ __forceinline__ void fast_low_terms(const double* m, const double* D, double* L, bool dipole) {
-#pragma unroll
-    for (int a = 0; a < 4; ++a) L[a] = fma(m[0], D[a], L[a]);
-    if (dipole) {
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            L[0] = fma(-m[1 + a], D[1 + a], L[0]);
-#pragma unroll
-            for (int b = 0; b < 3; ++b) L[1 + a] = fma(-m[1 + a], D[quad_row(a, b)], L[1 + a]);
-        }
-    }
-#pragma unroll
-    for (int q = 0; q < 6; ++q) {
-        L[0] = fma(m[4 + q], D[4 + q], L[0]);
-#pragma unroll
-        for (int a = 0; a < 3; ++a) L[1 + a] = fma(m[4 + q], D[quad_axis(q, a)], L[1 + a]);
-    }
-#pragma unroll
-    for (int k = 10; k < 20; ++k) L[0] = fma(-m[k], D[k], L[0]);
+// Derivative tensor of 1/r from dX and d0..d3 (any scalar type).
+template <class T>
+__device__ __forceinline__ void d_tensor(const T dX[3], T d0, T d1, T d2, T d3, T D[20]) {
+    const T X00 = dX[0] * dX[0], X11 = dX[1] * dX[1], X22 = dX[2] * dX[2];
+    const T X01 = dX[0] * dX[1], X02 = dX[0] * dX[2], X12 = dX[1] * dX[2];
+    D[0] = d0;
+    D[1] = dX[0] * d1;
+    D[2] = dX[1] * d1;
+    D[3] = dX[2] * d1;
+    D[4] = fmat(d2, X00, d1);
+    D[5] = d2 * X01;
+    D[6] = d2 * X02;
+    D[7] = fmat(d2, X11, d1);
+    D[8] = d2 * X12;
+    D[9] = fmat(d2, X22, d1);
+    const T d2_3 = T(3) * d2;
+    const T a0 = fmat(d3, X00, d2), a1 = fmat(d3, X11, d2), a2 = fmat(d3, X22, d2);
+    const T b0 = fmat(d3, X00, d2_3), b1 = fmat(d3, X11, d2_3), b2 = fmat(d3, X22, d2_3);
+    D[10] = dX[0] * b0;
+    D[11] = dX[1] * a0;
+    D[12] = dX[2] * a0;
+    D[13] = dX[0] * a1;
+    D[14] = d3 * dX[0] * X12;
+    D[15] = dX[0] * a2;
+    D[16] = dX[1] * b1;
+    D[17] = dX[2] * a1;
+    D[18] = dX[1] * a2;
+    D[19] = dX[2] * b2;
 }
 
-__device__ __forceinline__ void fast_high_terms(const double* m, const double* D, double* L) {
+// Contraction shared by M2L and P2M for L0..L3 (quadrupole/octupole partner
+// moments; Scaled moments carry the factors). The per-pair sums are split
+// into independent partial chains (L0 collects 17 terms per pair) so that
+// consecutive FMAs do not wait on each other.
+template <class T>
+__device__ __forceinline__ void fast_low_terms(const T* m, const T* D, T* L, bool dipole) {
+    // L0: monopole + quadrupole terms, octupole terms
+    T a = m[0] * D[0];
+    a = fmat(m[4], D[4], a);
+    a = fmat(m[5], D[5], a);
+    a = fmat(m[6], D[6], a);
+    T b = m[7] * D[7];
+    b = fmat(m[8], D[8], b);
+    b = fmat(m[9], D[9], b);
+    T c = m[10] * D[10];
+#pragma unroll
+    for (int k = 11; k < 15; ++k) c = fmat(m[k], D[k], c);
+    T e = m[15] * D[15];
+#pragma unroll
+    for (int k = 16; k < 20; ++k) e = fmat(m[k], D[k], e);
+    if (dipole) {
+        T g = m[1] * D[1];
+        g = fmat(m[2], D[2], g);
+        g = fmat(m[3], D[3], g);
+        c += g;
+    }
+    L[0] += (a + b) - (c + e);
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+        T u = m[0] * D[1 + ax];
+        u = fmat(m[4], D[quad_axis(0, ax)], u);
+        u = fmat(m[5], D[quad_axis(1, ax)], u);
+        u = fmat(m[6], D[quad_axis(2, ax)], u);
+        T v = m[7] * D[quad_axis(3, ax)];
+        v = fmat(m[8], D[quad_axis(4, ax)], v);
+        v = fmat(m[9], D[quad_axis(5, ax)], v);
+        if (dipole) {
+            // partner dipole block of compute_kernel_non_rho (:378-389)
+            T w = m[1 + ax] * D[quad_row(ax, 0)];
+            w = fmat(m[1 + ax], D[quad_row(ax, 1)], w);
+            w = fmat(m[1 + ax], D[quad_row(ax, 2)], w);
+            v -= w;
+        }
+        L[1 + ax] += u + v;
+    }
+}
+
+template <class T>
+__device__ __forceinline__ void fast_high_terms(const T* m, const T* D, T* L) {
 #pragma unroll
     for (int q = 0; q < 6; ++q) {
-        double t = fma(m[0], D[4 + q], L[4 + q]);
-#pragma unroll
-        for (int a = 0; a < 3; ++a) t = fma(-m[1 + a], D[quad_axis(q, a)], t);
-        L[4 + q] = t;
+        const T t = fmat(-m[1], D[quad_axis(q, 0)], m[0] * D[4 + q]);
+        const T u = fmat(m[2], D[quad_axis(q, 1)], m[3] * D[quad_axis(q, 2)]);
+        L[4 + q] += t - u;
     }
 #pragma unroll
-    for (int o = 0; o < 10; ++o) L[10 + o] = fma(m[0], D[10 + o], L[10 + o]);
+    for (int o = 0; o < 10; ++o) L[10 + o] = fmat(m[0], D[10 + o], L[10 + o]);
 }
 
 // Angular correction with Scaled octupoles g_k = f6_k (M_p - M_c n0).
@@ -312,10 +370,13 @@ __device__ __forceinline__ void fast_upper_correction(const FastDerivs& f, const
     U[14] = fma(d3_6, f.X22, d2_3);
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
-        double t = Lc[j];
+        double s = g[0] * U[upper_idx(0, j)];
+        double t = g[5] * U[upper_idx(5, j)];
 #pragma unroll
-        for (int o = 0; o < 10; ++o) t = fma(-g[o], U[upper_idx(o, j)], t);
-        Lc[j] = t;
+        for (int o = 1; o < 5; ++o) s = fma(g[o], U[upper_idx(o, j)], s);
+#pragma unroll
+        for (int o = 6; o < 10; ++o) t = fma(g[o], U[upper_idx(o, j)], t);
+        Lc[j] -= s + t;
     }
 }
 
@@ -352,6 +413,44 @@ __device__ __forceinline__ void fast_m2l_mass_pair(const double X[3], const doub
         double g[10];
 #pragma unroll
         for (int o = 0; o < 10; ++o) g[o] = -mc_oct[o] * n0;
+        fast_upper_correction(f, g, Lc);
+    }
+}
+
+// ------------------------------------------------------------------ FP32 split
+// Inputs in units of the subgrid cell size dx (exact for dx = 2^-k): X, Y
+// centres of mass / dx (FP64), partner moments M'_k = M_k dx^-n(k) with the
+// factors folded in, FP32 copies mpf and FP64 octupoles mp_oct for L_c.
+// The derivative factors d0..d3 and the angular correction stay FP64; the
+// derivative tensor and the D.M contraction run in FP32 into accf.
+template <bool RHO>
+__device__ __forceinline__ void split_m2l_pair(const double X[3], const double Y[3], const float mpf[20], double m0,
+                                               const double mp_oct[10], const double mc_oct[10], double inv_m0,
+                                               float accf[20], double Lc[3]) {
+    FastDerivs f;
+    const double dX[3] = {X[0] - Y[0], X[1] - Y[1], X[2] - Y[2]};
+    f.X00 = dX[0] * dX[0];
+    f.X11 = dX[1] * dX[1];
+    f.X22 = dX[2] * dX[2];
+    f.X01 = dX[0] * dX[1];
+    f.X02 = dX[0] * dX[2];
+    f.X12 = dX[1] * dX[2];
+    const double r2 = fmax(f.X00 + f.X11 + f.X22, 1.0e-20);
+    const double rs = rsqrt(r2);
+    const double r2inv = rs * rs;
+    const double d1 = rs * r2inv;
+    f.d2 = -3.0 * d1 * r2inv;
+    f.d3 = -5.0 * f.d2 * r2inv;
+    const float dXf[3] = {(float)dX[0], (float)dX[1], (float)dX[2]};
+    float Df[20];
+    d_tensor<float>(dXf, (float)(-rs), (float)d1, (float)f.d2, (float)f.d3, Df);
+    fast_low_terms<float>(mpf, Df, accf, !RHO);
+    fast_high_terms<float>(mpf, Df, accf);
+    if (RHO) {
+        const double n0 = m0 * inv_m0;
+        double g[10];
+#pragma unroll
+        for (int o = 0; o < 10; ++o) g[o] = fma(-mc_oct[o], n0, mp_oct[o]);
         fast_upper_correction(f, g, Lc);
     }
 }

@@ -197,3 +197,37 @@ def test_fma_peaks_measurable():
     from octotiger_b200.otfmm import measure_fma_peaks
     f64, f32 = measure_fma_peaks(0)
     assert 5.0 < f64 < 200.0 and 10.0 < f32 < 400.0
+
+
+def split_errors(L, Lc, Lo, Lco):
+    """Scaled max error per group: potential L0, force L1..3, higher L4..19, L_c."""
+    e = scaled_err(L, Lo)
+    out = {"L0": float(e[0]), "force": float(e[1:4].max()), "higher": float(e[4:].max())}
+    out["Lc"] = float(scaled_err(Lc, Lco).max()) if np.abs(Lco).max() > 0 else 0.0
+    return out
+
+
+SPLIT_CASES = ["single", "mixed", "uniform_level2", "leaf"]
+
+
+@pytest.mark.parametrize("solve", [RHO, DRHODT])
+@pytest.mark.parametrize("name", SPLIT_CASES)
+def test_batch_fp32_split_accuracy(ctx, oracle, name, solve):
+    """FP32 split form: <= 1e-6 on potential and force, <= 1e-10 on L_c
+    (which stays FP64), per component relative to its largest magnitude."""
+    b = CASES[name]()
+    L, Lc = run_batch(ctx, b, solve, "fp32_split")
+    Lo, Lco = oracle.batch(0.5, b.pool, b.items, rho=(solve == RHO))
+    sel = b.items["subgrid"]
+    err = split_errors(L[sel], Lc[sel], Lo[sel], Lco[sel])
+    assert err["L0"] <= 1e-6 and err["force"] <= 1e-6, err
+    assert err["higher"] <= 1e-5, err
+    assert err["Lc"] <= 1e-10, err
+
+
+def test_fp32_split_full_size_accuracy(ctx, oracle):
+    b = syn.uniform_level(3)
+    L, Lc = run_batch(ctx, b, RHO, "fp32_split")
+    Lo, Lco = oracle.batch(0.5, b.pool, b.items, rho=True)
+    err = split_errors(L, Lc, Lo, Lco)
+    assert err["L0"] <= 1e-6 and err["force"] <= 1e-6 and err["Lc"] <= 1e-10, err
