@@ -43,19 +43,28 @@ FLOPS_PER_PAIR = {("m2l", RHO): 406, ("m2l", DRHODT): 272, ("p2p", RHO): 12, ("p
 L2_FLUSH_BYTES = 256 << 20
 
 
+WORKLOADS = ("uniform_level3", "amr_polytrope", "amr_binary")
+
+
 def make_workload(name: str):
     if name == "uniform_level3":
         return syn.uniform_level(3)
+    from octotiger_b200 import amr
     if name == "amr_polytrope":
-        from octotiger_b200 import amr
         return amr.polytrope_batch()
+    if name == "amr_binary":
+        return amr.binary_batch()
     raise SystemExit(f"unknown workload {name}")
 
 
-def pair_counts(batch) -> dict:
-    from oracle.pyoracle import Oracle
-    o = Oracle()
-    total, per_kind = o.count_pairs(batch.theta, batch.pool, batch.items)
+def pair_counts(batch, ctx=None) -> dict:
+    """Evaluated cell-interactions of the work list, counted by the library
+    (host side); the CPU leg without a GPU context counts with the oracle."""
+    if ctx is not None:
+        total, per_kind = ctx.count_pairs(batch.pool.is_leaf, batch.items)
+    else:
+        from oracle.pyoracle import Oracle
+        total, per_kind = Oracle().count_pairs(batch.theta, batch.pool, batch.items)
     return {"total": total, "m2l": int(per_kind[0] + per_kind[1]), "p2p": int(per_kind[2]), "p2m": int(per_kind[3])}
 
 
@@ -223,8 +232,8 @@ def gpu_arm(args) -> None:
 
     batch = make_workload(args.workload)
     solve = RHO if args.gsolve == "rho" else DRHODT
-    counts = pair_counts(batch)
     ctx = Context(local, batch.theta)
+    counts = pair_counts(batch, ctx)
     solver = BatchSolver(ctx, batch.pool, batch.items)
     stream = torch.cuda.current_stream()
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
@@ -350,7 +359,7 @@ def gpu_arm(args) -> None:
         "precisions": others,
         "accuracy_vs_fp64_exact": accuracy,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
-        "gpu_launches": args.steps,
+        "gpu_launches": 3 * args.steps,
         "roofline": roof,
         "clocks": clk.summary(),
         "step_ms": [round(x, 4) for x in per],
@@ -372,7 +381,7 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="uniform_level3", choices=["uniform_level3", "amr_polytrope"])
+    ap.add_argument("--workload", default="uniform_level3", choices=list(WORKLOADS))
     ap.add_argument("--precision", default="fp32_split", choices=["fp32_split", "fp64", "fp64_exact"])
     ap.add_argument("--compare", nargs="*", default=["fp64", "fp64_exact"])
     ap.add_argument("--gsolve", default="rho", choices=["rho", "drhodt"])

@@ -129,16 +129,28 @@ int otfmm_p2m_soa(otfmm_context* ctx, int d, const double* neighbor_M, const dou
                   const double* inner_com, double* L4, double* L_c, int gsolve_type, int reset_lc, int precision,
                   void* stream);
 
-/* Batched solve: every work item of `items` (device array of n_items) in one
- * launch, reading the resident pool (device pointers, n_subgrids records) and
- * writing per subgrid L[n][20][512] and L_c[n][3][512] (leaf items fill
- * L[0..3], zero L[4..19]; L_c is zero for DRHODT and for leaves without a
- * refined neighbour). Work items are validated on the device; a bad item makes
- * the call return OTFMM_ERR_DEVICE (after the stream is synchronized) and
- * leaves its outputs unwritten. */
+/* Batched solve: every work item of `items` (device array of n_items),
+ * reading the resident pool (device pointers, n_subgrids records) and writing
+ * per subgrid L[n][20][512] and L_c[n][3][512] (leaf items fill L[0..3] and
+ * zero L[4..19]; L_c is zero for DRHODT and for leaves without a refined
+ * neighbour). Enqueues three stream-ordered launches: the multipole tiles of
+ * refined items, then P2P of leaf items, then P2M of leaves that have refined
+ * neighbours (the reference's P2P-then-P2M order). Asynchronous; work items
+ * are validated on the device and a bad item is reported by
+ * otfmm_batch_status (its outputs are left unwritten). Every subgrid may
+ * appear in at most one work item. Calls that overlap on the GPU must use
+ * distinct output arrays. */
 int otfmm_batch(otfmm_context* ctx, const double* pool_M, const double* pool_com, const double* pool_mon,
                 const uint8_t* pool_is_leaf, int32_t n_subgrids, const otfmm_work_item* items, int32_t n_items,
                 double* L, double* L_c, int gsolve_type, int precision, void* stream);
+
+/* Cell-interactions a work list evaluates (host-side count, no device
+ * work): the (cell, partner) pairs that pass the stencil and coarse-distance
+ * masks, which is what the reference's kernels evaluate. per_class (may be
+ * NULL) receives [M2L, root M2L, P2P, P2M]. is_leaf and items are host
+ * arrays. Returns the total, or a negative status. */
+long long otfmm_count_pairs(const otfmm_context* ctx, const uint8_t* is_leaf, int32_t n_subgrids,
+                            const otfmm_work_item* items, int32_t n_items, long long per_class[4]);
 
 /* Checks a device-side error flag written by the last otfmm_batch on `stream`
  * without synchronizing the whole device: returns OTFMM_OK or OTFMM_ERR_DEVICE. */

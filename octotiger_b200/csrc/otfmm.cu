@@ -93,6 +93,21 @@ static_assert(S_XS >= SUB_YZ * S_RB && (S_XS % 16 == 2 || S_XS % 16 == 6 || S_XS
               "split x stride");
 static_assert(S_SMEM_DOUBLES * 8 <= 232448, "split layout fits the 227 KB shared-memory limit");
 
+// P2P layout: one leaf subgrid per CTA (512 threads, one cell each); the
+// mass region -2..9 per axis split by parity into 6^3 sub-lattices with rows
+// padded to 12 doubles (4x4 lane blocks conflict-free).
+constexpr int P_THREADS = 512;
+constexpr int P_REG = INX + 4;
+constexpr int P_SUB = 6;
+constexpr int P_RS = 12;
+constexpr int P_XS = P_SUB * P_RS;
+constexpr int P_CLS = P_SUB * P_XS;
+constexpr int P_SMEM_DOUBLES = 8 * P_CLS;   // 3456 doubles = 27648 bytes
+
+// Monopole constants {-1/r, x/r^3, y/r^3, z/r^3} per stencil offset (they do
+// not depend on theta), read warp-uniformly through the constant cache.
+__constant__ double c_four[FULL][4];
+
 // Entry flags
 constexpr int F_FAR = 1;    // phase-one offset: full multipole partner
 constexpr int F_NEAR = 2;   // monopole-only offset
@@ -103,6 +118,7 @@ struct Tables {
     const int2* entries_fast;   // same entries, full-multipole (far) offsets first
     const int* count_far;       // [8] number of far offsets
     const int4* entries_split;  // far-first entries for the split layout: x = double delta, y = packed, z = float delta
+    const int2* entries_p2p;    // stencil-order entries for the P2P layout: x = smem delta, y = stencil index
     const double* four;      // [FULL][4] monopole constants
     const uint8_t* phase;    // [FULL] inner_stencil_masks (true outside the stencil)
 };
@@ -463,69 +479,6 @@ __device__ void m2l_tile_split(const double* sm, int x0, const Tables& t, uint32
     write_lc<RHO>(out, cf, corr);
 }
 
-// Leaf tile: P2P over own + leaf-neighbour masses, then P2M per refined
-// neighbour direction in direction order (monopole kokkos_kernel.hpp:1195-1273).
-template <int PREC, bool RHO>
-__device__ void leaf_tile(const double* sm, int x0, const Tables& t, uint32_t refmask, double dx, OutPtr out) {
-    const CellMap c = cell_map(x0);
-    double X[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) X[a] = sm[c.own + (20 + a) * SUB_YZ];
-    double acc[4] = {0.0, 0.0, 0.0, 0.0}, corr[3] = {0.0, 0.0, 0.0};
-    const int n = t.count[c.p];
-    const int2* ent = t.entries + c.p * MAX_ENTRIES;
-    const double dc0 = __ddiv_rn(1.0, dx), dc1 = __ddiv_rn(-1.0, dx);
-    // P2P (p2p_kernel_impl)
-    for (int e = 0; e < n; ++e) {
-        const int2 en = __ldg(ent + e);
-        const int ax = c.cx + entry_sx(en.y), ay = c.cy + entry_sy(en.y), az = c.cz + entry_sz(en.y);
-        if ((refmask >> raw_dir(ax, ay, az)) & 1u) continue;   // refined neighbour: no monopole
-        const double* four = t.four + 4 * entry_sidx(en.y);
-        const double m = sm[en.x + c.lane_off];
-        if (PREC == PREC_EXACT) {
-            const double ms = __dmul_rn(m, dc0);
-            acc[0] = __dadd_rn(acc[0], __dmul_rn(__ldg(four), ms));
-#pragma unroll
-            for (int a = 1; a < 4; ++a) acc[a] = __dadd_rn(acc[a], __dmul_rn(__dmul_rn(__ldg(four + a), ms), dc1));
-        } else {
-            const double ms = m * dc0;
-            const double ms1 = ms * dc1;
-            acc[0] = fma(__ldg(four), ms, acc[0]);
-#pragma unroll
-            for (int a = 1; a < 4; ++a) acc[a] = fma(__ldg(four + a), ms1, acc[a]);
-        }
-    }
-    // P2M, one refined direction after the other
-    if (refmask) {
-        for (int raw = 0; raw < 27; ++raw) {
-            if (!((refmask >> raw) & 1u)) continue;
-            for (int e = 0; e < n; ++e) {
-                const int2 en = __ldg(ent + e);
-                const int ax = c.cx + entry_sx(en.y), ay = c.cy + entry_sy(en.y), az = c.cz + entry_sz(en.y);
-                if (raw_dir(ax, ay, az) != raw) continue;
-                const int pb = en.x + c.lane_off;
-                double Y[3], mp[20];
-#pragma unroll
-                for (int a = 0; a < 3; ++a) Y[a] = sm[pb + (20 + a) * SUB_YZ];
-#pragma unroll
-                for (int q = 0; q < 20; ++q) mp[q] = sm[pb + q * SUB_YZ];
-                if (PREC == PREC_EXACT)
-                    exact_p2m_pair<RHO>(X, Y, mp, acc, corr);
-                else
-                    fast_p2m_pair<RHO>(X, Y, mp, acc, corr);
-            }
-        }
-    }
-    const int cf = c.cx * 64 + c.cy * 8 + c.cz;
-#pragma unroll
-    for (int q = 0; q < 4; ++q) out.L[q * out.stride + cf] = acc[q];
-    if (out.pool) {   // pool output: L4..L19 are zero for leaves
-#pragma unroll
-        for (int q = 4; q < 20; ++q) out.L[q * out.stride + cf] = 0.0;
-    }
-    write_lc<RHO>(out, cf, corr);
-}
-
 // Root node: partners are all own cells except the monopole-only stencil
 // offsets and the cell itself (multipole_kernel_root_*_impl).
 // Staged layout: sm[q * 512 + cell].
@@ -578,13 +531,10 @@ struct BatchArgs {
     int* err;
 };
 
-template <int PREC, bool RHO>
-__global__ void __launch_bounds__(THREADS, 1) batch_kernel(BatchArgs a) {
-    extern __shared__ double sm[];
-    __shared__ ItemInfo it;
-    __shared__ int bad;
-    const int item_idx = blockIdx.x >> 1;
-    const int half = blockIdx.x & 1;
+// Reads and validates one work item into shared memory (thread 0); returns
+// false for the whole CTA if the item is malformed (flag raised, nothing
+// accessed with its fields).
+__device__ bool load_item(const BatchArgs& a, int item_idx, ItemInfo& it, int& bad) {
     if (threadIdx.x == 0) {
         const otfmm_work_item& w = a.items[item_idx];
         it.subgrid = w.subgrid;
@@ -601,11 +551,24 @@ __global__ void __launch_bounds__(THREADS, 1) batch_kernel(BatchArgs a) {
         if (b) atomicOr(a.err, 1);
     }
     __syncthreads();
-    if (bad) return;
+    return !bad;
+}
+
+// Refined (multipole) items: M2L tiles, two CTAs per item. Leaf items are
+// left to the P2P / P2M kernels.
+template <int PREC, bool RHO>
+__global__ void __launch_bounds__(THREADS, 1) m2l_batch_kernel(BatchArgs a) {
+    extern __shared__ double sm[];
+    __shared__ ItemInfo it;
+    __shared__ int bad;
+    const int item_idx = blockIdx.x >> 1;
+    const int half = blockIdx.x & 1;
+    if (a.items[item_idx].kind == OTFMM_KIND_LEAF) return;   // uniform per CTA
+    if (!load_item(a, item_idx, it, bad)) return;
     const int x0 = TILE_X * half;
     const size_t sub = (size_t)it.subgrid;
     OutPtr out{a.L + sub * 20 * NCELL, a.Lc + sub * 3 * NCELL, NCELL, true};
-    // the split form covers multipole tiles; leaf and root tiles use fast FP64
+    // the split form covers the multipole tiles; the root tile uses fast FP64
     constexpr int P64 = (PREC == PREC_SPLIT) ? PREC_FAST : PREC;
     if (it.kind == OTFMM_KIND_M2L_ROOT) {
         const int base_sub = it.subgrid;
@@ -617,29 +580,144 @@ __global__ void __launch_bounds__(THREADS, 1) batch_kernel(BatchArgs a) {
         root_tile<P64, RHO>(sm, x0, a.t, out);
         return;
     }
-    const bool leaf = (it.kind == OTFMM_KIND_LEAF);
-    // direction masks indexed by raw direction: leaf neighbours (for M2L
-    // monopole-only offsets) or refined neighbours (leaf tiles)
-    uint32_t mask = 0;
+    // leaf neighbours, indexed by raw direction (monopole-only offsets)
+    uint32_t monomask = 0;
     for (int d = 0; d < 26; ++d) {
         const int nb = it.nb[d];
-        if (nb < 0) continue;
-        const bool nb_leaf = a.is_leaf[nb] != 0;
-        if (leaf ? !nb_leaf : nb_leaf) mask |= 1u << (d < 13 ? d : d + 1);
+        if (nb >= 0 && a.is_leaf[nb]) monomask |= 1u << (d < 13 ? d : d + 1);
     }
-    if (PREC == PREC_SPLIT && !leaf) {
+    if (PREC == PREC_SPLIT) {
         const double inv_dx = 1.0 / it.dx;
         stage_region_split(sm, it, x0, inv_dx, a.M, a.com, a.mon, a.is_leaf);
         __syncthreads();
-        m2l_tile_split<RHO>(sm, x0, a.t, mask, inv_dx, out);
+        m2l_tile_split<RHO>(sm, x0, a.t, monomask, inv_dx, out);
         return;
     }
-    stage_region_pool<P64>(sm, it, x0, leaf, a.M, a.com, a.mon, a.is_leaf);
+    stage_region_pool<P64>(sm, it, x0, false, a.M, a.com, a.mon, a.is_leaf);
     __syncthreads();
-    if (leaf) {
-        leaf_tile<P64, RHO>(sm, x0, a.t, mask, it.dx, out);
+    m2l_tile<P64, RHO>(sm, x0, a.t, monomask, nullptr, out);
+}
+
+// Leaf items: P2P (p2p_kernel_impl, monopole kokkos_kernel.hpp:143-320) over
+// the masses of the leaf and its leaf neighbours; refined and empty
+// neighbours are staged as zero mass (update_input,
+// monopole_interaction_interface.hpp:82-87), which adds exact zeros, so the
+// sweep has no branch. Writes L0..L3, zeroes L4..L19 and L_c (the P2M kernel
+// adds the refined-neighbour part afterwards).
+template <int PREC>
+__global__ void __launch_bounds__(P_THREADS) p2p_batch_kernel(BatchArgs a) {
+    __shared__ double pm[P_SMEM_DOUBLES];
+    __shared__ ItemInfo it;
+    __shared__ int bad;
+    if (a.items[blockIdx.x].kind != OTFMM_KIND_LEAF) return;
+    if (!load_item(a, blockIdx.x, it, bad)) return;
+    const double dc0 = __ddiv_rn(1.0, it.dx), dc1 = __ddiv_rn(-1.0, it.dx);
+    for (int r = threadIdx.x; r < P_REG * P_REG * P_REG; r += blockDim.x) {
+        const int ax = r / (P_REG * P_REG) - 2, ay = (r / P_REG) % P_REG - 2, az = r % P_REG - 2;
+        const int raw = raw_dir(ax, ay, az);
+        const int src = (raw == 13) ? it.subgrid : it.nb[raw < 13 ? raw : raw - 1];
+        double m = 0.0;
+        if (src >= 0 && (raw == 13 || a.is_leaf[src])) m = a.mon[(size_t)src * NCELL + (ax & 7) * 64 + (ay & 7) * 8 + (az & 7)];
+        if (PREC != PREC_EXACT) m *= dc0;   // 1/dx folded into the staged mass
+        const int cls = ((ax & 1) << 2) | ((ay & 1) << 1) | (az & 1);
+        pm[cls * P_CLS + ((ax + 2) >> 1) * P_XS + ((ay + 2) >> 1) * P_RS + ((az + 2) >> 1)] = m;
+    }
+    __syncthreads();
+    // thread -> cell: warp w covers parity class w/2, x' block w%2
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int p = w >> 1;
+    const int i = 2 * (w & 1) + (lane >> 4), j = (lane >> 2) & 3, k = lane & 3;
+    const int cx = ((p >> 2) & 1) + 2 * i, cy = ((p >> 1) & 1) + 2 * j, cz = (p & 1) + 2 * k;
+    const int lane_off = i * P_XS + j * P_RS + k;
+    const int n = a.t.count[p];
+    const int2* ent = a.t.entries_p2p + p * MAX_ENTRIES;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    if (PREC == PREC_EXACT) {
+        for (int e = 0; e < n; ++e) {
+            const int2 en = __ldg(ent + e);
+            const double ms = __dmul_rn(pm[en.x + lane_off], dc0);
+            acc[0] = __dadd_rn(acc[0], __dmul_rn(c_four[en.y][0], ms));
+#pragma unroll
+            for (int q = 1; q < 4; ++q) acc[q] = __dadd_rn(acc[q], __dmul_rn(__dmul_rn(c_four[en.y][q], ms), dc1));
+        }
     } else {
-        m2l_tile<P64, RHO>(sm, x0, a.t, mask, nullptr, out);
+#pragma unroll 4
+        for (int e = 0; e < n; ++e) {
+            const int2 en = __ldg(ent + e);
+            const double ms = pm[en.x + lane_off];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[q] = fma(c_four[en.y][q], ms, acc[q]);
+        }
+#pragma unroll
+        for (int q = 1; q < 4; ++q) acc[q] *= dc1;
+    }
+    const int cf = cx * 64 + cy * 8 + cz;
+    double* L = a.L + (size_t)it.subgrid * 20 * NCELL;
+    double* Lc = a.Lc + (size_t)it.subgrid * 3 * NCELL;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) L[q * NCELL + cf] = acc[q];
+#pragma unroll
+    for (int q = 4; q < 20; ++q) L[q * NCELL + cf] = 0.0;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) Lc[q * NCELL + cf] = 0.0;
+}
+
+// Leaf items with refined neighbours: P2M (p2m_kernel_impl_rho / _non_rho,
+// monopole kokkos_kernel.hpp:517-942) after P2P, one refined direction after
+// the other in direction order, partners in stencil order, partner moments
+// read from the pool. Adds to L0..L3, writes L_c.
+template <int PREC, bool RHO>
+__global__ void __launch_bounds__(P_THREADS) p2m_batch_kernel(BatchArgs a) {
+    __shared__ ItemInfo it;
+    __shared__ int bad;
+    if (a.items[blockIdx.x].kind != OTFMM_KIND_LEAF) return;
+    if (!load_item(a, blockIdx.x, it, bad)) return;
+    uint32_t refmask = 0;
+    for (int d = 0; d < 26; ++d) {
+        const int nb = it.nb[d];
+        if (nb >= 0 && !a.is_leaf[nb]) refmask |= 1u << (d < 13 ? d : d + 1);
+    }
+    if (!refmask) return;
+    const int cu = threadIdx.x;
+    const int cx = cu >> 6, cy = (cu >> 3) & 7, cz = cu & 7;
+    const int p = ((cx & 1) << 2) | ((cy & 1) << 1) | (cz & 1);
+    const size_t sub = (size_t)it.subgrid;
+    double* L = a.L + sub * 20 * NCELL;
+    double* Lc = a.Lc + sub * 3 * NCELL;
+    double X[3], acc[4], corr[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int q = 0; q < 3; ++q) X[q] = a.com[(sub * 3 + q) * NCELL + cu];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) acc[q] = L[q * NCELL + cu];
+    const int n = a.t.count[p];
+    const int2* ent = a.t.entries + p * MAX_ENTRIES;
+    for (int raw = 0; raw < 27; ++raw) {
+        if (!((refmask >> raw) & 1u)) continue;
+        const int nb = it.nb[raw < 13 ? raw : raw - 1];
+        for (int e = 0; e < n; ++e) {
+            const int y = __ldg(&ent[e].y);
+            const int ax = cx + entry_sx(y), ay = cy + entry_sy(y), az = cz + entry_sz(y);
+            if (raw_dir(ax, ay, az) != raw) continue;
+            const int u = (ax & 7) * 64 + (ay & 7) * 8 + (az & 7);
+            double Y[3], mp[20];
+#pragma unroll
+            for (int q = 0; q < 3; ++q) Y[q] = __ldg(a.com + ((size_t)nb * 3 + q) * NCELL + u);
+            if (PREC == PREC_EXACT) {
+#pragma unroll
+                for (int q = 0; q < 20; ++q) mp[q] = __ldg(a.M + ((size_t)nb * 20 + q) * NCELL + u);
+                exact_p2m_pair<RHO>(X, Y, mp, acc, corr);
+            } else {
+#pragma unroll
+                for (int q = 0; q < 20; ++q) mp[q] = __ldg(a.M + ((size_t)nb * 20 + q) * NCELL + u) * stage_scale<PREC_FAST>(q);
+                fast_p2m_pair<RHO>(X, Y, mp, acc, corr);
+            }
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) L[q * NCELL + cu] = acc[q];
+    if (RHO) {
+#pragma unroll
+        for (int q = 0; q < 3; ++q) Lc[q * NCELL + cu] = corr[q];
     }
 }
 
@@ -688,7 +766,7 @@ __global__ void soa_p2p_kernel(const double* __restrict__ mon, double dx, double
         const int y = __ldg(&ent[e].y);
         const int ax = cx + entry_sx(y), ay = cy + entry_sy(y), az = cz + entry_sz(y);
         const double m = mon[(ax + INX - PAD_OFF) * PSTRIDE * PSTRIDE + (ay + INX - PAD_OFF) * PSTRIDE + (az + INX - PAD_OFF)];
-        const double* four = t.four + 4 * entry_sidx(y);
+        const double* four = c_four[entry_sidx(y)];
         if (PREC == PREC_EXACT) {
             const double ms = __dmul_rn(m, dc0);
             acc[0] = __dadd_rn(acc[0], __dmul_rn(four[0], ms));
@@ -903,13 +981,14 @@ struct otfmm_context {
     int2* d_entries_fast = nullptr;
     int* d_count_far = nullptr;
     int4* d_entries_split = nullptr;
+    int2* d_entries_p2p = nullptr;
     int counts_far[8] = {};
     double* d_four = nullptr;
     uint8_t* d_phase = nullptr;
     int* d_err = nullptr;
     double* d_soa_scratch = nullptr;   // host-buffer path staging
     std::mutex mu;
-    Tables tables() const { return Tables{d_entries, d_count, d_entries_fast, d_count_far, d_entries_split, d_four, d_phase}; }
+    Tables tables() const { return Tables{d_entries, d_count, d_entries_fast, d_count_far, d_entries_split, d_entries_p2p, d_four, d_phase}; }
 };
 
 namespace {
@@ -943,12 +1022,12 @@ int ensure_attributes(int device) {
     if (g_attr_set[device]) return OTFMM_OK;
     const int bytes = SMEM_DOUBLES * (int)sizeof(double);
     int rc = OTFMM_OK;
-    rc = rc ? rc : set_smem(batch_kernel<PREC_EXACT, true>, bytes);
-    rc = rc ? rc : set_smem(batch_kernel<PREC_EXACT, false>, bytes);
-    rc = rc ? rc : set_smem(batch_kernel<PREC_FAST, true>, bytes);
-    rc = rc ? rc : set_smem(batch_kernel<PREC_FAST, false>, bytes);
-    rc = rc ? rc : set_smem(batch_kernel<PREC_SPLIT, true>, S_SMEM_DOUBLES * (int)sizeof(double));
-    rc = rc ? rc : set_smem(batch_kernel<PREC_SPLIT, false>, S_SMEM_DOUBLES * (int)sizeof(double));
+    rc = rc ? rc : set_smem(m2l_batch_kernel<PREC_EXACT, true>, bytes);
+    rc = rc ? rc : set_smem(m2l_batch_kernel<PREC_EXACT, false>, bytes);
+    rc = rc ? rc : set_smem(m2l_batch_kernel<PREC_FAST, true>, bytes);
+    rc = rc ? rc : set_smem(m2l_batch_kernel<PREC_FAST, false>, bytes);
+    rc = rc ? rc : set_smem(m2l_batch_kernel<PREC_SPLIT, true>, S_SMEM_DOUBLES * (int)sizeof(double));
+    rc = rc ? rc : set_smem(m2l_batch_kernel<PREC_SPLIT, false>, S_SMEM_DOUBLES * (int)sizeof(double));
     rc = rc ? rc : set_smem(soa_m2l_kernel<PREC_EXACT, true, false>, bytes);
     rc = rc ? rc : set_smem(soa_m2l_kernel<PREC_EXACT, false, false>, bytes);
     rc = rc ? rc : set_smem(soa_m2l_kernel<PREC_FAST, true, false>, bytes);
@@ -1000,6 +1079,17 @@ int otfmm_create(int device, double theta, otfmm_context** out) {
         return fail(OTFMM_ERR_UNSUPPORTED, "theta < 0.5 (coarse reach 2) is not built into this library");
     }
     ctx->reach = reach;
+    // P2P-layout table (stencil order)
+    std::vector<int2> entries_p2p(8 * MAX_ENTRIES, int2{0, 0});
+    for (int p = 0; p < 8; ++p)
+        for (int e = 0; e < ctx->counts[p]; ++e) {
+            const int2 en = entries[p * MAX_ENTRIES + e];
+            const int sx = (en.y & 15) - 8, sy = ((en.y >> 4) & 15) - 8, sz = ((en.y >> 8) & 15) - 8;
+            const int px = (p >> 2) & 1, py = (p >> 1) & 1, pz = p & 1;
+            const int cls = (((px + sx) & 1) << 2) | (((py + sy) & 1) << 1) | ((pz + sz) & 1);
+            const int delta = cls * P_CLS + ((px + sx + 2) >> 1) * P_XS + ((py + sy + 2) >> 1) * P_RS + ((pz + sz + 2) >> 1);
+            entries_p2p[p * MAX_ENTRIES + e] = int2{delta, (en.y >> 16) & 2047};
+        }
     // split-layout table (far first, like the fast one)
     std::vector<int4> entries_split(8 * MAX_ENTRIES, int4{0, 0, 0, 0});
     // fast-form table: far offsets first (accumulation order is free there)
@@ -1035,6 +1125,10 @@ int otfmm_create(int device, double theta, otfmm_context** out) {
                         cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemcpy(ctx->d_count_far, ctx->counts_far, sizeof(int) * 8, cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMalloc(&ctx->d_entries_split, sizeof(int4) * entries_split.size())) != cudaSuccess ||
+        (e = cudaMalloc(&ctx->d_entries_p2p, sizeof(int2) * entries_p2p.size())) != cudaSuccess ||
+        (e = cudaMemcpy(ctx->d_entries_p2p, entries_p2p.data(), sizeof(int2) * entries_p2p.size(),
+                        cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpyToSymbol(c_four, ctx->st.four, sizeof(double) * 4 * FULL)) != cudaSuccess ||
         (e = cudaMemcpy(ctx->d_entries_split, entries_split.data(), sizeof(int4) * entries_split.size(),
                         cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemcpy(ctx->d_entries, entries.data(), sizeof(int2) * entries.size(), cudaMemcpyHostToDevice)) !=
@@ -1063,6 +1157,7 @@ int otfmm_destroy(otfmm_context* ctx) {
     cudaFree(ctx->d_count);
     cudaFree(ctx->d_entries_fast);
     cudaFree(ctx->d_entries_split);
+    cudaFree(ctx->d_entries_p2p);
     cudaFree(ctx->d_count_far);
     cudaFree(ctx->d_four);
     cudaFree(ctx->d_phase);
@@ -1192,19 +1287,94 @@ int otfmm_batch(otfmm_context* ctx, const double* pool_M, const double* pool_com
     const size_t bytes = SMEM_DOUBLES * sizeof(double);
     const dim3 grid(2 * n_items);
     const bool rho = (gsolve_type == OTFMM_RHO);
+    // multipole tiles, then P2P of the leaves, then P2M (stream order keeps
+    // the reference's P2P-then-P2M accumulation order)
+    const dim3 pgrid(n_items);
     if (precision == OTFMM_FP64_EXACT) {
-        if (rho) batch_kernel<PREC_EXACT, true><<<grid, THREADS, bytes, s>>>(a);
-        else batch_kernel<PREC_EXACT, false><<<grid, THREADS, bytes, s>>>(a);
-    } else if (precision == OTFMM_FP32_SPLIT) {
-        const size_t sbytes = S_SMEM_DOUBLES * sizeof(double);
-        if (rho) batch_kernel<PREC_SPLIT, true><<<grid, THREADS, sbytes, s>>>(a);
-        else batch_kernel<PREC_SPLIT, false><<<grid, THREADS, sbytes, s>>>(a);
+        if (rho) m2l_batch_kernel<PREC_EXACT, true><<<grid, THREADS, bytes, s>>>(a);
+        else m2l_batch_kernel<PREC_EXACT, false><<<grid, THREADS, bytes, s>>>(a);
+        p2p_batch_kernel<PREC_EXACT><<<pgrid, P_THREADS, 0, s>>>(a);
+        if (rho) p2m_batch_kernel<PREC_EXACT, true><<<pgrid, P_THREADS, 0, s>>>(a);
+        else p2m_batch_kernel<PREC_EXACT, false><<<pgrid, P_THREADS, 0, s>>>(a);
     } else {
-        if (rho) batch_kernel<PREC_FAST, true><<<grid, THREADS, bytes, s>>>(a);
-        else batch_kernel<PREC_FAST, false><<<grid, THREADS, bytes, s>>>(a);
+        if (precision == OTFMM_FP32_SPLIT) {
+            const size_t sbytes = S_SMEM_DOUBLES * sizeof(double);
+            if (rho) m2l_batch_kernel<PREC_SPLIT, true><<<grid, THREADS, sbytes, s>>>(a);
+            else m2l_batch_kernel<PREC_SPLIT, false><<<grid, THREADS, sbytes, s>>>(a);
+        } else {
+            if (rho) m2l_batch_kernel<PREC_FAST, true><<<grid, THREADS, bytes, s>>>(a);
+            else m2l_batch_kernel<PREC_FAST, false><<<grid, THREADS, bytes, s>>>(a);
+        }
+        p2p_batch_kernel<PREC_FAST><<<pgrid, P_THREADS, 0, s>>>(a);
+        if (rho) p2m_batch_kernel<PREC_FAST, true><<<pgrid, P_THREADS, 0, s>>>(a);
+        else p2m_batch_kernel<PREC_FAST, false><<<pgrid, P_THREADS, 0, s>>>(a);
     }
     OT_CUDA(cudaGetLastError());
     return OTFMM_OK;
+}
+
+long long otfmm_count_pairs(const otfmm_context* ctx, const uint8_t* is_leaf, int32_t n_subgrids,
+                            const otfmm_work_item* items, int32_t n_items, long long per_class[4]) {
+    if (!ctx || !is_leaf || (!items && n_items > 0) || n_items < 0) return fail(OTFMM_ERR_INVALID, "bad arguments");
+    long long cls[4] = {0, 0, 0, 0};
+    // partners per cell of each parity, and per cell the offsets by direction
+    for (int i = 0; i < n_items; ++i) {
+        const otfmm_work_item& w = items[i];
+        if (w.subgrid < 0 || w.subgrid >= n_subgrids || w.kind < 0 || w.kind > 2)
+            return fail(OTFMM_ERR_INVALID, "work item out of range");
+        if (w.kind == OTFMM_KIND_M2L_ROOT) {
+            long long n = 0;
+            for (int c = 0; c < NCELL; ++c)
+                for (int q = 0; q < NCELL; ++q) {
+                    const int sx = (q >> 6) - (c >> 6), sy = ((q >> 3) & 7) - ((c >> 3) & 7), sz = (q & 7) - (c & 7);
+                    if (std::abs(sx) <= SMAX && std::abs(sy) <= SMAX && std::abs(sz) <= SMAX) {
+                        const int idx = (sx + SMAX) * SINX * SINX + (sy + SMAX) * SINX + (sz + SMAX);
+                        if (!ctx->st.phase[idx] || (sx == 0 && sy == 0 && sz == 0)) continue;
+                    }
+                    ++n;
+                }
+            cls[1] += n;
+            continue;
+        }
+        long long per_cell = 0;
+        for (int p = 0; p < 8; ++p) per_cell += ctx->counts[p];
+        const long long stencil_pairs = per_cell * (NCELL / 8);
+        if (w.kind == OTFMM_KIND_M2L) {
+            cls[0] += stencil_pairs;
+            continue;
+        }
+        cls[2] += stencil_pairs;
+        // P2M: stencil partners that fall into a refined neighbour
+        uint32_t refmask = 0;
+        for (int d = 0; d < 26; ++d) {
+            const int nb = w.neighbors[d];
+            if (nb < -1 || nb >= n_subgrids) return fail(OTFMM_ERR_INVALID, "neighbour out of range");
+            if (nb >= 0 && !is_leaf[nb]) refmask |= 1u << (d < 13 ? d : d + 1);
+        }
+        if (!refmask) continue;
+        for (int c = 0; c < NCELL; ++c) {
+            const int cx = c >> 6, cy = (c >> 3) & 7, cz = c & 7;
+            const int p = ((cx & 1) << 2) | ((cy & 1) << 1) | (cz & 1);
+            // host copy of the entry offsets (same order and filter as the device table)
+            for (int sx = -SMAX; sx <= SMAX; ++sx)
+                for (int sy = -SMAX; sy <= SMAX; ++sy)
+                    for (int sz = -SMAX; sz <= SMAX; ++sz) {
+                        const int idx = (sx + SMAX) * SINX * SINX + (sy + SMAX) * SINX + (sz + SMAX);
+                        if (!ctx->st.mask[idx]) continue;
+                        const int a = coarse_of(cx + INX) - coarse_of(cx + INX + sx);
+                        const int b = coarse_of(cy + INX) - coarse_of(cy + INX + sy);
+                        const int cc = coarse_of(cz + INX) - coarse_of(cz + INX + sz);
+                        if (!(double(a * a + b * b + cc * cc) < (1.0 / ctx->theta) * (1.0 / ctx->theta))) continue;
+                        const int ax = cx + sx, ay = cy + sy, az = cz + sz;
+                        const int raw = ((ax >> 3) + 1) + 3 * ((ay >> 3) + 1) + 9 * ((az >> 3) + 1);
+                        if ((refmask >> raw) & 1u) ++cls[3];
+                    }
+            (void)p;
+        }
+    }
+    if (per_class)
+        for (int c = 0; c < 4; ++c) per_class[c] = cls[c];
+    return cls[0] + cls[1] + cls[2] + cls[3];
 }
 
 int otfmm_batch_status(otfmm_context* ctx, void* stream) {

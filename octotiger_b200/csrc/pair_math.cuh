@@ -289,59 +289,38 @@ __device__ __forceinline__ void d_tensor(const T dX[3], T d0, T d1, T d2, T d3, 
 }
 
 // Contraction shared by M2L and P2M for L0..L3 (quadrupole/octupole partner
-// moments; Scaled moments carry the factors). The per-pair sums are split
-// into independent partial chains (L0 collects 17 terms per pair) so that
-// consecutive FMAs do not wait on each other.
+// moments; Scaled moments carry the factors): one FMA per term, straight
+// into the accumulators.
 template <class T>
 __device__ __forceinline__ void fast_low_terms(const T* m, const T* D, T* L, bool dipole) {
-    // L0: monopole + quadrupole terms, octupole terms
-    T a = m[0] * D[0];
-    a = fmat(m[4], D[4], a);
-    a = fmat(m[5], D[5], a);
-    a = fmat(m[6], D[6], a);
-    T b = m[7] * D[7];
-    b = fmat(m[8], D[8], b);
-    b = fmat(m[9], D[9], b);
-    T c = m[10] * D[10];
 #pragma unroll
-    for (int k = 11; k < 15; ++k) c = fmat(m[k], D[k], c);
-    T e = m[15] * D[15];
-#pragma unroll
-    for (int k = 16; k < 20; ++k) e = fmat(m[k], D[k], e);
+    for (int a = 0; a < 4; ++a) L[a] = fmat(m[0], D[a], L[a]);
     if (dipole) {
-        T g = m[1] * D[1];
-        g = fmat(m[2], D[2], g);
-        g = fmat(m[3], D[3], g);
-        c += g;
-    }
-    L[0] += (a + b) - (c + e);
 #pragma unroll
-    for (int ax = 0; ax < 3; ++ax) {
-        T u = m[0] * D[1 + ax];
-        u = fmat(m[4], D[quad_axis(0, ax)], u);
-        u = fmat(m[5], D[quad_axis(1, ax)], u);
-        u = fmat(m[6], D[quad_axis(2, ax)], u);
-        T v = m[7] * D[quad_axis(3, ax)];
-        v = fmat(m[8], D[quad_axis(4, ax)], v);
-        v = fmat(m[9], D[quad_axis(5, ax)], v);
-        if (dipole) {
-            // partner dipole block of compute_kernel_non_rho (:378-389)
-            T w = m[1 + ax] * D[quad_row(ax, 0)];
-            w = fmat(m[1 + ax], D[quad_row(ax, 1)], w);
-            w = fmat(m[1 + ax], D[quad_row(ax, 2)], w);
-            v -= w;
+        for (int a = 0; a < 3; ++a) {
+            L[0] = fmat(-m[1 + a], D[1 + a], L[0]);
+#pragma unroll
+            for (int b = 0; b < 3; ++b) L[1 + a] = fmat(-m[1 + a], D[quad_row(a, b)], L[1 + a]);
         }
-        L[1 + ax] += u + v;
     }
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+        L[0] = fmat(m[4 + q], D[4 + q], L[0]);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) L[1 + a] = fmat(m[4 + q], D[quad_axis(q, a)], L[1 + a]);
+    }
+#pragma unroll
+    for (int k = 10; k < 20; ++k) L[0] = fmat(-m[k], D[k], L[0]);
 }
 
 template <class T>
 __device__ __forceinline__ void fast_high_terms(const T* m, const T* D, T* L) {
 #pragma unroll
     for (int q = 0; q < 6; ++q) {
-        const T t = fmat(-m[1], D[quad_axis(q, 0)], m[0] * D[4 + q]);
-        const T u = fmat(m[2], D[quad_axis(q, 1)], m[3] * D[quad_axis(q, 2)]);
-        L[4 + q] += t - u;
+        T t = fmat(m[0], D[4 + q], L[4 + q]);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) t = fmat(-m[1 + a], D[quad_axis(q, a)], t);
+        L[4 + q] = t;
     }
 #pragma unroll
     for (int o = 0; o < 10; ++o) L[10 + o] = fmat(m[0], D[10 + o], L[10 + o]);
@@ -370,13 +349,10 @@ __device__ __forceinline__ void fast_upper_correction(const FastDerivs& f, const
     U[14] = fma(d3_6, f.X22, d2_3);
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
-        double s = g[0] * U[upper_idx(0, j)];
-        double t = g[5] * U[upper_idx(5, j)];
+        double t = Lc[j];
 #pragma unroll
-        for (int o = 1; o < 5; ++o) s = fma(g[o], U[upper_idx(o, j)], s);
-#pragma unroll
-        for (int o = 6; o < 10; ++o) t = fma(g[o], U[upper_idx(o, j)], t);
-        Lc[j] -= s + t;
+        for (int o = 0; o < 10; ++o) t = fma(-g[o], U[upper_idx(o, j)], t);
+        Lc[j] = t;
     }
 }
 
@@ -436,14 +412,25 @@ __device__ __forceinline__ void split_m2l_pair(const double X[3], const double Y
     f.X02 = dX[0] * dX[2];
     f.X12 = dX[1] * dX[2];
     const double r2 = fmax(f.X00 + f.X11 + f.X22, 1.0e-20);
-    const double rs = rsqrt(r2);
+    // 1/r: FP32 hardware estimate refined by one FP64 Newton step
+    // (relative error ~1e-14, far below what L_c needs)
+    const float r2f = (float)r2;
+    const float y0 = rsqrtf(r2f);
+    const double y = (double)y0;
+    const double rs = y * fma(-0.5 * r2 * y, y, 1.5);
     const double r2inv = rs * rs;
     const double d1 = rs * r2inv;
     f.d2 = -3.0 * d1 * r2inv;
     f.d3 = -5.0 * f.d2 * r2inv;
+    // FP32 factors from the refined 1/r (one conversion)
+    const float rsf = (float)rs;
+    const float r2invf = rsf * rsf;
+    const float d1f = rsf * r2invf;
+    const float d2f = -3.0f * d1f * r2invf;
+    const float d3f = -5.0f * d2f * r2invf;
     const float dXf[3] = {(float)dX[0], (float)dX[1], (float)dX[2]};
     float Df[20];
-    d_tensor<float>(dXf, (float)(-rs), (float)d1, (float)f.d2, (float)f.d3, Df);
+    d_tensor<float>(dXf, -rsf, d1f, d2f, d3f, Df);
     fast_low_terms<float>(mpf, Df, accf, !RHO);
     fast_high_terms<float>(mpf, Df, accf);
     if (RHO) {

@@ -24,7 +24,8 @@ FP64_EXACT, FP64, FP32_SPLIT = 0, 1, 2
 PRECISIONS = {"fp64_exact": FP64_EXACT, "fp64": FP64, "fp32_split": FP32_SPLIT}
 
 EXPORTED = ["otfmm_create", "otfmm_destroy", "otfmm_stencil_info", "otfmm_m2l_soa", "otfmm_m2l_soa_host",
-            "otfmm_p2p_soa", "otfmm_p2m_soa", "otfmm_batch", "otfmm_batch_status", "otfmm_last_error",
+            "otfmm_p2p_soa", "otfmm_p2m_soa", "otfmm_batch", "otfmm_batch_status", "otfmm_count_pairs",
+            "otfmm_last_error",
             "otfmm_build_info", "otfmm_measure_fma_peaks"]
 
 _lib = None
@@ -53,6 +54,8 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
         lib.otfmm_p2m_soa.argtypes = [vp, i, vp, vp, vp, vp, vp, i, i, i, vp]
         lib.otfmm_batch.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int32, vp, ctypes.c_int32, vp, vp, i, i, vp]
         lib.otfmm_batch_status.argtypes = [vp, vp]
+        lib.otfmm_count_pairs.argtypes = [vp, vp, ctypes.c_int32, vp, ctypes.c_int32, vp]
+        lib.otfmm_count_pairs.restype = ctypes.c_longlong
         lib.otfmm_last_error.restype = ctypes.c_char_p
         lib.otfmm_build_info.restype = ctypes.c_char_p
         lib.otfmm_measure_fma_peaks.argtypes = [i, ctypes.POINTER(dp), ctypes.POINTER(dp)]
@@ -155,6 +158,17 @@ class Context:
         _check(load_library().otfmm_batch(self.handle, _ptr(dev.M), _ptr(dev.com), _ptr(dev.mon), _ptr(dev.is_leaf),
                                           ctypes.c_int32(dev.n), _ptr(items_dev), ctypes.c_int32(n_items), _ptr(L),
                                           _ptr(Lc), int(gsolve_type), precision_code(precision), _stream(stream)))
+
+    def count_pairs(self, is_leaf: np.ndarray, items: np.ndarray) -> tuple[int, np.ndarray]:
+        """Cell-interactions of a work list: total and [M2L, root, P2P, P2M]."""
+        per = np.zeros(4, np.int64)
+        items = np.ascontiguousarray(items)
+        is_leaf = np.ascontiguousarray(is_leaf, dtype=np.uint8)
+        tot = load_library().otfmm_count_pairs(self.handle, is_leaf.ctypes.data, ctypes.c_int32(len(is_leaf)),
+                                               items.ctypes.data, ctypes.c_int32(len(items)), per.ctypes.data)
+        if tot < 0:
+            _check(int(tot))
+        return int(tot), per
 
     def batch_status(self, stream=None) -> None:
         _check(load_library().otfmm_batch_status(self.handle, _stream(stream)))

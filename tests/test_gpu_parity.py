@@ -52,6 +52,8 @@ CASES = {
     "leaf_all_refined": lambda: syn.single_subgrid(seed=25, leaf_centre=True),
     "leaf_only_leaves": lambda: syn.single_subgrid(seed=26, leaf_centre=True, leaf_dirs=tuple(range(26))),
     "uniform_level2": lambda: syn.uniform_level(2, seed=27),
+    "amr_small": lambda: __import__("octotiger_b200.amr", fromlist=["amr"]).polytrope_batch(radius=0.05, max_level=5,
+                                                                                             seed=28),
 }
 
 
@@ -207,7 +209,7 @@ def split_errors(L, Lc, Lo, Lco):
     return out
 
 
-SPLIT_CASES = ["single", "mixed", "uniform_level2", "leaf"]
+SPLIT_CASES = ["single", "mixed", "uniform_level2", "leaf", "amr_small"]
 
 
 @pytest.mark.parametrize("solve", [RHO, DRHODT])
@@ -231,3 +233,11 @@ def test_fp32_split_full_size_accuracy(ctx, oracle):
     Lo, Lco = oracle.batch(0.5, b.pool, b.items, rho=True)
     err = split_errors(L, Lc, Lo, Lco)
     assert err["L0"] <= 1e-6 and err["force"] <= 1e-6 and err["Lc"] <= 1e-10, err
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_library_pair_count_matches_oracle(ctx, oracle, name):
+    b = CASES[name]()
+    tot, per = ctx.count_pairs(b.pool.is_leaf, b.items)
+    tot_o, per_o = oracle.count_pairs(0.5, b.pool, b.items)
+    assert tot == tot_o and list(per) == list(per_o)
