@@ -604,25 +604,28 @@ __global__ void __launch_bounds__(THREADS, 1) m2l_batch_kernel(BatchArgs a) {
 // monopole_interaction_interface.hpp:82-87), which adds exact zeros, so the
 // sweep has no branch. Writes L0..L3, zeroes L4..L19 and L_c (the P2M kernel
 // adds the refined-neighbour part afterwards).
+// Persistent: each CTA stages the per-parity offset/constant table once and
+// then walks the work list with a grid stride (every leaf costs the same).
+constexpr int P2P_CTAS_PER_SM = 2;
+constexpr int P2P_TABLE_BYTES = 8 * MAX_ENTRIES * (4 * 8 + 4);
+constexpr int P2P_SMEM_BYTES = P_SMEM_DOUBLES * 8 + P2P_TABLE_BYTES;
+
 template <int PREC>
-__global__ void __launch_bounds__(P_THREADS) p2p_batch_kernel(BatchArgs a) {
-    __shared__ double pm[P_SMEM_DOUBLES];
+__global__ void __launch_bounds__(P_THREADS, P2P_CTAS_PER_SM) p2p_batch_kernel(BatchArgs a) {
+    extern __shared__ double dyn[];
+    double* pm = dyn;                                                  // mass region
+    double4* s_four = reinterpret_cast<double4*>(dyn + P_SMEM_DOUBLES);   // [8][MAX_ENTRIES]
+    int* s_delta = reinterpret_cast<int*>(s_four + 8 * MAX_ENTRIES);      // [8][MAX_ENTRIES]
     __shared__ ItemInfo it;
     __shared__ int bad;
-    if (a.items[blockIdx.x].kind != OTFMM_KIND_LEAF) return;
-    if (!load_item(a, blockIdx.x, it, bad)) return;
-    const double dc0 = __ddiv_rn(1.0, it.dx), dc1 = __ddiv_rn(-1.0, it.dx);
-    for (int r = threadIdx.x; r < P_REG * P_REG * P_REG; r += blockDim.x) {
-        const int ax = r / (P_REG * P_REG) - 2, ay = (r / P_REG) % P_REG - 2, az = r % P_REG - 2;
-        const int raw = raw_dir(ax, ay, az);
-        const int src = (raw == 13) ? it.subgrid : it.nb[raw < 13 ? raw : raw - 1];
-        double m = 0.0;
-        if (src >= 0 && (raw == 13 || a.is_leaf[src])) m = a.mon[(size_t)src * NCELL + (ax & 7) * 64 + (ay & 7) * 8 + (az & 7)];
-        if (PREC != PREC_EXACT) m *= dc0;   // 1/dx folded into the staged mass
-        const int cls = ((ax & 1) << 2) | ((ay & 1) << 1) | (az & 1);
-        pm[cls * P_CLS + ((ax + 2) >> 1) * P_XS + ((ay + 2) >> 1) * P_RS + ((az + 2) >> 1)] = m;
+    for (int e = threadIdx.x; e < 8 * MAX_ENTRIES; e += blockDim.x) {
+        const int p = e / MAX_ENTRIES, k = e % MAX_ENTRIES;
+        if (k < a.t.count[p]) {
+            const int2 en = a.t.entries_p2p[e];
+            s_delta[e] = en.x;
+            s_four[e] = make_double4(c_four[en.y][0], c_four[en.y][1], c_four[en.y][2], c_four[en.y][3]);
+        }
     }
-    __syncthreads();
     // thread -> cell: warp w covers parity class w/2, x' block w%2
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int p = w >> 1;
@@ -630,36 +633,58 @@ __global__ void __launch_bounds__(P_THREADS) p2p_batch_kernel(BatchArgs a) {
     const int cx = ((p >> 2) & 1) + 2 * i, cy = ((p >> 1) & 1) + 2 * j, cz = (p & 1) + 2 * k;
     const int lane_off = i * P_XS + j * P_RS + k;
     const int n = a.t.count[p];
-    const int2* ent = a.t.entries_p2p + p * MAX_ENTRIES;
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    if (PREC == PREC_EXACT) {
-        for (int e = 0; e < n; ++e) {
-            const int2 en = __ldg(ent + e);
-            const double ms = __dmul_rn(pm[en.x + lane_off], dc0);
-            acc[0] = __dadd_rn(acc[0], __dmul_rn(c_four[en.y][0], ms));
-#pragma unroll
-            for (int q = 1; q < 4; ++q) acc[q] = __dadd_rn(acc[q], __dmul_rn(__dmul_rn(c_four[en.y][q], ms), dc1));
+    const double4* four = s_four + p * MAX_ENTRIES;
+    const int* delta = s_delta + p * MAX_ENTRIES;
+    for (int item = blockIdx.x; item < a.n_items; item += gridDim.x) {
+        if (a.items[item].kind != OTFMM_KIND_LEAF) continue;   // uniform per CTA
+        __syncthreads();   // previous item's readers are done with pm / it
+        if (!load_item(a, item, it, bad)) continue;
+        const double dc0 = __ddiv_rn(1.0, it.dx), dc1 = __ddiv_rn(-1.0, it.dx);
+        for (int r = threadIdx.x; r < P_REG * P_REG * P_REG; r += blockDim.x) {
+            const int ax = r / (P_REG * P_REG) - 2, ay = (r / P_REG) % P_REG - 2, az = r % P_REG - 2;
+            const int raw = raw_dir(ax, ay, az);
+            const int src = (raw == 13) ? it.subgrid : it.nb[raw < 13 ? raw : raw - 1];
+            double m = 0.0;
+            if (src >= 0 && (raw == 13 || a.is_leaf[src]))
+                m = a.mon[(size_t)src * NCELL + (ax & 7) * 64 + (ay & 7) * 8 + (az & 7)];
+            if (PREC != PREC_EXACT) m *= dc0;   // 1/dx folded into the staged mass
+            const int cls = ((ax & 1) << 2) | ((ay & 1) << 1) | (az & 1);
+            pm[cls * P_CLS + ((ax + 2) >> 1) * P_XS + ((ay + 2) >> 1) * P_RS + ((az + 2) >> 1)] = m;
         }
-    } else {
+        __syncthreads();
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        if (PREC == PREC_EXACT) {
+            for (int e = 0; e < n; ++e) {
+                const double4 f = four[e];
+                const double ms = __dmul_rn(pm[delta[e] + lane_off], dc0);
+                acc[0] = __dadd_rn(acc[0], __dmul_rn(f.x, ms));
+                acc[1] = __dadd_rn(acc[1], __dmul_rn(__dmul_rn(f.y, ms), dc1));
+                acc[2] = __dadd_rn(acc[2], __dmul_rn(__dmul_rn(f.z, ms), dc1));
+                acc[3] = __dadd_rn(acc[3], __dmul_rn(__dmul_rn(f.w, ms), dc1));
+            }
+        } else {
 #pragma unroll 4
-        for (int e = 0; e < n; ++e) {
-            const int2 en = __ldg(ent + e);
-            const double ms = pm[en.x + lane_off];
+            for (int e = 0; e < n; ++e) {
+                const double4 f = four[e];
+                const double ms = pm[delta[e] + lane_off];
+                acc[0] = fma(f.x, ms, acc[0]);
+                acc[1] = fma(f.y, ms, acc[1]);
+                acc[2] = fma(f.z, ms, acc[2]);
+                acc[3] = fma(f.w, ms, acc[3]);
+            }
 #pragma unroll
-            for (int q = 0; q < 4; ++q) acc[q] = fma(c_four[en.y][q], ms, acc[q]);
+            for (int q = 1; q < 4; ++q) acc[q] *= dc1;
         }
+        const int cf = cx * 64 + cy * 8 + cz;
+        double* L = a.L + (size_t)it.subgrid * 20 * NCELL;
+        double* Lc = a.Lc + (size_t)it.subgrid * 3 * NCELL;
 #pragma unroll
-        for (int q = 1; q < 4; ++q) acc[q] *= dc1;
+        for (int q = 0; q < 4; ++q) L[q * NCELL + cf] = acc[q];
+#pragma unroll
+        for (int q = 4; q < 20; ++q) L[q * NCELL + cf] = 0.0;
+#pragma unroll
+        for (int q = 0; q < 3; ++q) Lc[q * NCELL + cf] = 0.0;
     }
-    const int cf = cx * 64 + cy * 8 + cz;
-    double* L = a.L + (size_t)it.subgrid * 20 * NCELL;
-    double* Lc = a.Lc + (size_t)it.subgrid * 3 * NCELL;
-#pragma unroll
-    for (int q = 0; q < 4; ++q) L[q * NCELL + cf] = acc[q];
-#pragma unroll
-    for (int q = 4; q < 20; ++q) L[q * NCELL + cf] = 0.0;
-#pragma unroll
-    for (int q = 0; q < 3; ++q) Lc[q * NCELL + cf] = 0.0;
 }
 
 // Leaf items with refined neighbours: P2M (p2m_kernel_impl_rho / _non_rho,
@@ -691,26 +716,39 @@ __global__ void __launch_bounds__(P_THREADS) p2m_batch_kernel(BatchArgs a) {
     for (int q = 0; q < 4; ++q) acc[q] = L[q * NCELL + cu];
     const int n = a.t.count[p];
     const int2* ent = a.t.entries + p * MAX_ENTRIES;
-    for (int raw = 0; raw < 27; ++raw) {
-        if (!((refmask >> raw) & 1u)) continue;
-        const int nb = it.nb[raw < 13 ? raw : raw - 1];
+    if (PREC == PREC_EXACT) {
+        // direction after direction, like the reference's one launch per neighbour
+        for (int raw = 0; raw < 27; ++raw) {
+            if (!((refmask >> raw) & 1u)) continue;
+            const int nb = it.nb[raw < 13 ? raw : raw - 1];
+            for (int e = 0; e < n; ++e) {
+                const int y = __ldg(&ent[e].y);
+                const int ax = cx + entry_sx(y), ay = cy + entry_sy(y), az = cz + entry_sz(y);
+                if (raw_dir(ax, ay, az) != raw) continue;
+                const int u = (ax & 7) * 64 + (ay & 7) * 8 + (az & 7);
+                double Y[3], mp[20];
+#pragma unroll
+                for (int q = 0; q < 3; ++q) Y[q] = __ldg(a.com + ((size_t)nb * 3 + q) * NCELL + u);
+#pragma unroll
+                for (int q = 0; q < 20; ++q) mp[q] = __ldg(a.M + ((size_t)nb * 20 + q) * NCELL + u);
+                exact_p2m_pair<RHO>(X, Y, mp, acc, corr);
+            }
+        }
+    } else {
+        // one pass: partners in any refined neighbour
         for (int e = 0; e < n; ++e) {
             const int y = __ldg(&ent[e].y);
             const int ax = cx + entry_sx(y), ay = cy + entry_sy(y), az = cz + entry_sz(y);
-            if (raw_dir(ax, ay, az) != raw) continue;
+            const int raw = raw_dir(ax, ay, az);
+            if (!((refmask >> raw) & 1u)) continue;
+            const int nb = it.nb[raw < 13 ? raw : raw - 1];
             const int u = (ax & 7) * 64 + (ay & 7) * 8 + (az & 7);
             double Y[3], mp[20];
 #pragma unroll
             for (int q = 0; q < 3; ++q) Y[q] = __ldg(a.com + ((size_t)nb * 3 + q) * NCELL + u);
-            if (PREC == PREC_EXACT) {
 #pragma unroll
-                for (int q = 0; q < 20; ++q) mp[q] = __ldg(a.M + ((size_t)nb * 20 + q) * NCELL + u);
-                exact_p2m_pair<RHO>(X, Y, mp, acc, corr);
-            } else {
-#pragma unroll
-                for (int q = 0; q < 20; ++q) mp[q] = __ldg(a.M + ((size_t)nb * 20 + q) * NCELL + u) * stage_scale<PREC_FAST>(q);
-                fast_p2m_pair<RHO>(X, Y, mp, acc, corr);
-            }
+            for (int q = 0; q < 20; ++q) mp[q] = __ldg(a.M + ((size_t)nb * 20 + q) * NCELL + u) * stage_scale<PREC_FAST>(q);
+            fast_p2m_pair<RHO>(X, Y, mp, acc, corr);
         }
     }
 #pragma unroll
@@ -1028,6 +1066,8 @@ int ensure_attributes(int device) {
     rc = rc ? rc : set_smem(m2l_batch_kernel<PREC_FAST, false>, bytes);
     rc = rc ? rc : set_smem(m2l_batch_kernel<PREC_SPLIT, true>, S_SMEM_DOUBLES * (int)sizeof(double));
     rc = rc ? rc : set_smem(m2l_batch_kernel<PREC_SPLIT, false>, S_SMEM_DOUBLES * (int)sizeof(double));
+    rc = rc ? rc : set_smem(p2p_batch_kernel<PREC_EXACT>, P2P_SMEM_BYTES);
+    rc = rc ? rc : set_smem(p2p_batch_kernel<PREC_FAST>, P2P_SMEM_BYTES);
     rc = rc ? rc : set_smem(soa_m2l_kernel<PREC_EXACT, true, false>, bytes);
     rc = rc ? rc : set_smem(soa_m2l_kernel<PREC_EXACT, false, false>, bytes);
     rc = rc ? rc : set_smem(soa_m2l_kernel<PREC_FAST, true, false>, bytes);
@@ -1290,10 +1330,13 @@ int otfmm_batch(otfmm_context* ctx, const double* pool_M, const double* pool_com
     // multipole tiles, then P2P of the leaves, then P2M (stream order keeps
     // the reference's P2P-then-P2M accumulation order)
     const dim3 pgrid(n_items);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+    const dim3 p2p_grid(std::min(n_items, P2P_CTAS_PER_SM * sms));
     if (precision == OTFMM_FP64_EXACT) {
         if (rho) m2l_batch_kernel<PREC_EXACT, true><<<grid, THREADS, bytes, s>>>(a);
         else m2l_batch_kernel<PREC_EXACT, false><<<grid, THREADS, bytes, s>>>(a);
-        p2p_batch_kernel<PREC_EXACT><<<pgrid, P_THREADS, 0, s>>>(a);
+        p2p_batch_kernel<PREC_EXACT><<<p2p_grid, P_THREADS, P2P_SMEM_BYTES, s>>>(a);
         if (rho) p2m_batch_kernel<PREC_EXACT, true><<<pgrid, P_THREADS, 0, s>>>(a);
         else p2m_batch_kernel<PREC_EXACT, false><<<pgrid, P_THREADS, 0, s>>>(a);
     } else {
@@ -1305,7 +1348,7 @@ int otfmm_batch(otfmm_context* ctx, const double* pool_M, const double* pool_com
             if (rho) m2l_batch_kernel<PREC_FAST, true><<<grid, THREADS, bytes, s>>>(a);
             else m2l_batch_kernel<PREC_FAST, false><<<grid, THREADS, bytes, s>>>(a);
         }
-        p2p_batch_kernel<PREC_FAST><<<pgrid, P_THREADS, 0, s>>>(a);
+        p2p_batch_kernel<PREC_FAST><<<p2p_grid, P_THREADS, P2P_SMEM_BYTES, s>>>(a);
         if (rho) p2m_batch_kernel<PREC_FAST, true><<<pgrid, P_THREADS, 0, s>>>(a);
         else p2m_batch_kernel<PREC_FAST, false><<<pgrid, P_THREADS, 0, s>>>(a);
     }
