@@ -114,6 +114,25 @@ int otfmm_m2l_soa(otfmm_context* ctx, const double* mon, const double* M, const 
 int otfmm_m2l_soa_host(otfmm_context* ctx, const double* mon, const double* M, const double* com, double* L,
                        double* L_c, int gsolve_type, int use_root_stencil, int precision);
 
+/* No counterpart in the reference. Same as otfmm_m2l_soa_host for up to
+ * OTFMM_NOALLOC_MAX_SUBGRIDS subgrids per call (host buffers laid out one
+ * subgrid after the other: mon[n][5832], M[n][20*5851], com[n][3*5851] in,
+ * L[n][20*531], L_c[n][3*531] out), but it allocates nothing: its device
+ * staging is a fixed static array of OTFMM_NOALLOC_MAX_SUBGRIDS x 1.22 MB that
+ * every GPU loading the library holds until the process exits. For callers
+ * that must not allocate device memory while they run: code inside a
+ * pre-sized memory budget, threads that must not trigger the implicit device
+ * synchronisation of cudaMalloc/cudaFree, or HPX tasks on a hot path where the
+ * reference uses recycled buffers. The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress) and should come before any
+ * stream capture. Larger n_subgrids is rejected (OTFMM_ERR_INVALID). All calls
+ * share the one array: calls that overlap on the GPU would race, so calls
+ * from this library are serialised and each waits for its stream. */
+#define OTFMM_NOALLOC_MAX_SUBGRIDS 4
+int otfmm_m2l_soa_host_noalloc(otfmm_context* ctx, int32_t n_subgrids, const double* mon, const double* M,
+                               const double* com, double* L, double* L_c, int gsolve_type, int use_root_stencil,
+                               int precision, void* stream);
+
 /* P2P of one leaf subgrid from its staged monopole buffer (mon[5832], device
  * pointer), p2p_kernel_impl + sum_p2p_results (monopole kokkos_kernel.hpp:118-320):
  * writes L4 (4 x 531). */

@@ -885,6 +885,13 @@ __global__ void fma_probe_kernel(T* out, int iters, T x, T y) {
     if (s == (T)-12345.0) out[blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
 
+// Staging for otfmm_m2l_soa_host_noalloc: up to NOALLOC_MAX_SUBGRIDS
+// subgrids' SoA inputs and outputs (1.22 MB each), resident in every device
+// that loads the library until the process exits.
+constexpr int NOALLOC_MAX_SUBGRIDS = 4;
+constexpr size_t NOALLOC_SLOT = ENTRIES + 23 * (size_t)CL + 23 * (size_t)CLU;   // doubles per subgrid
+static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_MAX_SUBGRIDS * NOALLOC_SLOT];
+
 }   // namespace otfmm
 
 // ======================================================================== host
@@ -1265,6 +1272,59 @@ int otfmm_m2l_soa_host(otfmm_context* ctx, const double* mon, const double* M, c
     if (rc) return rc;
     OT_CUDA(cudaMemcpy(L, d_L, sizeof(double) * 20 * CLU, cudaMemcpyDeviceToHost));
     if (gsolve_type == OTFMM_RHO && L_c) OT_CUDA(cudaMemcpy(L_c, d_Lc, sizeof(double) * 3 * CLU, cudaMemcpyDeviceToHost));
+    return OTFMM_OK;
+}
+
+// Host-buffer multipole call that allocates nothing: device staging comes
+// from the static g_noalloc_scratch array. Its device address is looked up
+// once per device (cudaGetSymbolAddress, on the first call on that device,
+// which should therefore come before any stream capture); later calls reuse
+// it. The array is shared by every call: calls are serialised here, and each
+// call clears the output staging it reads back.
+int otfmm_m2l_soa_host_noalloc(otfmm_context* ctx, int32_t n_subgrids, const double* mon, const double* M,
+                               const double* com, double* L, double* L_c, int gsolve_type, int use_root_stencil,
+                               int precision, void* stream) {
+    static std::mutex mu;
+    static double* scratch_ptr[64] = {};
+    if (!ctx || !M || !com || !L) return fail(OTFMM_ERR_INVALID, "NULL argument");
+    if (n_subgrids < 1 || n_subgrids > NOALLOC_MAX_SUBGRIDS)
+        return fail(OTFMM_ERR_INVALID, "n_subgrids must be 1.." + std::to_string(NOALLOC_MAX_SUBGRIDS) +
+                                           ": the static staging array holds at most that many subgrids");
+    const bool rho = (gsolve_type == OTFMM_RHO);
+    if (gsolve_type != OTFMM_RHO && gsolve_type != OTFMM_DRHODT) return fail(OTFMM_ERR_INVALID, "bad gsolve_type");
+    if (rho && !L_c) return fail(OTFMM_ERR_INVALID, "L_c is NULL for RHO");
+    if (!use_root_stencil && !mon) return fail(OTFMM_ERR_INVALID, "mon is NULL");
+    if (ctx->device < 0 || ctx->device >= 64) return fail(OTFMM_ERR_INVALID, "device index out of range");
+    int rc = check_precision(precision);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lock(mu);
+    DeviceGuard g(ctx->device);
+    if (!scratch_ptr[ctx->device]) {
+        double* ptr = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress((void**)&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+        scratch_ptr[ctx->device] = ptr;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    for (int i = 0; i < n_subgrids; ++i) {
+        double* d_mon = scratch_ptr[ctx->device] + i * NOALLOC_SLOT;
+        double* d_M = d_mon + ENTRIES;
+        double* d_com = d_M + 20 * (size_t)CL;
+        double* d_L = d_com + 3 * (size_t)CL;
+        double* d_Lc = d_L + 20 * (size_t)CLU;
+        if (!use_root_stencil)
+            OT_CUDA(cudaMemcpyAsync(d_mon, mon + (size_t)i * ENTRIES, sizeof(double) * ENTRIES, cudaMemcpyHostToDevice, s));
+        OT_CUDA(cudaMemcpyAsync(d_M, M + (size_t)i * 20 * CL, sizeof(double) * 20 * CL, cudaMemcpyHostToDevice, s));
+        OT_CUDA(cudaMemcpyAsync(d_com, com + (size_t)i * 3 * CL, sizeof(double) * 3 * CL, cudaMemcpyHostToDevice, s));
+        OT_CUDA(cudaMemsetAsync(d_L, 0, sizeof(double) * 23 * CLU, s));
+        rc = otfmm_m2l_soa(ctx, use_root_stencil ? nullptr : d_mon, d_M, d_com, d_L, d_Lc, gsolve_type,
+                           use_root_stencil, precision, stream);
+        if (rc) return rc;
+        OT_CUDA(cudaMemcpyAsync(L + (size_t)i * 20 * CLU, d_L, sizeof(double) * 20 * CLU, cudaMemcpyDeviceToHost, s));
+        if (rho)
+            OT_CUDA(cudaMemcpyAsync(L_c + (size_t)i * 3 * CLU, d_Lc, sizeof(double) * 3 * CLU, cudaMemcpyDeviceToHost, s));
+    }
+    OT_CUDA(cudaStreamSynchronize(s));
     return OTFMM_OK;
 }
 

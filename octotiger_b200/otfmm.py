@@ -25,7 +25,7 @@ PRECISIONS = {"fp64_exact": FP64_EXACT, "fp64": FP64, "fp32_split": FP32_SPLIT}
 
 EXPORTED = ["otfmm_create", "otfmm_destroy", "otfmm_stencil_info", "otfmm_m2l_soa", "otfmm_m2l_soa_host",
             "otfmm_p2p_soa", "otfmm_p2m_soa", "otfmm_batch", "otfmm_batch_status", "otfmm_count_pairs",
-            "otfmm_last_error",
+            "otfmm_m2l_soa_host_noalloc", "otfmm_last_error",
             "otfmm_build_info", "otfmm_measure_fma_peaks"]
 
 _lib = None
@@ -50,6 +50,7 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
         lib.otfmm_stencil_info.argtypes = [vp, vp, vp, vp, vp]
         lib.otfmm_m2l_soa.argtypes = [vp, vp, vp, vp, vp, vp, i, i, i, vp]
         lib.otfmm_m2l_soa_host.argtypes = [vp, vp, vp, vp, vp, vp, i, i, i]
+        lib.otfmm_m2l_soa_host_noalloc.argtypes = [vp, ctypes.c_int32, vp, vp, vp, vp, vp, i, i, i, vp]
         lib.otfmm_p2p_soa.argtypes = [vp, vp, dp, vp, i, vp]
         lib.otfmm_p2m_soa.argtypes = [vp, i, vp, vp, vp, vp, vp, i, i, i, vp]
         lib.otfmm_batch.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int32, vp, ctypes.c_int32, vp, vp, i, i, vp]
@@ -141,6 +142,28 @@ class Context:
         _check(load_library().otfmm_m2l_soa_host(
             self.handle, None if mon is None else mon.ctypes.data, M.ctypes.data, com.ctypes.data, L.ctypes.data,
             Lc.ctypes.data, int(gsolve_type), int(bool(use_root_stencil)), precision_code(precision)))
+        return L, Lc
+
+    def m2l_soa_host_noalloc(self, mon, M, com, gsolve_type=RHO, use_root_stencil=False, precision=FP64):
+        """Host-buffer multipole call for 1..4 subgrids that allocates no device
+        memory (its staging is a static device array). Inputs are stacked per
+        subgrid: mon [n, 5832] (None for the root stencil), M [n, 20*5851],
+        com [n, 3*5851]; returns L [n, 20*531], L_c [n, 3*531]."""
+        M = np.ascontiguousarray(M, dtype=np.float64).reshape(-1, 20 * COMPONENT_LENGTH)
+        com = np.ascontiguousarray(com, dtype=np.float64).reshape(-1, 3 * COMPONENT_LENGTH)
+        n = M.shape[0]
+        if mon is not None:
+            mon = np.ascontiguousarray(mon, dtype=np.float64).reshape(-1, ENTRIES)
+            if mon.shape[0] != n:
+                raise ValueError("mon and M disagree on the number of subgrids")
+        if com.shape[0] != n:
+            raise ValueError("com and M disagree on the number of subgrids")
+        L = np.zeros((n, 20 * COMPONENT_LENGTH_UNPADDED))
+        Lc = np.zeros((n, 3 * COMPONENT_LENGTH_UNPADDED))
+        _check(load_library().otfmm_m2l_soa_host_noalloc(
+            self.handle, ctypes.c_int32(n), None if mon is None else mon.ctypes.data, M.ctypes.data,
+            com.ctypes.data, L.ctypes.data, Lc.ctypes.data, int(gsolve_type), int(bool(use_root_stencil)),
+            precision_code(precision), None))
         return L, Lc
 
     def p2p_soa(self, mon, dx, L4, precision=FP64, stream=None):
