@@ -175,6 +175,14 @@ long long otfmm_count_pairs(const otfmm_context* ctx, const uint8_t* is_leaf, in
  * without synchronizing the whole device: returns OTFMM_OK or OTFMM_ERR_DEVICE. */
 int otfmm_batch_status(otfmm_context* ctx, void* stream);
 
+/* Device memory helpers for host adapters that do not link the CUDA runtime
+ * themselves (include/otfmm_octotiger.hpp): allocate / free on the context's
+ * device, and blocking copies between host and device. */
+int otfmm_device_alloc(otfmm_context* ctx, size_t bytes, void** ptr);
+int otfmm_device_free(void* ptr);
+int otfmm_copy_to_device(otfmm_context* ctx, void* dst, const void* src, size_t bytes);
+int otfmm_copy_to_host(otfmm_context* ctx, void* dst, const void* src, size_t bytes);
+
 /* Message for the last error on the calling thread ("" if none). */
 const char* otfmm_last_error(void);
 

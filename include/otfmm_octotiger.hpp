@@ -1,0 +1,257 @@
+// otfmm_octotiger.hpp — drop-in host adapter for Octo-Tiger (header only).
+//
+// The bodies of a new `interaction_device_kernel_type` branch in
+//   octotiger::fmm::multipole_interactions::multipole_kernel_interface
+//     (src/multipole_interactions/multipole_kernel_interface.cpp:73-169)
+//   octotiger::fmm::monopole_interactions::monopole_kernel_interface
+//     (src/monopole_interactions/monopole_kernel_interface.cpp:97-198)
+// on top of the C ABI in otfmm.h. The functions take the same arguments with
+// the same meaning as the reference's interfaces and leave the grid in the
+// same state:
+//   * multipole: L += M2L result (all 20 components), L_c = correction (RHO);
+//   * monopole: L[0..3] += P2P + P2M, L_c = P2M correction when a neighbour is
+//     refined (RHO), otherwise L_c untouched;
+// and stage the 26-neighbour halo the way update_input does
+// (octotiger/multipole_interactions/legacy/multipole_interaction_interface.hpp:88-281,
+//  octotiger/monopole_interactions/legacy/monopole_interaction_interface.hpp:64-143,
+//  octotiger/monopole_interactions/legacy/p2m_interaction_interface.hpp:102-160).
+// Neighbour payloads must be full size (512 cells); the compressed
+// ilist_n_bnd payloads of remote neighbours are expanded by the caller.
+//
+// Template parameters are Octo-Tiger's own types (multipole = taylor<4>,
+// expansion = taylor<4>, space_vector, neighbor_gravity_type with
+// .data.M / .data.m / .data.x and .is_monopole), so the header compiles inside
+// the reference tree; tests/cpp instantiates it with plain stand-ins.
+//
+// Errors: every function returns the otfmm status; the *_or_abort wrappers
+// print to std::cerr and abort(), which is what the reference does on
+// misconfiguration (multipole_kernel_interface.cpp:107-158).
+#pragma once
+
+#include <array>
+#include <cstdio>
+#include <cstdlib>
+#include <iostream>
+#include <memory>
+#include <vector>
+
+#include "otfmm.h"
+
+namespace otfmm_octotiger {
+
+constexpr int INX = 8;
+constexpr int NCELL = 512;
+constexpr int SMAX = 5;
+constexpr int PSTRIDE = INX + 2 * SMAX;
+constexpr int ENTRIES = PSTRIDE * PSTRIDE * PSTRIDE;
+constexpr int CL = ENTRIES + 19;
+constexpr int CLU = NCELL + 19;
+
+inline int flat_padded(int x, int y, int z) { return (x - 3) * PSTRIDE * PSTRIDE + (y - 3) * PSTRIDE + (z - 3); }
+inline int flat_inner(int x, int y, int z) { return x * INX * INX + y * INX + z; }
+inline void dir_offsets(int d, int o[3]) {
+    const int r = d < 13 ? d : d + 1;
+    o[0] = r % 3 - 1;
+    o[1] = (r / 3) % 3 - 1;
+    o[2] = r / 9 - 1;
+}
+// neighbour-local cell range inside the 18^3 halo and the padded index of
+// local cell 0 (iterate_inner_cells_padding, interactions_iterators.hpp:65-128)
+inline void padding_range(const int o[3], int s[3], int e[3], int p[3]) {
+    for (int a = 0; a < 3; ++a) {
+        s[a] = (o[a] == -1) ? INX - SMAX : 0;
+        e[a] = (o[a] == 1) ? SMAX : INX;
+        p[a] = (o[a] == 1) ? 2 * INX : (o[a] == 0 ? INX : 0);
+    }
+}
+
+// Host and device staging of one subgrid, reused across calls of a thread
+// (the reference recycles its buffers through CPPuddle).
+struct Staging {
+    std::vector<double> mon, M, com, L, Lc;
+    Staging() : mon(ENTRIES), M(20 * CL), com(3 * CL), L(20 * CLU), Lc(3 * CLU) {}
+};
+inline Staging& thread_staging() {
+    thread_local Staging s;
+    return s;
+}
+
+template <class Multipole, class SpaceVector, class Neighbor>
+void stage_multipole_input(const std::vector<Multipole>& M_ptr, const SpaceVector* com0,
+                           const std::vector<Neighbor>& neighbors, double dx, const std::array<double, 3>& xbase,
+                           bool is_root, Staging& st) {
+    std::fill(st.mon.begin(), st.mon.end(), 0.0);
+    std::fill(st.M.begin(), st.M.end(), 0.0);
+    std::fill(st.com.begin(), st.com.end(), 0.0);
+    for (int x = 0; x < INX; ++x)
+        for (int y = 0; y < INX; ++y)
+            for (int z = 0; z < INX; ++z) {
+                const int f = flat_padded(x + INX, y + INX, z + INX), u = flat_inner(x, y, z);
+                for (int c = 0; c < 20; ++c) st.M[c * CL + f] = M_ptr[u][c];
+                for (int c = 0; c < 3; ++c) st.com[c * CL + f] = com0[u][c];
+            }
+    if (is_root) return;
+    for (int d = 0; d < 26; ++d) {
+        const Neighbor& nb = neighbors[d];
+        int o[3], s[3], e[3], p[3];
+        dir_offsets(d, o);
+        padding_range(o, s, e, p);
+        for (int x = s[0]; x < e[0]; ++x)
+            for (int y = s[1]; y < e[1]; ++y)
+                for (int z = s[2]; z < e[2]; ++z) {
+                    const int ix = x + p[0], iy = y + p[1], iz = z + p[2];
+                    const int f = flat_padded(ix, iy, iz), u = flat_inner(x, y, z);
+                    if (!nb.is_monopole) {
+                        if (!nb.data.M) continue;   // empty direction: zeros
+                        for (int c = 0; c < 20; ++c) st.M[c * CL + f] = (*nb.data.M)[u][c];
+                        for (int c = 0; c < 3; ++c) st.com[c * CL + f] = (*nb.data.x)[u][c];
+                    } else {
+                        if (!nb.data.m) continue;
+                        st.com[0 * CL + f] = ix * dx + xbase[0] - INX * dx;
+                        st.com[1 * CL + f] = iy * dx + xbase[1] - INX * dx;
+                        st.com[2 * CL + f] = iz * dx + xbase[2] - INX * dx;
+                        st.mon[f] = (*nb.data.m)[u];
+                    }
+                }
+    }
+}
+
+// multipole_kernel_interface(monopoles, M_ptr, com_ptr, neighbors, type, dx,
+// is_direction_empty, xbase, grid, use_root_stencil): L += result,
+// L_c = correction (RHO). `monopoles` is not read: a refined node's own cells
+// enter as multipoles (update_input sets their monopole slots to zero).
+template <class Multipole, class SpaceVector, class Neighbor, class Expansion>
+int multipole_kernel_interface(otfmm_context* ctx, const std::vector<double>& /*monopoles*/,
+                               const std::vector<Multipole>& M_ptr,
+                               const std::vector<std::shared_ptr<std::vector<SpaceVector>>>& com_ptr,
+                               const std::vector<Neighbor>& neighbors, int type, double dx,
+                               const std::array<bool, 26>& /*is_direction_empty*/, std::array<double, 3> xbase,
+                               std::vector<Expansion>& L, std::vector<SpaceVector>& L_c, bool use_root_stencil,
+                               int precision = OTFMM_FP64) {
+    Staging& st = thread_staging();
+    stage_multipole_input(M_ptr, com_ptr[0]->data(), neighbors, dx, xbase, use_root_stencil, st);
+    const int rc = otfmm_m2l_soa_host(ctx, use_root_stencil ? nullptr : st.mon.data(), st.M.data(), st.com.data(),
+                                      st.L.data(), st.Lc.data(), type, use_root_stencil ? 1 : 0, precision);
+    if (rc != OTFMM_OK) return rc;
+    for (int c = 0; c < 20; ++c)
+        for (int u = 0; u < NCELL; ++u) L[u][c] += st.L[c * CLU + u];
+    if (type == OTFMM_RHO)
+        for (int c = 0; c < 3; ++c)
+            for (int u = 0; u < NCELL; ++u) L_c[u][c] = st.Lc[c * CLU + u];
+    return OTFMM_OK;
+}
+
+template <class Multipole, class SpaceVector, class Neighbor, class Expansion>
+void multipole_kernel_interface_or_abort(otfmm_context* ctx, const std::vector<double>& monopoles,
+                                         const std::vector<Multipole>& M_ptr,
+                                         const std::vector<std::shared_ptr<std::vector<SpaceVector>>>& com_ptr,
+                                         const std::vector<Neighbor>& neighbors, int type, double dx,
+                                         const std::array<bool, 26>& empty, std::array<double, 3> xbase,
+                                         std::vector<Expansion>& L, std::vector<SpaceVector>& L_c,
+                                         bool use_root_stencil, int precision = OTFMM_FP64) {
+    const int rc = multipole_kernel_interface(ctx, monopoles, M_ptr, com_ptr, neighbors, type, dx, empty, xbase, L,
+                                              L_c, use_root_stencil, precision);
+    if (rc != OTFMM_OK) {
+        std::cerr << "otfmm multipole kernel failed (" << rc << "): " << otfmm_last_error() << std::endl;
+        std::abort();
+    }
+}
+
+// monopole_kernel_interface(monopoles, com_ptr, neighbors, type, dx,
+// is_direction_empty, grid, contains_multipole_neighbor): L[0..3] += P2P (+ P2M),
+// L_c = P2M correction when a neighbour is refined (RHO). Device staging is
+// allocated once per thread.
+template <class SpaceVector, class Neighbor, class Expansion>
+int monopole_kernel_interface(otfmm_context* ctx, const std::vector<double>& monopoles,
+                              const std::vector<std::shared_ptr<std::vector<SpaceVector>>>& com_ptr,
+                              const std::vector<Neighbor>& neighbors, int type, double dx,
+                              const std::array<bool, 26>& /*is_direction_empty*/, std::vector<Expansion>& L,
+                              std::vector<SpaceVector>& L_c, bool contains_multipole_neighbor,
+                              int precision = OTFMM_FP64) {
+    struct Dev {
+        double* buf = nullptr;
+        ~Dev() { if (buf) otfmm_device_free(buf); }
+    };
+    thread_local Dev dev;
+    constexpr size_t n_mon = ENTRIES, n_L4 = 4 * CLU, n_Lc = 3 * CLU, n_icom = 3 * CLU, n_nM = 20 * 419,
+                     n_ncom = 3 * 419;
+    constexpr size_t total = n_mon + n_L4 + n_Lc + n_icom + n_nM + n_ncom;
+    if (!dev.buf) {
+        const int rc = otfmm_device_alloc(ctx, total * sizeof(double), reinterpret_cast<void**>(&dev.buf));
+        if (rc != OTFMM_OK) return rc;
+    }
+    double* d_mon = dev.buf;
+    double* d_L4 = d_mon + n_mon;
+    double* d_Lc = d_L4 + n_L4;
+    double* d_icom = d_Lc + n_Lc;
+    double* d_nM = d_icom + n_icom;
+    double* d_ncom = d_nM + n_nM;
+    // monopole update_input: own masses, leaf neighbours' masses, zeros else
+    std::vector<double> mon(ENTRIES, 0.0);
+    for (int x = 0; x < INX; ++x)
+        for (int y = 0; y < INX; ++y)
+            for (int z = 0; z < INX; ++z) mon[flat_padded(x + INX, y + INX, z + INX)] = monopoles[flat_inner(x, y, z)];
+    for (int d = 0; d < 26; ++d) {
+        const Neighbor& nb = neighbors[d];
+        if (!nb.is_monopole || !nb.data.m) continue;
+        int o[3], s[3], e[3], p[3];
+        dir_offsets(d, o);
+        padding_range(o, s, e, p);
+        for (int x = s[0]; x < e[0]; ++x)
+            for (int y = s[1]; y < e[1]; ++y)
+                for (int z = s[2]; z < e[2]; ++z)
+                    mon[flat_padded(x + p[0], y + p[1], z + p[2])] = (*nb.data.m)[flat_inner(x, y, z)];
+    }
+    int rc = otfmm_copy_to_device(ctx, d_mon, mon.data(), sizeof(double) * ENTRIES);
+    if (rc == OTFMM_OK) rc = otfmm_p2p_soa(ctx, d_mon, dx, d_L4, precision == OTFMM_FP64_EXACT ? OTFMM_FP64_EXACT : OTFMM_FP64, nullptr);
+    if (rc != OTFMM_OK) return rc;
+    bool any_p2m = false;
+    if (contains_multipole_neighbor) {
+        std::vector<double> icom(3 * CLU, 0.0), nM(20 * 419, 0.0), ncom(3 * 419, 0.0);
+        const SpaceVector* com0 = com_ptr[0]->data();
+        for (int c = 0; c < 3; ++c)
+            for (int u = 0; u < NCELL; ++u) icom[c * CLU + u] = com0[u][c];
+        rc = otfmm_copy_to_device(ctx, d_icom, icom.data(), sizeof(double) * 3 * CLU);
+        if (rc != OTFMM_OK) return rc;
+        for (int d = 0; d < 26; ++d) {
+            const Neighbor& nb = neighbors[d];
+            if (nb.is_monopole || !nb.data.M) continue;
+            // update_neighbor_input: the refined neighbour's slab, own SoA stride
+            int o[3], s[3], e[3], sz[3];
+            dir_offsets(d, o);
+            for (int a = 0; a < 3; ++a) {
+                s[a] = (o[a] == -1) ? INX - SMAX : 0;
+                e[a] = (o[a] == 1) ? SMAX : INX;
+                sz[a] = e[a] - s[a];
+            }
+            const int stride = sz[0] * sz[1] * sz[2] + 19;
+            for (int x = s[0]; x < e[0]; ++x)
+                for (int y = s[1]; y < e[1]; ++y)
+                    for (int z = s[2]; z < e[2]; ++z) {
+                        const int f = (x - s[0]) * (sz[1] * sz[2]) + (y - s[1]) * sz[2] + (z - s[2]);
+                        const int u = flat_inner(x, y, z);
+                        for (int c = 0; c < 20; ++c) nM[c * stride + f] = (*nb.data.M)[u][c];
+                        for (int c = 0; c < 3; ++c) ncom[c * stride + f] = (*nb.data.x)[u][c];
+                    }
+            rc = otfmm_copy_to_device(ctx, d_nM, nM.data(), sizeof(double) * 20 * stride);
+            if (rc == OTFMM_OK) rc = otfmm_copy_to_device(ctx, d_ncom, ncom.data(), sizeof(double) * 3 * stride);
+            if (rc == OTFMM_OK)
+                rc = otfmm_p2m_soa(ctx, d, d_nM, d_ncom, d_icom, d_L4, d_Lc, type, any_p2m ? 0 : 1,
+                                   precision == OTFMM_FP64_EXACT ? OTFMM_FP64_EXACT : OTFMM_FP64, nullptr);
+            if (rc != OTFMM_OK) return rc;
+            any_p2m = true;
+        }
+    }
+    Staging& st = thread_staging();
+    rc = otfmm_copy_to_host(ctx, st.L.data(), d_L4, sizeof(double) * 4 * CLU);
+    if (rc == OTFMM_OK && any_p2m && type == OTFMM_RHO) rc = otfmm_copy_to_host(ctx, st.Lc.data(), d_Lc, sizeof(double) * 3 * CLU);
+    if (rc != OTFMM_OK) return rc;
+    for (int c = 0; c < 4; ++c)
+        for (int u = 0; u < NCELL; ++u) L[u][c] += st.L[c * CLU + u];
+    if (any_p2m && type == OTFMM_RHO)
+        for (int c = 0; c < 3; ++c)
+            for (int u = 0; u < NCELL; ++u) L_c[u][c] = st.Lc[c * CLU + u];
+    return OTFMM_OK;
+}
+
+}   // namespace otfmm_octotiger

@@ -517,6 +517,17 @@ __device__ void root_tile(const double* sm, int x0, const Tables& t, OutPtr out)
 }
 
 // ---------------------------------------------------------------- kernels
+// Device-side work lists, filled by classify_kernel: item indices per kind
+// and the counters the persistent launches take their tiles from.
+enum : int { WL_M2L = 0, WL_LEAF = 1, WL_P2M = 2, WL_M2L_NEXT = 3, WL_P2M_NEXT = 4, WL_ROOT = 5, WL_COUNTERS = 8 };
+struct WorkLists {
+    int* m2l;      // refined, non-root items
+    int* root;     // level-0 items
+    int* leaf;     // leaf items
+    int* p2m;      // leaf items with a refined neighbour
+    int* counts;   // WL_* counters
+};
+
 struct BatchArgs {
     const double* M;
     const double* com;
@@ -529,73 +540,100 @@ struct BatchArgs {
     double* Lc;
     Tables t;
     int* err;
+    WorkLists wl;
 };
 
-// Reads and validates one work item into shared memory (thread 0); returns
-// false for the whole CTA if the item is malformed (flag raised, nothing
-// accessed with its fields).
-__device__ bool load_item(const BatchArgs& a, int item_idx, ItemInfo& it, int& bad) {
+__device__ __forceinline__ bool item_valid(const BatchArgs& a, const otfmm_work_item& w) {
+    bool b = (w.subgrid < 0 || w.subgrid >= a.n_sub || w.kind < 0 || w.kind > 2 || !(w.dx > 0.0));
+    for (int d = 0; d < 26; ++d) b |= (w.neighbors[d] < -1 || w.neighbors[d] >= a.n_sub);
+    if (!b && w.kind != OTFMM_KIND_M2L_ROOT) b |= (a.is_leaf[w.subgrid] != 0) != (w.kind == OTFMM_KIND_LEAF);
+    return !b;
+}
+
+// One thread per work item: validates it (a malformed item raises the error
+// flag and is dropped before anything reads with its fields) and appends it
+// to the list of its kind.
+__global__ void classify_kernel(BatchArgs a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n_items) return;
+    const otfmm_work_item& w = a.items[i];
+    if (!item_valid(a, w)) {
+        atomicOr(a.err, 1);
+        return;
+    }
+    if (w.kind == OTFMM_KIND_M2L) {
+        a.wl.m2l[atomicAdd(a.wl.counts + WL_M2L, 1)] = i;
+    } else if (w.kind == OTFMM_KIND_M2L_ROOT) {
+        a.wl.root[atomicAdd(a.wl.counts + WL_ROOT, 1)] = i;
+    } else {
+        a.wl.leaf[atomicAdd(a.wl.counts + WL_LEAF, 1)] = i;
+        bool refined_nb = false;
+        for (int d = 0; d < 26; ++d) refined_nb |= (w.neighbors[d] >= 0 && !a.is_leaf[w.neighbors[d]]);
+        if (refined_nb) a.wl.p2m[atomicAdd(a.wl.counts + WL_P2M, 1)] = i;
+    }
+}
+
+// Copies an item (already validated by classify_kernel) into shared memory.
+__device__ __forceinline__ void load_item(const BatchArgs& a, int item_idx, ItemInfo& it) {
     if (threadIdx.x == 0) {
         const otfmm_work_item& w = a.items[item_idx];
         it.subgrid = w.subgrid;
         it.kind = w.kind;
         it.dx = w.dx;
         for (int q = 0; q < 3; ++q) it.xbase[q] = w.xbase[q];
-        int b = (w.subgrid < 0 || w.subgrid >= a.n_sub || w.kind < 0 || w.kind > 2 || !(w.dx > 0.0));
-        for (int d = 0; d < 26; ++d) {
-            it.nb[d] = w.neighbors[d];
-            b |= (w.neighbors[d] < -1 || w.neighbors[d] >= a.n_sub);
-        }
-        if (!b && w.kind != OTFMM_KIND_M2L_ROOT) b |= (a.is_leaf[w.subgrid] != 0) != (w.kind == OTFMM_KIND_LEAF);
-        bad = b;
-        if (b) atomicOr(a.err, 1);
+        for (int d = 0; d < 26; ++d) it.nb[d] = w.neighbors[d];
     }
     __syncthreads();
-    return !bad;
 }
 
-// Refined (multipole) items: M2L tiles, two CTAs per item. Leaf items are
-// left to the P2P / P2M kernels.
+// Multipole tiles (two per refined item), persistent: one CTA per SM takes
+// tiles from an atomic counter, root tiles (longest) first.
 template <int PREC, bool RHO>
 __global__ void __launch_bounds__(THREADS, 1) m2l_batch_kernel(BatchArgs a) {
     extern __shared__ double sm[];
     __shared__ ItemInfo it;
-    __shared__ int bad;
-    const int item_idx = blockIdx.x >> 1;
-    const int half = blockIdx.x & 1;
-    if (a.items[item_idx].kind == OTFMM_KIND_LEAF) return;   // uniform per CTA
-    if (!load_item(a, item_idx, it, bad)) return;
-    const int x0 = TILE_X * half;
-    const size_t sub = (size_t)it.subgrid;
-    OutPtr out{a.L + sub * 20 * NCELL, a.Lc + sub * 3 * NCELL, NCELL, true};
+    __shared__ int tile;
+    const int nroot = a.wl.counts[WL_ROOT], nm2l = a.wl.counts[WL_M2L];
+    const int total = 2 * (nroot + nm2l);
     // the split form covers the multipole tiles; the root tile uses fast FP64
     constexpr int P64 = (PREC == PREC_SPLIT) ? PREC_FAST : PREC;
-    if (it.kind == OTFMM_KIND_M2L_ROOT) {
-        const int base_sub = it.subgrid;
-        for (int r = threadIdx.x; r < NCELL; r += blockDim.x)
-            for (int q = 0; q < NCOMP; ++q)
-                sm[q * NCELL + r] = (q < 20) ? a.M[((size_t)base_sub * 20 + q) * NCELL + r] * stage_scale<P64>(q)
-                                             : a.com[((size_t)base_sub * 3 + (q - 20)) * NCELL + r];
+    for (;;) {
+        if (threadIdx.x == 0) tile = atomicAdd(a.wl.counts + WL_M2L_NEXT, 1);
         __syncthreads();
-        root_tile<P64, RHO>(sm, x0, a.t, out);
-        return;
+        const int t = tile;
+        if (t >= total) break;
+        const int item_idx = (t < 2 * nroot) ? a.wl.root[t >> 1] : a.wl.m2l[(t - 2 * nroot) >> 1];
+        load_item(a, item_idx, it);
+        const int x0 = TILE_X * (t & 1);
+        const size_t sub = (size_t)it.subgrid;
+        OutPtr out{a.L + sub * 20 * NCELL, a.Lc + sub * 3 * NCELL, NCELL, true};
+        if (it.kind == OTFMM_KIND_M2L_ROOT) {
+            for (int r = threadIdx.x; r < NCELL; r += blockDim.x)
+                for (int q = 0; q < NCOMP; ++q)
+                    sm[q * NCELL + r] = (q < 20) ? a.M[(sub * 20 + q) * NCELL + r] * stage_scale<P64>(q)
+                                                 : a.com[(sub * 3 + (q - 20)) * NCELL + r];
+            __syncthreads();
+            root_tile<P64, RHO>(sm, x0, a.t, out);
+        } else {
+            // leaf neighbours, indexed by raw direction (monopole-only offsets)
+            uint32_t monomask = 0;
+            for (int d = 0; d < 26; ++d) {
+                const int nb = it.nb[d];
+                if (nb >= 0 && a.is_leaf[nb]) monomask |= 1u << (d < 13 ? d : d + 1);
+            }
+            if (PREC == PREC_SPLIT) {
+                const double inv_dx = 1.0 / it.dx;
+                stage_region_split(sm, it, x0, inv_dx, a.M, a.com, a.mon, a.is_leaf);
+                __syncthreads();
+                m2l_tile_split<RHO>(sm, x0, a.t, monomask, inv_dx, out);
+            } else {
+                stage_region_pool<P64>(sm, it, x0, false, a.M, a.com, a.mon, a.is_leaf);
+                __syncthreads();
+                m2l_tile<P64, RHO>(sm, x0, a.t, monomask, nullptr, out);
+            }
+        }
+        __syncthreads();   // shared memory and `it` are reused by the next tile
     }
-    // leaf neighbours, indexed by raw direction (monopole-only offsets)
-    uint32_t monomask = 0;
-    for (int d = 0; d < 26; ++d) {
-        const int nb = it.nb[d];
-        if (nb >= 0 && a.is_leaf[nb]) monomask |= 1u << (d < 13 ? d : d + 1);
-    }
-    if (PREC == PREC_SPLIT) {
-        const double inv_dx = 1.0 / it.dx;
-        stage_region_split(sm, it, x0, inv_dx, a.M, a.com, a.mon, a.is_leaf);
-        __syncthreads();
-        m2l_tile_split<RHO>(sm, x0, a.t, monomask, inv_dx, out);
-        return;
-    }
-    stage_region_pool<P64>(sm, it, x0, false, a.M, a.com, a.mon, a.is_leaf);
-    __syncthreads();
-    m2l_tile<P64, RHO>(sm, x0, a.t, monomask, nullptr, out);
 }
 
 // Leaf items: P2P (p2p_kernel_impl, monopole kokkos_kernel.hpp:143-320) over
@@ -605,19 +643,19 @@ __global__ void __launch_bounds__(THREADS, 1) m2l_batch_kernel(BatchArgs a) {
 // sweep has no branch. Writes L0..L3, zeroes L4..L19 and L_c (the P2M kernel
 // adds the refined-neighbour part afterwards).
 // Persistent: each CTA stages the per-parity offset/constant table once and
-// then walks the work list with a grid stride (every leaf costs the same).
+// then walks the leaf list with a grid stride (every leaf costs the same).
 constexpr int P2P_CTAS_PER_SM = 2;
+constexpr int P2P_THREADS = 256;   // 8 warps: one per parity class, two cells per thread
 constexpr int P2P_TABLE_BYTES = 8 * MAX_ENTRIES * (4 * 8 + 4);
 constexpr int P2P_SMEM_BYTES = P_SMEM_DOUBLES * 8 + P2P_TABLE_BYTES;
 
 template <int PREC>
-__global__ void __launch_bounds__(P_THREADS, P2P_CTAS_PER_SM) p2p_batch_kernel(BatchArgs a) {
+__global__ void __launch_bounds__(P2P_THREADS, P2P_CTAS_PER_SM) p2p_batch_kernel(BatchArgs a) {
     extern __shared__ double dyn[];
-    double* pm = dyn;                                                  // mass region
+    double* pm = dyn;                                                      // mass region
     double4* s_four = reinterpret_cast<double4*>(dyn + P_SMEM_DOUBLES);   // [8][MAX_ENTRIES]
-    int* s_delta = reinterpret_cast<int*>(s_four + 8 * MAX_ENTRIES);      // [8][MAX_ENTRIES]
+    int* s_delta = reinterpret_cast<int*>(s_four + 8 * MAX_ENTRIES);       // [8][MAX_ENTRIES]
     __shared__ ItemInfo it;
-    __shared__ int bad;
     for (int e = threadIdx.x; e < 8 * MAX_ENTRIES; e += blockDim.x) {
         const int p = e / MAX_ENTRIES, k = e % MAX_ENTRIES;
         if (k < a.t.count[p]) {
@@ -626,19 +664,23 @@ __global__ void __launch_bounds__(P_THREADS, P2P_CTAS_PER_SM) p2p_batch_kernel(B
             s_four[e] = make_double4(c_four[en.y][0], c_four[en.y][1], c_four[en.y][2], c_four[en.y][3]);
         }
     }
-    // thread -> cell: warp w covers parity class w/2, x' block w%2
+    // thread -> two cells: warp w owns parity class w (64 cells); lane covers
+    // sub-lattice x' = i and i + 2 at (j, k), so each table read serves two pairs
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int p = w >> 1;
-    const int i = 2 * (w & 1) + (lane >> 4), j = (lane >> 2) & 3, k = lane & 3;
-    const int cx = ((p >> 2) & 1) + 2 * i, cy = ((p >> 1) & 1) + 2 * j, cz = (p & 1) + 2 * k;
+    const int p = w;
+    const int i = lane >> 4, j = (lane >> 2) & 3, k = lane & 3;
+    const int px = (p >> 2) & 1, py = (p >> 1) & 1, pz = p & 1;
+    const int cy = py + 2 * j, cz = pz + 2 * k;
+    const int cxa = px + 2 * i, cxb = px + 2 * (i + 2);
     const int lane_off = i * P_XS + j * P_RS + k;
+    constexpr int OFF_B = 2 * P_XS;   // second cell: two sub-lattice planes further in x
     const int n = a.t.count[p];
     const double4* four = s_four + p * MAX_ENTRIES;
     const int* delta = s_delta + p * MAX_ENTRIES;
-    for (int item = blockIdx.x; item < a.n_items; item += gridDim.x) {
-        if (a.items[item].kind != OTFMM_KIND_LEAF) continue;   // uniform per CTA
-        __syncthreads();   // previous item's readers are done with pm / it
-        if (!load_item(a, item, it, bad)) continue;
+    const int nleaf = a.wl.counts[WL_LEAF];
+    for (int kk = blockIdx.x; kk < nleaf; kk += gridDim.x) {
+        __syncthreads();   // previous leaf's readers are done with pm / it
+        load_item(a, a.wl.leaf[kk], it);
         const double dc0 = __ddiv_rn(1.0, it.dx), dc1 = __ddiv_rn(-1.0, it.dx);
         for (int r = threadIdx.x; r < P_REG * P_REG * P_REG; r += blockDim.x) {
             const int ax = r / (P_REG * P_REG) - 2, ay = (r / P_REG) % P_REG - 2, az = r % P_REG - 2;
@@ -652,110 +694,128 @@ __global__ void __launch_bounds__(P_THREADS, P2P_CTAS_PER_SM) p2p_batch_kernel(B
             pm[cls * P_CLS + ((ax + 2) >> 1) * P_XS + ((ay + 2) >> 1) * P_RS + ((az + 2) >> 1)] = m;
         }
         __syncthreads();
-        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        double ga[4] = {0.0, 0.0, 0.0, 0.0}, gb[4] = {0.0, 0.0, 0.0, 0.0};
         if (PREC == PREC_EXACT) {
             for (int e = 0; e < n; ++e) {
                 const double4 f = four[e];
-                const double ms = __dmul_rn(pm[delta[e] + lane_off], dc0);
-                acc[0] = __dadd_rn(acc[0], __dmul_rn(f.x, ms));
-                acc[1] = __dadd_rn(acc[1], __dmul_rn(__dmul_rn(f.y, ms), dc1));
-                acc[2] = __dadd_rn(acc[2], __dmul_rn(__dmul_rn(f.z, ms), dc1));
-                acc[3] = __dadd_rn(acc[3], __dmul_rn(__dmul_rn(f.w, ms), dc1));
+                const int d = delta[e] + lane_off;
+                const double ma = __dmul_rn(pm[d], dc0), mb = __dmul_rn(pm[d + OFF_B], dc0);
+                ga[0] = __dadd_rn(ga[0], __dmul_rn(f.x, ma));
+                ga[1] = __dadd_rn(ga[1], __dmul_rn(__dmul_rn(f.y, ma), dc1));
+                ga[2] = __dadd_rn(ga[2], __dmul_rn(__dmul_rn(f.z, ma), dc1));
+                ga[3] = __dadd_rn(ga[3], __dmul_rn(__dmul_rn(f.w, ma), dc1));
+                gb[0] = __dadd_rn(gb[0], __dmul_rn(f.x, mb));
+                gb[1] = __dadd_rn(gb[1], __dmul_rn(__dmul_rn(f.y, mb), dc1));
+                gb[2] = __dadd_rn(gb[2], __dmul_rn(__dmul_rn(f.z, mb), dc1));
+                gb[3] = __dadd_rn(gb[3], __dmul_rn(__dmul_rn(f.w, mb), dc1));
             }
         } else {
 #pragma unroll 4
             for (int e = 0; e < n; ++e) {
                 const double4 f = four[e];
-                const double ms = pm[delta[e] + lane_off];
-                acc[0] = fma(f.x, ms, acc[0]);
-                acc[1] = fma(f.y, ms, acc[1]);
-                acc[2] = fma(f.z, ms, acc[2]);
-                acc[3] = fma(f.w, ms, acc[3]);
+                const int d = delta[e] + lane_off;
+                const double ma = pm[d], mb = pm[d + OFF_B];
+                ga[0] = fma(f.x, ma, ga[0]);
+                ga[1] = fma(f.y, ma, ga[1]);
+                ga[2] = fma(f.z, ma, ga[2]);
+                ga[3] = fma(f.w, ma, ga[3]);
+                gb[0] = fma(f.x, mb, gb[0]);
+                gb[1] = fma(f.y, mb, gb[1]);
+                gb[2] = fma(f.z, mb, gb[2]);
+                gb[3] = fma(f.w, mb, gb[3]);
             }
 #pragma unroll
-            for (int q = 1; q < 4; ++q) acc[q] *= dc1;
+            for (int q = 1; q < 4; ++q) {
+                ga[q] *= dc1;
+                gb[q] *= dc1;
+            }
         }
-        const int cf = cx * 64 + cy * 8 + cz;
         double* L = a.L + (size_t)it.subgrid * 20 * NCELL;
         double* Lc = a.Lc + (size_t)it.subgrid * 3 * NCELL;
+        const int cfa = cxa * 64 + cy * 8 + cz, cfb = cxb * 64 + cy * 8 + cz;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) L[q * NCELL + cf] = acc[q];
+        for (int q = 0; q < 4; ++q) {
+            L[q * NCELL + cfa] = ga[q];
+            L[q * NCELL + cfb] = gb[q];
+        }
 #pragma unroll
-        for (int q = 4; q < 20; ++q) L[q * NCELL + cf] = 0.0;
+        for (int q = 4; q < 20; ++q) {
+            L[q * NCELL + cfa] = 0.0;
+            L[q * NCELL + cfb] = 0.0;
+        }
 #pragma unroll
-        for (int q = 0; q < 3; ++q) Lc[q * NCELL + cf] = 0.0;
+        for (int q = 0; q < 3; ++q) {
+            Lc[q * NCELL + cfa] = 0.0;
+            Lc[q * NCELL + cfb] = 0.0;
+        }
     }
 }
 
 // Leaf items with refined neighbours: P2M (p2m_kernel_impl_rho / _non_rho,
-// monopole kokkos_kernel.hpp:517-942) after P2P, one refined direction after
-// the other in direction order, partners in stencil order, partner moments
-// read from the pool. Adds to L0..L3, writes L_c.
+// monopole kokkos_kernel.hpp:517-942) after P2P: one CTA per leaf of the P2M
+// work list (grid stride), one thread per cell, partner moments read through
+// L2. The exact form goes direction after direction in direction order, like
+// the reference's one launch per refined neighbour; the fast form takes all
+// refined directions in one stencil pass.
 template <int PREC, bool RHO>
 __global__ void __launch_bounds__(P_THREADS) p2m_batch_kernel(BatchArgs a) {
     __shared__ ItemInfo it;
-    __shared__ int bad;
-    if (a.items[blockIdx.x].kind != OTFMM_KIND_LEAF) return;
-    if (!load_item(a, blockIdx.x, it, bad)) return;
-    uint32_t refmask = 0;
-    for (int d = 0; d < 26; ++d) {
-        const int nb = it.nb[d];
-        if (nb >= 0 && !a.is_leaf[nb]) refmask |= 1u << (d < 13 ? d : d + 1);
-    }
-    if (!refmask) return;
+    constexpr int P64 = (PREC == PREC_EXACT) ? PREC_EXACT : PREC_FAST;
     const int cu = threadIdx.x;
     const int cx = cu >> 6, cy = (cu >> 3) & 7, cz = cu & 7;
     const int p = ((cx & 1) << 2) | ((cy & 1) << 1) | (cz & 1);
-    const size_t sub = (size_t)it.subgrid;
-    double* L = a.L + sub * 20 * NCELL;
-    double* Lc = a.Lc + sub * 3 * NCELL;
-    double X[3], acc[4], corr[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-    for (int q = 0; q < 3; ++q) X[q] = a.com[(sub * 3 + q) * NCELL + cu];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) acc[q] = L[q * NCELL + cu];
     const int n = a.t.count[p];
     const int2* ent = a.t.entries + p * MAX_ENTRIES;
-    if (PREC == PREC_EXACT) {
-        // direction after direction, like the reference's one launch per neighbour
-        for (int raw = 0; raw < 27; ++raw) {
-            if (!((refmask >> raw) & 1u)) continue;
-            const int nb = it.nb[raw < 13 ? raw : raw - 1];
+    const int np2m = a.wl.counts[WL_P2M];
+    for (int kk = blockIdx.x; kk < np2m; kk += gridDim.x) {
+        __syncthreads();   // `it` is reused
+        load_item(a, a.wl.p2m[kk], it);
+        uint32_t refmask = 0;
+        for (int d = 0; d < 26; ++d) {
+            const int nb = it.nb[d];
+            if (nb >= 0 && !a.is_leaf[nb]) refmask |= 1u << (d < 13 ? d : d + 1);
+        }
+        const size_t sub = (size_t)it.subgrid;
+        double* L = a.L + sub * 20 * NCELL;
+        double* Lc = a.Lc + sub * 3 * NCELL;
+        double X[3], acc[4], corr[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int q = 0; q < 3; ++q) X[q] = a.com[(sub * 3 + q) * NCELL + cu];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[q] = L[q * NCELL + cu];
+        for (int raw_sel = (P64 == PREC_EXACT ? 0 : 27); raw_sel < 28; ++raw_sel) {
+            uint32_t want;   // refined directions served in this sweep
+            if (P64 == PREC_EXACT) {
+                if (raw_sel == 27) break;
+                if (!((refmask >> raw_sel) & 1u)) continue;
+                want = 1u << raw_sel;
+            } else {
+                want = refmask;
+            }
             for (int e = 0; e < n; ++e) {
                 const int y = __ldg(&ent[e].y);
                 const int ax = cx + entry_sx(y), ay = cy + entry_sy(y), az = cz + entry_sz(y);
-                if (raw_dir(ax, ay, az) != raw) continue;
+                const int raw = raw_dir(ax, ay, az);
+                if (!((want >> raw) & 1u)) continue;
+                const size_t nb = (size_t)it.nb[raw < 13 ? raw : raw - 1];
                 const int u = (ax & 7) * 64 + (ay & 7) * 8 + (az & 7);
                 double Y[3], mp[20];
 #pragma unroll
-                for (int q = 0; q < 3; ++q) Y[q] = __ldg(a.com + ((size_t)nb * 3 + q) * NCELL + u);
+                for (int q = 0; q < 3; ++q) Y[q] = __ldg(a.com + (nb * 3 + q) * NCELL + u);
 #pragma unroll
-                for (int q = 0; q < 20; ++q) mp[q] = __ldg(a.M + ((size_t)nb * 20 + q) * NCELL + u);
-                exact_p2m_pair<RHO>(X, Y, mp, acc, corr);
+                for (int q = 0; q < 20; ++q) mp[q] = __ldg(a.M + (nb * 20 + q) * NCELL + u) * stage_scale<P64>(q);
+                if (P64 == PREC_EXACT)
+                    exact_p2m_pair<RHO>(X, Y, mp, acc, corr);
+                else
+                    fast_p2m_pair<RHO>(X, Y, mp, acc, corr);
             }
         }
-    } else {
-        // one pass: partners in any refined neighbour
-        for (int e = 0; e < n; ++e) {
-            const int y = __ldg(&ent[e].y);
-            const int ax = cx + entry_sx(y), ay = cy + entry_sy(y), az = cz + entry_sz(y);
-            const int raw = raw_dir(ax, ay, az);
-            if (!((refmask >> raw) & 1u)) continue;
-            const int nb = it.nb[raw < 13 ? raw : raw - 1];
-            const int u = (ax & 7) * 64 + (ay & 7) * 8 + (az & 7);
-            double Y[3], mp[20];
 #pragma unroll
-            for (int q = 0; q < 3; ++q) Y[q] = __ldg(a.com + ((size_t)nb * 3 + q) * NCELL + u);
+        for (int q = 0; q < 4; ++q) L[q * NCELL + cu] = acc[q];
+        if (RHO) {
 #pragma unroll
-            for (int q = 0; q < 20; ++q) mp[q] = __ldg(a.M + ((size_t)nb * 20 + q) * NCELL + u) * stage_scale<PREC_FAST>(q);
-            fast_p2m_pair<RHO>(X, Y, mp, acc, corr);
+            for (int q = 0; q < 3; ++q) Lc[q * NCELL + cu] = corr[q];
         }
-    }
-#pragma unroll
-    for (int q = 0; q < 4; ++q) L[q * NCELL + cu] = acc[q];
-    if (RHO) {
-#pragma unroll
-        for (int q = 0; q < 3; ++q) Lc[q * NCELL + cu] = corr[q];
     }
 }
 
@@ -1032,6 +1092,8 @@ struct otfmm_context {
     uint8_t* d_phase = nullptr;
     int* d_err = nullptr;
     double* d_soa_scratch = nullptr;   // host-buffer path staging
+    int* d_lists = nullptr;            // batched work lists (grown on demand)
+    int list_capacity = 0;
     std::mutex mu;
     Tables tables() const { return Tables{d_entries, d_count, d_entries_fast, d_count_far, d_entries_split, d_entries_p2p, d_four, d_phase}; }
 };
@@ -1210,6 +1272,7 @@ int otfmm_destroy(otfmm_context* ctx) {
     cudaFree(ctx->d_phase);
     cudaFree(ctx->d_err);
     cudaFree(ctx->d_soa_scratch);
+    cudaFree(ctx->d_lists);
     delete ctx;
     return OTFMM_OK;
 }
@@ -1381,36 +1444,52 @@ int otfmm_batch(otfmm_context* ctx, const double* pool_M, const double* pool_com
     if (n_items == 0) return OTFMM_OK;
     DeviceGuard g(ctx->device);
     cudaStream_t s = (cudaStream_t)stream;
+    {
+        // work-list storage: 4 lists of n_items + counters; grown (reallocated)
+        // only when a larger work list arrives, serialised per context
+        std::lock_guard<std::mutex> lock(ctx->mu);
+        if (n_items > ctx->list_capacity) {
+            OT_CUDA(cudaStreamSynchronize(s));
+            cudaFree(ctx->d_lists);
+            ctx->d_lists = nullptr;
+            const int cap = std::max(n_items, 2 * ctx->list_capacity);
+            OT_CUDA(cudaMalloc(&ctx->d_lists, sizeof(int) * (4 * (size_t)cap + WL_COUNTERS)));
+            ctx->list_capacity = cap;
+        }
+    }
+    const int cap = ctx->list_capacity;
+    WorkLists wl{ctx->d_lists, ctx->d_lists + cap, ctx->d_lists + 2 * (size_t)cap, ctx->d_lists + 3 * (size_t)cap,
+                 ctx->d_lists + 4 * (size_t)cap};
     OT_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), s));
+    OT_CUDA(cudaMemsetAsync(wl.counts, 0, sizeof(int) * WL_COUNTERS, s));
     BatchArgs a{pool_M, pool_com, pool_mon, pool_is_leaf, n_subgrids, items, n_items, L, L_c, ctx->tables(),
-                ctx->d_err};
+                ctx->d_err, wl};
     const size_t bytes = SMEM_DOUBLES * sizeof(double);
-    const dim3 grid(2 * n_items);
     const bool rho = (gsolve_type == OTFMM_RHO);
-    // multipole tiles, then P2P of the leaves, then P2M (stream order keeps
-    // the reference's P2P-then-P2M accumulation order)
-    const dim3 pgrid(n_items);
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
-    const dim3 p2p_grid(std::min(n_items, P2P_CTAS_PER_SM * sms));
+    // classify, then multipole tiles, P2P of the leaves and P2M (stream
+    // order keeps the reference's P2P-then-P2M accumulation order)
+    classify_kernel<<<(n_items + 255) / 256, 256, 0, s>>>(a);
+    const dim3 tiles_grid(sms), p2p_grid(P2P_CTAS_PER_SM * sms), p2m_grid(std::min(n_items, 8 * sms));
     if (precision == OTFMM_FP64_EXACT) {
-        if (rho) m2l_batch_kernel<PREC_EXACT, true><<<grid, THREADS, bytes, s>>>(a);
-        else m2l_batch_kernel<PREC_EXACT, false><<<grid, THREADS, bytes, s>>>(a);
-        p2p_batch_kernel<PREC_EXACT><<<p2p_grid, P_THREADS, P2P_SMEM_BYTES, s>>>(a);
-        if (rho) p2m_batch_kernel<PREC_EXACT, true><<<pgrid, P_THREADS, 0, s>>>(a);
-        else p2m_batch_kernel<PREC_EXACT, false><<<pgrid, P_THREADS, 0, s>>>(a);
+        if (rho) m2l_batch_kernel<PREC_EXACT, true><<<tiles_grid, THREADS, bytes, s>>>(a);
+        else m2l_batch_kernel<PREC_EXACT, false><<<tiles_grid, THREADS, bytes, s>>>(a);
+        p2p_batch_kernel<PREC_EXACT><<<p2p_grid, P2P_THREADS, P2P_SMEM_BYTES, s>>>(a);
+        if (rho) p2m_batch_kernel<PREC_EXACT, true><<<p2m_grid, P_THREADS, 0, s>>>(a);
+        else p2m_batch_kernel<PREC_EXACT, false><<<p2m_grid, P_THREADS, 0, s>>>(a);
     } else {
         if (precision == OTFMM_FP32_SPLIT) {
             const size_t sbytes = S_SMEM_DOUBLES * sizeof(double);
-            if (rho) m2l_batch_kernel<PREC_SPLIT, true><<<grid, THREADS, sbytes, s>>>(a);
-            else m2l_batch_kernel<PREC_SPLIT, false><<<grid, THREADS, sbytes, s>>>(a);
+            if (rho) m2l_batch_kernel<PREC_SPLIT, true><<<tiles_grid, THREADS, sbytes, s>>>(a);
+            else m2l_batch_kernel<PREC_SPLIT, false><<<tiles_grid, THREADS, sbytes, s>>>(a);
         } else {
-            if (rho) m2l_batch_kernel<PREC_FAST, true><<<grid, THREADS, bytes, s>>>(a);
-            else m2l_batch_kernel<PREC_FAST, false><<<grid, THREADS, bytes, s>>>(a);
+            if (rho) m2l_batch_kernel<PREC_FAST, true><<<tiles_grid, THREADS, bytes, s>>>(a);
+            else m2l_batch_kernel<PREC_FAST, false><<<tiles_grid, THREADS, bytes, s>>>(a);
         }
-        p2p_batch_kernel<PREC_FAST><<<p2p_grid, P_THREADS, P2P_SMEM_BYTES, s>>>(a);
-        if (rho) p2m_batch_kernel<PREC_FAST, true><<<pgrid, P_THREADS, 0, s>>>(a);
-        else p2m_batch_kernel<PREC_FAST, false><<<pgrid, P_THREADS, 0, s>>>(a);
+        p2p_batch_kernel<PREC_FAST><<<p2p_grid, P2P_THREADS, P2P_SMEM_BYTES, s>>>(a);
+        if (rho) p2m_batch_kernel<PREC_FAST, true><<<p2m_grid, P_THREADS, 0, s>>>(a);
+        else p2m_batch_kernel<PREC_FAST, false><<<p2m_grid, P_THREADS, 0, s>>>(a);
     }
     OT_CUDA(cudaGetLastError());
     return OTFMM_OK;
@@ -1487,6 +1566,32 @@ int otfmm_batch_status(otfmm_context* ctx, void* stream) {
     OT_CUDA(cudaMemcpyAsync(&h, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
     OT_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
     if (h) return fail(OTFMM_ERR_DEVICE, "a work item failed validation on the device");
+    return OTFMM_OK;
+}
+
+int otfmm_device_alloc(otfmm_context* ctx, size_t bytes, void** ptr) {
+    if (!ctx || !ptr) return fail(OTFMM_ERR_INVALID, "NULL argument");
+    DeviceGuard g(ctx->device);
+    OT_CUDA(cudaMalloc(ptr, bytes));
+    return OTFMM_OK;
+}
+
+int otfmm_device_free(void* ptr) {
+    OT_CUDA(cudaFree(ptr));
+    return OTFMM_OK;
+}
+
+int otfmm_copy_to_device(otfmm_context* ctx, void* dst, const void* src, size_t bytes) {
+    if (!ctx || !dst || !src) return fail(OTFMM_ERR_INVALID, "NULL argument");
+    DeviceGuard g(ctx->device);
+    OT_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice));
+    return OTFMM_OK;
+}
+
+int otfmm_copy_to_host(otfmm_context* ctx, void* dst, const void* src, size_t bytes) {
+    if (!ctx || !dst || !src) return fail(OTFMM_ERR_INVALID, "NULL argument");
+    DeviceGuard g(ctx->device);
+    OT_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost));
     return OTFMM_OK;
 }
 
