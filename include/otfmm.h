@@ -150,15 +150,20 @@ int otfmm_p2m_soa(otfmm_context* ctx, int d, const double* neighbor_M, const dou
 
 /* Batched solve: every work item of `items` (device array of n_items),
  * reading the resident pool (device pointers, n_subgrids records) and writing
- * per subgrid L[n][20][512] and L_c[n][3][512] (leaf items fill L[0..3] and
- * zero L[4..19]; L_c is zero for DRHODT and for leaves without a refined
- * neighbour). Enqueues three stream-ordered launches: the multipole tiles of
- * refined items, then P2P of leaf items, then P2M of leaves that have refined
- * neighbours (the reference's P2P-then-P2M order). Asynchronous; work items
- * are validated on the device and a bad item is reported by
- * otfmm_batch_status (its outputs are left unwritten). Every subgrid may
- * appear in at most one work item. Calls that overlap on the GPU must use
- * distinct output arrays. */
+ * per subgrid into L[n][20][512] and L_c[n][3][512]:
+ *   refined items: all 20 L components and the 3 L_c components (zeros for DRHODT);
+ *   leaf items:    L[0..3] (P2P + P2M), and L_c when a neighbour is refined.
+ * Everything else is left untouched: as node_server::compute_fmm does before
+ * the reference's kernels (src/node_server.cpp:701-705), the caller zeroes L
+ * and L_c once; later solves of work lists with the same kinds overwrite the
+ * same entries. Enqueues a classification kernel that builds device-side work
+ * lists, then persistent launches for the multipole tiles of refined items,
+ * P2P of the leaves and P2M of leaves with refined neighbours (the reference's
+ * P2P-then-P2M order). Work-list storage lives in the context and grows (a
+ * device allocation) when a larger work list arrives. Asynchronous; work items
+ * are validated on the device and a bad one is reported by otfmm_batch_status
+ * (its outputs are left unwritten). Every subgrid may appear in at most one
+ * work item. Calls that overlap on the GPU must use distinct contexts. */
 int otfmm_batch(otfmm_context* ctx, const double* pool_M, const double* pool_com, const double* pool_mon,
                 const uint8_t* pool_is_leaf, int32_t n_subgrids, const otfmm_work_item* items, int32_t n_items,
                 double* L, double* L_c, int gsolve_type, int precision, void* stream);

@@ -640,8 +640,9 @@ __global__ void __launch_bounds__(THREADS, 1) m2l_batch_kernel(BatchArgs a) {
 // the masses of the leaf and its leaf neighbours; refined and empty
 // neighbours are staged as zero mass (update_input,
 // monopole_interaction_interface.hpp:82-87), which adds exact zeros, so the
-// sweep has no branch. Writes L0..L3, zeroes L4..L19 and L_c (the P2M kernel
-// adds the refined-neighbour part afterwards).
+// sweep has no branch. Writes L0..L3 only, like the reference's monopole path
+// (L4..L19 and L_c of a leaf are left as the caller zeroed them; the P2M
+// kernel adds the refined-neighbour part afterwards).
 // Persistent: each CTA stages the per-parity offset/constant table once and
 // then walks the leaf list with a grid stride (every leaf costs the same).
 constexpr int P2P_CTAS_PER_SM = 2;
@@ -738,16 +739,7 @@ __global__ void __launch_bounds__(P2P_THREADS, P2P_CTAS_PER_SM) p2p_batch_kernel
             L[q * NCELL + cfa] = ga[q];
             L[q * NCELL + cfb] = gb[q];
         }
-#pragma unroll
-        for (int q = 4; q < 20; ++q) {
-            L[q * NCELL + cfa] = 0.0;
-            L[q * NCELL + cfb] = 0.0;
-        }
-#pragma unroll
-        for (int q = 0; q < 3; ++q) {
-            Lc[q * NCELL + cfa] = 0.0;
-            Lc[q * NCELL + cfb] = 0.0;
-        }
+        (void)Lc;   // L4..L19 and L_c of a leaf are not written here (see otfmm_batch)
     }
 }
 
@@ -812,10 +804,9 @@ __global__ void __launch_bounds__(P_THREADS) p2m_batch_kernel(BatchArgs a) {
         }
 #pragma unroll
         for (int q = 0; q < 4; ++q) L[q * NCELL + cu] = acc[q];
-        if (RHO) {
+        // L_c of a leaf with a refined neighbour: the P2M correction (zero for DRHODT)
 #pragma unroll
-            for (int q = 0; q < 3; ++q) Lc[q * NCELL + cu] = corr[q];
-        }
+        for (int q = 0; q < 3; ++q) Lc[q * NCELL + cu] = RHO ? corr[q] : 0.0;
     }
 }
 
