@@ -119,6 +119,8 @@ struct Tables {
     const int* count_far;       // [8] number of far offsets
     const int4* entries_split;  // far-first entries for the split layout: x = double delta, y = packed, z = float delta
     const int2* entries_p2p;    // stencil-order entries for the P2P layout: x = smem delta, y = stencil index
+    const int4* entries_ws;     // far-first entries for the warp-specialised split layout: x = float2 delta,
+                                // y = double2 delta, z = packed
     const double* four;      // [FULL][4] monopole constants
     const uint8_t* phase;    // [FULL] inner_stencil_masks (true outside the stencil)
 };
@@ -479,6 +481,292 @@ __device__ void m2l_tile_split(const double* sm, int x0, const Tables& t, uint32
     write_lc<RHO>(out, cf, corr);
 }
 
+// ------------------------------------------------ FP32 split, warp-specialised
+// RHO multipole tiles with 16 warps on one staged region. Warps 0-7
+// ("contraction warps") build each pair's derivative tensor in FP32 from the
+// FP64 centre-of-mass difference and contract it with the FP32 partner
+// moments, promoting FP32 partial sums to FP64 every CHUNK partners; warps
+// 8-15 ("correction warps") compute the angular-momentum correction L_c of
+// the same pairs entirely in FP64. Warp w serves the 32 target cells of
+// parity class w & 7 in either role, so the FP64 pipe (correction warps) and
+// the FP32 pipe (contraction warps) work side by side on every SM.
+// Shared memory per parity class (4 x 6 x 6 sub-lattice), rows of 6 z-cells:
+//   FP32 part: pairs (M0,M1) .. (M18,M19) as float2, [10 pairs][6 z] = 60 float2 per row;
+//   FP64 part: (Px,Py) (Pz,m0) (O0,O1) .. (O8,O9) as double2, [7][6 z] = 42 per row.
+// P = (centre of mass - xbase) / dx, moments in units of dx with the multinomial
+// factors folded in (exact rescaling for dx = 2^-k). Lane l of a warp serves
+// sub-lattice cell (i, j, k) = ((l >> 2) & 1, l >> 3, l & 3): a half-warp
+// (16 lanes: k, i, two j) reads float2 at offsets k + {0, 8, 12, 4} mod 16
+// (x stride 360, row stride 60), a quarter-warp (8 lanes: k, i) reads double2
+// at k + {0, 4} mod 8 (x stride 252): both without bank conflicts. The stencil
+// table follows the two parts: per parity class and entry, the float2 and
+// double2 partner deltas packed as 16 + 16 bits.
+constexpr int WS_THREADS = 512;
+constexpr int WA_ROW = 10 * SUB_YZ;            // 60 float2
+constexpr int WA_XS = SUB_YZ * WA_ROW;
+constexpr int WA_CLS = (REG_X / 2) * WA_XS;
+constexpr int WB_ROW = 7 * SUB_YZ;             // 42 double2
+constexpr int WB_XS = SUB_YZ * WB_ROW;
+constexpr int WB_CLS = (REG_X / 2) * WB_XS;
+constexpr int WS_A_BYTES = 8 * WA_CLS * 8;
+constexpr int WS_B_BYTES = 8 * WB_CLS * 16;
+constexpr int WS_TABLE_BYTES = 8 * MAX_ENTRIES * 4;
+constexpr int WS_SMEM_BYTES = WS_A_BYTES + WS_B_BYTES + WS_TABLE_BYTES;   // 92160 + 129024 + 6912 = 228096
+static_assert(WA_ROW % 16 == 12 && WA_XS % 16 == 8, "float2 half-warps (k, i, j pair) conflict-free");
+static_assert(WB_XS % 8 == 4, "double2 quarter-warps (k, i) conflict-free");
+static_assert(8 * WA_CLS < 65536 && 8 * WB_CLS < 65536, "deltas fit 16 bits");
+static_assert(WS_SMEM_BYTES + 256 <= 232448, "warp-specialised layout fits the 227 KB shared-memory limit");
+static_assert(ROOT_SMEM_DOUBLES * 8 <= WS_A_BYTES + WS_B_BYTES, "root staging leaves the stencil table intact");
+// Smallest squared distance (in dx^2) the FP32 derivative tensor accepts; it
+// keeps d3 ~ r^-7 finite in FP32. Cells of one grid have distinct centres of
+// mass at least ~0.2 dx apart; the FP64 forms clamp at 1e-20 like the reference.
+constexpr float WS_R2_MIN = 1.0e-6f;
+
+__device__ void stage_region_ws(float2* sa, double2* sb, const ItemInfo& it, int x0, double inv_dx,
+                                const double* __restrict__ M, const double* __restrict__ com,
+                                const double* __restrict__ mon, const uint8_t* __restrict__ is_leaf) {
+    const double inv2 = inv_dx * inv_dx, inv3 = inv2 * inv_dx;
+    for (int r = threadIdx.x; r < REG_CELLS; r += blockDim.x) {
+        const int rx = r / (REG_YZ * REG_YZ), ry = (r / REG_YZ) % REG_YZ, rz = r % REG_YZ;
+        const int ax = x0 - 2 + rx, ay = ry - 2, az = rz - 2;
+        const int raw = raw_dir(ax, ay, az);
+        const bool centre = (raw == 13);
+        const int src = centre ? it.subgrid : it.nb[raw < 13 ? raw : raw - 1];
+        const int u = (ax & 7) * 64 + (ay & 7) * 8 + (az & 7);
+        double m[20], P[3];
+        if (src < 0) {
+            // empty direction: zero moments at the cell's own centre (never at a
+            // target's centre of mass, so the pair stays finite)
+#pragma unroll
+            for (int q = 0; q < 20; ++q) m[q] = 0.0;
+            P[0] = ax;
+            P[1] = ay;
+            P[2] = az;
+        } else if (!centre && is_leaf[src]) {
+            m[0] = mon[(size_t)src * NCELL + u];
+#pragma unroll
+            for (int q = 1; q < 20; ++q) m[q] = 0.0;
+            // leaf cell centre i*dx + xbase - INX*dx (monopole_interaction_interface.hpp:221-234)
+            const int ip[3] = {ax + INX, ay + INX, az + INX};
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                const double c = __dsub_rn(__dadd_rn(__dmul_rn((double)ip[a], it.dx), it.xbase[a]),
+                                           __dmul_rn((double)INX, it.dx));
+                P[a] = (c - it.xbase[a]) * inv_dx;
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < 20; ++q) m[q] = M[((size_t)src * 20 + q) * NCELL + u];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) P[a] = (com[((size_t)src * 3 + a) * NCELL + u] - it.xbase[a]) * inv_dx;
+        }
+#pragma unroll
+        for (int q = 1; q < 4; ++q) m[q] *= inv_dx;
+#pragma unroll
+        for (int q = 4; q < 10; ++q) m[q] *= (factor_of(q) / 2.0) * inv2;
+#pragma unroll
+        for (int q = 10; q < 20; ++q) m[q] *= (factor_of(q) / 6.0) * inv3;
+        const int cls = ((ax & 1) << 2) | ((ay & 1) << 1) | (az & 1);
+        const int ua = cls * WA_CLS + (rx >> 1) * WA_XS + (ry >> 1) * WA_ROW + (rz >> 1);
+        const int ub = cls * WB_CLS + (rx >> 1) * WB_XS + (ry >> 1) * WB_ROW + (rz >> 1);
+#pragma unroll
+        for (int q = 0; q < 10; ++q) sa[ua + q * SUB_YZ] = make_float2((float)m[2 * q], (float)m[2 * q + 1]);
+        sb[ub] = make_double2(P[0], P[1]);
+        sb[ub + SUB_YZ] = make_double2(P[2], m[0]);
+#pragma unroll
+        for (int o = 0; o < 5; ++o) sb[ub + (2 + o) * SUB_YZ] = make_double2(m[10 + 2 * o], m[11 + 2 * o]);
+    }
+}
+
+// FP32 derivative tensor and contraction of one pair (dX in units of dx).
+// 1/r: hardware estimate plus one Newton step with an FMA residual
+// (within about one FP32 ulp).
+__device__ __forceinline__ void ws_contract_pair(const float dX[3], const float m[20], float acc[20]) {
+    const float r2 = fmaxf(fmaf(dX[0], dX[0], fmaf(dX[1], dX[1], dX[2] * dX[2])), WS_R2_MIN);
+    const float y0 = rsqrtf(r2);
+    const float h = fmaf(-r2 * y0, y0, 1.0f);
+    const float rs = fmaf(0.5f * y0, h, y0);
+    const float r2inv = rs * rs;
+    const float d1 = rs * r2inv;
+    const float d2 = -3.0f * d1 * r2inv;
+    const float d3 = -5.0f * d2 * r2inv;
+    float D[20];
+    d_tensor<float>(dX, -rs, d1, d2, d3, D);
+    fast_low_terms<float>(m, D, acc, false);
+    fast_high_terms<float>(m, D, acc);
+}
+
+// Partner with mass only (monopole-only entries, leaf-neighbour partners).
+__device__ __forceinline__ void ws_contract_mass(const float dX[3], float m0, float acc[20]) {
+    const float r2 = fmaxf(fmaf(dX[0], dX[0], fmaf(dX[1], dX[1], dX[2] * dX[2])), WS_R2_MIN);
+    const float y0 = rsqrtf(r2);
+    const float h = fmaf(-r2 * y0, y0, 1.0f);
+    const float rs = fmaf(0.5f * y0, h, y0);
+    const float r2inv = rs * rs;
+    const float d1 = rs * r2inv;
+    const float d2 = -3.0f * d1 * r2inv;
+    const float d3 = -5.0f * d2 * r2inv;
+    float D[20];
+    d_tensor<float>(dX, -rs, d1, d2, d3, D);
+#pragma unroll
+    for (int q = 0; q < 20; ++q) acc[q] = fmaf(m0, D[q], acc[q]);
+}
+
+// FP64 angular-momentum correction of one pair: g = O_p - O_c m_p / m_c
+// against the fourth-order slice (compute_kernel_templates.hpp:232-334).
+__device__ __forceinline__ void ws_correction_pair(const double dX[3], double m0p, const double op[10],
+                                                   const double mc_oct[10], double inv_m0, double Lc[3]) {
+    FastDerivs f;
+    f.X00 = dX[0] * dX[0];
+    f.X11 = dX[1] * dX[1];
+    f.X22 = dX[2] * dX[2];
+    f.X01 = dX[0] * dX[1];
+    f.X02 = dX[0] * dX[2];
+    f.X12 = dX[1] * dX[2];
+    const double r2 = fmax(f.X00 + f.X11 + f.X22, 1.0e-20);
+    const double y = (double)rsqrtf((float)r2);
+    const double rs = y * fma(-0.5 * r2 * y, y, 1.5);   // one Newton step: ~1e-14 relative
+    const double r2inv = rs * rs;
+    const double d1 = rs * r2inv;
+    f.d2 = -3.0 * d1 * r2inv;
+    f.d3 = -5.0 * f.d2 * r2inv;
+    const double n0 = m0p * inv_m0;
+    double g[10];
+#pragma unroll
+    for (int o = 0; o < 10; ++o) g[o] = fma(-mc_oct[o], n0, op[o]);
+    fast_upper_correction(f, g, Lc);
+}
+
+// Lane -> sub-lattice cell of the warp's parity class (see the layout above).
+struct WsLane {
+    int i, j, k;
+};
+__device__ __forceinline__ WsLane ws_lane() {
+    const int lane = threadIdx.x & 31;
+    return WsLane{(lane >> 2) & 1, lane >> 3, lane & 3};
+}
+
+template <int CHUNK>
+__device__ void ws_contraction_warp(const float2* sa, const double2* sb, const unsigned* s_ent, int x0, int p,
+                                    const Tables& t, uint32_t monomask, double inv_dx, const OutPtr& out) {
+    const WsLane l = ws_lane();
+    const int lane_a = l.i * WA_XS + l.j * WA_ROW + l.k;
+    const int lane_b = l.i * WB_XS + l.j * WB_ROW + l.k;
+    const int own_b = p * WB_CLS + WB_XS + WB_ROW + 1 + lane_b;
+    const double2 o0 = sb[own_b], o1 = sb[own_b + SUB_YZ];
+    const double Pc0 = o0.x, Pc1 = o0.y, Pc2 = o1.x;
+    double acc[20];
+    float accf[20];
+#pragma unroll
+    for (int q = 0; q < 20; ++q) {
+        acc[q] = 0.0;
+        accf[q] = 0.0f;
+    }
+    const int n = t.count[p], nfar = t.count_far[p];
+    const unsigned* ent = s_ent + p * MAX_ENTRIES;
+#pragma unroll 1
+    for (int e0 = 0; e0 < nfar; e0 += CHUNK) {
+        const int e1 = min(e0 + CHUNK, nfar);
+#pragma unroll 2
+        for (int e = e0; e < e1; ++e) {
+            const unsigned en = ent[e];
+            const double2* pb = sb + (en >> 16) + lane_b;
+            const double2 q0 = pb[0], q1 = pb[SUB_YZ];
+            const float dX[3] = {(float)(Pc0 - q0.x), (float)(Pc1 - q0.y), (float)(Pc2 - q1.x)};
+            const float2* pa = sa + (en & 0xffffu) + lane_a;
+            float m[20];
+#pragma unroll
+            for (int q = 0; q < 10; ++q) {
+                const float2 v = pa[q * SUB_YZ];
+                m[2 * q] = v.x;
+                m[2 * q + 1] = v.y;
+            }
+            ws_contract_pair(dX, m, accf);
+        }
+#pragma unroll
+        for (int q = 0; q < 20; ++q) {
+            acc[q] += (double)accf[q];
+            accf[q] = 0.0f;
+        }
+    }
+    const int cx = x0 + ((p >> 2) & 1) + 2 * l.i, cy = ((p >> 1) & 1) + 2 * l.j, cz = (p & 1) + 2 * l.k;
+    if (monomask) {
+        // monopole-only offsets: only leaf-neighbour partners contribute
+        const int4* gent = t.entries_ws + p * MAX_ENTRIES;
+#pragma unroll 1
+        for (int e = nfar; e < n; ++e) {
+            const int4 en = __ldg(gent + e);
+            const int ax = cx + entry_sx(en.z), ay = cy + entry_sy(en.z), az = cz + entry_sz(en.z);
+            if (!((monomask >> raw_dir(ax, ay, az)) & 1u)) continue;
+            const double2 q0 = sb[en.y + lane_b], q1 = sb[en.y + lane_b + SUB_YZ];
+            const float dX[3] = {(float)(Pc0 - q0.x), (float)(Pc1 - q0.y), (float)(Pc2 - q1.x)};
+            ws_contract_mass(dX, sa[en.x + lane_a].x, accf);
+        }
+#pragma unroll
+        for (int q = 0; q < 20; ++q) acc[q] += (double)accf[q];
+    }
+    // back to physical units: L_(n) = L'_(n) dx^-(n+1)
+    const double s1 = inv_dx, s2 = s1 * inv_dx, s3 = s2 * inv_dx, s4 = s3 * inv_dx;
+    const int cf = cx * 64 + cy * 8 + cz;
+#pragma unroll
+    for (int q = 0; q < 20; ++q) out.L[q * out.stride + cf] = acc[q] * (q == 0 ? s1 : q < 4 ? s2 : q < 10 ? s3 : s4);
+}
+
+__device__ void ws_correction_warp(const double2* sb, const unsigned* s_ent, int x0, int p, const Tables& t,
+                                   uint32_t monomask, double inv_dx, const OutPtr& out) {
+    const WsLane l = ws_lane();
+    const int lane_b = l.i * WB_XS + l.j * WB_ROW + l.k;
+    const int own_b = p * WB_CLS + WB_XS + WB_ROW + 1 + lane_b;
+    const double2 o0 = sb[own_b], o1 = sb[own_b + SUB_YZ];
+    const double Pc0 = o0.x, Pc1 = o0.y, Pc2 = o1.x;
+    const double inv_m0 = 1.0 / o1.y;
+    double mc_oct[10];
+#pragma unroll
+    for (int o = 0; o < 5; ++o) {
+        const double2 v = sb[own_b + (2 + o) * SUB_YZ];
+        mc_oct[2 * o] = v.x;
+        mc_oct[2 * o + 1] = v.y;
+    }
+    double corr[3] = {0.0, 0.0, 0.0};
+    const int n = t.count[p], nfar = t.count_far[p];
+    const unsigned* ent = s_ent + p * MAX_ENTRIES;
+#pragma unroll 2
+    for (int e = 0; e < nfar; ++e) {
+        const double2* pb = sb + (ent[e] >> 16) + lane_b;
+        const double2 q0 = pb[0], q1 = pb[SUB_YZ];
+        const double dX[3] = {Pc0 - q0.x, Pc1 - q0.y, Pc2 - q1.x};
+        double op[10];
+#pragma unroll
+        for (int o = 0; o < 5; ++o) {
+            const double2 v = pb[(2 + o) * SUB_YZ];
+            op[2 * o] = v.x;
+            op[2 * o + 1] = v.y;
+        }
+        ws_correction_pair(dX, q1.y, op, mc_oct, inv_m0, corr);
+    }
+    const int cx = x0 + ((p >> 2) & 1) + 2 * l.i, cy = ((p >> 1) & 1) + 2 * l.j, cz = (p & 1) + 2 * l.k;
+    if (monomask) {
+        const int4* gent = t.entries_ws + p * MAX_ENTRIES;
+#pragma unroll 1
+        for (int e = nfar; e < n; ++e) {
+            const int4 en = __ldg(gent + e);
+            const int ax = cx + entry_sx(en.z), ay = cy + entry_sy(en.z), az = cz + entry_sz(en.z);
+            if (!((monomask >> raw_dir(ax, ay, az)) & 1u)) continue;
+            const int pb = en.y + lane_b;
+            const double2 q0 = sb[pb], q1 = sb[pb + SUB_YZ];
+            const double dX[3] = {Pc0 - q0.x, Pc1 - q0.y, Pc2 - q1.x};
+            double op[10];
+#pragma unroll
+            for (int o = 0; o < 10; ++o) op[o] = 0.0;   // leaf partners carry no octupole
+            ws_correction_pair(dX, q1.y, op, mc_oct, inv_m0, corr);
+        }
+    }
+    const double s2 = inv_dx * inv_dx;
+    const int cf = cx * 64 + cy * 8 + cz;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) out.Lc[a * out.stride + cf] = corr[a] * s2;
+}
+
 // Root node: partners are all own cells except the monopole-only stencil
 // offsets and the cell itself (multipole_kernel_root_*_impl).
 // Staged layout: sm[q * 512 + cell].
@@ -631,6 +919,62 @@ __global__ void __launch_bounds__(THREADS, 1) m2l_batch_kernel(BatchArgs a) {
                 __syncthreads();
                 m2l_tile<P64, RHO>(sm, x0, a.t, monomask, nullptr, out);
             }
+        }
+        __syncthreads();   // shared memory and `it` are reused by the next tile
+    }
+}
+
+// RHO multipole tiles in the FP32 split precision, warp-specialised (see
+// stage_region_ws): persistent over the same tile counter as m2l_batch_kernel,
+// 512 threads, one CTA per SM. The root tile runs the fast FP64 form on the
+// first 256 threads.
+template <int CHUNK>
+__global__ void __launch_bounds__(WS_THREADS, 1) m2l_split_ws_kernel(BatchArgs a) {
+    extern __shared__ __align__(16) unsigned char ws_dyn[];
+    float2* sa = reinterpret_cast<float2*>(ws_dyn);
+    double2* sb = reinterpret_cast<double2*>(ws_dyn + WS_A_BYTES);
+    unsigned* s_ent = reinterpret_cast<unsigned*>(ws_dyn + WS_A_BYTES + WS_B_BYTES);
+    __shared__ ItemInfo it;
+    __shared__ int tile;
+    const int nroot = a.wl.counts[WL_ROOT], nm2l = a.wl.counts[WL_M2L];
+    const int total = 2 * (nroot + nm2l);
+    const int warp = threadIdx.x >> 5;
+    // far-first partner deltas of the 8 parity classes, resident for the whole launch
+    for (int e = threadIdx.x; e < 8 * MAX_ENTRIES; e += blockDim.x) {
+        const int4 en = a.t.entries_ws[e];
+        s_ent[e] = (unsigned)en.x | ((unsigned)en.y << 16);
+    }
+    for (;;) {
+        if (threadIdx.x == 0) tile = atomicAdd(a.wl.counts + WL_M2L_NEXT, 1);
+        __syncthreads();
+        const int t = tile;
+        if (t >= total) break;
+        const int item_idx = (t < 2 * nroot) ? a.wl.root[t >> 1] : a.wl.m2l[(t - 2 * nroot) >> 1];
+        load_item(a, item_idx, it);
+        const int x0 = TILE_X * (t & 1);
+        const size_t sub = (size_t)it.subgrid;
+        OutPtr out{a.L + sub * 20 * NCELL, a.Lc + sub * 3 * NCELL, NCELL, true};
+        if (it.kind == OTFMM_KIND_M2L_ROOT) {
+            double* sm = reinterpret_cast<double*>(ws_dyn);
+            for (int r = threadIdx.x; r < NCELL; r += blockDim.x)
+                for (int q = 0; q < NCOMP; ++q)
+                    sm[q * NCELL + r] = (q < 20) ? a.M[(sub * 20 + q) * NCELL + r] * stage_scale<PREC_FAST>(q)
+                                                 : a.com[(sub * 3 + (q - 20)) * NCELL + r];
+            __syncthreads();
+            if (threadIdx.x < THREADS) root_tile<PREC_FAST, true>(sm, x0, a.t, out);
+        } else {
+            uint32_t monomask = 0;
+            for (int d = 0; d < 26; ++d) {
+                const int nb = it.nb[d];
+                if (nb >= 0 && a.is_leaf[nb]) monomask |= 1u << (d < 13 ? d : d + 1);
+            }
+            const double inv_dx = 1.0 / it.dx;
+            stage_region_ws(sa, sb, it, x0, inv_dx, a.M, a.com, a.mon, a.is_leaf);
+            __syncthreads();
+            if (warp < 8)
+                ws_contraction_warp<CHUNK>(sa, sb, s_ent, x0, warp, a.t, monomask, inv_dx, out);
+            else
+                ws_correction_warp(sb, s_ent, x0, warp & 7, a.t, monomask, inv_dx, out);
         }
         __syncthreads();   // shared memory and `it` are reused by the next tile
     }
@@ -1078,6 +1422,7 @@ struct otfmm_context {
     int* d_count_far = nullptr;
     int4* d_entries_split = nullptr;
     int2* d_entries_p2p = nullptr;
+    int4* d_entries_ws = nullptr;
     int counts_far[8] = {};
     double* d_four = nullptr;
     uint8_t* d_phase = nullptr;
@@ -1086,7 +1431,8 @@ struct otfmm_context {
     int* d_lists = nullptr;            // batched work lists (grown on demand)
     int list_capacity = 0;
     std::mutex mu;
-    Tables tables() const { return Tables{d_entries, d_count, d_entries_fast, d_count_far, d_entries_split, d_entries_p2p, d_four, d_phase}; }
+    Tables tables() const { return Tables{d_entries, d_count, d_entries_fast, d_count_far, d_entries_split, d_entries_p2p, d_entries_ws, d_four,
+                                          d_phase}; }
 };
 
 namespace {
@@ -1126,6 +1472,8 @@ int ensure_attributes(int device) {
     rc = rc ? rc : set_smem(m2l_batch_kernel<PREC_FAST, false>, bytes);
     rc = rc ? rc : set_smem(m2l_batch_kernel<PREC_SPLIT, true>, S_SMEM_DOUBLES * (int)sizeof(double));
     rc = rc ? rc : set_smem(m2l_batch_kernel<PREC_SPLIT, false>, S_SMEM_DOUBLES * (int)sizeof(double));
+    rc = rc ? rc : set_smem(m2l_split_ws_kernel<16>, WS_SMEM_BYTES);
+    rc = rc ? rc : set_smem(m2l_split_ws_kernel<8>, WS_SMEM_BYTES);
     rc = rc ? rc : set_smem(p2p_batch_kernel<PREC_EXACT>, P2P_SMEM_BYTES);
     rc = rc ? rc : set_smem(p2p_batch_kernel<PREC_FAST>, P2P_SMEM_BYTES);
     rc = rc ? rc : set_smem(soa_m2l_kernel<PREC_EXACT, true, false>, bytes);
@@ -1192,6 +1540,7 @@ int otfmm_create(int device, double theta, otfmm_context** out) {
         }
     // split-layout table (far first, like the fast one)
     std::vector<int4> entries_split(8 * MAX_ENTRIES, int4{0, 0, 0, 0});
+    std::vector<int4> entries_ws(8 * MAX_ENTRIES, int4{0, 0, 0, 0});
     // fast-form table: far offsets first (accumulation order is free there)
     std::vector<int2> entries_fast(entries.size(), int2{0, 0});
     for (int p = 0; p < 8; ++p) {
@@ -1207,6 +1556,9 @@ int otfmm_create(int device, double theta, otfmm_context** out) {
                     const int cls = (((px + sx) & 1) << 2) | (((py + sy) & 1) << 1) | ((pz + sz) & 1);
                     const int row = cls * S_CLS + (qx >> 1) * S_XS + (qy >> 1) * S_RB;
                     entries_split[p * MAX_ENTRIES + k] = int4{row + (qz >> 1), en.y, 2 * row + S_FOFF + (qz >> 1), 0};
+                    entries_ws[p * MAX_ENTRIES + k] =
+                        int4{cls * WA_CLS + (qx >> 1) * WA_XS + (qy >> 1) * WA_ROW + (qz >> 1),
+                             cls * WB_CLS + (qx >> 1) * WB_XS + (qy >> 1) * WB_ROW + (qz >> 1), en.y, 0};
                     entries_fast[p * MAX_ENTRIES + k++] = en;
                 }
                 if (pass == 0 && far) ++ctx->counts_far[p];
@@ -1226,6 +1578,9 @@ int otfmm_create(int device, double theta, otfmm_context** out) {
         (e = cudaMemcpy(ctx->d_count_far, ctx->counts_far, sizeof(int) * 8, cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMalloc(&ctx->d_entries_split, sizeof(int4) * entries_split.size())) != cudaSuccess ||
         (e = cudaMalloc(&ctx->d_entries_p2p, sizeof(int2) * entries_p2p.size())) != cudaSuccess ||
+        (e = cudaMalloc(&ctx->d_entries_ws, sizeof(int4) * entries_ws.size())) != cudaSuccess ||
+        (e = cudaMemcpy(ctx->d_entries_ws, entries_ws.data(), sizeof(int4) * entries_ws.size(),
+                        cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemcpy(ctx->d_entries_p2p, entries_p2p.data(), sizeof(int2) * entries_p2p.size(),
                         cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemcpyToSymbol(c_four, ctx->st.four, sizeof(double) * 4 * FULL)) != cudaSuccess ||
@@ -1258,6 +1613,7 @@ int otfmm_destroy(otfmm_context* ctx) {
     cudaFree(ctx->d_entries_fast);
     cudaFree(ctx->d_entries_split);
     cudaFree(ctx->d_entries_p2p);
+    cudaFree(ctx->d_entries_ws);
     cudaFree(ctx->d_count_far);
     cudaFree(ctx->d_four);
     cudaFree(ctx->d_phase);
@@ -1472,7 +1828,7 @@ int otfmm_batch(otfmm_context* ctx, const double* pool_M, const double* pool_com
     } else {
         if (precision == OTFMM_FP32_SPLIT) {
             const size_t sbytes = S_SMEM_DOUBLES * sizeof(double);
-            if (rho) m2l_batch_kernel<PREC_SPLIT, true><<<tiles_grid, THREADS, sbytes, s>>>(a);
+            if (rho) m2l_split_ws_kernel<16><<<tiles_grid, WS_THREADS, WS_SMEM_BYTES, s>>>(a);
             else m2l_batch_kernel<PREC_SPLIT, false><<<tiles_grid, THREADS, sbytes, s>>>(a);
         } else {
             if (rho) m2l_batch_kernel<PREC_FAST, true><<<tiles_grid, THREADS, bytes, s>>>(a);
