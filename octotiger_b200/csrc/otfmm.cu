@@ -100,9 +100,12 @@ constexpr int P_THREADS = 512;
 constexpr int P_REG = INX + 4;
 constexpr int P_SUB = 6;
 constexpr int P_RS = 12;
-constexpr int P_XS = P_SUB * P_RS;
+constexpr int P_XS = 80;                    // >= 6 rows of 12; = 16 mod 32 for the FP32 copy
 constexpr int P_CLS = P_SUB * P_XS;
-constexpr int P_SMEM_DOUBLES = 8 * P_CLS;   // 3456 doubles = 27648 bytes
+constexpr int P_SMEM_DOUBLES = 8 * P_CLS;   // 3840 elements
+// Lane (i, j, k) = (l >> 4, (l >> 2) & 3, l & 3) reads element k + 12 j + 80 i:
+// distinct 8-byte slots per half-warp and distinct 4-byte banks per warp.
+static_assert(P_XS >= P_SUB * P_RS && P_RS % 16 == 12 && P_XS % 32 == 16, "P2P region strides");
 
 // Monopole constants {-1/r, x/r^3, y/r^3, z/r^3} per stencil offset (they do
 // not depend on theta), read warp-uniformly through the constant cache.
@@ -123,6 +126,8 @@ struct Tables {
                                 // y = double2 delta, z = packed
     const double* four;      // [FULL][4] monopole constants
     const uint8_t* phase;    // [FULL] inner_stencil_masks (true outside the stencil)
+    const int* p2m_start;    // [512][28]: per cell, start of the entries of raw direction r in p2m_list
+    const uint16_t* p2m_list;   // partner cell index (in its neighbour) of every entry, grouped by direction
 };
 
 __device__ __forceinline__ int entry_sx(int y) { return (y & 15) - 8; }
@@ -1087,21 +1092,160 @@ __global__ void __launch_bounds__(P2P_THREADS, P2P_CTAS_PER_SM) p2p_batch_kernel
     }
 }
 
+// Leaf items, P2P in the fast FP64 form (T = double) or the FP32 split form
+// (T = float, FP32 partial sums promoted to FP64 every CHUNK partners):
+// persistent, one CTA of 1024 threads per SM made of 4 groups of 8 warps.
+// Every group solves one leaf at a time (warp = parity class, two cells per
+// thread, the partner mass of each stencil entry read from the staged
+// region); the 4 groups share one copy of the per-parity delta and monopole
+// constant table, and synchronise among themselves with named barriers.
+constexpr int P2_GROUPS = 4;
+constexpr int P2_THREADS = 256 * P2_GROUPS;
+template <class T>
+struct P2Vec;
+template <>
+struct P2Vec<double> {
+    using type = double4;
+};
+template <>
+struct P2Vec<float> {
+    using type = float4;
+};
+template <class T>
+constexpr int p2_smem_bytes() {
+    return 8 * MAX_ENTRIES * (int)(sizeof(typename P2Vec<T>::type) + sizeof(int)) +
+           P2_GROUPS * P_SMEM_DOUBLES * (int)sizeof(T);
+}
+static_assert(p2_smem_bytes<double>() <= 232448 - 1024, "FP64 P2P groups fit");
+
+__device__ __forceinline__ void group_sync(int g) {
+    asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "r"(256) : "memory");
+}
+
+template <class T, int CHUNK>
+__global__ void __launch_bounds__(P2_THREADS, 1) p2p_leaf_kernel(BatchArgs a) {
+    using V4 = typename P2Vec<T>::type;
+    extern __shared__ __align__(16) unsigned char p2_dyn[];
+    V4* s_four = reinterpret_cast<V4*>(p2_dyn);
+    int* s_delta = reinterpret_cast<int*>(p2_dyn + 8 * MAX_ENTRIES * sizeof(V4));
+    T* regions = reinterpret_cast<T*>(p2_dyn + 8 * MAX_ENTRIES * (sizeof(V4) + sizeof(int)));
+    __shared__ ItemInfo its[P2_GROUPS];
+    for (int e = threadIdx.x; e < 8 * MAX_ENTRIES; e += blockDim.x) {
+        const int p = e / MAX_ENTRIES, k = e % MAX_ENTRIES;
+        if (k < a.t.count[p]) {
+            const int2 en = a.t.entries_p2p[e];
+            s_delta[e] = en.x;
+            s_four[e] = V4{(T)c_four[en.y][0], (T)c_four[en.y][1], (T)c_four[en.y][2], (T)c_four[en.y][3]};
+        }
+    }
+    __syncthreads();
+    const int g = threadIdx.x >> 8, tid = threadIdx.x & 255;
+    T* pm = regions + g * P_SMEM_DOUBLES;
+    ItemInfo& it = its[g];
+    const int p = tid >> 5, lane = tid & 31;
+    const int i = lane >> 4, j = (lane >> 2) & 3, k = lane & 3;
+    const int px = (p >> 2) & 1, py = (p >> 1) & 1, pz = p & 1;
+    const int cy = py + 2 * j, cz = pz + 2 * k;
+    const int cxa = px + 2 * i, cxb = px + 2 * (i + 2);
+    const int lane_off = i * P_XS + j * P_RS + k;
+    constexpr int OFF_B = 2 * P_XS;   // second cell: two sub-lattice planes further in x
+    const int n = a.t.count[p];
+    const V4* four = s_four + p * MAX_ENTRIES;
+    const int* delta = s_delta + p * MAX_ENTRIES;
+    const int nleaf = a.wl.counts[WL_LEAF];
+    for (int kk = blockIdx.x * P2_GROUPS + g; kk < nleaf; kk += gridDim.x * P2_GROUPS) {
+        group_sync(g);   // the group's previous leaf is done with pm / it
+        if (tid == 0) {
+            const otfmm_work_item& w = a.items[a.wl.leaf[kk]];
+            it.subgrid = w.subgrid;
+            it.dx = w.dx;
+            for (int d = 0; d < 26; ++d) it.nb[d] = w.neighbors[d];
+        }
+        group_sync(g);
+        const double dc0 = 1.0 / it.dx;
+        for (int r = tid; r < P_REG * P_REG * P_REG; r += 256) {
+            const int ax = r / (P_REG * P_REG) - 2, ay = (r / P_REG) % P_REG - 2, az = r % P_REG - 2;
+            const int raw = raw_dir(ax, ay, az);
+            const int src = (raw == 13) ? it.subgrid : it.nb[raw < 13 ? raw : raw - 1];
+            double m = 0.0;
+            if (src >= 0 && (raw == 13 || a.is_leaf[src]))
+                m = a.mon[(size_t)src * NCELL + (ax & 7) * 64 + (ay & 7) * 8 + (az & 7)];
+            const int cls = ((ax & 1) << 2) | ((ay & 1) << 1) | (az & 1);
+            pm[cls * P_CLS + ((ax + 2) >> 1) * P_XS + ((ay + 2) >> 1) * P_RS + ((az + 2) >> 1)] = (T)(m * dc0);
+        }
+        group_sync(g);
+        double ga[4] = {0.0, 0.0, 0.0, 0.0}, gb[4] = {0.0, 0.0, 0.0, 0.0};
+        if (sizeof(T) == 8) {
+#pragma unroll 4
+            for (int e = 0; e < n; ++e) {
+                const V4 f = four[e];
+                const int d = delta[e] + lane_off;
+                const double ma = pm[d], mb = pm[d + OFF_B];
+                ga[0] = fma((double)f.x, ma, ga[0]);
+                ga[1] = fma((double)f.y, ma, ga[1]);
+                ga[2] = fma((double)f.z, ma, ga[2]);
+                ga[3] = fma((double)f.w, ma, ga[3]);
+                gb[0] = fma((double)f.x, mb, gb[0]);
+                gb[1] = fma((double)f.y, mb, gb[1]);
+                gb[2] = fma((double)f.z, mb, gb[2]);
+                gb[3] = fma((double)f.w, mb, gb[3]);
+            }
+        } else {
+#pragma unroll 1
+            for (int e0 = 0; e0 < n; e0 += CHUNK) {
+                const int e1 = min(e0 + CHUNK, n);
+                float fa[4] = {0.f, 0.f, 0.f, 0.f}, fb[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll 4
+                for (int e = e0; e < e1; ++e) {
+                    const V4 f = four[e];
+                    const int d = delta[e] + lane_off;
+                    const float ma = (float)pm[d], mb = (float)pm[d + OFF_B];
+                    fa[0] = fmaf((float)f.x, ma, fa[0]);
+                    fa[1] = fmaf((float)f.y, ma, fa[1]);
+                    fa[2] = fmaf((float)f.z, ma, fa[2]);
+                    fa[3] = fmaf((float)f.w, ma, fa[3]);
+                    fb[0] = fmaf((float)f.x, mb, fb[0]);
+                    fb[1] = fmaf((float)f.y, mb, fb[1]);
+                    fb[2] = fmaf((float)f.z, mb, fb[2]);
+                    fb[3] = fmaf((float)f.w, mb, fb[3]);
+                }
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    ga[q] += (double)fa[q];
+                    gb[q] += (double)fb[q];
+                }
+            }
+        }
+        const double dc1 = -dc0;
+#pragma unroll
+        for (int q = 1; q < 4; ++q) {
+            ga[q] *= dc1;
+            gb[q] *= dc1;
+        }
+        double* L = a.L + (size_t)it.subgrid * 20 * NCELL;
+        const int cfa = cxa * 64 + cy * 8 + cz, cfb = cxb * 64 + cy * 8 + cz;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            L[q * NCELL + cfa] = ga[q];
+            L[q * NCELL + cfb] = gb[q];
+        }
+    }
+}
+
 // Leaf items with refined neighbours: P2M (p2m_kernel_impl_rho / _non_rho,
 // monopole kokkos_kernel.hpp:517-942) after P2P: one CTA per leaf of the P2M
-// work list (grid stride), one thread per cell, partner moments read through
-// L2. The exact form goes direction after direction in direction order, like
-// the reference's one launch per refined neighbour; the fast form takes all
-// refined directions in one stencil pass.
+// work list (grid stride), one thread per cell. Every cell walks only the
+// stencil entries whose partner lies in a refined neighbour: per cell, the
+// entries are kept grouped by the partner's direction (stencil order inside
+// a group, table built at context creation), so a lane visits direction after
+// direction in direction order, which is also the order of the reference's
+// one launch per refined neighbour. Partner moments come through L1/L2.
 template <int PREC, bool RHO>
 __global__ void __launch_bounds__(P_THREADS) p2m_batch_kernel(BatchArgs a) {
     __shared__ ItemInfo it;
     constexpr int P64 = (PREC == PREC_EXACT) ? PREC_EXACT : PREC_FAST;
     const int cu = threadIdx.x;
-    const int cx = cu >> 6, cy = (cu >> 3) & 7, cz = cu & 7;
-    const int p = ((cx & 1) << 2) | ((cy & 1) << 1) | (cz & 1);
-    const int n = a.t.count[p];
-    const int2* ent = a.t.entries + p * MAX_ENTRIES;
+    const int* start = a.t.p2m_start + cu * 28;
     const int np2m = a.wl.counts[WL_P2M];
     for (int kk = blockIdx.x; kk < np2m; kk += gridDim.x) {
         __syncthreads();   // `it` is reused
@@ -1119,27 +1263,20 @@ __global__ void __launch_bounds__(P_THREADS) p2m_batch_kernel(BatchArgs a) {
         for (int q = 0; q < 3; ++q) X[q] = a.com[(sub * 3 + q) * NCELL + cu];
 #pragma unroll
         for (int q = 0; q < 4; ++q) acc[q] = L[q * NCELL + cu];
-        for (int raw_sel = (P64 == PREC_EXACT ? 0 : 27); raw_sel < 28; ++raw_sel) {
-            uint32_t want;   // refined directions served in this sweep
-            if (P64 == PREC_EXACT) {
-                if (raw_sel == 27) break;
-                if (!((refmask >> raw_sel) & 1u)) continue;
-                want = 1u << raw_sel;
-            } else {
-                want = refmask;
-            }
-            for (int e = 0; e < n; ++e) {
-                const int y = __ldg(&ent[e].y);
-                const int ax = cx + entry_sx(y), ay = cy + entry_sy(y), az = cz + entry_sz(y);
-                const int raw = raw_dir(ax, ay, az);
-                if (!((want >> raw) & 1u)) continue;
-                const size_t nb = (size_t)it.nb[raw < 13 ? raw : raw - 1];
-                const int u = (ax & 7) * 64 + (ay & 7) * 8 + (az & 7);
+        for (uint32_t rm = refmask; rm; rm &= rm - 1) {
+            const int raw = __ffs(rm) - 1;
+            const size_t nb = (size_t)it.nb[raw < 13 ? raw : raw - 1];
+            const double* __restrict__ nM = a.M + nb * 20 * NCELL;
+            const double* __restrict__ ncom = a.com + nb * 3 * NCELL;
+            const int beg = __ldg(start + raw), end = __ldg(start + raw + 1);
+#pragma unroll 1
+            for (int q = beg; q < end; ++q) {
+                const int u = __ldg(a.t.p2m_list + q);
                 double Y[3], mp[20];
 #pragma unroll
-                for (int q = 0; q < 3; ++q) Y[q] = __ldg(a.com + (nb * 3 + q) * NCELL + u);
+                for (int c = 0; c < 3; ++c) Y[c] = __ldg(ncom + c * NCELL + u);
 #pragma unroll
-                for (int q = 0; q < 20; ++q) mp[q] = __ldg(a.M + (nb * 20 + q) * NCELL + u) * stage_scale<P64>(q);
+                for (int c = 0; c < 20; ++c) mp[c] = __ldg(nM + c * NCELL + u) * stage_scale<P64>(c);
                 if (P64 == PREC_EXACT)
                     exact_p2m_pair<RHO>(X, Y, mp, acc, corr);
                 else
@@ -1423,6 +1560,8 @@ struct otfmm_context {
     int4* d_entries_split = nullptr;
     int2* d_entries_p2p = nullptr;
     int4* d_entries_ws = nullptr;
+    int* d_p2m_start = nullptr;
+    uint16_t* d_p2m_list = nullptr;
     int counts_far[8] = {};
     double* d_four = nullptr;
     uint8_t* d_phase = nullptr;
@@ -1431,8 +1570,8 @@ struct otfmm_context {
     int* d_lists = nullptr;            // batched work lists (grown on demand)
     int list_capacity = 0;
     std::mutex mu;
-    Tables tables() const { return Tables{d_entries, d_count, d_entries_fast, d_count_far, d_entries_split, d_entries_p2p, d_entries_ws, d_four,
-                                          d_phase}; }
+    Tables tables() const { return Tables{d_entries,    d_count, d_entries_fast, d_count_far, d_entries_split, d_entries_p2p,
+                      d_entries_ws, d_four,  d_phase,        d_p2m_start, d_p2m_list}; }
 };
 
 namespace {
@@ -1476,6 +1615,8 @@ int ensure_attributes(int device) {
     rc = rc ? rc : set_smem(m2l_split_ws_kernel<8>, WS_SMEM_BYTES);
     rc = rc ? rc : set_smem(p2p_batch_kernel<PREC_EXACT>, P2P_SMEM_BYTES);
     rc = rc ? rc : set_smem(p2p_batch_kernel<PREC_FAST>, P2P_SMEM_BYTES);
+    rc = rc ? rc : set_smem(p2p_leaf_kernel<double, 0>, p2_smem_bytes<double>());
+    rc = rc ? rc : set_smem(p2p_leaf_kernel<float, 32>, p2_smem_bytes<float>());
     rc = rc ? rc : set_smem(soa_m2l_kernel<PREC_EXACT, true, false>, bytes);
     rc = rc ? rc : set_smem(soa_m2l_kernel<PREC_EXACT, false, false>, bytes);
     rc = rc ? rc : set_smem(soa_m2l_kernel<PREC_FAST, true, false>, bytes);
@@ -1564,9 +1705,35 @@ int otfmm_create(int device, double theta, otfmm_context** out) {
                 if (pass == 0 && far) ++ctx->counts_far[p];
             }
     }
+    // P2M: per target cell, its stencil entries grouped by the raw direction of
+    // the partner (stencil order inside a group), as partner cell indices
+    std::vector<int> p2m_start(NCELL * 28, 0);
+    std::vector<uint16_t> p2m_list;
+    p2m_list.reserve((size_t)NCELL * MAX_ENTRIES);
+    for (int cu = 0; cu < NCELL; ++cu) {
+        const int cx = cu >> 6, cy = (cu >> 3) & 7, cz = cu & 7;
+        const int p = ((cx & 1) << 2) | ((cy & 1) << 1) | (cz & 1);
+        for (int r = 0; r < 27; ++r) {
+            p2m_start[cu * 28 + r] = (int)p2m_list.size();
+            if (r == 13) continue;
+            for (int e2 = 0; e2 < ctx->counts[p]; ++e2) {
+                const int y = entries[p * MAX_ENTRIES + e2].y;
+                const int ax = cx + (y & 15) - 8, ay = cy + ((y >> 4) & 15) - 8, az = cz + ((y >> 8) & 15) - 8;
+                const int raw = ((ax >> 3) + 1) + 3 * ((ay >> 3) + 1) + 9 * ((az >> 3) + 1);
+                if (raw == r) p2m_list.push_back((uint16_t)((ax & 7) * 64 + (ay & 7) * 8 + (az & 7)));
+            }
+        }
+        p2m_start[cu * 28 + 27] = (int)p2m_list.size();
+    }
     DeviceGuard g(device);
     cudaError_t e;
-    if ((e = cudaMalloc(&ctx->d_entries, sizeof(int2) * entries.size())) != cudaSuccess ||
+    if ((e = cudaMalloc(&ctx->d_p2m_start, sizeof(int) * p2m_start.size())) != cudaSuccess ||
+        (e = cudaMemcpy(ctx->d_p2m_start, p2m_start.data(), sizeof(int) * p2m_start.size(),
+                        cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMalloc(&ctx->d_p2m_list, sizeof(uint16_t) * p2m_list.size())) != cudaSuccess ||
+        (e = cudaMemcpy(ctx->d_p2m_list, p2m_list.data(), sizeof(uint16_t) * p2m_list.size(),
+                        cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMalloc(&ctx->d_entries, sizeof(int2) * entries.size())) != cudaSuccess ||
         (e = cudaMalloc(&ctx->d_count, sizeof(int) * 8)) != cudaSuccess ||
         (e = cudaMalloc(&ctx->d_four, sizeof(double) * 4 * FULL)) != cudaSuccess ||
         (e = cudaMalloc(&ctx->d_phase, FULL)) != cudaSuccess ||
@@ -1614,6 +1781,8 @@ int otfmm_destroy(otfmm_context* ctx) {
     cudaFree(ctx->d_entries_split);
     cudaFree(ctx->d_entries_p2p);
     cudaFree(ctx->d_entries_ws);
+    cudaFree(ctx->d_p2m_start);
+    cudaFree(ctx->d_p2m_list);
     cudaFree(ctx->d_count_far);
     cudaFree(ctx->d_four);
     cudaFree(ctx->d_phase);
@@ -1834,7 +2003,10 @@ int otfmm_batch(otfmm_context* ctx, const double* pool_M, const double* pool_com
             if (rho) m2l_batch_kernel<PREC_FAST, true><<<tiles_grid, THREADS, bytes, s>>>(a);
             else m2l_batch_kernel<PREC_FAST, false><<<tiles_grid, THREADS, bytes, s>>>(a);
         }
-        p2p_batch_kernel<PREC_FAST><<<p2p_grid, P2P_THREADS, P2P_SMEM_BYTES, s>>>(a);
+        if (precision == OTFMM_FP32_SPLIT)
+            p2p_leaf_kernel<float, 32><<<sms, P2_THREADS, p2_smem_bytes<float>(), s>>>(a);
+        else
+            p2p_leaf_kernel<double, 0><<<sms, P2_THREADS, p2_smem_bytes<double>(), s>>>(a);
         if (rho) p2m_batch_kernel<PREC_FAST, true><<<p2m_grid, P_THREADS, 0, s>>>(a);
         else p2m_batch_kernel<PREC_FAST, false><<<p2m_grid, P_THREADS, 0, s>>>(a);
     }
