@@ -128,6 +128,8 @@ struct Tables {
     const uint8_t* phase;    // [FULL] inner_stencil_masks (true outside the stencil)
     const int* p2m_start;    // [512][28]: per cell, start of the entries of raw direction r in p2m_list
     const uint16_t* p2m_list;   // partner cell index (in its neighbour) of every entry, grouped by direction
+    const int* p2m_perm_start;  // [28]: start of raw direction r in p2m_perm
+    const uint16_t* p2m_perm;   // per direction, the cells with partners there, most partners first
 };
 
 __device__ __forceinline__ int entry_sx(int y) { return (y & 15) - 8; }
@@ -1234,21 +1236,23 @@ __global__ void __launch_bounds__(P2_THREADS, 1) p2p_leaf_kernel(BatchArgs a) {
 
 // Leaf items with refined neighbours: P2M (p2m_kernel_impl_rho / _non_rho,
 // monopole kokkos_kernel.hpp:517-942) after P2P: one CTA per leaf of the P2M
-// work list (grid stride), one thread per cell. Every cell walks only the
-// stencil entries whose partner lies in a refined neighbour: per cell, the
-// entries are kept grouped by the partner's direction (stencil order inside
-// a group, table built at context creation), so a lane visits direction after
-// direction in direction order, which is also the order of the reference's
-// one launch per refined neighbour. Partner moments come through L1/L2.
+// work list (grid stride). The refined directions are taken one after the
+// other in direction order, like the reference's one launch per refined
+// neighbour; within a direction only the cells that have partners there
+// work, ordered by their partner count (a table built at context creation),
+// so the lanes of a warp run loops of similar length. The exact form visits a
+// cell's entries of that direction in stencil order on one lane; the fast
+// form spreads them over F lanes (as many as the CTA holds, up to 16) and
+// sums the F partial results in a fixed butterfly order. The per-cell sums
+// live in shared memory between directions. Partner moments come through L1/L2.
 template <int PREC, bool RHO>
 __global__ void __launch_bounds__(P_THREADS) p2m_batch_kernel(BatchArgs a) {
     __shared__ ItemInfo it;
+    __shared__ double s_acc[7][NCELL];   // L0..L3, then L_c x, y, z
     constexpr int P64 = (PREC == PREC_EXACT) ? PREC_EXACT : PREC_FAST;
-    const int cu = threadIdx.x;
-    const int* start = a.t.p2m_start + cu * 28;
     const int np2m = a.wl.counts[WL_P2M];
     for (int kk = blockIdx.x; kk < np2m; kk += gridDim.x) {
-        __syncthreads();   // `it` is reused
+        __syncthreads();   // `it` and s_acc are reused
         load_item(a, a.wl.p2m[kk], it);
         uint32_t refmask = 0;
         for (int d = 0; d < 26; ++d) {
@@ -1258,19 +1262,38 @@ __global__ void __launch_bounds__(P_THREADS) p2m_batch_kernel(BatchArgs a) {
         const size_t sub = (size_t)it.subgrid;
         double* L = a.L + sub * 20 * NCELL;
         double* Lc = a.Lc + sub * 3 * NCELL;
-        double X[3], acc[4], corr[3] = {0.0, 0.0, 0.0};
+        for (int cu = threadIdx.x; cu < NCELL; cu += blockDim.x) {
 #pragma unroll
-        for (int q = 0; q < 3; ++q) X[q] = a.com[(sub * 3 + q) * NCELL + cu];
+            for (int q = 0; q < 4; ++q) s_acc[q][cu] = L[q * NCELL + cu];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) acc[q] = L[q * NCELL + cu];
+            for (int q = 4; q < 7; ++q) s_acc[q][cu] = 0.0;
+        }
         for (uint32_t rm = refmask; rm; rm &= rm - 1) {
             const int raw = __ffs(rm) - 1;
+            __syncthreads();   // the previous direction's sums are in place
             const size_t nb = (size_t)it.nb[raw < 13 ? raw : raw - 1];
             const double* __restrict__ nM = a.M + nb * 20 * NCELL;
             const double* __restrict__ ncom = a.com + nb * 3 * NCELL;
-            const int beg = __ldg(start + raw), end = __ldg(start + raw + 1);
+            const int t0 = __ldg(a.t.p2m_perm_start + raw), nt = __ldg(a.t.p2m_perm_start + raw + 1) - t0;
+            // F lanes share a cell's entries of this direction (fast form; F divides 32);
+            // the exact form keeps one lane per cell and the stencil order
+            int F = 1;
+            if (P64 != PREC_EXACT)
+                while (F < 16 && nt * 2 * F <= (int)blockDim.x) F <<= 1;
+            const int tgt = threadIdx.x / F, f = threadIdx.x % F;
+            const bool active = tgt < nt;
+            const int cu = active ? __ldg(a.t.p2m_perm + t0 + tgt) : 0;
+            double X[3], acc[4], corr[3];
+#pragma unroll
+            for (int q = 0; q < 3; ++q) X[q] = __ldg(a.com + (sub * 3 + q) * NCELL + cu);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[q] = (P64 == PREC_EXACT && active) ? s_acc[q][cu] : 0.0;
+#pragma unroll
+            for (int q = 0; q < 3; ++q) corr[q] = (P64 == PREC_EXACT && active) ? s_acc[4 + q][cu] : 0.0;
+            const int beg = active ? __ldg(a.t.p2m_start + cu * 28 + raw) : 0;
+            const int end = active ? __ldg(a.t.p2m_start + cu * 28 + raw + 1) : 0;
 #pragma unroll 1
-            for (int q = beg; q < end; ++q) {
+            for (int q = beg + f; q < end; q += F) {
                 const int u = __ldg(a.t.p2m_list + q);
                 double Y[3], mp[20];
 #pragma unroll
@@ -1282,12 +1305,35 @@ __global__ void __launch_bounds__(P_THREADS) p2m_batch_kernel(BatchArgs a) {
                 else
                     fast_p2m_pair<RHO>(X, Y, mp, acc, corr);
             }
+            if (P64 != PREC_EXACT) {
+                // fixed-order butterfly over the F lanes of each cell
+                for (int o = F >> 1; o > 0; o >>= 1) {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) corr[q] += __shfl_xor_sync(0xffffffffu, corr[q], o);
+                }
+                if (active && f == 0) {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) s_acc[q][cu] += acc[q];
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) s_acc[4 + q][cu] += corr[q];
+                }
+            } else if (active) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) s_acc[q][cu] = acc[q];
+#pragma unroll
+                for (int q = 0; q < 3; ++q) s_acc[4 + q][cu] = corr[q];
+            }
         }
+        __syncthreads();
+        for (int cu = threadIdx.x; cu < NCELL; cu += blockDim.x) {
 #pragma unroll
-        for (int q = 0; q < 4; ++q) L[q * NCELL + cu] = acc[q];
-        // L_c of a leaf with a refined neighbour: the P2M correction (zero for DRHODT)
+            for (int q = 0; q < 4; ++q) L[q * NCELL + cu] = s_acc[q][cu];
+            // L_c of a leaf with a refined neighbour: the P2M correction (zero for DRHODT)
 #pragma unroll
-        for (int q = 0; q < 3; ++q) Lc[q * NCELL + cu] = RHO ? corr[q] : 0.0;
+            for (int q = 0; q < 3; ++q) Lc[q * NCELL + cu] = RHO ? s_acc[4 + q][cu] : 0.0;
+        }
     }
 }
 
@@ -1562,6 +1608,8 @@ struct otfmm_context {
     int4* d_entries_ws = nullptr;
     int* d_p2m_start = nullptr;
     uint16_t* d_p2m_list = nullptr;
+    int* d_p2m_perm_start = nullptr;
+    uint16_t* d_p2m_perm = nullptr;
     int counts_far[8] = {};
     double* d_four = nullptr;
     uint8_t* d_phase = nullptr;
@@ -1571,7 +1619,8 @@ struct otfmm_context {
     int list_capacity = 0;
     std::mutex mu;
     Tables tables() const { return Tables{d_entries,    d_count, d_entries_fast, d_count_far, d_entries_split, d_entries_p2p,
-                      d_entries_ws, d_four,  d_phase,        d_p2m_start, d_p2m_list}; }
+                      d_entries_ws, d_four,  d_phase,        d_p2m_start,     d_p2m_list,    d_p2m_perm_start,
+                      d_p2m_perm}; }
 };
 
 namespace {
@@ -1725,9 +1774,29 @@ int otfmm_create(int device, double theta, otfmm_context** out) {
         }
         p2m_start[cu * 28 + 27] = (int)p2m_list.size();
     }
+    // per direction: the cells with partners there, most partners first
+    std::vector<int> p2m_perm_start(28, 0);
+    std::vector<uint16_t> p2m_perm;
+    for (int r = 0; r < 27; ++r) {
+        p2m_perm_start[r] = (int)p2m_perm.size();
+        std::vector<std::pair<int, int>> cells;
+        for (int cu = 0; cu < NCELL; ++cu) {
+            const int cnt = p2m_start[cu * 28 + r + 1] - p2m_start[cu * 28 + r];
+            if (cnt > 0) cells.push_back({-cnt, cu});
+        }
+        std::sort(cells.begin(), cells.end());
+        for (const auto& c : cells) p2m_perm.push_back((uint16_t)c.second);
+    }
+    p2m_perm_start[27] = (int)p2m_perm.size();
     DeviceGuard g(device);
     cudaError_t e;
-    if ((e = cudaMalloc(&ctx->d_p2m_start, sizeof(int) * p2m_start.size())) != cudaSuccess ||
+    if ((e = cudaMalloc(&ctx->d_p2m_perm_start, sizeof(int) * p2m_perm_start.size())) != cudaSuccess ||
+        (e = cudaMemcpy(ctx->d_p2m_perm_start, p2m_perm_start.data(), sizeof(int) * p2m_perm_start.size(),
+                        cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMalloc(&ctx->d_p2m_perm, sizeof(uint16_t) * std::max<size_t>(1, p2m_perm.size()))) != cudaSuccess ||
+        (e = cudaMemcpy(ctx->d_p2m_perm, p2m_perm.data(), sizeof(uint16_t) * p2m_perm.size(),
+                        cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMalloc(&ctx->d_p2m_start, sizeof(int) * p2m_start.size())) != cudaSuccess ||
         (e = cudaMemcpy(ctx->d_p2m_start, p2m_start.data(), sizeof(int) * p2m_start.size(),
                         cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMalloc(&ctx->d_p2m_list, sizeof(uint16_t) * p2m_list.size())) != cudaSuccess ||
@@ -1783,6 +1852,8 @@ int otfmm_destroy(otfmm_context* ctx) {
     cudaFree(ctx->d_entries_ws);
     cudaFree(ctx->d_p2m_start);
     cudaFree(ctx->d_p2m_list);
+    cudaFree(ctx->d_p2m_perm_start);
+    cudaFree(ctx->d_p2m_perm);
     cudaFree(ctx->d_count_far);
     cudaFree(ctx->d_four);
     cudaFree(ctx->d_phase);
