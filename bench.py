@@ -278,6 +278,34 @@ def gpu_arm(args) -> None:
         others[prec] = {"value": counts["total"] * max(3, args.steps // 2) / (ms * 1e-3),
                         "ms_per_step": ms / max(3, args.steps // 2)}
 
+    # the reference's call pattern: one FP64 entry-point call per node (per
+    # subgrid), round-robin over a stream pool, halos staged on the device
+    # beforehand; the "plain FP64" side of the batched-split comparison
+    per_subgrid = None
+    if not args.no_per_subgrid:
+        from octotiger_b200.otfmm import PerSubgridSolver
+        plain = PerSubgridSolver(ctx, batch.pool, batch.items, n_streams=32)
+        for _ in range(2):
+            plain.run(solve, "fp64")
+        torch.cuda.synchronize()
+        reps, ms_plain = 3, 0.0
+        for _ in range(reps):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            plain.run(solve, "fp64")
+            e1.record(stream)
+            e1.synchronize()
+            ms_plain += e0.elapsed_time(e1)
+        ms_plain /= reps
+        per_subgrid = {"value": counts["total"] / (ms_plain * 1e-3), "ms_per_step": ms_plain, "precision": "fp64",
+                       "calls_per_step": plain.n_launches, "streams": 32,
+                       "what": "one otfmm_m2l_soa / otfmm_p2p_soa / otfmm_p2m_soa call per node and refined "
+                               "neighbour (the reference's per-node call pattern), halos pre-staged on the device"}
+        del plain
+        torch.cuda.empty_cache()
+
     # accuracy of the headline form against the exact FP64 form (bit-identical
     # to the reference arithmetic) on this workload
     accuracy = None
@@ -357,9 +385,12 @@ def gpu_arm(args) -> None:
                    "l2": "flushed (256 MiB write) before every timed step",
                    "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU"},
         "precisions": others,
+        "per_subgrid_fp64": per_subgrid,
+        "ratios": {"vs_batched_fp64": (value / world / others["fp64"]["value"]) if "fp64" in others else None,
+                   "vs_per_subgrid_fp64": (value / world / per_subgrid["value"]) if per_subgrid else None},
         "accuracy_vs_fp64_exact": accuracy,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
-        "gpu_launches": 3 * args.steps,
+        "gpu_launches": 4 * args.steps,
         "roofline": roof,
         "clocks": clk.summary(),
         "step_ms": [round(x, 4) for x in per],
@@ -387,6 +418,7 @@ def main() -> None:
     ap.add_argument("--gsolve", default="rho", choices=["rho", "drhodt"])
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-per-subgrid", action="store_true", help="skip the per-subgrid FP64 comparison")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -148,6 +148,25 @@ int otfmm_p2m_soa(otfmm_context* ctx, int d, const double* neighbor_M, const dou
                   const double* inner_com, double* L4, double* L_c, int gsolve_type, int reset_lc, int precision,
                   void* stream);
 
+/* Halo staging for the per-subgrid entry points, on the device from the
+ * resident pool: the reference's update_input restated
+ * (octotiger/multipole_interactions/legacy/multipole_interaction_interface.hpp:88-281
+ * for refined and root items -> mon[5832], M[20][5851], com[3][5851];
+ * octotiger/monopole_interactions/legacy/monopole_interaction_interface.hpp:64-143
+ * for leaf items -> mon[5832], M and com unused and may be NULL). `item` is a
+ * host pointer; the output buffers are device pointers. Asynchronous. */
+int otfmm_stage_soa(otfmm_context* ctx, const double* pool_M, const double* pool_com, const double* pool_mon,
+                    const uint8_t* pool_is_leaf, int32_t n_subgrids, const otfmm_work_item* item, double* mon,
+                    double* M, double* com, void* stream);
+
+/* Slab of refined neighbour `neighbor` seen in direction d (0..25) by a leaf,
+ * in the layout otfmm_p2m_soa reads (update_neighbor_input,
+ * octotiger/monopole_interactions/legacy/p2m_interaction_interface.hpp:102-160):
+ * 20 / 3 components of stride *stride = cells + 19 (at most 320 cells, stride 339). */
+int otfmm_stage_p2m_soa(otfmm_context* ctx, const double* pool_M, const double* pool_com, int32_t n_subgrids,
+                        int32_t neighbor, int d, double* neighbor_M, double* neighbor_com, int32_t* stride,
+                        void* stream);
+
 /* Batched solve: every work item of `items` (device array of n_items),
  * reading the resident pool (device pointers, n_subgrids records) and writing
  * per subgrid into L[n][20][512] and L_c[n][3][512]:

@@ -1443,6 +1443,81 @@ __global__ void soa_p2m_kernel(int d, const double* __restrict__ nM, const doubl
         for (int a = 0; a < 3; ++a) Lc[a * CLU + cu] = corr[a];
 }
 
+// Device restatement of the reference's halo staging for the per-subgrid
+// entry points, from the resident pool: multipole update_input
+// (multipole_interaction_interface.hpp:88-281) into mon[5832], M[20][5851],
+// com[3][5851] (own and refined cells: moments and centres of mass; leaf
+// neighbours: mass at the cell centre; empty directions and the root's halo:
+// zeros), or monopole update_input (monopole_interaction_interface.hpp:64-143)
+// into mon[5832] (own and leaf cells' masses). One thread per padded entry.
+__global__ void stage_soa_kernel(const double* __restrict__ M, const double* __restrict__ com,
+                                 const double* __restrict__ mon, const uint8_t* __restrict__ is_leaf,
+                                 otfmm_work_item it, double* mon_out, double* M_out, double* com_out) {
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool leaf_item = (it.kind == OTFMM_KIND_LEAF);
+    if (f >= CL) return;
+    if (f >= ENTRIES) {   // SoA padding tail of the component arrays
+        if (!leaf_item) {
+            for (int q = 0; q < 20; ++q) M_out[q * CL + f] = 0.0;
+            for (int a = 0; a < 3; ++a) com_out[a * CL + f] = 0.0;
+        }
+        return;
+    }
+    const int ax = f / (PSTRIDE * PSTRIDE) - (INX - PAD_OFF), ay = (f / PSTRIDE) % PSTRIDE - (INX - PAD_OFF),
+              az = f % PSTRIDE - (INX - PAD_OFF);
+    const int raw = raw_dir(ax, ay, az);
+    const bool centre = (raw == 13);
+    const int src = centre ? it.subgrid
+                           : (it.kind == OTFMM_KIND_M2L_ROOT ? -1 : it.neighbors[raw < 13 ? raw : raw - 1]);
+    const int u = (ax & 7) * 64 + (ay & 7) * 8 + (az & 7);
+    if (leaf_item) {
+        mon_out[f] = (src >= 0 && (centre || is_leaf[src])) ? mon[(size_t)src * NCELL + u] : 0.0;
+        return;
+    }
+    double m0 = 0.0, c[3] = {0.0, 0.0, 0.0};
+    bool moments = false;
+    if (src >= 0) {
+        if (centre || !is_leaf[src]) {
+            moments = true;
+            for (int a = 0; a < 3; ++a) c[a] = com[((size_t)src * 3 + a) * NCELL + u];
+        } else {
+            m0 = mon[(size_t)src * NCELL + u];
+            const int ip[3] = {ax + INX, ay + INX, az + INX};
+            for (int a = 0; a < 3; ++a)
+                c[a] = __dsub_rn(__dadd_rn(__dmul_rn((double)ip[a], it.dx), it.xbase[a]), __dmul_rn((double)INX, it.dx));
+        }
+    }
+    mon_out[f] = m0;
+    for (int q = 0; q < 20; ++q) M_out[q * CL + f] = moments ? M[((size_t)src * 20 + q) * NCELL + u] : 0.0;
+    for (int a = 0; a < 3; ++a) com_out[a * CL + f] = c[a];
+}
+
+// Slab of refined neighbour nb in direction d for the per-subgrid P2M entry
+// point (update_neighbor_input, p2m_interaction_interface.hpp:102-160): the
+// cells within reach, component-major with stride size + 19.
+__global__ void stage_p2m_kernel(const double* __restrict__ M, const double* __restrict__ com, int nb, int d,
+                                 double* nM, double* ncom) {
+    const int r = d < 13 ? d : d + 1;
+    const int o[3] = {r % 3 - 1, (r / 3) % 3 - 1, r / 9 - 1};
+    int s[3], sz[3];
+    for (int a = 0; a < 3; ++a) {
+        s[a] = (o[a] == -1) ? INX - SMAX : 0;
+        sz[a] = ((o[a] == 1) ? SMAX : INX) - s[a];
+    }
+    const int size = sz[0] * sz[1] * sz[2], stride = size + 19;
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= stride) return;
+    if (f >= size) {
+        for (int q = 0; q < 20; ++q) nM[q * stride + f] = 0.0;
+        for (int a = 0; a < 3; ++a) ncom[a * stride + f] = 0.0;
+        return;
+    }
+    const int x = f / (sz[1] * sz[2]) + s[0], y = (f / sz[2]) % sz[1] + s[1], z = f % sz[2] + s[2];
+    const int u = x * 64 + y * 8 + z;
+    for (int q = 0; q < 20; ++q) nM[q * stride + f] = M[((size_t)nb * 20 + q) * NCELL + u];
+    for (int a = 0; a < 3; ++a) ncom[a * stride + f] = com[((size_t)nb * 3 + a) * NCELL + u];
+}
+
 __global__ void zero_kernel(double* p, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) p[i] = 0.0;
@@ -2015,6 +2090,41 @@ int otfmm_p2m_soa(otfmm_context* ctx, int d, const double* neighbor_M, const dou
         if (rho) soa_p2m_kernel<PREC_FAST, true><<<4, 128, 0, s>>>(d, neighbor_M, neighbor_com, inner_com, L4, L_c, t);
         else soa_p2m_kernel<PREC_FAST, false><<<4, 128, 0, s>>>(d, neighbor_M, neighbor_com, inner_com, L4, L_c, t);
     }
+    OT_CUDA(cudaGetLastError());
+    return OTFMM_OK;
+}
+
+int otfmm_stage_soa(otfmm_context* ctx, const double* pool_M, const double* pool_com, const double* pool_mon,
+                    const uint8_t* pool_is_leaf, int32_t n_subgrids, const otfmm_work_item* item, double* mon,
+                    double* M, double* com, void* stream) {
+    if (!ctx || !pool_M || !pool_com || !pool_mon || !pool_is_leaf || !item || !mon)
+        return fail(OTFMM_ERR_INVALID, "NULL argument");
+    const otfmm_work_item& w = *item;
+    if (w.kind < 0 || w.kind > 2 || w.subgrid < 0 || w.subgrid >= n_subgrids)
+        return fail(OTFMM_ERR_INVALID, "work item out of range");
+    for (int d = 0; d < 26; ++d)
+        if (w.neighbors[d] < -1 || w.neighbors[d] >= n_subgrids) return fail(OTFMM_ERR_INVALID, "neighbour out of range");
+    if (w.kind != OTFMM_KIND_LEAF && (!M || !com)) return fail(OTFMM_ERR_INVALID, "M / com NULL for a multipole item");
+    DeviceGuard g(ctx->device);
+    stage_soa_kernel<<<(CL + 255) / 256, 256, 0, (cudaStream_t)stream>>>(pool_M, pool_com, pool_mon, pool_is_leaf, w,
+                                                                         mon, M, com);
+    OT_CUDA(cudaGetLastError());
+    return OTFMM_OK;
+}
+
+int otfmm_stage_p2m_soa(otfmm_context* ctx, const double* pool_M, const double* pool_com, int32_t n_subgrids,
+                        int32_t neighbor, int d, double* neighbor_M, double* neighbor_com, int32_t* stride,
+                        void* stream) {
+    if (!ctx || !pool_M || !pool_com || !neighbor_M || !neighbor_com) return fail(OTFMM_ERR_INVALID, "NULL argument");
+    if (d < 0 || d >= 26) return fail(OTFMM_ERR_INVALID, "direction out of range");
+    if (neighbor < 0 || neighbor >= n_subgrids) return fail(OTFMM_ERR_INVALID, "neighbour out of range");
+    const int r = d < 13 ? d : d + 1;
+    int size = 1;
+    for (int a = 0; a < 3; ++a) size *= ((r / (a == 0 ? 1 : a == 1 ? 3 : 9)) % 3 == 1) ? INX : SMAX;
+    if (stride) *stride = size + 19;
+    DeviceGuard g(ctx->device);
+    stage_p2m_kernel<<<(size + 19 + 127) / 128, 128, 0, (cudaStream_t)stream>>>(pool_M, pool_com, neighbor, d,
+                                                                                 neighbor_M, neighbor_com);
     OT_CUDA(cudaGetLastError());
     return OTFMM_OK;
 }

@@ -25,7 +25,7 @@ PRECISIONS = {"fp64_exact": FP64_EXACT, "fp64": FP64, "fp32_split": FP32_SPLIT}
 
 EXPORTED = ["otfmm_create", "otfmm_destroy", "otfmm_stencil_info", "otfmm_m2l_soa", "otfmm_m2l_soa_host",
             "otfmm_p2p_soa", "otfmm_p2m_soa", "otfmm_batch", "otfmm_batch_status", "otfmm_count_pairs",
-            "otfmm_m2l_soa_host_noalloc", "otfmm_last_error",
+            "otfmm_m2l_soa_host_noalloc", "otfmm_stage_soa", "otfmm_stage_p2m_soa", "otfmm_last_error",
             "otfmm_build_info", "otfmm_measure_fma_peaks"]
 
 _lib = None
@@ -55,6 +55,9 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
         lib.otfmm_p2m_soa.argtypes = [vp, i, vp, vp, vp, vp, vp, i, i, i, vp]
         lib.otfmm_batch.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int32, vp, ctypes.c_int32, vp, vp, i, i, vp]
         lib.otfmm_batch_status.argtypes = [vp, vp]
+        lib.otfmm_stage_soa.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int32, vp, vp, vp, vp, vp]
+        lib.otfmm_stage_p2m_soa.argtypes = [vp, vp, vp, ctypes.c_int32, ctypes.c_int32, i, vp, vp,
+                                            ctypes.POINTER(ctypes.c_int32), vp]
         lib.otfmm_count_pairs.argtypes = [vp, vp, ctypes.c_int32, vp, ctypes.c_int32, vp]
         lib.otfmm_count_pairs.restype = ctypes.c_longlong
         lib.otfmm_last_error.restype = ctypes.c_char_p
@@ -175,6 +178,22 @@ class Context:
                                             _ptr(Lc), int(gsolve_type), int(bool(reset_lc)),
                                             precision_code(precision), _stream(stream)))
 
+    def stage_soa(self, dev: "DevicePool", item: np.ndarray, mon, M=None, com=None, stream=None) -> None:
+        """Device-side update_input of one work item (numpy record) from a
+        resident pool into the reference's SoA buffers (device tensors)."""
+        it = np.ascontiguousarray(np.asarray(item).reshape(1))
+        _check(load_library().otfmm_stage_soa(self.handle, _ptr(dev.M), _ptr(dev.com), _ptr(dev.mon),
+                                              _ptr(dev.is_leaf), ctypes.c_int32(dev.n), it.ctypes.data, _ptr(mon),
+                                              _ptr(M), _ptr(com), _stream(stream)))
+
+    def stage_p2m_soa(self, dev: "DevicePool", neighbor: int, d: int, nM, ncom, stream=None) -> int:
+        """Refined neighbour slab for otfmm_p2m_soa; returns its component stride."""
+        stride = ctypes.c_int32()
+        _check(load_library().otfmm_stage_p2m_soa(self.handle, _ptr(dev.M), _ptr(dev.com), ctypes.c_int32(dev.n),
+                                                  ctypes.c_int32(int(neighbor)), int(d), _ptr(nM), _ptr(ncom),
+                                                  ctypes.byref(stride), _stream(stream)))
+        return stride.value
+
     # ---------------------------------------------------------------- batched
     def batch(self, dev: "DevicePool", items_dev, n_items: int, L, Lc, gsolve_type=RHO, precision=FP64,
               stream=None):
@@ -251,6 +270,112 @@ class BatchSolver:
     def results(self):
         self.ctx.batch_status()
         return self.L.cpu().numpy(), self.Lc.cpu().numpy()
+
+
+P2M_SLAB_STRIDE_MAX = 8 * 8 * 5 + 19
+
+
+class PerSubgridSolver:
+    """The reference's call pattern on the GPU: one call of the per-subgrid
+    entry points per node (multipole_kernel_interface -> otfmm_m2l_soa for
+    refined nodes; monopole_kernel_interface -> otfmm_p2p_soa, then
+    otfmm_p2m_soa per refined neighbour, for leaves), launched round-robin
+    over a pool of streams like the reference's stream pool. The halo buffers
+    are staged on the device once at construction (otfmm_stage_soa), so run()
+    times the kernels and their launches only."""
+
+    def __init__(self, ctx: Context, pool: SubgridPool, items: np.ndarray, n_streams: int = 32):
+        torch = _require_cuda()
+        self.ctx = ctx
+        self.dev = DevicePool.upload(pool, ctx.device)
+        d = torch.device("cuda", ctx.device)
+        items = np.ascontiguousarray(items)
+        validate_work_list(items, pool.n)
+        self.items = items
+        kinds = items["kind"]
+        self.mpole = np.nonzero(kinds != 2)[0]
+        self.leaves = np.nonzero(kinds == 2)[0]
+        nm, nl = len(self.mpole), len(self.leaves)
+        f64 = dict(dtype=torch.float64, device=d)
+        self.m_mon = torch.zeros((nm, ENTRIES), **f64)
+        self.m_M = torch.zeros((nm, 20 * COMPONENT_LENGTH), **f64)
+        self.m_com = torch.zeros((nm, 3 * COMPONENT_LENGTH), **f64)
+        self.m_L = torch.zeros((nm, 20 * COMPONENT_LENGTH_UNPADDED), **f64)
+        self.m_Lc = torch.zeros((nm, 3 * COMPONENT_LENGTH_UNPADDED), **f64)
+        self.l_mon = torch.zeros((nl, ENTRIES), **f64)
+        self.l_icom = torch.zeros((nl, 3, COMPONENT_LENGTH_UNPADDED), **f64)
+        self.l_L4 = torch.zeros((nl, 4 * COMPONENT_LENGTH_UNPADDED), **f64)
+        self.l_Lc = torch.zeros((nl, 3 * COMPONENT_LENGTH_UNPADDED), **f64)
+        self.p2m = []   # (leaf slot, direction, slab index)
+        for k, i in enumerate(self.leaves):
+            nbs = items[i]["neighbors"]
+            for dd in range(26):
+                nb = int(nbs[dd])
+                if nb >= 0 and not pool.is_leaf[nb]:
+                    self.p2m.append((k, dd, nb))
+        ns = max(1, len(self.p2m))
+        self.s_M = torch.zeros((ns, 20 * P2M_SLAB_STRIDE_MAX), **f64)
+        self.s_com = torch.zeros((ns, 3 * P2M_SLAB_STRIDE_MAX), **f64)
+        for k, i in enumerate(self.mpole):
+            ctx.stage_soa(self.dev, items[i], self.m_mon[k], self.m_M[k], self.m_com[k])
+        for k, i in enumerate(self.leaves):
+            ctx.stage_soa(self.dev, items[i], self.l_mon[k])
+            self.l_icom[k, :, :NCELL] = self.dev.com[int(items[i]["subgrid"])]
+        self.p2m_by_leaf = [[] for _ in range(nl)]
+        for j, (k, dd, nb) in enumerate(self.p2m):
+            ctx.stage_p2m_soa(self.dev, nb, dd, self.s_M[j], self.s_com[j])
+            self.p2m_by_leaf[k].append((j, dd))
+        self.streams = [torch.cuda.Stream(device=d) for _ in range(n_streams)]
+        torch.cuda.synchronize(d)
+
+    def run(self, gsolve_type=RHO, precision=FP64) -> None:
+        """Every node's calls, round-robin over the stream pool; the calling
+        stream waits for all of them."""
+        torch = _require_cuda()
+        main = torch.cuda.current_stream()
+        start = torch.cuda.Event()
+        start.record(main)
+        for st in self.streams:
+            st.wait_event(start)
+        ns = len(self.streams)
+        for k, i in enumerate(self.mpole):
+            root = int(self.items[i]["kind"]) == 1
+            self.ctx.m2l_soa(None if root else self.m_mon[k], self.m_M[k], self.m_com[k], self.m_L[k], self.m_Lc[k],
+                             gsolve_type, root, precision, self.streams[k % ns])
+        off = len(self.mpole)
+        for k, i in enumerate(self.leaves):
+            st = self.streams[(off + k) % ns]
+            self.ctx.p2p_soa(self.l_mon[k], float(self.items[i]["dx"]), self.l_L4[k], precision, st)
+            first = True
+            for j, dd in self.p2m_by_leaf[k]:
+                self.ctx.p2m_soa(dd, self.s_M[j], self.s_com[j], self.l_icom[k], self.l_L4[k], self.l_Lc[k],
+                                 gsolve_type, first, precision, st)
+                first = False
+        for st in self.streams:
+            ev = torch.cuda.Event()
+            ev.record(st)
+            main.wait_event(ev)
+
+    @property
+    def n_launches(self) -> int:
+        return len(self.mpole) + len(self.leaves) + len(self.p2m)
+
+    def results(self):
+        """L [n, 20, 512] and L_c [n, 3, 512] per subgrid, as the batched path writes them."""
+        n = self.dev.n
+        L = np.zeros((n, 20, NCELL))
+        Lc = np.zeros((n, 3, NCELL))
+        mL = self.m_L.cpu().numpy().reshape(-1, 20, COMPONENT_LENGTH_UNPADDED)[:, :, :NCELL]
+        mLc = self.m_Lc.cpu().numpy().reshape(-1, 3, COMPONENT_LENGTH_UNPADDED)[:, :, :NCELL]
+        sub = self.items["subgrid"]
+        L[sub[self.mpole]] = mL
+        Lc[sub[self.mpole]] = mLc
+        l4 = self.l_L4.cpu().numpy().reshape(-1, 4, COMPONENT_LENGTH_UNPADDED)[:, :, :NCELL]
+        lc = self.l_Lc.cpu().numpy().reshape(-1, 3, COMPONENT_LENGTH_UNPADDED)[:, :, :NCELL]
+        L[sub[self.leaves], :4] = l4
+        has_p2m = np.array([len(x) > 0 for x in self.p2m_by_leaf], dtype=bool)
+        Lc[sub[self.leaves][has_p2m]] = lc[has_p2m]
+        return L, Lc
 
 
 def build_info() -> str:
