@@ -238,9 +238,22 @@ def gpu_arm(args) -> None:
     stream = torch.cuda.current_stream()
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
 
-    def timed_steps(precision: str, steps: int, warmup: int):
+    # every precision is autotuned on this work list, then captured into a
+    # CUDA graph (otfmm_plan) and replayed: the production path of a solve
+    tunings, tuned, plans = {}, {}, {}
+
+    def prepare(precision: str):
+        if precision not in plans:
+            tuned[precision] = solver.autotune(solve, precision, repeats=3)
+            tunings[precision] = tuned[precision].as_dict()
+            plans[precision] = solver.plan(solve, precision)
+        return plans[precision]
+
+    def timed_steps(precision: str, steps: int, warmup: int, graph: bool = True):
+        plan = prepare(precision)
+        step = plan.launch if graph else (lambda: solver.run(solve, precision))
         for _ in range(warmup):
-            solver.run(solve, precision)
+            step()
         torch.cuda.synchronize()
         total_ms, per = 0.0, []
         for _ in range(steps):
@@ -248,16 +261,18 @@ def gpu_arm(args) -> None:
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            solver.run(solve, precision)
+            step()
             e1.record(stream)
             e1.synchronize()
             ms = e0.elapsed_time(e1)
             per.append(ms)
             total_ms += ms
+        plan.status()
         solver.ctx.batch_status()
         return total_ms, per
 
     # device-resident timing of the headline precision, clocks sampled meanwhile
+    prepare(args.precision)
     if pg:
         pg.barrier()
     torch.cuda.synchronize()
@@ -268,6 +283,8 @@ def gpu_arm(args) -> None:
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         total_ms = float(t.item())
     value = world * counts["total"] * args.steps / (total_ms * 1e-3)
+    direct_ms, _ = timed_steps(args.precision, max(3, args.steps // 2), 3, graph=False)
+    direct_ms /= max(3, args.steps // 2)
 
     # the other precisions on the same workload (device-resident, same method)
     others = {}
@@ -312,7 +329,7 @@ def gpu_arm(args) -> None:
     if args.precision != "fp64_exact":
         solver.run(solve, "fp64_exact")
         Le, Lce = solver.L.clone(), solver.Lc.clone()
-        solver.run(solve, args.precision)
+        plans[args.precision].launch()
         torch.cuda.synchronize()
         accuracy = accuracy_report(solver.L, solver.Lc, Le, Lce)
 
@@ -339,6 +356,7 @@ def gpu_arm(args) -> None:
         L_pin.copy_(solver.L, non_blocking=True)
         Lc_pin.copy_(solver.Lc, non_blocking=True)
 
+    ctx.set_tuning(tuned[args.precision])
     for _ in range(args.warmup):
         e2e_step()
     torch.cuda.synchronize()
@@ -383,8 +401,12 @@ def gpu_arm(args) -> None:
                    "pairs_p2m": counts["p2m"],
                    "theta": batch.theta, "gsolve": args.gsolve, "precision": args.precision,
                    "l2": "flushed (256 MiB write) before every timed step",
+                   "launch": "one CUDA graph replay per step (otfmm_plan: classify + 3 persistent kernels)",
+                   "tuning": tunings.get(args.precision),
                    "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU"},
         "precisions": others,
+        "direct_launch_ms_per_step": direct_ms,
+        "tunings": tunings,
         "per_subgrid_fp64": per_subgrid,
         "ratios": {"vs_batched_fp64": (value / world / others["fp64"]["value"]) if "fp64" in others else None,
                    "vs_per_subgrid_fp64": (value / world / per_subgrid["value"]) if per_subgrid else None},

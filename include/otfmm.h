@@ -187,6 +187,46 @@ int otfmm_batch(otfmm_context* ctx, const double* pool_M, const double* pool_com
                 const uint8_t* pool_is_leaf, int32_t n_subgrids, const otfmm_work_item* items, int32_t n_items,
                 double* L, double* L_c, int gsolve_type, int precision, void* stream);
 
+/* Kernel variants of the batched solve. Every variant computes the same
+ * interactions within its precision's tolerance; they differ in speed only.
+ * No counterpart in the reference (its kernels have fixed launch shapes). */
+#define OTFMM_SPLIT_WARP_SPECIALISED 0 /* FP32-split RHO tiles: FP32 contraction warps + FP64 L_c warps */
+#define OTFMM_SPLIT_SINGLE_ROLE 1      /* FP32-split RHO tiles: every warp does both */
+typedef struct otfmm_tuning {
+    int32_t split_m2l_form;  /* OTFMM_SPLIT_WARP_SPECIALISED or OTFMM_SPLIT_SINGLE_ROLE */
+    int32_t split_m2l_chunk; /* FP32 partial sums of the warp-specialised tiles promoted every 8 or 16 partners */
+    int32_t split_p2p_chunk; /* FP32 P2P partial sums promoted every 16 or 32 partners */
+    int32_t p2m_lanes;       /* fast-form P2M: at most 4, 8 or 16 lanes share one cell's entries */
+} otfmm_tuning;
+
+/* The context's current variants (defaults: warp-specialised, 16, 32, 16). */
+int otfmm_get_tuning(const otfmm_context* ctx, otfmm_tuning* out);
+int otfmm_set_tuning(otfmm_context* ctx, const otfmm_tuning* t);
+
+/* Autotuner: times the variants on the caller's own batch (same arguments as
+ * otfmm_batch; L and L_c are overwritten) by coordinate descent, median of
+ * `repeats` solves per candidate, keeps the fastest in the context and
+ * returns it in *chosen (may be NULL). Synchronises the stream. */
+int otfmm_autotune(otfmm_context* ctx, const double* pool_M, const double* pool_com, const double* pool_mon,
+                   const uint8_t* pool_is_leaf, int32_t n_subgrids, const otfmm_work_item* items, int32_t n_items,
+                   double* L, double* L_c, int gsolve_type, int precision, int repeats, otfmm_tuning* chosen,
+                   void* stream);
+
+/* A batched solve captured once into a CUDA graph (the counter resets, the
+ * classification and the three persistent launches of otfmm_batch with the
+ * context's variants at creation), replayed by otfmm_plan_launch with one
+ * graph launch. The plan binds the given device pointers and owns its own
+ * work-list storage and error flag, so plans of one context may run
+ * concurrently when their outputs are disjoint; otfmm_plan_status reads the
+ * flag of the last launch. No counterpart in the reference. */
+typedef struct otfmm_plan otfmm_plan;
+int otfmm_plan_create(otfmm_context* ctx, const double* pool_M, const double* pool_com, const double* pool_mon,
+                      const uint8_t* pool_is_leaf, int32_t n_subgrids, const otfmm_work_item* items, int32_t n_items,
+                      double* L, double* L_c, int gsolve_type, int precision, otfmm_plan** out);
+int otfmm_plan_launch(otfmm_plan* plan, void* stream);
+int otfmm_plan_status(otfmm_plan* plan, void* stream);
+int otfmm_plan_destroy(otfmm_plan* plan);
+
 /* Cell-interactions a work list evaluates (host-side count, no device
  * work): the (cell, partner) pairs that pass the stencil and coarse-distance
  * masks, which is what the reference's kernels evaluate. per_class (may be

@@ -836,6 +836,7 @@ struct BatchArgs {
     Tables t;
     int* err;
     WorkLists wl;
+    int p2m_lanes;   // fast-form P2M: at most this many lanes share one cell's entries (1..16, power of two)
 };
 
 __device__ __forceinline__ bool item_valid(const BatchArgs& a, const otfmm_work_item& w) {
@@ -1279,7 +1280,7 @@ __global__ void __launch_bounds__(P_THREADS) p2m_batch_kernel(BatchArgs a) {
             // the exact form keeps one lane per cell and the stencil order
             int F = 1;
             if (P64 != PREC_EXACT)
-                while (F < 16 && nt * 2 * F <= (int)blockDim.x) F <<= 1;
+                while (F < a.p2m_lanes && nt * 2 * F <= (int)blockDim.x) F <<= 1;
             const int tgt = threadIdx.x / F, f = threadIdx.x % F;
             const bool active = tgt < nt;
             const int cu = active ? __ldg(a.t.p2m_perm + t0 + tgt) : 0;
@@ -1692,6 +1693,7 @@ struct otfmm_context {
     double* d_soa_scratch = nullptr;   // host-buffer path staging
     int* d_lists = nullptr;            // batched work lists (grown on demand)
     int list_capacity = 0;
+    otfmm_tuning tuning = {OTFMM_SPLIT_WARP_SPECIALISED, 16, 32, 16};
     std::mutex mu;
     Tables tables() const { return Tables{d_entries,    d_count, d_entries_fast, d_count_far, d_entries_split, d_entries_p2p,
                       d_entries_ws, d_four,  d_phase,        d_p2m_start,     d_p2m_list,    d_p2m_perm_start,
@@ -1741,6 +1743,7 @@ int ensure_attributes(int device) {
     rc = rc ? rc : set_smem(p2p_batch_kernel<PREC_FAST>, P2P_SMEM_BYTES);
     rc = rc ? rc : set_smem(p2p_leaf_kernel<double, 0>, p2_smem_bytes<double>());
     rc = rc ? rc : set_smem(p2p_leaf_kernel<float, 32>, p2_smem_bytes<float>());
+    rc = rc ? rc : set_smem(p2p_leaf_kernel<float, 16>, p2_smem_bytes<float>());
     rc = rc ? rc : set_smem(soa_m2l_kernel<PREC_EXACT, true, false>, bytes);
     rc = rc ? rc : set_smem(soa_m2l_kernel<PREC_EXACT, false, false>, bytes);
     rc = rc ? rc : set_smem(soa_m2l_kernel<PREC_FAST, true, false>, bytes);
@@ -2129,38 +2132,42 @@ int otfmm_stage_p2m_soa(otfmm_context* ctx, const double* pool_M, const double* 
     return OTFMM_OK;
 }
 
-int otfmm_batch(otfmm_context* ctx, const double* pool_M, const double* pool_com, const double* pool_mon,
-                const uint8_t* pool_is_leaf, int32_t n_subgrids, const otfmm_work_item* items, int32_t n_items,
-                double* L, double* L_c, int gsolve_type, int precision, void* stream) {
+}   // extern "C"
+
+namespace {
+
+int check_tuning(const otfmm_tuning& t) {
+    if (t.split_m2l_form != OTFMM_SPLIT_WARP_SPECIALISED && t.split_m2l_form != OTFMM_SPLIT_SINGLE_ROLE)
+        return fail(OTFMM_ERR_INVALID, "unknown split M2L form");
+    if (t.split_m2l_chunk != 8 && t.split_m2l_chunk != 16) return fail(OTFMM_ERR_INVALID, "split M2L chunk must be 8 or 16");
+    if (t.split_p2p_chunk != 16 && t.split_p2p_chunk != 32) return fail(OTFMM_ERR_INVALID, "split P2P chunk must be 16 or 32");
+    if (t.p2m_lanes != 4 && t.p2m_lanes != 8 && t.p2m_lanes != 16) return fail(OTFMM_ERR_INVALID, "P2M lanes must be 4, 8 or 16");
+    return OTFMM_OK;
+}
+
+int check_batch_args(otfmm_context* ctx, const double* pool_M, const double* pool_com, const double* pool_mon,
+                     const uint8_t* pool_is_leaf, int32_t n_subgrids, const otfmm_work_item* items, int32_t n_items,
+                     double* L, double* L_c, int gsolve_type, int precision) {
     if (!ctx || !pool_M || !pool_com || !pool_mon || !pool_is_leaf || !items || !L || !L_c)
         return fail(OTFMM_ERR_INVALID, "NULL argument");
     if (n_subgrids <= 0 || n_items < 0 || n_items > (1 << 29)) return fail(OTFMM_ERR_INVALID, "bad sizes");
     if (gsolve_type != OTFMM_RHO && gsolve_type != OTFMM_DRHODT) return fail(OTFMM_ERR_INVALID, "bad gsolve_type");
-    int rc = check_precision(precision, true);
-    if (rc) return rc;
-    if (n_items == 0) return OTFMM_OK;
-    DeviceGuard g(ctx->device);
-    cudaStream_t s = (cudaStream_t)stream;
-    {
-        // work-list storage: 4 lists of n_items + counters; grown (reallocated)
-        // only when a larger work list arrives, serialised per context
-        std::lock_guard<std::mutex> lock(ctx->mu);
-        if (n_items > ctx->list_capacity) {
-            OT_CUDA(cudaStreamSynchronize(s));
-            cudaFree(ctx->d_lists);
-            ctx->d_lists = nullptr;
-            const int cap = std::max(n_items, 2 * ctx->list_capacity);
-            OT_CUDA(cudaMalloc(&ctx->d_lists, sizeof(int) * (4 * (size_t)cap + WL_COUNTERS)));
-            ctx->list_capacity = cap;
-        }
-    }
-    const int cap = ctx->list_capacity;
-    WorkLists wl{ctx->d_lists, ctx->d_lists + cap, ctx->d_lists + 2 * (size_t)cap, ctx->d_lists + 3 * (size_t)cap,
-                 ctx->d_lists + 4 * (size_t)cap};
-    OT_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), s));
+    return check_precision(precision, true);
+}
+
+// Enqueues one batched solve on `s`: counter resets, classification into the
+// device work lists `lists` (capacity `cap` items), then the persistent
+// multipole, P2P and P2M launches with the variants of `tu`. Only stream
+// operations: safe inside a stream capture.
+int enqueue_batch(otfmm_context* ctx, const double* pool_M, const double* pool_com, const double* pool_mon,
+                  const uint8_t* pool_is_leaf, int32_t n_subgrids, const otfmm_work_item* items, int32_t n_items,
+                  double* L, double* L_c, int gsolve_type, int precision, int* lists, int cap, int* err,
+                  const otfmm_tuning& tu, cudaStream_t s) {
+    WorkLists wl{lists, lists + cap, lists + 2 * (size_t)cap, lists + 3 * (size_t)cap, lists + 4 * (size_t)cap};
+    OT_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
     OT_CUDA(cudaMemsetAsync(wl.counts, 0, sizeof(int) * WL_COUNTERS, s));
     BatchArgs a{pool_M, pool_com, pool_mon, pool_is_leaf, n_subgrids, items, n_items, L, L_c, ctx->tables(),
-                ctx->d_err, wl};
+                err, wl, tu.p2m_lanes};
     const size_t bytes = SMEM_DOUBLES * sizeof(double);
     const bool rho = (gsolve_type == OTFMM_RHO);
     int sms = 148;
@@ -2178,20 +2185,215 @@ int otfmm_batch(otfmm_context* ctx, const double* pool_M, const double* pool_com
     } else {
         if (precision == OTFMM_FP32_SPLIT) {
             const size_t sbytes = S_SMEM_DOUBLES * sizeof(double);
-            if (rho) m2l_split_ws_kernel<16><<<tiles_grid, WS_THREADS, WS_SMEM_BYTES, s>>>(a);
-            else m2l_batch_kernel<PREC_SPLIT, false><<<tiles_grid, THREADS, sbytes, s>>>(a);
+            if (rho && tu.split_m2l_form == OTFMM_SPLIT_WARP_SPECIALISED) {
+                if (tu.split_m2l_chunk == 8) m2l_split_ws_kernel<8><<<tiles_grid, WS_THREADS, WS_SMEM_BYTES, s>>>(a);
+                else m2l_split_ws_kernel<16><<<tiles_grid, WS_THREADS, WS_SMEM_BYTES, s>>>(a);
+            } else if (rho) {
+                m2l_batch_kernel<PREC_SPLIT, true><<<tiles_grid, THREADS, sbytes, s>>>(a);
+            } else {
+                m2l_batch_kernel<PREC_SPLIT, false><<<tiles_grid, THREADS, sbytes, s>>>(a);
+            }
+            if (tu.split_p2p_chunk == 16) p2p_leaf_kernel<float, 16><<<sms, P2_THREADS, p2_smem_bytes<float>(), s>>>(a);
+            else p2p_leaf_kernel<float, 32><<<sms, P2_THREADS, p2_smem_bytes<float>(), s>>>(a);
         } else {
             if (rho) m2l_batch_kernel<PREC_FAST, true><<<tiles_grid, THREADS, bytes, s>>>(a);
             else m2l_batch_kernel<PREC_FAST, false><<<tiles_grid, THREADS, bytes, s>>>(a);
-        }
-        if (precision == OTFMM_FP32_SPLIT)
-            p2p_leaf_kernel<float, 32><<<sms, P2_THREADS, p2_smem_bytes<float>(), s>>>(a);
-        else
             p2p_leaf_kernel<double, 0><<<sms, P2_THREADS, p2_smem_bytes<double>(), s>>>(a);
+        }
         if (rho) p2m_batch_kernel<PREC_FAST, true><<<p2m_grid, P_THREADS, 0, s>>>(a);
         else p2m_batch_kernel<PREC_FAST, false><<<p2m_grid, P_THREADS, 0, s>>>(a);
     }
     OT_CUDA(cudaGetLastError());
+    return OTFMM_OK;
+}
+
+// Grows the context's work-list storage to hold n_items (a device allocation,
+// after the stream's earlier work is done).
+int ensure_list_capacity(otfmm_context* ctx, int32_t n_items, cudaStream_t s) {
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    if (n_items <= ctx->list_capacity) return OTFMM_OK;
+    OT_CUDA(cudaStreamSynchronize(s));
+    cudaFree(ctx->d_lists);
+    ctx->d_lists = nullptr;
+    const int cap = std::max(n_items, 2 * ctx->list_capacity);
+    OT_CUDA(cudaMalloc(&ctx->d_lists, sizeof(int) * (4 * (size_t)cap + WL_COUNTERS)));
+    ctx->list_capacity = cap;
+    return OTFMM_OK;
+}
+
+}   // namespace
+
+struct otfmm_plan {
+    otfmm_context* ctx = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int* lists = nullptr;
+    int* err = nullptr;
+};
+
+extern "C" {
+
+int otfmm_batch(otfmm_context* ctx, const double* pool_M, const double* pool_com, const double* pool_mon,
+                const uint8_t* pool_is_leaf, int32_t n_subgrids, const otfmm_work_item* items, int32_t n_items,
+                double* L, double* L_c, int gsolve_type, int precision, void* stream) {
+    int rc = check_batch_args(ctx, pool_M, pool_com, pool_mon, pool_is_leaf, n_subgrids, items, n_items, L, L_c,
+                              gsolve_type, precision);
+    if (rc) return rc;
+    if (n_items == 0) return OTFMM_OK;
+    DeviceGuard g(ctx->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    rc = ensure_list_capacity(ctx, n_items, s);
+    if (rc) return rc;
+    return enqueue_batch(ctx, pool_M, pool_com, pool_mon, pool_is_leaf, n_subgrids, items, n_items, L, L_c,
+                         gsolve_type, precision, ctx->d_lists, ctx->list_capacity, ctx->d_err, ctx->tuning, s);
+}
+
+int otfmm_get_tuning(const otfmm_context* ctx, otfmm_tuning* out) {
+    if (!ctx || !out) return fail(OTFMM_ERR_INVALID, "NULL argument");
+    *out = ctx->tuning;
+    return OTFMM_OK;
+}
+
+int otfmm_set_tuning(otfmm_context* ctx, const otfmm_tuning* t) {
+    if (!ctx || !t) return fail(OTFMM_ERR_INVALID, "NULL argument");
+    const int rc = check_tuning(*t);
+    if (rc) return rc;
+    ctx->tuning = *t;
+    return OTFMM_OK;
+}
+
+int otfmm_plan_create(otfmm_context* ctx, const double* pool_M, const double* pool_com, const double* pool_mon,
+                      const uint8_t* pool_is_leaf, int32_t n_subgrids, const otfmm_work_item* items, int32_t n_items,
+                      double* L, double* L_c, int gsolve_type, int precision, otfmm_plan** out) {
+    if (!out) return fail(OTFMM_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    int rc = check_batch_args(ctx, pool_M, pool_com, pool_mon, pool_is_leaf, n_subgrids, items, n_items, L, L_c,
+                              gsolve_type, precision);
+    if (rc) return rc;
+    if (n_items == 0) return fail(OTFMM_ERR_INVALID, "empty work list");
+    DeviceGuard g(ctx->device);
+    auto* plan = new otfmm_plan();
+    plan->ctx = ctx;
+    cudaStream_t cs = nullptr;
+    cudaError_t e;
+    if ((e = cudaMalloc(&plan->lists, sizeof(int) * (4 * (size_t)n_items + WL_COUNTERS))) != cudaSuccess ||
+        (e = cudaMalloc(&plan->err, sizeof(int))) != cudaSuccess ||
+        (e = cudaMemset(plan->err, 0, sizeof(int))) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) {
+        if (cs) cudaStreamDestroy(cs);
+        otfmm_plan_destroy(plan);
+        return cuda_fail(e, "otfmm_plan_create");
+    }
+    rc = enqueue_batch(ctx, pool_M, pool_com, pool_mon, pool_is_leaf, n_subgrids, items, n_items, L, L_c,
+                       gsolve_type, precision, plan->lists, n_items, plan->err, ctx->tuning, cs);
+    cudaGraph_t graph = nullptr;
+    e = cudaStreamEndCapture(cs, &graph);
+    cudaStreamDestroy(cs);
+    plan->graph = graph;
+    if (rc == OTFMM_OK && e != cudaSuccess) rc = cuda_fail(e, "cudaStreamEndCapture");
+    if (rc == OTFMM_OK && (e = cudaGraphInstantiate(&plan->exec, plan->graph, 0)) != cudaSuccess)
+        rc = cuda_fail(e, "cudaGraphInstantiate");
+    if (rc != OTFMM_OK) {
+        const std::string msg = g_last_error;
+        otfmm_plan_destroy(plan);
+        return fail(rc, msg);
+    }
+    *out = plan;
+    return OTFMM_OK;
+}
+
+int otfmm_plan_launch(otfmm_plan* plan, void* stream) {
+    if (!plan || !plan->exec) return fail(OTFMM_ERR_INVALID, "NULL plan");
+    DeviceGuard g(plan->ctx->device);
+    OT_CUDA(cudaGraphLaunch(plan->exec, (cudaStream_t)stream));
+    return OTFMM_OK;
+}
+
+int otfmm_plan_status(otfmm_plan* plan, void* stream) {
+    if (!plan) return fail(OTFMM_ERR_INVALID, "NULL plan");
+    DeviceGuard g(plan->ctx->device);
+    int h = 0;
+    OT_CUDA(cudaMemcpyAsync(&h, plan->err, sizeof(int), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    OT_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    if (h) return fail(OTFMM_ERR_DEVICE, "a work item failed validation on the device");
+    return OTFMM_OK;
+}
+
+int otfmm_plan_destroy(otfmm_plan* plan) {
+    if (!plan) return OTFMM_OK;
+    DeviceGuard g(plan->ctx->device);
+    if (plan->exec) cudaGraphExecDestroy(plan->exec);
+    if (plan->graph) cudaGraphDestroy(plan->graph);
+    cudaFree(plan->lists);
+    cudaFree(plan->err);
+    delete plan;
+    return OTFMM_OK;
+}
+
+int otfmm_autotune(otfmm_context* ctx, const double* pool_M, const double* pool_com, const double* pool_mon,
+                   const uint8_t* pool_is_leaf, int32_t n_subgrids, const otfmm_work_item* items, int32_t n_items,
+                   double* L, double* L_c, int gsolve_type, int precision, int repeats, otfmm_tuning* chosen,
+                   void* stream) {
+    int rc = check_batch_args(ctx, pool_M, pool_com, pool_mon, pool_is_leaf, n_subgrids, items, n_items, L, L_c,
+                              gsolve_type, precision);
+    if (rc) return rc;
+    if (n_items == 0 || repeats < 1) return fail(OTFMM_ERR_INVALID, "empty work list or repeats < 1");
+    DeviceGuard g(ctx->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    rc = ensure_list_capacity(ctx, n_items, s);
+    if (rc) return rc;
+    cudaEvent_t e0, e1;
+    OT_CUDA(cudaEventCreate(&e0));
+    OT_CUDA(cudaEventCreate(&e1));
+    // median of `repeats` timed solves after one warm-up
+    auto time_of = [&](const otfmm_tuning& tu, float& med) -> int {
+        std::vector<float> ts;
+        for (int r = 0; r <= repeats; ++r) {
+            OT_CUDA(cudaEventRecord(e0, s));
+            int rc2 = enqueue_batch(ctx, pool_M, pool_com, pool_mon, pool_is_leaf, n_subgrids, items, n_items, L,
+                                    L_c, gsolve_type, precision, ctx->d_lists, ctx->list_capacity, ctx->d_err, tu, s);
+            if (rc2) return rc2;
+            OT_CUDA(cudaEventRecord(e1, s));
+            OT_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            OT_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            if (r > 0) ts.push_back(ms);
+        }
+        std::sort(ts.begin(), ts.end());
+        med = ts[ts.size() / 2];
+        return OTFMM_OK;
+    };
+    // coordinate descent over the variant dimensions, starting from the current choice
+    otfmm_tuning best = ctx->tuning;
+    float tbest = 0.f;
+    rc = time_of(best, tbest);
+    const int forms[2] = {OTFMM_SPLIT_WARP_SPECIALISED, OTFMM_SPLIT_SINGLE_ROLE};
+    const int m2l_chunks[2] = {8, 16}, p2p_chunks[2] = {16, 32}, lanes[3] = {4, 8, 16};
+    const bool split = (precision == OTFMM_FP32_SPLIT), fast = (precision != OTFMM_FP64_EXACT);
+    for (int dim = 0; dim < 4 && rc == OTFMM_OK; ++dim) {
+        const int nvar = (dim == 3) ? 3 : 2;
+        if ((dim < 3 && !split) || (dim == 3 && !fast)) continue;
+        for (int v = 0; v < nvar && rc == OTFMM_OK; ++v) {
+            otfmm_tuning tu = best;
+            if (dim == 0) tu.split_m2l_form = forms[v];
+            if (dim == 1) tu.split_m2l_chunk = m2l_chunks[v];
+            if (dim == 2) tu.split_p2p_chunk = p2p_chunks[v];
+            if (dim == 3) tu.p2m_lanes = lanes[v];
+            if (std::memcmp(&tu, &best, sizeof tu) == 0) continue;
+            float t = 0.f;
+            rc = time_of(tu, t);
+            if (rc == OTFMM_OK && t < tbest) {
+                tbest = t;
+                best = tu;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    ctx->tuning = best;
+    if (chosen) *chosen = best;
     return OTFMM_OK;
 }
 

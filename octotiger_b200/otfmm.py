@@ -25,10 +25,25 @@ PRECISIONS = {"fp64_exact": FP64_EXACT, "fp64": FP64, "fp32_split": FP32_SPLIT}
 
 EXPORTED = ["otfmm_create", "otfmm_destroy", "otfmm_stencil_info", "otfmm_m2l_soa", "otfmm_m2l_soa_host",
             "otfmm_p2p_soa", "otfmm_p2m_soa", "otfmm_batch", "otfmm_batch_status", "otfmm_count_pairs",
-            "otfmm_m2l_soa_host_noalloc", "otfmm_stage_soa", "otfmm_stage_p2m_soa", "otfmm_last_error",
+            "otfmm_m2l_soa_host_noalloc", "otfmm_stage_soa", "otfmm_stage_p2m_soa", "otfmm_get_tuning",
+            "otfmm_set_tuning", "otfmm_autotune", "otfmm_plan_create", "otfmm_plan_launch", "otfmm_plan_status",
+            "otfmm_plan_destroy", "otfmm_last_error",
             "otfmm_build_info", "otfmm_measure_fma_peaks"]
 
 _lib = None
+
+SPLIT_WARP_SPECIALISED, SPLIT_SINGLE_ROLE = 0, 1
+
+
+class Tuning(ctypes.Structure):
+    """otfmm_tuning: the kernel variants of the batched solve."""
+    _fields_ = [("split_m2l_form", ctypes.c_int32), ("split_m2l_chunk", ctypes.c_int32),
+                ("split_p2p_chunk", ctypes.c_int32), ("p2m_lanes", ctypes.c_int32)]
+
+    def as_dict(self) -> dict:
+        return {"split_m2l_form": "warp_specialised" if self.split_m2l_form == 0 else "single_role",
+                "split_m2l_chunk": self.split_m2l_chunk, "split_p2p_chunk": self.split_p2p_chunk,
+                "p2m_lanes": self.p2m_lanes}
 
 
 class OtfmmError(RuntimeError):
@@ -55,6 +70,15 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
         lib.otfmm_p2m_soa.argtypes = [vp, i, vp, vp, vp, vp, vp, i, i, i, vp]
         lib.otfmm_batch.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int32, vp, ctypes.c_int32, vp, vp, i, i, vp]
         lib.otfmm_batch_status.argtypes = [vp, vp]
+        lib.otfmm_get_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]
+        lib.otfmm_set_tuning.argtypes = [vp, ctypes.POINTER(Tuning)]
+        lib.otfmm_autotune.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int32, vp, ctypes.c_int32, vp, vp, i, i, i,
+                                       ctypes.POINTER(Tuning), vp]
+        lib.otfmm_plan_create.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int32, vp, ctypes.c_int32, vp, vp, i, i,
+                                          ctypes.POINTER(vp)]
+        lib.otfmm_plan_launch.argtypes = [vp, vp]
+        lib.otfmm_plan_status.argtypes = [vp, vp]
+        lib.otfmm_plan_destroy.argtypes = [vp]
         lib.otfmm_stage_soa.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int32, vp, vp, vp, vp, vp]
         lib.otfmm_stage_p2m_soa.argtypes = [vp, vp, vp, ctypes.c_int32, ctypes.c_int32, i, vp, vp,
                                             ctypes.POINTER(ctypes.c_int32), vp]
@@ -201,6 +225,25 @@ class Context:
                                           ctypes.c_int32(dev.n), _ptr(items_dev), ctypes.c_int32(n_items), _ptr(L),
                                           _ptr(Lc), int(gsolve_type), precision_code(precision), _stream(stream)))
 
+    def get_tuning(self) -> Tuning:
+        t = Tuning()
+        _check(load_library().otfmm_get_tuning(self.handle, ctypes.byref(t)))
+        return t
+
+    def set_tuning(self, t: Tuning) -> None:
+        _check(load_library().otfmm_set_tuning(self.handle, ctypes.byref(t)))
+
+    def autotune(self, dev: "DevicePool", items_dev, n_items: int, L, Lc, gsolve_type=RHO, precision=FP64,
+                 repeats: int = 3, stream=None) -> Tuning:
+        """Times the kernel variants on this batch and keeps the fastest."""
+        t = Tuning()
+        _check(load_library().otfmm_autotune(self.handle, _ptr(dev.M), _ptr(dev.com), _ptr(dev.mon),
+                                             _ptr(dev.is_leaf), ctypes.c_int32(dev.n), _ptr(items_dev),
+                                             ctypes.c_int32(n_items), _ptr(L), _ptr(Lc), int(gsolve_type),
+                                             precision_code(precision), int(repeats), ctypes.byref(t),
+                                             _stream(stream)))
+        return t
+
     def count_pairs(self, is_leaf: np.ndarray, items: np.ndarray) -> tuple[int, np.ndarray]:
         """Cell-interactions of a work list: total and [M2L, root, P2P, P2M]."""
         per = np.zeros(4, np.int64)
@@ -270,6 +313,45 @@ class BatchSolver:
     def results(self):
         self.ctx.batch_status()
         return self.L.cpu().numpy(), self.Lc.cpu().numpy()
+
+    def autotune(self, gsolve_type=RHO, precision=FP64, repeats: int = 3) -> Tuning:
+        return self.ctx.autotune(self.dev, self.items, self.n_items, self.L, self.Lc, gsolve_type, precision, repeats)
+
+    def plan(self, gsolve_type=RHO, precision=FP64) -> "Plan":
+        """This solve captured into a CUDA graph (see otfmm_plan_create)."""
+        return Plan(self.ctx, self.dev, self.items, self.n_items, self.L, self.Lc, gsolve_type, precision)
+
+
+class Plan:
+    """A batched solve captured into a CUDA graph; launch() replays it."""
+
+    def __init__(self, ctx: Context, dev: DevicePool, items_dev, n_items: int, L, Lc, gsolve_type=RHO,
+                 precision=FP64):
+        self.ctx = ctx
+        self._keep = (dev, items_dev, L, Lc)   # the graph binds these device pointers
+        h = ctypes.c_void_p()
+        _check(load_library().otfmm_plan_create(ctx.handle, _ptr(dev.M), _ptr(dev.com), _ptr(dev.mon),
+                                                _ptr(dev.is_leaf), ctypes.c_int32(dev.n), _ptr(items_dev),
+                                                ctypes.c_int32(n_items), _ptr(L), _ptr(Lc), int(gsolve_type),
+                                                precision_code(precision), ctypes.byref(h)))
+        self.handle = h
+
+    def launch(self, stream=None) -> None:
+        _check(load_library().otfmm_plan_launch(self.handle, _stream(stream)))
+
+    def status(self, stream=None) -> None:
+        _check(load_library().otfmm_plan_status(self.handle, _stream(stream)))
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            load_library().otfmm_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 P2M_SLAB_STRIDE_MAX = 8 * 8 * 5 + 19

@@ -1,0 +1,109 @@
+"""CUDA-graph plans and kernel variants of the batched solve:
+* a plan replays exactly the launches of otfmm_batch (bit-identical results);
+* every variant the autotuner may choose stays within its precision's
+  tolerance against the oracle (FP64 fast: 1e-12; FP32 split: 1e-6 potential
+  and force, 1e-10 L_c);
+* the autotuner returns one of the allowed variants and the context keeps it;
+* invalid variants are rejected."""
+from __future__ import annotations
+
+import itertools
+
+import numpy as np
+import pytest
+
+from octotiger_b200 import synthetic as syn
+from octotiger_b200.layout import DRHODT, RHO
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    from octotiger_b200.otfmm import Context
+    c = Context(0, 0.5)
+    yield c
+    c.close()
+
+
+def amr_small():
+    from octotiger_b200 import amr
+    return amr.polytrope_batch(radius=0.05, max_level=5, seed=71)
+
+
+def scaled(a, ref):
+    num = np.abs(a - ref).max(axis=(0, 2))
+    den = np.abs(ref).max(axis=(0, 2))
+    return np.where(den > 0, num / np.where(den > 0, den, 1), num)
+
+
+@pytest.mark.parametrize("precision", ["fp64_exact", "fp64", "fp32_split"])
+@pytest.mark.parametrize("solve", [RHO, DRHODT])
+def test_plan_replays_batch(ctx, precision, solve):
+    import torch
+    from octotiger_b200.otfmm import BatchSolver
+    b = amr_small()
+    s = BatchSolver(ctx, b.pool, b.items)
+    s.run(solve, precision)
+    L0, Lc0 = s.results()
+    s.L.zero_()
+    s.Lc.zero_()
+    plan = s.plan(solve, precision)
+    for _ in range(2):
+        plan.launch()
+    plan.status()
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(s.L.cpu().numpy(), L0)
+    np.testing.assert_array_equal(s.Lc.cpu().numpy(), Lc0)
+    plan.close()
+
+
+VARIANTS = list(itertools.product([0, 1], [8, 16], [16, 32], [4, 8, 16]))
+
+
+@pytest.mark.parametrize("form,m2l_chunk,p2p_chunk,lanes", VARIANTS)
+def test_every_variant_within_tolerance(ctx, oracle, form, m2l_chunk, p2p_chunk, lanes):
+    from octotiger_b200.otfmm import BatchSolver, Tuning
+    b = amr_small()
+    Lo, Lco = oracle.batch(0.5, b.pool, b.items, rho=True)
+    keep = ctx.get_tuning()
+    try:
+        ctx.set_tuning(Tuning(form, m2l_chunk, p2p_chunk, lanes))
+        s = BatchSolver(ctx, b.pool, b.items)
+        s.run(RHO, "fp32_split")
+        L, Lc = s.results()
+        e = scaled(L, Lo)
+        assert e[:4].max() <= 1e-6 and e[4:].max() <= 1e-5, e
+        assert scaled(Lc, Lco).max() <= 1e-10
+        s.run(RHO, "fp64")
+        L, Lc = s.results()
+        assert scaled(L, Lo).max() <= 1e-12 and scaled(Lc, Lco).max() <= 1e-12
+    finally:
+        ctx.set_tuning(keep)
+
+
+def test_autotune_keeps_an_allowed_variant(ctx, oracle):
+    from octotiger_b200.otfmm import BatchSolver
+    b = amr_small()
+    keep = ctx.get_tuning()
+    try:
+        s = BatchSolver(ctx, b.pool, b.items)
+        t = s.autotune(RHO, "fp32_split", repeats=2)
+        assert (t.split_m2l_form, t.split_m2l_chunk, t.split_p2p_chunk, t.p2m_lanes) in VARIANTS
+        got = ctx.get_tuning()
+        assert got.as_dict() == t.as_dict()
+        s.run(RHO, "fp32_split")
+        L, Lc = s.results()
+        Lo, Lco = oracle.batch(0.5, b.pool, b.items, rho=True)
+        assert scaled(L, Lo)[:4].max() <= 1e-6 and scaled(Lc, Lco).max() <= 1e-10
+    finally:
+        ctx.set_tuning(keep)
+
+
+def test_invalid_variants_rejected(ctx):
+    from octotiger_b200.otfmm import OtfmmError, Tuning
+    keep = ctx.get_tuning()
+    for bad in (Tuning(2, 16, 32, 16), Tuning(0, 12, 32, 16), Tuning(0, 16, 8, 16), Tuning(0, 16, 32, 3)):
+        with pytest.raises(OtfmmError):
+            ctx.set_tuning(bad)
+    assert ctx.get_tuning().as_dict() == keep.as_dict()
