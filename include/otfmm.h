@@ -192,8 +192,9 @@ int otfmm_batch(otfmm_context* ctx, const double* pool_M, const double* pool_com
  * No counterpart in the reference (its kernels have fixed launch shapes). */
 #define OTFMM_SPLIT_WARP_SPECIALISED 0 /* FP32-split RHO tiles: FP32 contraction warps + FP64 L_c warps */
 #define OTFMM_SPLIT_SINGLE_ROLE 1      /* FP32-split RHO tiles: every warp does both */
+#define OTFMM_SPLIT_WARP_SPECIALISED_PACKED 2 /* warp-specialised, contraction in packed FP32 pairs */
 typedef struct otfmm_tuning {
-    int32_t split_m2l_form;  /* OTFMM_SPLIT_WARP_SPECIALISED or OTFMM_SPLIT_SINGLE_ROLE */
+    int32_t split_m2l_form;  /* one of the OTFMM_SPLIT_* forms above */
     int32_t split_m2l_chunk; /* FP32 partial sums of the warp-specialised tiles promoted every 8 or 16 partners */
     int32_t split_p2p_chunk; /* FP32 P2P partial sums promoted every 16 or 32 partners */
     int32_t p2m_lanes;       /* fast-form P2M: at most 4, 8 or 16 lanes share one cell's entries */

@@ -130,6 +130,7 @@ struct Tables {
     const uint16_t* p2m_list;   // partner cell index (in its neighbour) of every entry, grouped by direction
     const int* p2m_perm_start;  // [28]: start of raw direction r in p2m_perm
     const uint16_t* p2m_perm;   // per direction, the cells with partners there, most partners first
+    const double4* p2p_four;    // [8][MAX_ENTRIES]: monopole constants of entries_p2p (zeros past the count)
 };
 
 __device__ __forceinline__ int entry_sx(int y) { return (y & 15) - 8; }
@@ -603,6 +604,79 @@ __device__ __forceinline__ void ws_contract_pair(const float dX[3], const float 
     fast_high_terms<float>(m, D, acc);
 }
 
+// Same contraction with packed FP32 FMAs (two products per instruction; on
+// sm_100 these co-issue with the FP64 pipe far better than scalar FMAs).
+// Accumulator pairs: A[k] = (L_2k, L_2k+1) for k = 0..9; A[10] = L0 quadrupole
+// part, A[11] = L0 octupole part (subtracted), A[12..14] = L1..L3 quadrupole
+// parts, each as two partial sums. The derivative tensor is used as its
+// natural pairs (D_2k, D_2k+1) plus the five pairs the quadrupole/dipole terms
+// of L2, L3 and L4..L9 need: (D11,D13) (D14,D16) (D17,D18) (D12,D14) (D15,D17).
+constexpr int WS_PACKED_ACC = 15;
+__device__ __forceinline__ void ws_contract_pair_packed(const float dX[3], const float2 mm[10],
+                                                        float2 A[WS_PACKED_ACC]) {
+    const float r2 = fmaxf(fmaf(dX[0], dX[0], fmaf(dX[1], dX[1], dX[2] * dX[2])), WS_R2_MIN);
+    const float y0 = rsqrtf(r2);
+    const float h = fmaf(-r2 * y0, y0, 1.0f);
+    const float rs = fmaf(0.5f * y0, h, y0);
+    const float r2inv = rs * rs;
+    const float d1 = rs * r2inv;
+    const float d2 = -3.0f * d1 * r2inv;
+    const float d3 = -5.0f * d2 * r2inv;
+    float D[20];
+    d_tensor<float>(dX, -rs, d1, d2, d3, D);
+    float2 P[10];
+#pragma unroll
+    for (int k = 0; k < 10; ++k) P[k] = make_float2(D[2 * k], D[2 * k + 1]);
+    const float2 Q1 = make_float2(D[11], D[13]), Q2 = make_float2(D[14], D[16]), Q3 = make_float2(D[17], D[18]);
+    const float2 R1 = make_float2(D[12], D[14]), R2 = make_float2(D[15], D[17]);
+    const float2 b0 = make_float2(mm[0].x, mm[0].x);
+    const float2 n1 = make_float2(-mm[0].y, -mm[0].y), n2 = make_float2(-mm[1].x, -mm[1].x),
+                 n3 = make_float2(-mm[1].y, -mm[1].y);
+    // monopole: L0..L19 += M0 D0..D19
+#pragma unroll
+    for (int k = 0; k < 10; ++k) A[k] = __ffma2_rn(b0, P[k], A[k]);
+    // dipole part of L4..L9: -= M_(1+a) D[quad_axis(q, a)]
+    A[2] = __ffma2_rn(n1, P[5], A[2]);
+    A[3] = __ffma2_rn(n1, P[6], A[3]);
+    A[4] = __ffma2_rn(n1, P[7], A[4]);
+    A[2] = __ffma2_rn(n2, Q1, A[2]);
+    A[3] = __ffma2_rn(n2, Q2, A[3]);
+    A[4] = __ffma2_rn(n2, Q3, A[4]);
+    A[2] = __ffma2_rn(n3, R1, A[2]);
+    A[3] = __ffma2_rn(n3, R2, A[3]);
+    A[4] = __ffma2_rn(n3, P[9], A[4]);
+    // quadrupole part of L0 and L1..L3
+#pragma unroll
+    for (int q = 0; q < 3; ++q) A[10] = __ffma2_rn(mm[2 + q], P[2 + q], A[10]);
+    A[12] = __ffma2_rn(mm[2], P[5], A[12]);
+    A[12] = __ffma2_rn(mm[3], P[6], A[12]);
+    A[12] = __ffma2_rn(mm[4], P[7], A[12]);
+    A[13] = __ffma2_rn(mm[2], Q1, A[13]);
+    A[13] = __ffma2_rn(mm[3], Q2, A[13]);
+    A[13] = __ffma2_rn(mm[4], Q3, A[13]);
+    A[14] = __ffma2_rn(mm[2], R1, A[14]);
+    A[14] = __ffma2_rn(mm[3], R2, A[14]);
+    A[14] = __ffma2_rn(mm[4], P[9], A[14]);
+    // octupole part of L0 (subtracted when the pairs are folded)
+#pragma unroll
+    for (int o = 0; o < 5; ++o) A[11] = __ffma2_rn(mm[5 + o], P[5 + o], A[11]);
+}
+
+// Folds the packed accumulators into the FP64 sums of L0..L19 and clears them.
+__device__ __forceinline__ void ws_fold_packed(float2 A[WS_PACKED_ACC], double acc[20]) {
+    acc[0] += (double)((A[0].x + (A[10].x + A[10].y)) - (A[11].x + A[11].y));
+    acc[1] += (double)(A[0].y + (A[12].x + A[12].y));
+    acc[2] += (double)(A[1].x + (A[13].x + A[13].y));
+    acc[3] += (double)(A[1].y + (A[14].x + A[14].y));
+#pragma unroll
+    for (int k = 2; k < 10; ++k) {
+        acc[2 * k] += (double)A[k].x;
+        acc[2 * k + 1] += (double)A[k].y;
+    }
+#pragma unroll
+    for (int k = 0; k < WS_PACKED_ACC; ++k) A[k] = make_float2(0.0f, 0.0f);
+}
+
 // Partner with mass only (monopole-only entries, leaf-neighbour partners).
 __device__ __forceinline__ void ws_contract_mass(const float dX[3], float m0, float acc[20]) {
     const float r2 = fmaxf(fmaf(dX[0], dX[0], fmaf(dX[1], dX[1], dX[2] * dX[2])), WS_R2_MIN);
@@ -653,7 +727,7 @@ __device__ __forceinline__ WsLane ws_lane() {
     return WsLane{(lane >> 2) & 1, lane >> 3, lane & 3};
 }
 
-template <int CHUNK>
+template <int CHUNK, bool PACKED>
 __device__ void ws_contraction_warp(const float2* sa, const double2* sb, const unsigned* s_ent, int x0, int p,
                                     const Tables& t, uint32_t monomask, double inv_dx, const OutPtr& out) {
     const WsLane l = ws_lane();
@@ -671,29 +745,52 @@ __device__ void ws_contraction_warp(const float2* sa, const double2* sb, const u
     }
     const int n = t.count[p], nfar = t.count_far[p];
     const unsigned* ent = s_ent + p * MAX_ENTRIES;
+    if (PACKED) {
+        float2 A[WS_PACKED_ACC];
+#pragma unroll
+        for (int k = 0; k < WS_PACKED_ACC; ++k) A[k] = make_float2(0.0f, 0.0f);
 #pragma unroll 1
-    for (int e0 = 0; e0 < nfar; e0 += CHUNK) {
-        const int e1 = min(e0 + CHUNK, nfar);
+        for (int e0 = 0; e0 < nfar; e0 += CHUNK) {
+            const int e1 = min(e0 + CHUNK, nfar);
 #pragma unroll 2
-        for (int e = e0; e < e1; ++e) {
-            const unsigned en = ent[e];
-            const double2* pb = sb + (en >> 16) + lane_b;
-            const double2 q0 = pb[0], q1 = pb[SUB_YZ];
-            const float dX[3] = {(float)(Pc0 - q0.x), (float)(Pc1 - q0.y), (float)(Pc2 - q1.x)};
-            const float2* pa = sa + (en & 0xffffu) + lane_a;
-            float m[20];
+            for (int e = e0; e < e1; ++e) {
+                const unsigned en = ent[e];
+                const double2* pb = sb + (en >> 16) + lane_b;
+                const double2 q0 = pb[0], q1 = pb[SUB_YZ];
+                const float dX[3] = {(float)(Pc0 - q0.x), (float)(Pc1 - q0.y), (float)(Pc2 - q1.x)};
+                const float2* pa = sa + (en & 0xffffu) + lane_a;
+                float2 mm[10];
 #pragma unroll
-            for (int q = 0; q < 10; ++q) {
-                const float2 v = pa[q * SUB_YZ];
-                m[2 * q] = v.x;
-                m[2 * q + 1] = v.y;
+                for (int q = 0; q < 10; ++q) mm[q] = pa[q * SUB_YZ];
+                ws_contract_pair_packed(dX, mm, A);
             }
-            ws_contract_pair(dX, m, accf);
+            ws_fold_packed(A, acc);
         }
+    } else {
+#pragma unroll 1
+        for (int e0 = 0; e0 < nfar; e0 += CHUNK) {
+            const int e1 = min(e0 + CHUNK, nfar);
+#pragma unroll 2
+            for (int e = e0; e < e1; ++e) {
+                const unsigned en = ent[e];
+                const double2* pb = sb + (en >> 16) + lane_b;
+                const double2 q0 = pb[0], q1 = pb[SUB_YZ];
+                const float dX[3] = {(float)(Pc0 - q0.x), (float)(Pc1 - q0.y), (float)(Pc2 - q1.x)};
+                const float2* pa = sa + (en & 0xffffu) + lane_a;
+                float m[20];
 #pragma unroll
-        for (int q = 0; q < 20; ++q) {
-            acc[q] += (double)accf[q];
-            accf[q] = 0.0f;
+                for (int q = 0; q < 10; ++q) {
+                    const float2 v = pa[q * SUB_YZ];
+                    m[2 * q] = v.x;
+                    m[2 * q + 1] = v.y;
+                }
+                ws_contract_pair(dX, m, accf);
+            }
+#pragma unroll
+            for (int q = 0; q < 20; ++q) {
+                acc[q] += (double)accf[q];
+                accf[q] = 0.0f;
+            }
         }
     }
     const int cx = x0 + ((p >> 2) & 1) + 2 * l.i, cy = ((p >> 1) & 1) + 2 * l.j, cz = (p & 1) + 2 * l.k;
@@ -936,7 +1033,7 @@ __global__ void __launch_bounds__(THREADS, 1) m2l_batch_kernel(BatchArgs a) {
 // stage_region_ws): persistent over the same tile counter as m2l_batch_kernel,
 // 512 threads, one CTA per SM. The root tile runs the fast FP64 form on the
 // first 256 threads.
-template <int CHUNK>
+template <int CHUNK, bool PACKED>
 __global__ void __launch_bounds__(WS_THREADS, 1) m2l_split_ws_kernel(BatchArgs a) {
     extern __shared__ __align__(16) unsigned char ws_dyn[];
     float2* sa = reinterpret_cast<float2*>(ws_dyn);
@@ -980,7 +1077,7 @@ __global__ void __launch_bounds__(WS_THREADS, 1) m2l_split_ws_kernel(BatchArgs a
             stage_region_ws(sa, sb, it, x0, inv_dx, a.M, a.com, a.mon, a.is_leaf);
             __syncthreads();
             if (warp < 8)
-                ws_contraction_warp<CHUNK>(sa, sb, s_ent, x0, warp, a.t, monomask, inv_dx, out);
+                ws_contraction_warp<CHUNK, PACKED>(sa, sb, s_ent, x0, warp, a.t, monomask, inv_dx, out);
             else
                 ws_correction_warp(sb, s_ent, x0, warp & 7, a.t, monomask, inv_dx, out);
         }
@@ -1133,13 +1230,13 @@ __global__ void __launch_bounds__(P2_THREADS, 1) p2p_leaf_kernel(BatchArgs a) {
     int* s_delta = reinterpret_cast<int*>(p2_dyn + 8 * MAX_ENTRIES * sizeof(V4));
     T* regions = reinterpret_cast<T*>(p2_dyn + 8 * MAX_ENTRIES * (sizeof(V4) + sizeof(int)));
     __shared__ ItemInfo its[P2_GROUPS];
+    const int nleaf = a.wl.counts[WL_LEAF];
+    if (blockIdx.x * P2_GROUPS >= nleaf) return;   // no leaf for this CTA (uniform for the block)
+    // per-parity monopole constants and deltas, prebuilt in stencil order at context creation
     for (int e = threadIdx.x; e < 8 * MAX_ENTRIES; e += blockDim.x) {
-        const int p = e / MAX_ENTRIES, k = e % MAX_ENTRIES;
-        if (k < a.t.count[p]) {
-            const int2 en = a.t.entries_p2p[e];
-            s_delta[e] = en.x;
-            s_four[e] = V4{(T)c_four[en.y][0], (T)c_four[en.y][1], (T)c_four[en.y][2], (T)c_four[en.y][3]};
-        }
+        const double4 f = a.t.p2p_four[e];
+        s_four[e] = V4{(T)f.x, (T)f.y, (T)f.z, (T)f.w};
+        s_delta[e] = a.t.entries_p2p[e].x;
     }
     __syncthreads();
     const int g = threadIdx.x >> 8, tid = threadIdx.x & 255;
@@ -1155,7 +1252,6 @@ __global__ void __launch_bounds__(P2_THREADS, 1) p2p_leaf_kernel(BatchArgs a) {
     const int n = a.t.count[p];
     const V4* four = s_four + p * MAX_ENTRIES;
     const int* delta = s_delta + p * MAX_ENTRIES;
-    const int nleaf = a.wl.counts[WL_LEAF];
     for (int kk = blockIdx.x * P2_GROUPS + g; kk < nleaf; kk += gridDim.x * P2_GROUPS) {
         group_sync(g);   // the group's previous leaf is done with pm / it
         if (tid == 0) {
@@ -1686,6 +1782,7 @@ struct otfmm_context {
     uint16_t* d_p2m_list = nullptr;
     int* d_p2m_perm_start = nullptr;
     uint16_t* d_p2m_perm = nullptr;
+    double4* d_p2p_four = nullptr;
     int counts_far[8] = {};
     double* d_four = nullptr;
     uint8_t* d_phase = nullptr;
@@ -1697,7 +1794,7 @@ struct otfmm_context {
     std::mutex mu;
     Tables tables() const { return Tables{d_entries,    d_count, d_entries_fast, d_count_far, d_entries_split, d_entries_p2p,
                       d_entries_ws, d_four,  d_phase,        d_p2m_start,     d_p2m_list,    d_p2m_perm_start,
-                      d_p2m_perm}; }
+                      d_p2m_perm,   d_p2p_four}; }
 };
 
 namespace {
@@ -1737,8 +1834,10 @@ int ensure_attributes(int device) {
     rc = rc ? rc : set_smem(m2l_batch_kernel<PREC_FAST, false>, bytes);
     rc = rc ? rc : set_smem(m2l_batch_kernel<PREC_SPLIT, true>, S_SMEM_DOUBLES * (int)sizeof(double));
     rc = rc ? rc : set_smem(m2l_batch_kernel<PREC_SPLIT, false>, S_SMEM_DOUBLES * (int)sizeof(double));
-    rc = rc ? rc : set_smem(m2l_split_ws_kernel<16>, WS_SMEM_BYTES);
-    rc = rc ? rc : set_smem(m2l_split_ws_kernel<8>, WS_SMEM_BYTES);
+    rc = rc ? rc : set_smem(m2l_split_ws_kernel<16, false>, WS_SMEM_BYTES);
+    rc = rc ? rc : set_smem(m2l_split_ws_kernel<8, false>, WS_SMEM_BYTES);
+    rc = rc ? rc : set_smem(m2l_split_ws_kernel<16, true>, WS_SMEM_BYTES);
+    rc = rc ? rc : set_smem(m2l_split_ws_kernel<8, true>, WS_SMEM_BYTES);
     rc = rc ? rc : set_smem(p2p_batch_kernel<PREC_EXACT>, P2P_SMEM_BYTES);
     rc = rc ? rc : set_smem(p2p_batch_kernel<PREC_FAST>, P2P_SMEM_BYTES);
     rc = rc ? rc : set_smem(p2p_leaf_kernel<double, 0>, p2_smem_bytes<double>());
@@ -1797,6 +1896,7 @@ int otfmm_create(int device, double theta, otfmm_context** out) {
     ctx->reach = reach;
     // P2P-layout table (stencil order)
     std::vector<int2> entries_p2p(8 * MAX_ENTRIES, int2{0, 0});
+    std::vector<double4> p2p_four(8 * MAX_ENTRIES, double4{0.0, 0.0, 0.0, 0.0});
     for (int p = 0; p < 8; ++p)
         for (int e = 0; e < ctx->counts[p]; ++e) {
             const int2 en = entries[p * MAX_ENTRIES + e];
@@ -1805,6 +1905,8 @@ int otfmm_create(int device, double theta, otfmm_context** out) {
             const int cls = (((px + sx) & 1) << 2) | (((py + sy) & 1) << 1) | ((pz + sz) & 1);
             const int delta = cls * P_CLS + ((px + sx + 2) >> 1) * P_XS + ((py + sy + 2) >> 1) * P_RS + ((pz + sz + 2) >> 1);
             entries_p2p[p * MAX_ENTRIES + e] = int2{delta, (en.y >> 16) & 2047};
+            const double* f = ctx->st.four[(en.y >> 16) & 2047];
+            p2p_four[p * MAX_ENTRIES + e] = double4{f[0], f[1], f[2], f[3]};
         }
     // split-layout table (far first, like the fast one)
     std::vector<int4> entries_split(8 * MAX_ENTRIES, int4{0, 0, 0, 0});
@@ -1868,7 +1970,10 @@ int otfmm_create(int device, double theta, otfmm_context** out) {
     p2m_perm_start[27] = (int)p2m_perm.size();
     DeviceGuard g(device);
     cudaError_t e;
-    if ((e = cudaMalloc(&ctx->d_p2m_perm_start, sizeof(int) * p2m_perm_start.size())) != cudaSuccess ||
+    if ((e = cudaMalloc(&ctx->d_p2p_four, sizeof(double4) * p2p_four.size())) != cudaSuccess ||
+        (e = cudaMemcpy(ctx->d_p2p_four, p2p_four.data(), sizeof(double4) * p2p_four.size(),
+                        cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMalloc(&ctx->d_p2m_perm_start, sizeof(int) * p2m_perm_start.size())) != cudaSuccess ||
         (e = cudaMemcpy(ctx->d_p2m_perm_start, p2m_perm_start.data(), sizeof(int) * p2m_perm_start.size(),
                         cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMalloc(&ctx->d_p2m_perm, sizeof(uint16_t) * std::max<size_t>(1, p2m_perm.size()))) != cudaSuccess ||
@@ -1932,6 +2037,7 @@ int otfmm_destroy(otfmm_context* ctx) {
     cudaFree(ctx->d_p2m_list);
     cudaFree(ctx->d_p2m_perm_start);
     cudaFree(ctx->d_p2m_perm);
+    cudaFree(ctx->d_p2p_four);
     cudaFree(ctx->d_count_far);
     cudaFree(ctx->d_four);
     cudaFree(ctx->d_phase);
@@ -2137,7 +2243,8 @@ int otfmm_stage_p2m_soa(otfmm_context* ctx, const double* pool_M, const double* 
 namespace {
 
 int check_tuning(const otfmm_tuning& t) {
-    if (t.split_m2l_form != OTFMM_SPLIT_WARP_SPECIALISED && t.split_m2l_form != OTFMM_SPLIT_SINGLE_ROLE)
+    if (t.split_m2l_form != OTFMM_SPLIT_WARP_SPECIALISED && t.split_m2l_form != OTFMM_SPLIT_SINGLE_ROLE &&
+        t.split_m2l_form != OTFMM_SPLIT_WARP_SPECIALISED_PACKED)
         return fail(OTFMM_ERR_INVALID, "unknown split M2L form");
     if (t.split_m2l_chunk != 8 && t.split_m2l_chunk != 16) return fail(OTFMM_ERR_INVALID, "split M2L chunk must be 8 or 16");
     if (t.split_p2p_chunk != 16 && t.split_p2p_chunk != 32) return fail(OTFMM_ERR_INVALID, "split P2P chunk must be 16 or 32");
@@ -2185,9 +2292,15 @@ int enqueue_batch(otfmm_context* ctx, const double* pool_M, const double* pool_c
     } else {
         if (precision == OTFMM_FP32_SPLIT) {
             const size_t sbytes = S_SMEM_DOUBLES * sizeof(double);
-            if (rho && tu.split_m2l_form == OTFMM_SPLIT_WARP_SPECIALISED) {
-                if (tu.split_m2l_chunk == 8) m2l_split_ws_kernel<8><<<tiles_grid, WS_THREADS, WS_SMEM_BYTES, s>>>(a);
-                else m2l_split_ws_kernel<16><<<tiles_grid, WS_THREADS, WS_SMEM_BYTES, s>>>(a);
+            if (rho && tu.split_m2l_form != OTFMM_SPLIT_SINGLE_ROLE) {
+                const bool packed = (tu.split_m2l_form == OTFMM_SPLIT_WARP_SPECIALISED_PACKED);
+                if (tu.split_m2l_chunk == 8) {
+                    if (packed) m2l_split_ws_kernel<8, true><<<tiles_grid, WS_THREADS, WS_SMEM_BYTES, s>>>(a);
+                    else m2l_split_ws_kernel<8, false><<<tiles_grid, WS_THREADS, WS_SMEM_BYTES, s>>>(a);
+                } else {
+                    if (packed) m2l_split_ws_kernel<16, true><<<tiles_grid, WS_THREADS, WS_SMEM_BYTES, s>>>(a);
+                    else m2l_split_ws_kernel<16, false><<<tiles_grid, WS_THREADS, WS_SMEM_BYTES, s>>>(a);
+                }
             } else if (rho) {
                 m2l_batch_kernel<PREC_SPLIT, true><<<tiles_grid, THREADS, sbytes, s>>>(a);
             } else {
@@ -2368,11 +2481,11 @@ int otfmm_autotune(otfmm_context* ctx, const double* pool_M, const double* pool_
     otfmm_tuning best = ctx->tuning;
     float tbest = 0.f;
     rc = time_of(best, tbest);
-    const int forms[2] = {OTFMM_SPLIT_WARP_SPECIALISED, OTFMM_SPLIT_SINGLE_ROLE};
+    const int forms[3] = {OTFMM_SPLIT_WARP_SPECIALISED_PACKED, OTFMM_SPLIT_WARP_SPECIALISED, OTFMM_SPLIT_SINGLE_ROLE};
     const int m2l_chunks[2] = {8, 16}, p2p_chunks[2] = {16, 32}, lanes[3] = {4, 8, 16};
     const bool split = (precision == OTFMM_FP32_SPLIT), fast = (precision != OTFMM_FP64_EXACT);
     for (int dim = 0; dim < 4 && rc == OTFMM_OK; ++dim) {
-        const int nvar = (dim == 3) ? 3 : 2;
+        const int nvar = (dim == 3 || dim == 0) ? 3 : 2;
         if ((dim < 3 && !split) || (dim == 3 && !fast)) continue;
         for (int v = 0; v < nvar && rc == OTFMM_OK; ++v) {
             otfmm_tuning tu = best;

@@ -32,7 +32,8 @@ EXPORTED = ["otfmm_create", "otfmm_destroy", "otfmm_stencil_info", "otfmm_m2l_so
 
 _lib = None
 
-SPLIT_WARP_SPECIALISED, SPLIT_SINGLE_ROLE = 0, 1
+SPLIT_WARP_SPECIALISED, SPLIT_SINGLE_ROLE, SPLIT_WARP_SPECIALISED_PACKED = 0, 1, 2
+SPLIT_FORMS = {0: "warp_specialised", 1: "single_role", 2: "warp_specialised_packed"}
 
 
 class Tuning(ctypes.Structure):
@@ -41,7 +42,7 @@ class Tuning(ctypes.Structure):
                 ("split_p2p_chunk", ctypes.c_int32), ("p2m_lanes", ctypes.c_int32)]
 
     def as_dict(self) -> dict:
-        return {"split_m2l_form": "warp_specialised" if self.split_m2l_form == 0 else "single_role",
+        return {"split_m2l_form": SPLIT_FORMS.get(self.split_m2l_form, str(self.split_m2l_form)),
                 "split_m2l_chunk": self.split_m2l_chunk, "split_p2p_chunk": self.split_p2p_chunk,
                 "p2m_lanes": self.p2m_lanes}
 

@@ -58,7 +58,7 @@ def test_plan_replays_batch(ctx, precision, solve):
     plan.close()
 
 
-VARIANTS = list(itertools.product([0, 1], [8, 16], [16, 32], [4, 8, 16]))
+VARIANTS = list(itertools.product([0, 1, 2], [8, 16], [16, 32], [4, 8, 16]))
 
 
 @pytest.mark.parametrize("form,m2l_chunk,p2p_chunk,lanes", VARIANTS)
@@ -103,7 +103,7 @@ def test_autotune_keeps_an_allowed_variant(ctx, oracle):
 def test_invalid_variants_rejected(ctx):
     from octotiger_b200.otfmm import OtfmmError, Tuning
     keep = ctx.get_tuning()
-    for bad in (Tuning(2, 16, 32, 16), Tuning(0, 12, 32, 16), Tuning(0, 16, 8, 16), Tuning(0, 16, 32, 3)):
+    for bad in (Tuning(3, 16, 32, 16), Tuning(0, 12, 32, 16), Tuning(0, 16, 8, 16), Tuning(0, 16, 32, 3)):
         with pytest.raises(OtfmmError):
             ctx.set_tuning(bad)
     assert ctx.get_tuning().as_dict() == keep.as_dict()
