@@ -42,6 +42,13 @@ FLOPS_PER_PAIR = {("m2l", RHO): 406, ("m2l", DRHODT): 272, ("p2p", RHO): 12, ("p
 
 L2_FLUSH_BYTES = 256 << 20
 
+# DRAM bytes (read + write) of one launch of the multipole-tile kernel, from
+# ncu captures (dram__bytes_read.sum + dram__bytes_write.sum) of this command
+# on a B200; the algorithmic bytes are the pool read once plus L and L_c written
+# (uniform level 3: 50.3 MB + 48.2 MB).
+PROFILED_TRAFFIC = {("uniform_level3", "fp32_split"): 61.0e6, ("uniform_level3", "fp64"): 57.9e6,
+                    ("amr_polytrope_l6", "fp32_split"): 78.6e6, ("amr_polytrope_l6", "fp64"): 77.4e6}
+
 
 WORKLOADS = ("uniform_level3", "amr_polytrope", "amr_binary")
 
@@ -377,18 +384,32 @@ def gpu_arm(args) -> None:
         e2e_ms = float(t.item())
     e2e_value = world * counts["total"] * args.steps / (e2e_ms * 1e-3)
 
-    # roofline: nominal reference FLOPs of one launch / its device time vs the
-    # FP64 FMA issue rate measured on this GPU in this run
+    # roofline of the dominant kernel (the multipole tiles): nominal reference
+    # FLOPs of one launch / its device time (CUDA events between the launches
+    # of one solve, median of 5, L2 flushed) vs the FMA issue rate measured on
+    # this GPU in this run
+    ctx.set_tuning(tuned[args.precision])
+    kms = []
+    for _ in range(5):
+        flush.zero_()
+        kms.append(solver.profile(solve, args.precision))
+    kernel_ms = {k: float(np.median([x[k] for x in kms])) for k in kms[0]}
+    flops_m2l = counts["m2l"] * FLOPS_PER_PAIR[("m2l", solve)]
     flops = sum(counts[k] * FLOPS_PER_PAIR[(k, solve)] for k in ("m2l", "p2p", "p2m"))
-    ms_launch = total_ms / args.steps
-    achieved = flops / (ms_launch * 1e-3) / 1e12
+    achieved = flops_m2l / (kernel_ms["m2l"] * 1e-3) / 1e12
     fp64_peak, fp32_peak = measure_fma_peaks(local)
     peak = fp32_peak if args.precision == "fp32_split" else fp64_peak
+    traffic = PROFILED_TRAFFIC.get((batch.name, args.precision))
     roof = {"bound": "fp64_fma" if args.precision != "fp32_split" else "fp32_fma", "achieved": achieved,
-            "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
-            "flops_per_launch": flops,
+            "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
+            "kernel": "multipole tiles (m2l)", "flops_per_launch": flops_m2l,
+            "flops_per_pair": FLOPS_PER_PAIR[("m2l", solve)], "kernel_ms": kernel_ms,
+            "step_flops_per_s": flops / (total_ms / args.steps * 1e-3) / 1e12,
+            "fp64_equivalent_frac": achieved / fp64_peak,
             "peak_source": "measured in this run: register-resident FMA loop (otfmm_measure_fma_peaks); "
                            "MEASURED_PEAKS.json has no FP64/FP32 figure",
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of the same kernel "
+                              "on this workload (tuned variant)" if traffic else None,
             "fp64_peak_tflops": fp64_peak, "fp32_peak_tflops": fp32_peak}
 
     line = {

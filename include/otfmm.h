@@ -200,6 +200,15 @@ typedef struct otfmm_tuning {
     int32_t p2m_lanes;       /* fast-form P2M: at most 4, 8 or 16 lanes share one cell's entries */
 } otfmm_tuning;
 
+/* One otfmm_batch with CUDA events between its launches: kernel_ms receives the
+ * device time of the classification, multipole-tile, P2P and P2M kernels of
+ * this solve (roofline reporting). Synchronises the stream. No counterpart in
+ * the reference. */
+int otfmm_batch_profile(otfmm_context* ctx, const double* pool_M, const double* pool_com, const double* pool_mon,
+                        const uint8_t* pool_is_leaf, int32_t n_subgrids, const otfmm_work_item* items,
+                        int32_t n_items, double* L, double* L_c, int gsolve_type, int precision, float kernel_ms[4],
+                        void* stream);
+
 /* The context's current variants (defaults: warp-specialised, 16, 32, 16). */
 int otfmm_get_tuning(const otfmm_context* ctx, otfmm_tuning* out);
 int otfmm_set_tuning(otfmm_context* ctx, const otfmm_tuning* t);

@@ -2269,7 +2269,11 @@ int check_batch_args(otfmm_context* ctx, const double* pool_M, const double* poo
 int enqueue_batch(otfmm_context* ctx, const double* pool_M, const double* pool_com, const double* pool_mon,
                   const uint8_t* pool_is_leaf, int32_t n_subgrids, const otfmm_work_item* items, int32_t n_items,
                   double* L, double* L_c, int gsolve_type, int precision, int* lists, int cap, int* err,
-                  const otfmm_tuning& tu, cudaStream_t s) {
+                  const otfmm_tuning& tu, cudaStream_t s, cudaEvent_t* marks = nullptr) {
+    // marks (optional): 5 events recorded around the 4 kernel launches
+    auto mark = [&](int i) {
+        if (marks) cudaEventRecord(marks[i], s);
+    };
     WorkLists wl{lists, lists + cap, lists + 2 * (size_t)cap, lists + 3 * (size_t)cap, lists + 4 * (size_t)cap};
     OT_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
     OT_CUDA(cudaMemsetAsync(wl.counts, 0, sizeof(int) * WL_COUNTERS, s));
@@ -2281,12 +2285,16 @@ int enqueue_batch(otfmm_context* ctx, const double* pool_M, const double* pool_c
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
     // classify, then multipole tiles, P2P of the leaves and P2M (stream
     // order keeps the reference's P2P-then-P2M accumulation order)
+    mark(0);
     classify_kernel<<<(n_items + 255) / 256, 256, 0, s>>>(a);
+    mark(1);
     const dim3 tiles_grid(sms), p2p_grid(P2P_CTAS_PER_SM * sms), p2m_grid(std::min(n_items, 8 * sms));
     if (precision == OTFMM_FP64_EXACT) {
         if (rho) m2l_batch_kernel<PREC_EXACT, true><<<tiles_grid, THREADS, bytes, s>>>(a);
         else m2l_batch_kernel<PREC_EXACT, false><<<tiles_grid, THREADS, bytes, s>>>(a);
+        mark(2);
         p2p_batch_kernel<PREC_EXACT><<<p2p_grid, P2P_THREADS, P2P_SMEM_BYTES, s>>>(a);
+        mark(3);
         if (rho) p2m_batch_kernel<PREC_EXACT, true><<<p2m_grid, P_THREADS, 0, s>>>(a);
         else p2m_batch_kernel<PREC_EXACT, false><<<p2m_grid, P_THREADS, 0, s>>>(a);
     } else {
@@ -2306,16 +2314,20 @@ int enqueue_batch(otfmm_context* ctx, const double* pool_M, const double* pool_c
             } else {
                 m2l_batch_kernel<PREC_SPLIT, false><<<tiles_grid, THREADS, sbytes, s>>>(a);
             }
+            mark(2);
             if (tu.split_p2p_chunk == 16) p2p_leaf_kernel<float, 16><<<sms, P2_THREADS, p2_smem_bytes<float>(), s>>>(a);
             else p2p_leaf_kernel<float, 32><<<sms, P2_THREADS, p2_smem_bytes<float>(), s>>>(a);
         } else {
             if (rho) m2l_batch_kernel<PREC_FAST, true><<<tiles_grid, THREADS, bytes, s>>>(a);
             else m2l_batch_kernel<PREC_FAST, false><<<tiles_grid, THREADS, bytes, s>>>(a);
+            mark(2);
             p2p_leaf_kernel<double, 0><<<sms, P2_THREADS, p2_smem_bytes<double>(), s>>>(a);
         }
+        mark(3);
         if (rho) p2m_batch_kernel<PREC_FAST, true><<<p2m_grid, P_THREADS, 0, s>>>(a);
         else p2m_batch_kernel<PREC_FAST, false><<<p2m_grid, P_THREADS, 0, s>>>(a);
     }
+    mark(4);
     OT_CUDA(cudaGetLastError());
     return OTFMM_OK;
 }
@@ -2359,6 +2371,31 @@ int otfmm_batch(otfmm_context* ctx, const double* pool_M, const double* pool_com
     if (rc) return rc;
     return enqueue_batch(ctx, pool_M, pool_com, pool_mon, pool_is_leaf, n_subgrids, items, n_items, L, L_c,
                          gsolve_type, precision, ctx->d_lists, ctx->list_capacity, ctx->d_err, ctx->tuning, s);
+}
+
+int otfmm_batch_profile(otfmm_context* ctx, const double* pool_M, const double* pool_com, const double* pool_mon,
+                        const uint8_t* pool_is_leaf, int32_t n_subgrids, const otfmm_work_item* items,
+                        int32_t n_items, double* L, double* L_c, int gsolve_type, int precision, float kernel_ms[4],
+                        void* stream) {
+    if (!kernel_ms) return fail(OTFMM_ERR_INVALID, "kernel_ms is NULL");
+    int rc = check_batch_args(ctx, pool_M, pool_com, pool_mon, pool_is_leaf, n_subgrids, items, n_items, L, L_c,
+                              gsolve_type, precision);
+    if (rc) return rc;
+    if (n_items == 0) return fail(OTFMM_ERR_INVALID, "empty work list");
+    DeviceGuard g(ctx->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    rc = ensure_list_capacity(ctx, n_items, s);
+    if (rc) return rc;
+    cudaEvent_t ev[5] = {};
+    for (auto& e : ev) OT_CUDA(cudaEventCreate(&e));
+    rc = enqueue_batch(ctx, pool_M, pool_com, pool_mon, pool_is_leaf, n_subgrids, items, n_items, L, L_c,
+                       gsolve_type, precision, ctx->d_lists, ctx->list_capacity, ctx->d_err, ctx->tuning, s, ev);
+    cudaError_t e = cudaEventSynchronize(ev[4]);
+    for (int k = 0; k < 4 && rc == OTFMM_OK && e == cudaSuccess; ++k) e = cudaEventElapsedTime(&kernel_ms[k], ev[k], ev[k + 1]);
+    for (auto& x : ev) cudaEventDestroy(x);
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_fail(e, "otfmm_batch_profile");
+    return OTFMM_OK;
 }
 
 int otfmm_get_tuning(const otfmm_context* ctx, otfmm_tuning* out) {

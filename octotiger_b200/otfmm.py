@@ -26,7 +26,7 @@ PRECISIONS = {"fp64_exact": FP64_EXACT, "fp64": FP64, "fp32_split": FP32_SPLIT}
 EXPORTED = ["otfmm_create", "otfmm_destroy", "otfmm_stencil_info", "otfmm_m2l_soa", "otfmm_m2l_soa_host",
             "otfmm_p2p_soa", "otfmm_p2m_soa", "otfmm_batch", "otfmm_batch_status", "otfmm_count_pairs",
             "otfmm_m2l_soa_host_noalloc", "otfmm_stage_soa", "otfmm_stage_p2m_soa", "otfmm_get_tuning",
-            "otfmm_set_tuning", "otfmm_autotune", "otfmm_plan_create", "otfmm_plan_launch", "otfmm_plan_status",
+            "otfmm_set_tuning", "otfmm_autotune", "otfmm_batch_profile", "otfmm_plan_create", "otfmm_plan_launch", "otfmm_plan_status",
             "otfmm_plan_destroy", "otfmm_last_error",
             "otfmm_build_info", "otfmm_measure_fma_peaks"]
 
@@ -78,6 +78,8 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
         lib.otfmm_plan_create.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int32, vp, ctypes.c_int32, vp, vp, i, i,
                                           ctypes.POINTER(vp)]
         lib.otfmm_plan_launch.argtypes = [vp, vp]
+        lib.otfmm_batch_profile.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int32, vp, ctypes.c_int32, vp, vp, i, i,
+                                            ctypes.POINTER(ctypes.c_float), vp]
         lib.otfmm_plan_status.argtypes = [vp, vp]
         lib.otfmm_plan_destroy.argtypes = [vp]
         lib.otfmm_stage_soa.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int32, vp, vp, vp, vp, vp]
@@ -226,6 +228,16 @@ class Context:
                                           ctypes.c_int32(dev.n), _ptr(items_dev), ctypes.c_int32(n_items), _ptr(L),
                                           _ptr(Lc), int(gsolve_type), precision_code(precision), _stream(stream)))
 
+    def batch_profile(self, dev: "DevicePool", items_dev, n_items: int, L, Lc, gsolve_type=RHO, precision=FP64,
+                      stream=None) -> dict:
+        """One batched solve with per-kernel device times (ms)."""
+        ms = (ctypes.c_float * 4)()
+        _check(load_library().otfmm_batch_profile(self.handle, _ptr(dev.M), _ptr(dev.com), _ptr(dev.mon),
+                                                  _ptr(dev.is_leaf), ctypes.c_int32(dev.n), _ptr(items_dev),
+                                                  ctypes.c_int32(n_items), _ptr(L), _ptr(Lc), int(gsolve_type),
+                                                  precision_code(precision), ms, _stream(stream)))
+        return {"classify": ms[0], "m2l": ms[1], "p2p": ms[2], "p2m": ms[3]}
+
     def get_tuning(self) -> Tuning:
         t = Tuning()
         _check(load_library().otfmm_get_tuning(self.handle, ctypes.byref(t)))
@@ -314,6 +326,9 @@ class BatchSolver:
     def results(self):
         self.ctx.batch_status()
         return self.L.cpu().numpy(), self.Lc.cpu().numpy()
+
+    def profile(self, gsolve_type=RHO, precision=FP64) -> dict:
+        return self.ctx.batch_profile(self.dev, self.items, self.n_items, self.L, self.Lc, gsolve_type, precision)
 
     def autotune(self, gsolve_type=RHO, precision=FP64, repeats: int = 3) -> Tuning:
         return self.ctx.autotune(self.dev, self.items, self.n_items, self.L, self.Lc, gsolve_type, precision, repeats)

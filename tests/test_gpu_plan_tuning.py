@@ -107,3 +107,17 @@ def test_invalid_variants_rejected(ctx):
         with pytest.raises(OtfmmError):
             ctx.set_tuning(bad)
     assert ctx.get_tuning().as_dict() == keep.as_dict()
+
+
+def test_batch_profile_times_each_kernel_and_matches_batch(ctx):
+    from octotiger_b200.otfmm import BatchSolver
+    b = amr_small()
+    s = BatchSolver(ctx, b.pool, b.items)
+    s.run(RHO, "fp64")
+    L0, Lc0 = s.results()
+    ms = s.profile(RHO, "fp64")
+    assert set(ms) == {"classify", "m2l", "p2p", "p2m"}
+    assert all(v > 0.0 for v in ms.values()), ms
+    L, Lc = s.results()
+    np.testing.assert_array_equal(L, L0)
+    np.testing.assert_array_equal(Lc, Lc0)
