@@ -237,6 +237,22 @@ int otfmm_plan_launch(otfmm_plan* plan, void* stream);
 int otfmm_plan_status(otfmm_plan* plan, void* stream);
 int otfmm_plan_destroy(otfmm_plan* plan);
 
+/* Batched solve from host buffers (pinned memory lets the copies overlap):
+ * pool and work list as for otfmm_batch but in host memory; writes the whole
+ * of the host outputs L[n][20][512] and L_c[n][3][512]: the solve's results,
+ * zeros elsewhere (node_server::compute_fmm zeroes L / L_c before the
+ * reference's kernels, src/node_server.cpp:701-705). The pool is uploaded in
+ * chunks of consecutive subgrids; each work item runs once the records it
+ * reads have arrived and each output range is copied back once final, on two
+ * copy streams, so uploads, kernels and downloads overlap when neighbours have
+ * nearby pool indices. Device copies live in the context (grown on demand).
+ * Asynchronous: the outputs are valid once `stream` has completed; a later
+ * call waits for the earlier call's uploads. Work items are re-validated on the
+ * device (otfmm_batch_status). No counterpart in the reference. */
+int otfmm_batch_host(otfmm_context* ctx, const double* pool_M, const double* pool_com, const double* pool_mon,
+                     const uint8_t* pool_is_leaf, int32_t n_subgrids, const otfmm_work_item* items, int32_t n_items,
+                     double* L, double* L_c, int gsolve_type, int precision, void* stream);
+
 /* Cell-interactions a work list evaluates (host-side count, no device
  * work): the (cell, partner) pairs that pass the stencil and coarse-distance
  * masks, which is what the reference's kernels evaluate. per_class (may be

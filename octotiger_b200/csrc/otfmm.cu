@@ -1791,6 +1791,19 @@ struct otfmm_context {
     int* d_lists = nullptr;            // batched work lists (grown on demand)
     int list_capacity = 0;
     otfmm_tuning tuning = {OTFMM_SPLIT_WARP_SPECIALISED, 16, 32, 16};
+    // otfmm_batch_host: device copies of the pool, work list and outputs, a
+    // pinned host copy of the reordered work list, two copy streams and events
+    struct HostPath {
+        int n_sub = 0, n_items = 0;
+        double *M = nullptr, *com = nullptr, *mon = nullptr, *L = nullptr, *Lc = nullptr;
+        uint8_t* is_leaf = nullptr;
+        otfmm_work_item* items = nullptr;
+        otfmm_work_item* items_pinned = nullptr;
+        cudaStream_t h2d = nullptr, d2h = nullptr;
+        cudaEvent_t ev[3 * 16 + 4] = {};
+        bool ready = false;
+        std::mutex mu;   // one host-path call at a time per context
+    } hp;
     std::mutex mu;
     Tables tables() const { return Tables{d_entries,    d_count, d_entries_fast, d_count_far, d_entries_split, d_entries_p2p,
                       d_entries_ws, d_four,  d_phase,        d_p2m_start,     d_p2m_list,    d_p2m_perm_start,
@@ -2038,6 +2051,24 @@ int otfmm_destroy(otfmm_context* ctx) {
     cudaFree(ctx->d_p2m_perm_start);
     cudaFree(ctx->d_p2m_perm);
     cudaFree(ctx->d_p2p_four);
+    {
+        auto& hp = ctx->hp;
+        if (hp.ready) {
+            cudaStreamSynchronize(hp.h2d);
+            cudaStreamSynchronize(hp.d2h);
+            for (auto& e : hp.ev) cudaEventDestroy(e);
+            cudaStreamDestroy(hp.h2d);
+            cudaStreamDestroy(hp.d2h);
+        }
+        cudaFree(hp.M);
+        cudaFree(hp.com);
+        cudaFree(hp.mon);
+        cudaFree(hp.L);
+        cudaFree(hp.Lc);
+        cudaFree(hp.is_leaf);
+        cudaFree(hp.items);
+        cudaFreeHost(hp.items_pinned);
+    }
     cudaFree(ctx->d_count_far);
     cudaFree(ctx->d_four);
     cudaFree(ctx->d_phase);
@@ -2269,13 +2300,13 @@ int check_batch_args(otfmm_context* ctx, const double* pool_M, const double* poo
 int enqueue_batch(otfmm_context* ctx, const double* pool_M, const double* pool_com, const double* pool_mon,
                   const uint8_t* pool_is_leaf, int32_t n_subgrids, const otfmm_work_item* items, int32_t n_items,
                   double* L, double* L_c, int gsolve_type, int precision, int* lists, int cap, int* err,
-                  const otfmm_tuning& tu, cudaStream_t s, cudaEvent_t* marks = nullptr) {
+                  const otfmm_tuning& tu, cudaStream_t s, cudaEvent_t* marks = nullptr, bool reset_err = true) {
     // marks (optional): 5 events recorded around the 4 kernel launches
     auto mark = [&](int i) {
         if (marks) cudaEventRecord(marks[i], s);
     };
     WorkLists wl{lists, lists + cap, lists + 2 * (size_t)cap, lists + 3 * (size_t)cap, lists + 4 * (size_t)cap};
-    OT_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
+    if (reset_err) OT_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
     OT_CUDA(cudaMemsetAsync(wl.counts, 0, sizeof(int) * WL_COUNTERS, s));
     BatchArgs a{pool_M, pool_com, pool_mon, pool_is_leaf, n_subgrids, items, n_items, L, L_c, ctx->tables(),
                 err, wl, tu.p2m_lanes};
@@ -2395,6 +2426,147 @@ int otfmm_batch_profile(otfmm_context* ctx, const double* pool_M, const double* 
     for (auto& x : ev) cudaEventDestroy(x);
     if (rc) return rc;
     if (e != cudaSuccess) return cuda_fail(e, "otfmm_batch_profile");
+    return OTFMM_OK;
+}
+
+int otfmm_batch_host(otfmm_context* ctx, const double* pool_M, const double* pool_com, const double* pool_mon,
+                     const uint8_t* pool_is_leaf, int32_t n_subgrids, const otfmm_work_item* items, int32_t n_items,
+                     double* L, double* L_c, int gsolve_type, int precision, void* stream) {
+    int rc = check_batch_args(ctx, pool_M, pool_com, pool_mon, pool_is_leaf, n_subgrids, items, n_items, L, L_c,
+                              gsolve_type, precision);
+    if (rc) return rc;
+    // host-side checks of the fields used to order the work (the device re-validates everything)
+    for (int i = 0; i < n_items; ++i) {
+        const otfmm_work_item& w = items[i];
+        if (w.subgrid < 0 || w.subgrid >= n_subgrids) return fail(OTFMM_ERR_INVALID, "work item out of range");
+        for (int d = 0; d < 26; ++d)
+            if (w.neighbors[d] < -1 || w.neighbors[d] >= n_subgrids)
+                return fail(OTFMM_ERR_INVALID, "neighbour out of range");
+    }
+    DeviceGuard g(ctx->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    auto& hp = ctx->hp;
+    std::lock_guard<std::mutex> lock(hp.mu);
+    if (!hp.ready) {
+        OT_CUDA(cudaStreamCreateWithFlags(&hp.h2d, cudaStreamNonBlocking));
+        OT_CUDA(cudaStreamCreateWithFlags(&hp.d2h, cudaStreamNonBlocking));
+        for (auto& e : hp.ev) OT_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        hp.ready = true;
+    }
+    cudaEvent_t* ev_h2d = hp.ev;          // [16] pool chunk k arrived
+    cudaEvent_t* ev_comp = hp.ev + 16;    // [16] item chunk c computed
+    cudaEvent_t* ev_d2h = hp.ev + 32;     // [16] outputs of pool chunk k copied
+    cudaEvent_t ev_start = hp.ev[48], ev_items = hp.ev[49], ev_done = hp.ev[50];
+    // the previous call's copies out of the pinned work list and into the host outputs are done
+    OT_CUDA(cudaEventSynchronize(ev_items));
+    // device buffers and the work-list storage, grown on demand
+    if (n_subgrids > hp.n_sub) {
+        OT_CUDA(cudaStreamSynchronize(s));
+        OT_CUDA(cudaDeviceSynchronize());
+        cudaFree(hp.M);
+        cudaFree(hp.com);
+        cudaFree(hp.mon);
+        cudaFree(hp.L);
+        cudaFree(hp.Lc);
+        cudaFree(hp.is_leaf);
+        hp.M = hp.com = hp.mon = hp.L = hp.Lc = nullptr;
+        hp.is_leaf = nullptr;
+        hp.n_sub = 0;
+        const size_t n = (size_t)n_subgrids;
+        OT_CUDA(cudaMalloc(&hp.M, sizeof(double) * 20 * NCELL * n));
+        OT_CUDA(cudaMalloc(&hp.com, sizeof(double) * 3 * NCELL * n));
+        OT_CUDA(cudaMalloc(&hp.mon, sizeof(double) * NCELL * n));
+        OT_CUDA(cudaMalloc(&hp.L, sizeof(double) * 20 * NCELL * n));
+        OT_CUDA(cudaMalloc(&hp.Lc, sizeof(double) * 3 * NCELL * n));
+        OT_CUDA(cudaMalloc(&hp.is_leaf, n));
+        hp.n_sub = n_subgrids;
+    }
+    if (n_items > hp.n_items) {
+        OT_CUDA(cudaDeviceSynchronize());
+        cudaFree(hp.items);
+        cudaFreeHost(hp.items_pinned);
+        hp.items = nullptr;
+        hp.items_pinned = nullptr;
+        hp.n_items = 0;
+        OT_CUDA(cudaMalloc(&hp.items, sizeof(otfmm_work_item) * (size_t)n_items));
+        OT_CUDA(cudaMallocHost(&hp.items_pinned, sizeof(otfmm_work_item) * (size_t)n_items));
+        hp.n_items = n_items;
+    }
+    if (n_items == 0) return OTFMM_OK;
+    rc = ensure_list_capacity(ctx, n_items, s);
+    if (rc) return rc;
+    // Pool chunks [bnd[k], bnd[k+1]); an item runs once every pool record it reads
+    // has arrived, i.e. in the chunk of the largest index it reads; the outputs
+    // of pool chunk k are final after the last item chunk writing them.
+    const int K = std::max(1, std::min(16, n_subgrids / 64));
+    std::vector<int> bnd(K + 1);
+    for (int k = 0; k <= K; ++k) bnd[k] = (int)((long long)n_subgrids * k / K);
+    auto chunk_of = [&](int idx) { return (int)((long long)idx * K / n_subgrids); };
+    std::vector<int> cidx(n_items), need(K, 0);
+    for (int i = 0; i < n_items; ++i) {
+        const otfmm_work_item& w = items[i];
+        int mx = w.subgrid;
+        for (int d = 0; d < 26; ++d) mx = std::max(mx, w.neighbors[d]);
+        int c = chunk_of(mx);
+        while (c + 1 <= K - 1 && bnd[c + 1] <= mx) ++c;   // exact chunk of mx
+        while (c > 0 && bnd[c] > mx) --c;
+        cidx[i] = c;
+        int ks = chunk_of(w.subgrid);
+        while (ks + 1 <= K - 1 && bnd[ks + 1] <= w.subgrid) ++ks;
+        while (ks > 0 && bnd[ks] > w.subgrid) --ks;
+        need[ks] = std::max(need[ks], c);
+    }
+    std::vector<int> first(K + 1, 0);
+    for (int i = 0; i < n_items; ++i) ++first[cidx[i] + 1];
+    for (int c = 0; c < K; ++c) first[c + 1] += first[c];
+    {
+        std::vector<int> fill(first.begin(), first.end() - 1);
+        for (int i = 0; i < n_items; ++i) hp.items_pinned[fill[cidx[i]]++] = items[i];
+    }
+    for (int k = 1; k < K; ++k) need[k] = std::max(need[k], need[k - 1]);   // copy out in pool order
+    const size_t cell = NCELL * sizeof(double);
+    OT_CUDA(cudaEventRecord(ev_start, s));
+    OT_CUDA(cudaStreamWaitEvent(hp.h2d, ev_start, 0));
+    OT_CUDA(cudaStreamWaitEvent(hp.d2h, ev_start, 0));
+    OT_CUDA(cudaMemcpyAsync(hp.is_leaf, pool_is_leaf, (size_t)n_subgrids, cudaMemcpyHostToDevice, hp.h2d));
+    OT_CUDA(cudaMemcpyAsync(hp.items, hp.items_pinned, sizeof(otfmm_work_item) * (size_t)n_items,
+                            cudaMemcpyHostToDevice, hp.h2d));
+    for (int k = 0; k < K; ++k) {
+        const size_t a = bnd[k], n = bnd[k + 1] - bnd[k];
+        OT_CUDA(cudaMemcpyAsync(hp.M + a * 20 * NCELL, pool_M + a * 20 * NCELL, n * 20 * cell, cudaMemcpyHostToDevice,
+                                hp.h2d));
+        OT_CUDA(cudaMemcpyAsync(hp.com + a * 3 * NCELL, pool_com + a * 3 * NCELL, n * 3 * cell,
+                                cudaMemcpyHostToDevice, hp.h2d));
+        OT_CUDA(cudaMemcpyAsync(hp.mon + a * NCELL, pool_mon + a * NCELL, n * cell, cudaMemcpyHostToDevice, hp.h2d));
+        OT_CUDA(cudaEventRecord(ev_h2d[k], hp.h2d));
+    }
+    OT_CUDA(cudaEventRecord(ev_items, hp.h2d));
+    // outputs start from zero, as compute_fmm zeroes L / L_c (src/node_server.cpp:701-705)
+    OT_CUDA(cudaMemsetAsync(hp.L, 0, sizeof(double) * 20 * NCELL * (size_t)n_subgrids, s));
+    OT_CUDA(cudaMemsetAsync(hp.Lc, 0, sizeof(double) * 3 * NCELL * (size_t)n_subgrids, s));
+    OT_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), s));
+    for (int c = 0; c < K; ++c) {
+        OT_CUDA(cudaStreamWaitEvent(s, ev_h2d[c], 0));
+        const int n = first[c + 1] - first[c];
+        if (n > 0) {
+            rc = enqueue_batch(ctx, hp.M, hp.com, hp.mon, hp.is_leaf, n_subgrids, hp.items + first[c], n, hp.L,
+                               hp.Lc, gsolve_type, precision, ctx->d_lists, ctx->list_capacity, ctx->d_err,
+                               ctx->tuning, s, nullptr, false);
+            if (rc) return rc;
+        }
+        OT_CUDA(cudaEventRecord(ev_comp[c], s));
+    }
+    for (int k = 0; k < K; ++k) {
+        OT_CUDA(cudaStreamWaitEvent(hp.d2h, ev_comp[need[k]], 0));
+        const size_t a = bnd[k], n = bnd[k + 1] - bnd[k];
+        OT_CUDA(cudaMemcpyAsync(L + a * 20 * NCELL, hp.L + a * 20 * NCELL, n * 20 * cell, cudaMemcpyDeviceToHost,
+                                hp.d2h));
+        OT_CUDA(cudaMemcpyAsync(L_c + a * 3 * NCELL, hp.Lc + a * 3 * NCELL, n * 3 * cell, cudaMemcpyDeviceToHost,
+                                hp.d2h));
+        OT_CUDA(cudaEventRecord(ev_d2h[k], hp.d2h));
+    }
+    OT_CUDA(cudaEventRecord(ev_done, hp.d2h));
+    OT_CUDA(cudaStreamWaitEvent(s, ev_done, 0));
     return OTFMM_OK;
 }
 

@@ -26,7 +26,7 @@ PRECISIONS = {"fp64_exact": FP64_EXACT, "fp64": FP64, "fp32_split": FP32_SPLIT}
 EXPORTED = ["otfmm_create", "otfmm_destroy", "otfmm_stencil_info", "otfmm_m2l_soa", "otfmm_m2l_soa_host",
             "otfmm_p2p_soa", "otfmm_p2m_soa", "otfmm_batch", "otfmm_batch_status", "otfmm_count_pairs",
             "otfmm_m2l_soa_host_noalloc", "otfmm_stage_soa", "otfmm_stage_p2m_soa", "otfmm_get_tuning",
-            "otfmm_set_tuning", "otfmm_autotune", "otfmm_batch_profile", "otfmm_plan_create", "otfmm_plan_launch", "otfmm_plan_status",
+            "otfmm_set_tuning", "otfmm_autotune", "otfmm_batch_profile", "otfmm_batch_host", "otfmm_plan_create", "otfmm_plan_launch", "otfmm_plan_status",
             "otfmm_plan_destroy", "otfmm_last_error",
             "otfmm_build_info", "otfmm_measure_fma_peaks"]
 
@@ -78,6 +78,7 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
         lib.otfmm_plan_create.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int32, vp, ctypes.c_int32, vp, vp, i, i,
                                           ctypes.POINTER(vp)]
         lib.otfmm_plan_launch.argtypes = [vp, vp]
+        lib.otfmm_batch_host.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int32, vp, ctypes.c_int32, vp, vp, i, i, vp]
         lib.otfmm_batch_profile.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int32, vp, ctypes.c_int32, vp, vp, i, i,
                                             ctypes.POINTER(ctypes.c_float), vp]
         lib.otfmm_plan_status.argtypes = [vp, vp]
@@ -227,6 +228,26 @@ class Context:
         _check(load_library().otfmm_batch(self.handle, _ptr(dev.M), _ptr(dev.com), _ptr(dev.mon), _ptr(dev.is_leaf),
                                           ctypes.c_int32(dev.n), _ptr(items_dev), ctypes.c_int32(n_items), _ptr(L),
                                           _ptr(Lc), int(gsolve_type), precision_code(precision), _stream(stream)))
+
+    def batch_host(self, M, com, mon, is_leaf, n_subgrids: int, items, n_items: int, L, Lc, gsolve_type=RHO,
+                   precision=FP64, stream=None) -> None:
+        """Batched solve from host buffers (numpy arrays or pinned CPU torch
+        tensors): pipelined uploads, kernels and downloads; L / Lc are
+        complete once `stream` has finished."""
+        def hp(a):
+            if a is None:
+                return None
+            if hasattr(a, "data_ptr"):
+                if a.is_cuda:
+                    raise ValueError("batch_host takes host buffers")
+                return ctypes.c_void_p(a.data_ptr())
+            if not a.flags.c_contiguous:
+                raise ValueError("host buffers must be C-contiguous")
+            return ctypes.c_void_p(a.ctypes.data)
+        _check(load_library().otfmm_batch_host(self.handle, hp(M), hp(com), hp(mon), hp(is_leaf),
+                                               ctypes.c_int32(n_subgrids), hp(items), ctypes.c_int32(n_items),
+                                               hp(L), hp(Lc), int(gsolve_type), precision_code(precision),
+                                               _stream(stream)))
 
     def batch_profile(self, dev: "DevicePool", items_dev, n_items: int, L, Lc, gsolve_type=RHO, precision=FP64,
                       stream=None) -> dict:

@@ -121,3 +121,37 @@ def test_batch_profile_times_each_kernel_and_matches_batch(ctx):
     L, Lc = s.results()
     np.testing.assert_array_equal(L, L0)
     np.testing.assert_array_equal(Lc, Lc0)
+
+
+@pytest.mark.parametrize("precision", ["fp64_exact", "fp32_split"])
+@pytest.mark.parametrize("pinned", [False, True])
+def test_batch_host_matches_device_batch(ctx, precision, pinned):
+    """otfmm_batch_host (chunked uploads, kernels and downloads) gives the
+    device batch's results, and zeros where the solve writes nothing."""
+    import torch
+    from octotiger_b200.otfmm import BatchSolver, order_work_list
+    b = amr_small()
+    s = BatchSolver(ctx, b.pool, b.items)
+    s.run(RHO, precision)
+    L0, Lc0 = s.results()
+    n = b.pool.n
+    items = order_work_list(b.items)
+    if pinned:
+        arrs = {k: torch.from_numpy(getattr(b.pool, k)).pin_memory() for k in ("M", "com", "mon", "is_leaf")}
+        it = torch.from_numpy(items.view(np.uint8).reshape(-1).copy()).pin_memory()
+        L = torch.full((n, 20, 512), np.nan, dtype=torch.float64).pin_memory()
+        Lc = torch.full((n, 3, 512), np.nan, dtype=torch.float64).pin_memory()
+    else:
+        arrs = {k: np.ascontiguousarray(getattr(b.pool, k)) for k in ("M", "com", "mon", "is_leaf")}
+        it = items
+        L = np.full((n, 20, 512), np.nan)
+        Lc = np.full((n, 3, 512), np.nan)
+    for _ in range(2):   # the second call reuses the context's buffers
+        ctx.batch_host(arrs["M"], arrs["com"], arrs["mon"], arrs["is_leaf"], n, it, len(items), L, Lc, RHO,
+                       precision)
+        torch.cuda.synchronize()
+        ctx.batch_status()
+        Lh = L.numpy() if pinned else L
+        Lch = Lc.numpy() if pinned else Lc
+        np.testing.assert_array_equal(Lh, L0)
+        np.testing.assert_array_equal(Lch, Lc0)
