@@ -253,6 +253,46 @@ int otfmm_batch_host(otfmm_context* ctx, const double* pool_M, const double* poo
                      const uint8_t* pool_is_leaf, int32_t n_subgrids, const otfmm_work_item* items, int32_t n_items,
                      double* L, double* L_c, int gsolve_type, int precision, void* stream);
 
+/* ------------------------------------------------------------------ tree passes
+ * The two passes around the interaction kernels of a gravity solve, on the
+ * device from the resident pool. One node of the octree (48 bytes): */
+typedef struct otfmm_tree_node {
+    int32_t subgrid;  /* pool index of the node */
+    int32_t parent;   /* pool index of its parent, -1 for the root */
+    int32_t octant;   /* its octant in the parent: x + 2y + 4z (geo::octant) */
+    int32_t reserved;
+    double dx;        /* cell size */
+    double xbase[3];  /* centre of inner cell (0,0,0) */
+} otfmm_tree_node;
+
+/* Upward pass (M2M): grid::compute_multipoles (src/grid_fmm.cpp:1639-1803)
+ * with the octant gather of node_server::compute_fmm (src/node_server.cpp:613-640).
+ * `nodes` (device) are ordered by level, root first; level l is
+ * [level_start[l], level_start[l+1]) (host array of n_levels + 1). Levels run
+ * finest first: every node forms the centres of mass of its 4^3 coarse cells
+ * (RHO; written to com1[n][3][64]) and the multipoles of its children shifted
+ * to them (taylor::operator>>=), written into its parent's cells of its octant
+ * (pool M and com). Leaves take pool mon as their cell masses and, for RHO,
+ * their cell centres as centres of mass. DRHODT reuses com / com1 of the
+ * preceding RHO pass. Arithmetic in the reference's order (bit-identical to
+ * the oracle). Asynchronous; malformed nodes raise the flag otfmm_batch_status
+ * reports. */
+int otfmm_upward(otfmm_context* ctx, double* pool_M, double* pool_com, const double* pool_mon,
+                 const uint8_t* pool_is_leaf, double* com1, int32_t n_subgrids, const otfmm_tree_node* nodes,
+                 const int32_t* level_start, int32_t n_levels, int gsolve_type, void* stream);
+
+/* Downward pass (L2L): grid::compute_expansions (src/grid_fmm.cpp:1525-1637)
+ * with the octant scatter of node_server (src/node_server.cpp:756-786), root
+ * first: every fine cell adds its parent cell's expansion shifted to the cell's
+ * centre of mass (taylor::operator<<=) and the parent's L_c (RHO) to L / L_c
+ * (the interaction outputs, [n][20][512] / [n][3][512]); leaves then write
+ * G[n][4][512]: RHO phi = gconst L0, g = -gconst (L1..3 + L_c if
+ * correct_am_grav); DRHODT d(phi)/dt = gconst L0 in slot 0. */
+int otfmm_downward(otfmm_context* ctx, const double* pool_com, const uint8_t* pool_is_leaf, const double* com1,
+                   int32_t n_subgrids, const otfmm_tree_node* nodes, const int32_t* level_start, int32_t n_levels,
+                   double* L, double* L_c, double* G, double gconst, int correct_am_grav, int gsolve_type,
+                   void* stream);
+
 /* Cell-interactions a work list evaluates (host-side count, no device
  * work): the (cell, partner) pairs that pass the stencil and coarse-distance
  * masks, which is what the reference's kernels evaluate. per_class (may be

@@ -26,7 +26,8 @@ PRECISIONS = {"fp64_exact": FP64_EXACT, "fp64": FP64, "fp32_split": FP32_SPLIT}
 EXPORTED = ["otfmm_create", "otfmm_destroy", "otfmm_stencil_info", "otfmm_m2l_soa", "otfmm_m2l_soa_host",
             "otfmm_p2p_soa", "otfmm_p2m_soa", "otfmm_batch", "otfmm_batch_status", "otfmm_count_pairs",
             "otfmm_m2l_soa_host_noalloc", "otfmm_stage_soa", "otfmm_stage_p2m_soa", "otfmm_get_tuning",
-            "otfmm_set_tuning", "otfmm_autotune", "otfmm_batch_profile", "otfmm_batch_host", "otfmm_plan_create", "otfmm_plan_launch", "otfmm_plan_status",
+            "otfmm_set_tuning", "otfmm_autotune", "otfmm_batch_profile", "otfmm_batch_host", "otfmm_upward",
+            "otfmm_downward", "otfmm_plan_create", "otfmm_plan_launch", "otfmm_plan_status",
             "otfmm_plan_destroy", "otfmm_last_error",
             "otfmm_build_info", "otfmm_measure_fma_peaks"]
 
@@ -78,6 +79,9 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
         lib.otfmm_plan_create.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int32, vp, ctypes.c_int32, vp, vp, i, i,
                                           ctypes.POINTER(vp)]
         lib.otfmm_plan_launch.argtypes = [vp, vp]
+        lib.otfmm_upward.argtypes = [vp, vp, vp, vp, vp, vp, ctypes.c_int32, vp, vp, ctypes.c_int32, i, vp]
+        lib.otfmm_downward.argtypes = [vp, vp, vp, vp, ctypes.c_int32, vp, vp, ctypes.c_int32, vp, vp, vp, dp, i, i,
+                                       vp]
         lib.otfmm_batch_host.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int32, vp, ctypes.c_int32, vp, vp, i, i, vp]
         lib.otfmm_batch_profile.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int32, vp, ctypes.c_int32, vp, vp, i, i,
                                             ctypes.POINTER(ctypes.c_float), vp]
@@ -249,6 +253,24 @@ class Context:
                                                hp(L), hp(Lc), int(gsolve_type), precision_code(precision),
                                                _stream(stream)))
 
+    def upward(self, dev: "DevicePool", com1, nodes_dev, level_start: np.ndarray, gsolve_type=RHO,
+               stream=None) -> None:
+        """M2M pass (see otfmm_upward): fills the refined nodes' M / com and com1."""
+        ls = np.ascontiguousarray(level_start, dtype=np.int32)
+        _check(load_library().otfmm_upward(self.handle, _ptr(dev.M), _ptr(dev.com), _ptr(dev.mon), _ptr(dev.is_leaf),
+                                           _ptr(com1), ctypes.c_int32(dev.n), _ptr(nodes_dev), ls.ctypes.data,
+                                           ctypes.c_int32(len(ls) - 1), int(gsolve_type), _stream(stream)))
+
+    def downward(self, dev: "DevicePool", com1, nodes_dev, level_start: np.ndarray, L, Lc, G, gconst=1.0,
+                 correct_am_grav=True, gsolve_type=RHO, stream=None) -> None:
+        """L2L pass (see otfmm_downward): adds the parents' expansions to L / L_c, writes G of leaves."""
+        ls = np.ascontiguousarray(level_start, dtype=np.int32)
+        _check(load_library().otfmm_downward(self.handle, _ptr(dev.com), _ptr(dev.is_leaf), _ptr(com1),
+                                             ctypes.c_int32(dev.n), _ptr(nodes_dev), ls.ctypes.data,
+                                             ctypes.c_int32(len(ls) - 1), _ptr(L), _ptr(Lc), _ptr(G),
+                                             float(gconst), int(bool(correct_am_grav)), int(gsolve_type),
+                                             _stream(stream)))
+
     def batch_profile(self, dev: "DevicePool", items_dev, n_items: int, L, Lc, gsolve_type=RHO, precision=FP64,
                       stream=None) -> dict:
         """One batched solve with per-kernel device times (ms)."""
@@ -357,6 +379,42 @@ class BatchSolver:
     def plan(self, gsolve_type=RHO, precision=FP64) -> "Plan":
         """This solve captured into a CUDA graph (see otfmm_plan_create)."""
         return Plan(self.ctx, self.dev, self.items, self.n_items, self.L, self.Lc, gsolve_type, precision)
+
+
+class GravitySolver:
+    """A whole gravity solve on the device (node_server::solve_gravity's
+    order): the upward pass (M2M) fills the refined nodes' multipoles from the
+    leaves' masses, the batched interaction kernels fill L / L_c, the downward
+    pass (L2L) adds the parents' expansions and writes the leaves' potential
+    and acceleration G[n][4][512]."""
+
+    def __init__(self, ctx: Context, pool: SubgridPool, items: np.ndarray, nodes: np.ndarray,
+                 level_start: np.ndarray, gconst: float = 1.0, correct_am_grav: bool = True):
+        torch = _require_cuda()
+        self.batch = BatchSolver(ctx, pool, items)
+        self.ctx = ctx
+        d = torch.device("cuda", ctx.device)
+        raw = np.ascontiguousarray(nodes).view(np.uint8).reshape(-1)
+        self.nodes = torch.from_numpy(raw.copy()).to(d)
+        self.level_start = np.ascontiguousarray(level_start, dtype=np.int32)
+        self.com1 = torch.zeros((pool.n, 3, 64), dtype=torch.float64, device=d)
+        self.G = torch.zeros((pool.n, 4, NCELL), dtype=torch.float64, device=d)
+        self.gconst = gconst
+        self.correct_am_grav = correct_am_grav
+
+    def run(self, gsolve_type=RHO, precision=FP64, stream=None) -> None:
+        b = self.batch
+        self.ctx.upward(b.dev, self.com1, self.nodes, self.level_start, gsolve_type, stream)
+        b.L.zero_()
+        b.Lc.zero_()
+        b.run(gsolve_type, precision, stream)
+        self.ctx.downward(b.dev, self.com1, self.nodes, self.level_start, b.L, b.Lc, self.G, self.gconst,
+                          self.correct_am_grav, gsolve_type, stream)
+
+    def results(self):
+        """(L, L_c, G) as numpy arrays after checking the device error flag."""
+        self.ctx.batch_status()
+        return self.batch.L.cpu().numpy(), self.batch.Lc.cpu().numpy(), self.G.cpu().numpy()
 
 
 class Plan:

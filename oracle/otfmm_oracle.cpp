@@ -15,6 +15,7 @@
 // Parity is pinned against the reference's own templates compiled by
 // oracle/build_ref.sh (bit-for-bit) and against the committed golden vectors.
 #include "oracle_core.hpp"
+#include "tree_passes.hpp"
 
 namespace ora {
 namespace {
@@ -321,7 +322,77 @@ struct OracleKernels {
 }   // namespace ora
 
 // ---------------------------------------------------------------- C ABI (ctypes)
+// Shift operators of taylor<4> (octotiger/taylor.hpp:222-318) restated with
+// the reference's operation order; component order of src/taylor.cpp:10-56.
+struct ScalarShift {
+    static int i2(int a, int b) { return ora::kQuadRow[a][b]; }
+    static int i3(int a, int b, int c) {
+        static constexpr int m3[3][3][3] = {{{10, 11, 12}, {11, 13, 14}, {12, 14, 15}},
+                                            {{11, 13, 14}, {13, 16, 17}, {14, 17, 18}},
+                                            {{12, 14, 15}, {14, 17, 18}, {15, 18, 19}}};
+        return m3[a][b][c];
+    }
+    // B = A >> X (operator>>=, :222-255)
+    void up(const double A[20], const double X[3], double B[20]) const {
+        for (int j = 0; j < 20; ++j) B[j] = A[j];
+        for (int a = 0; a < 3; ++a) B[1 + a] += A[0] * X[a];
+        for (int a = 0; a < 3; ++a)
+            for (int b = a; b < 3; ++b) {
+                B[i2(a, b)] += A[1 + a] * X[b] + X[a] * A[1 + b];
+                B[i2(a, b)] += A[0] * X[a] * X[b];
+            }
+        for (int a = 0; a < 3; ++a)
+            for (int b = a; b < 3; ++b)
+                for (int c = b; c < 3; ++c) {
+                    B[i3(a, b, c)] += A[i2(a, b)] * X[c] + A[i2(b, c)] * X[a] + A[i2(c, a)] * X[b];
+                    B[i3(a, b, c)] += A[1 + a] * X[b] * X[c] + A[1 + b] * X[c] * X[a] + A[1 + c] * X[a] * X[b];
+                    B[i3(a, b, c)] += A[0] * X[a] * X[b] * X[c];
+                }
+    }
+    // B = A << X (operator<<=, :263-318)
+    void down(const double A[20], const double X[3], double B[20]) const {
+        constexpr double half = 1.0 / 2.0, sixth = 1.0 / 6.0;
+        for (int j = 0; j < 20; ++j) B[j] = A[j];
+        for (int a = 0; a < 3; ++a) B[0] += A[1 + a] * X[a];
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) B[0] += A[i2(a, b)] * X[a] * X[b] * half;
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) B[1 + a] += A[i2(a, b)] * X[b];
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b)
+                for (int c = 0; c < 3; ++c) B[0] += A[i3(a, b, c)] * X[a] * X[b] * X[c] * sixth;
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b)
+                for (int c = 0; c < 3; ++c) B[1 + a] += A[i3(a, b, c)] * X[b] * X[c] * half;
+        for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b)
+                for (int c = a; c < 3; ++c) B[i2(a, c)] += A[i3(a, b, c)] * X[b];
+    }
+};
+
 extern "C" {
+
+int oracle_shift(const double* A, const double* X, double* B, int down) {
+    ScalarShift S;
+    if (down) S.down(A, X, B);
+    else S.up(A, X, B);
+    return 0;
+}
+
+int oracle_upward(double* M, double* com, const double* mon, const uint8_t* is_leaf, double* com1, int n,
+                  const ora::TreeNode* nodes, const int32_t* level_start, int n_levels, int rho) {
+    ora::TreePool P{M, com, mon, is_leaf, com1, n};
+    ora::upward_pass(ScalarShift{}, P, nodes, level_start, n_levels, rho != 0);
+    return 0;
+}
+
+int oracle_downward(const double* com, const uint8_t* is_leaf, const double* com1, int n, const ora::TreeNode* nodes,
+                    const int32_t* level_start, int n_levels, double* L, double* Lc, double* G, double gconst,
+                    int correct_am, int rho) {
+    ora::TreePool P{nullptr, const_cast<double*>(com), nullptr, is_leaf, const_cast<double*>(com1), n};
+    ora::downward_pass(ScalarShift{}, P, nodes, level_start, n_levels, L, Lc, G, gconst, correct_am != 0, rho != 0);
+    return 0;
+}
 
 int oracle_build_stencil(double theta, uint8_t* mpole_mask, uint8_t* mpole_phase, uint8_t* p2p_mask,
                          double* four, int* counts) {

@@ -45,6 +45,52 @@ class _Common:
         pool.validate()
         return (_ptr(pool.M), _ptr(pool.com), _ptr(pool.mon), _ptr(pool.is_leaf, _u8p), ctypes.c_int(pool.n))
 
+    # ------------------------------------------------------------ tree passes
+    _up = "oracle_upward"
+    _down = "oracle_downward"
+    _shift = "oracle_shift"
+
+    def shift(self, A: np.ndarray, X: np.ndarray, down: bool) -> np.ndarray:
+        """taylor<4> shift of 20 moments / expansion coefficients by X."""
+        A = np.ascontiguousarray(A, dtype=np.float64)
+        X = np.ascontiguousarray(X, dtype=np.float64)
+        B = np.zeros(20)
+        getattr(self.lib, self._shift)(_ptr(A), _ptr(X), _ptr(B), int(down))
+        return B
+
+    def upward(self, pool: SubgridPool, nodes: np.ndarray, level_start: np.ndarray, rho: bool = True,
+               com1: np.ndarray | None = None):
+        """Upward pass on copies of the pool: returns (M, com, com1)."""
+        M = pool.M.copy()
+        com = pool.com.copy()
+        com1 = np.zeros((pool.n, 3, 64)) if com1 is None else com1.copy()
+        nodes = np.ascontiguousarray(nodes)
+        ls = np.ascontiguousarray(level_start, dtype=np.int32)
+        rc = getattr(self.lib, self._up)(_ptr(M), _ptr(com), _ptr(pool.mon), _ptr(pool.is_leaf, _u8p),
+                                         _ptr(com1), ctypes.c_int(pool.n), nodes.ctypes.data_as(ctypes.c_void_p),
+                                         _ptr(ls, _ip), ctypes.c_int(len(ls) - 1), int(rho))
+        _check(rc, self._up)
+        return M, com, com1
+
+    def downward(self, com, is_leaf, com1, nodes, level_start, L, Lc, gconst: float = 1.0,
+                 correct_am: bool = True, rho: bool = True):
+        """Downward pass on copies of L, L_c: returns (L, L_c, G)."""
+        L = np.ascontiguousarray(L, dtype=np.float64).copy()
+        Lc = np.ascontiguousarray(Lc, dtype=np.float64).copy()
+        G = np.zeros((L.shape[0], 4, NCELL))
+        com = np.ascontiguousarray(com, dtype=np.float64)
+        com1 = np.ascontiguousarray(com1, dtype=np.float64)
+        is_leaf = np.ascontiguousarray(is_leaf, dtype=np.uint8)
+        nodes = np.ascontiguousarray(nodes)
+        ls = np.ascontiguousarray(level_start, dtype=np.int32)
+        rc = getattr(self.lib, self._down)(_ptr(com), _ptr(is_leaf, _u8p), _ptr(com1), ctypes.c_int(L.shape[0]),
+                                           nodes.ctypes.data_as(ctypes.c_void_p), _ptr(ls, _ip),
+                                           ctypes.c_int(len(ls) - 1), _ptr(L), _ptr(Lc), _ptr(G),
+                                           ctypes.c_double(gconst), int(correct_am), int(rho))
+        _check(rc, self._down)
+        return L, Lc, G
+
+
 
 class Oracle(_Common):
     def __init__(self, path: Path = ORACLE_SO):
@@ -148,7 +194,12 @@ def ref_library_path() -> Path | None:
 
 
 class RefMath(_Common):
-    """The reference's own kernel arithmetic (SIMD lanes along z)."""
+    """The reference's own kernel arithmetic (SIMD lanes along z; the tree
+    passes through its taylor<4> shift operators)."""
+
+    _up = "ref_upward"
+    _down = "ref_downward"
+    _shift = "ref_shift"
 
     def __init__(self, path: Path | None = None):
         path = path or ref_library_path()

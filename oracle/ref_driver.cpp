@@ -1,12 +1,14 @@
 // TEST INFRASTRUCTURE ONLY — compiled by oracle/build_ref.sh into oracle/_ref/.
 //
-// Runs Octo-Tiger's own kernel arithmetic on the CPU. The per-pair math and
-// the stencil generators are the reference's, included from its source tree
-// at build time (nothing of it is copied into this repository):
+// Runs Octo-Tiger's own kernel arithmetic on the CPU. The per-pair math, the
+// stencil generators and the multipole shift operators are the reference's,
+// included from its source tree at build time (nothing of it is copied into
+// this repository):
 //   octotiger/multipole_interactions/kernel/compute_kernel_templates.hpp
 //   octotiger/monopole_interactions/kernel/monopole_kernel_templates.hpp
 //   src/multipole_interactions/util/calculate_stencil.cpp
 //   src/monopole_interactions/util/calculate_stencil.cpp
+//   octotiger/taylor.hpp, src/taylor.cpp (tree passes, oracle/tree_passes.hpp)
 // The sweep loops of the reference live in its Kokkos kernels
 // (octotiger/multipole_interactions/kernel/kokkos_kernel.hpp:137-764,
 // octotiger/monopole_interactions/kernel/kokkos_kernel.hpp:143-943), which need
@@ -29,6 +31,12 @@
 
 #include "src/monopole_interactions/util/calculate_stencil.cpp"
 #include "src/multipole_interactions/util/calculate_stencil.cpp"
+
+// The shift operators of the tree passes: the reference's taylor<4> class and
+// its index maps (octotiger/taylor.hpp, src/taylor.cpp), included in place.
+#include "octotiger/taylor.hpp"
+#include "src/taylor.cpp"
+#include "tree_passes.hpp"
 
 namespace stdx = std::experimental;
 namespace ofmm = octotiger::fmm;
@@ -372,7 +380,41 @@ struct RefKernels {
 
 }   // namespace
 
+// Upward / downward shifts through the reference's taylor<4, double> operators.
+struct RefShift {
+    static void run(const double A[20], const double X[3], double B[20], bool down) {
+        taylor<4, double> t;
+        for (int j = 0; j < 20; ++j) t[j] = A[j];
+        const std::array<double, 3> x{X[0], X[1], X[2]};
+        if (down) t <<= x;
+        else t >>= x;
+        for (int j = 0; j < 20; ++j) B[j] = t[j];
+    }
+    void up(const double A[20], const double X[3], double B[20]) const { run(A, X, B, false); }
+    void down(const double A[20], const double X[3], double B[20]) const { run(A, X, B, true); }
+};
+
 extern "C" {
+
+int ref_shift(const double* A, const double* X, double* B, int down) {
+    RefShift::run(A, X, B, down != 0);
+    return 0;
+}
+
+int ref_upward(double* M, double* com, const double* mon, const uint8_t* is_leaf, double* com1, int n,
+               const ora::TreeNode* nodes, const int32_t* level_start, int n_levels, int rho) {
+    ora::TreePool P{M, com, mon, is_leaf, com1, n};
+    ora::upward_pass(RefShift{}, P, nodes, level_start, n_levels, rho != 0);
+    return 0;
+}
+
+int ref_downward(const double* com, const uint8_t* is_leaf, const double* com1, int n, const ora::TreeNode* nodes,
+                 const int32_t* level_start, int n_levels, double* L, double* Lc, double* G, double gconst,
+                 int correct_am, int rho) {
+    ora::TreePool P{nullptr, const_cast<double*>(com), nullptr, is_leaf, const_cast<double*>(com1), n};
+    ora::downward_pass(RefShift{}, P, nodes, level_start, n_levels, L, Lc, G, gconst, correct_am != 0, rho != 0);
+    return 0;
+}
 
 // simd_mode: 0 = scalar lanes, 1 = native SIMD lanes of this build.
 int ref_simd_width(int simd_mode) { return simd_mode ? int(native_simd::size()) : 1; }

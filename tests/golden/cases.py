@@ -27,3 +27,9 @@ def input_digest(batch) -> str:
     for a in (batch.pool.M, batch.pool.com, batch.pool.mon, batch.pool.is_leaf, batch.items):
         h.update(a.tobytes())
     return h.hexdigest()
+
+
+def tree_case():
+    """A small polytrope octree (levels 0-4) for the tree-pass goldens."""
+    from octotiger_b200 import amr
+    return amr.polytrope_batch(radius=0.05, max_level=4, seed=81)
