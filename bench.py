@@ -377,6 +377,47 @@ def gpu_arm(args) -> None:
         e2e_ms = float(t.item())
     e2e_value = world * counts["total"] * args.steps / (e2e_ms * 1e-3)
 
+    # a whole gravity solve where the workload is a full octree (upward M2M,
+    # the interaction solve replayed from its graph, downward L2L with the
+    # leaves' potential and acceleration), device time per solve
+    gravity = None
+    levels = getattr(batch, "levels", None)
+    if levels is not None and len(levels) and int(np.min(levels)) == 0:
+        from octotiger_b200.tree import batch_tree
+        nodes, level_start = batch_tree(batch)
+        nodes_dev = torch.from_numpy(np.ascontiguousarray(nodes).view(np.uint8).reshape(-1).copy()).to(dev)
+        com1 = torch.zeros((batch.pool.n, 3, 64), dtype=torch.float64, device=dev)
+        G = torch.zeros((batch.pool.n, 4, 512), dtype=torch.float64, device=dev)
+        plan = plans[args.precision]
+
+        def gravity_solve(marks):
+            marks[0].record(stream)
+            ctx.upward(solver.dev, com1, nodes_dev, level_start, solve)
+            marks[1].record(stream)
+            solver.L.zero_()
+            solver.Lc.zero_()
+            plan.launch()
+            marks[2].record(stream)
+            ctx.downward(solver.dev, com1, nodes_dev, level_start, solver.L, solver.Lc, G, 1.0, True, solve)
+            marks[3].record(stream)
+
+        marks = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        for _ in range(3):
+            gravity_solve(marks)
+        parts = []
+        for _ in range(max(3, args.steps // 2)):
+            flush.zero_()
+            gravity_solve(marks)
+            marks[3].synchronize()
+            parts.append([marks[0].elapsed_time(marks[1]), marks[1].elapsed_time(marks[2]),
+                          marks[2].elapsed_time(marks[3])])
+        plan.status()
+        solver.ctx.batch_status()
+        med = np.median(np.array(parts), axis=0)
+        gravity = {"ms_per_solve": float(med.sum()), "upward_ms": float(med[0]), "interactions_ms": float(med[1]),
+                   "downward_ms": float(med[2]), "n_nodes": int(len(nodes)), "levels": int(len(level_start) - 1),
+                   "what": "upward M2M + interaction solve (graph) + downward L2L and leaf potential/acceleration"}
+
     # roofline of the dominant kernel (the multipole tiles): nominal reference
     # FLOPs of one launch / its device time (CUDA events between the launches
     # of one solve, median of 5, L2 flushed) vs the FMA issue rate measured on
@@ -422,6 +463,7 @@ def gpu_arm(args) -> None:
         "direct_launch_ms_per_step": direct_ms,
         "tunings": tunings,
         "per_subgrid_fp64": per_subgrid,
+        "gravity_solve": gravity,
         "ratios": {"vs_batched_fp64": (value / world / others["fp64"]["value"]) if "fp64" in others else None,
                    "vs_per_subgrid_fp64": (value / world / per_subgrid["value"]) if per_subgrid else None},
         "accuracy_vs_fp64_exact": accuracy,
