@@ -130,6 +130,7 @@ struct Tables {
     const uint16_t* p2m_list;   // partner cell index (in its neighbour) of every entry, grouped by direction
     const int* p2m_perm_start;  // [28]: start of raw direction r in p2m_perm
     const uint16_t* p2m_perm;   // per direction, the cells with partners there, most partners first
+    const int16_t* p2m_slot;    // [27][512]: position of a cell in its direction's p2m_perm list, -1 if absent
     const double4* p2p_four;    // [8][MAX_ENTRIES]: monopole constants of entries_p2p (zeros past the count)
 };
 
@@ -1434,6 +1435,110 @@ __global__ void __launch_bounds__(P_THREADS) p2m_batch_kernel(BatchArgs a) {
     }
 }
 
+// Fast-form P2M with every refined direction of a leaf in flight at once:
+// one CTA per leaf of the P2M work list (grid stride). The work of a leaf is
+// the list of (direction, cell, lane) slots of its refined directions, F lanes
+// per cell (F = the tuning's P2M lane count), walked in rounds of the CTA's
+// threads; the F lanes of a cell sum their partners' contributions in a fixed
+// butterfly order into one partial per (direction, cell) in shared memory.
+// After one barrier every cell adds its partials to its P2P result in direction
+// order. Deterministic; no barrier between directions.
+template <bool RHO>
+__global__ void __launch_bounds__(P_THREADS) p2m_fast_kernel(BatchArgs a) {
+    extern __shared__ double s_part[];   // [groups][7]: L0..L3, L_c x, y, z
+    __shared__ ItemInfo it;
+    __shared__ int s_dir[27], s_cum[28];
+    __shared__ int s_ndir;
+    const int F = a.p2m_lanes;
+    const int np2m = a.wl.counts[WL_P2M];
+    for (int kk = blockIdx.x; kk < np2m; kk += gridDim.x) {
+        __syncthreads();   // `it`, the direction list and s_part are reused
+        load_item(a, a.wl.p2m[kk], it);
+        if (threadIdx.x == 0) {
+            int n = 0, cum = 0;
+            for (int d = 0; d < 26; ++d) {
+                const int nb = it.nb[d];
+                if (nb >= 0 && !a.is_leaf[nb]) {
+                    const int r = d < 13 ? d : d + 1;
+                    s_dir[n] = r;
+                    s_cum[n] = cum;
+                    cum += (a.t.p2m_perm_start[r + 1] - a.t.p2m_perm_start[r]) * F;
+                    ++n;
+                }
+            }
+            s_cum[n] = cum;
+            s_ndir = n;
+        }
+        __syncthreads();
+        const int ndir = s_ndir, total = s_cum[ndir];
+        const size_t sub = (size_t)it.subgrid;
+        for (int g0 = 0; g0 < total; g0 += blockDim.x) {
+            const int g = g0 + threadIdx.x;
+            double acc[4] = {0.0, 0.0, 0.0, 0.0}, corr[3] = {0.0, 0.0, 0.0};
+            int k = 0;
+            if (g < total) {
+                while (s_cum[k + 1] <= g) ++k;
+                const int r = s_dir[k];
+                const int local = g - s_cum[k], tgt = local / F, f = local % F;
+                const int cu = __ldg(a.t.p2m_perm + a.t.p2m_perm_start[r] + tgt);
+                const size_t nb = (size_t)it.nb[r < 13 ? r : r - 1];
+                const double* __restrict__ nM = a.M + nb * 20 * NCELL;
+                const double* __restrict__ ncom = a.com + nb * 3 * NCELL;
+                double X[3];
+#pragma unroll
+                for (int q = 0; q < 3; ++q) X[q] = __ldg(a.com + (sub * 3 + q) * NCELL + cu);
+                const int beg = __ldg(a.t.p2m_start + cu * 28 + r), end = __ldg(a.t.p2m_start + cu * 28 + r + 1);
+#pragma unroll 1
+                for (int q = beg + f; q < end; q += F) {
+                    const int u = __ldg(a.t.p2m_list + q);
+                    double Y[3], mp[20];
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) Y[c] = __ldg(ncom + c * NCELL + u);
+#pragma unroll
+                    for (int c = 0; c < 20; ++c) mp[c] = __ldg(nM + c * NCELL + u) * stage_scale<PREC_FAST>(c);
+                    fast_p2m_pair<RHO>(X, Y, mp, acc, corr);
+                }
+            }
+            // F lanes of a cell are aligned within the warp (F divides 32, every
+            // direction's slot count is a multiple of F)
+            for (int o = F >> 1; o > 0; o >>= 1) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+#pragma unroll
+                for (int q = 0; q < 3; ++q) corr[q] += __shfl_xor_sync(0xffffffffu, corr[q], o);
+            }
+            if (g < total && (g % F) == 0) {
+                double* part = s_part + (size_t)(g / F) * 7;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) part[q] = acc[q];
+#pragma unroll
+                for (int q = 0; q < 3; ++q) part[4 + q] = corr[q];
+            }
+        }
+        __syncthreads();
+        double* L = a.L + sub * 20 * NCELL;
+        double* Lc = a.Lc + sub * 3 * NCELL;
+        for (int cu = threadIdx.x; cu < NCELL; cu += blockDim.x) {
+            double acc[4], corr[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[q] = L[q * NCELL + cu];
+            for (int k = 0; k < ndir; ++k) {
+                const int t = __ldg(a.t.p2m_slot + s_dir[k] * NCELL + cu);
+                if (t < 0) continue;
+                const double* part = s_part + (size_t)(s_cum[k] / F + t) * 7;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) acc[q] += part[q];
+#pragma unroll
+                for (int q = 0; q < 3; ++q) corr[q] += part[4 + q];
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) L[q * NCELL + cu] = acc[q];
+#pragma unroll
+            for (int q = 0; q < 3; ++q) Lc[q * NCELL + cu] = RHO ? corr[q] : 0.0;
+        }
+    }
+}
+
 struct SoaArgs {
     const double* mon;
     const double* M;
@@ -2009,6 +2114,8 @@ struct otfmm_context {
     uint16_t* d_p2m_list = nullptr;
     int* d_p2m_perm_start = nullptr;
     uint16_t* d_p2m_perm = nullptr;
+    int16_t* d_p2m_slot = nullptr;
+    int p2m_groups_max = 0;   // cells with partners summed over the 26 directions
     double4* d_p2p_four = nullptr;
     int counts_far[8] = {};
     double* d_four = nullptr;
@@ -2034,7 +2141,7 @@ struct otfmm_context {
     std::mutex mu;
     Tables tables() const { return Tables{d_entries,    d_count, d_entries_fast, d_count_far, d_entries_split, d_entries_p2p,
                       d_entries_ws, d_four,  d_phase,        d_p2m_start,     d_p2m_list,    d_p2m_perm_start,
-                      d_p2m_perm,   d_p2p_four}; }
+                      d_p2m_perm,   d_p2m_slot,     d_p2p_four}; }
 };
 
 namespace {
@@ -2083,6 +2190,8 @@ int ensure_attributes(int device) {
     rc = rc ? rc : set_smem(p2p_leaf_kernel<double, 0>, p2_smem_bytes<double>());
     rc = rc ? rc : set_smem(p2p_leaf_kernel<float, 32>, p2_smem_bytes<float>());
     rc = rc ? rc : set_smem(p2p_leaf_kernel<float, 16>, p2_smem_bytes<float>());
+    rc = rc ? rc : set_smem(p2m_fast_kernel<true>, 7 * 8 * 6 * NCELL);
+    rc = rc ? rc : set_smem(p2m_fast_kernel<false>, 7 * 8 * 6 * NCELL);
     rc = rc ? rc : set_smem(soa_m2l_kernel<PREC_EXACT, true, false>, bytes);
     rc = rc ? rc : set_smem(soa_m2l_kernel<PREC_EXACT, false, false>, bytes);
     rc = rc ? rc : set_smem(soa_m2l_kernel<PREC_FAST, true, false>, bytes);
@@ -2208,9 +2317,17 @@ int otfmm_create(int device, double theta, otfmm_context** out) {
         for (const auto& c : cells) p2m_perm.push_back((uint16_t)c.second);
     }
     p2m_perm_start[27] = (int)p2m_perm.size();
+    std::vector<int16_t> p2m_slot(27 * NCELL, -1);
+    for (int r = 0; r < 27; ++r)
+        for (int t = p2m_perm_start[r]; t < p2m_perm_start[r + 1]; ++t)
+            p2m_slot[r * NCELL + p2m_perm[t]] = (int16_t)(t - p2m_perm_start[r]);
+    ctx->p2m_groups_max = (int)p2m_perm.size();
     DeviceGuard g(device);
     cudaError_t e;
-    if ((e = cudaMalloc(&ctx->d_p2p_four, sizeof(double4) * p2p_four.size())) != cudaSuccess ||
+    if ((e = cudaMalloc(&ctx->d_p2m_slot, sizeof(int16_t) * p2m_slot.size())) != cudaSuccess ||
+        (e = cudaMemcpy(ctx->d_p2m_slot, p2m_slot.data(), sizeof(int16_t) * p2m_slot.size(),
+                        cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMalloc(&ctx->d_p2p_four, sizeof(double4) * p2p_four.size())) != cudaSuccess ||
         (e = cudaMemcpy(ctx->d_p2p_four, p2p_four.data(), sizeof(double4) * p2p_four.size(),
                         cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMalloc(&ctx->d_p2m_perm_start, sizeof(int) * p2m_perm_start.size())) != cudaSuccess ||
@@ -2278,6 +2395,7 @@ int otfmm_destroy(otfmm_context* ctx) {
     cudaFree(ctx->d_p2m_perm_start);
     cudaFree(ctx->d_p2m_perm);
     cudaFree(ctx->d_p2p_four);
+    cudaFree(ctx->d_p2m_slot);
     {
         auto& hp = ctx->hp;
         if (hp.ready) {
@@ -2582,8 +2700,9 @@ int enqueue_batch(otfmm_context* ctx, const double* pool_M, const double* pool_c
             p2p_leaf_kernel<double, 0><<<sms, P2_THREADS, p2_smem_bytes<double>(), s>>>(a);
         }
         mark(3);
-        if (rho) p2m_batch_kernel<PREC_FAST, true><<<p2m_grid, P_THREADS, 0, s>>>(a);
-        else p2m_batch_kernel<PREC_FAST, false><<<p2m_grid, P_THREADS, 0, s>>>(a);
+        const size_t part_bytes = sizeof(double) * 7 * (size_t)ctx->p2m_groups_max;
+        if (rho) p2m_fast_kernel<true><<<p2m_grid, P_THREADS, part_bytes, s>>>(a);
+        else p2m_fast_kernel<false><<<p2m_grid, P_THREADS, part_bytes, s>>>(a);
     }
     mark(4);
     OT_CUDA(cudaGetLastError());
