@@ -17,7 +17,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libotfmm.so"
 SOURCES = [CSRC / "otfmm.cu"]
-DEPS = SOURCES + [CSRC / "pair_math.cuh", ROOT / "include" / "otfmm.h", Path(__file__)]
+DEPS = SOURCES + sorted(CSRC.glob("*.cuh")) + [ROOT / "include" / "otfmm.h", Path(__file__)]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -1,0 +1,213 @@
+// Layout of the FMM interaction kernels: reference constants (GRIDDIM 8), the
+// tile geometry and shared-memory layouts, the per-context stencil tables, and
+// the batched-solve arguments with the device-side work lists and the work-item
+// classification kernel.
+// Part of libotfmm.so; included once, in order, by otfmm.cu (one translation unit).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "../../include/otfmm.h"
+#include "pair_math.cuh"
+
+namespace otfmm {
+
+constexpr int INX = 8;
+constexpr int NCELL = 512;
+constexpr int SMAX = 5;
+constexpr int SINX = 11;
+constexpr int FULL = SINX * SINX * SINX;
+constexpr int PSTRIDE = 18;
+constexpr int ENTRIES = PSTRIDE * PSTRIDE * PSTRIDE;
+constexpr int CL = ENTRIES + 19;   // reference input component stride
+constexpr int CLU = NCELL + 19;    // reference output component stride
+constexpr int PAD_OFF = 3;
+constexpr double THETA_MIN = 0.34;
+
+// Tile geometry for coarse reach 1 (theta >= 0.5).
+constexpr int THREADS = 256;
+constexpr int TILE_X = 4;
+constexpr int REG_X = TILE_X + 4;          // region x extent, origin x0 - 2
+constexpr int REG_YZ = INX + 4;            // region y, z extent, origin -2
+constexpr int REG_CELLS = REG_X * REG_YZ * REG_YZ;   // 1152
+constexpr int SUB_YZ = REG_YZ / 2;         // 6
+constexpr int NCOMP = 23;                  // m0, M1..M19, com x/y/z
+constexpr int RB = NCOMP * SUB_YZ + 2;     // 140 doubles per (x', y') row
+constexpr int XS = SUB_YZ * RB;            // 840
+constexpr int CLS = (REG_X / 2) * XS;      // 3360 doubles per parity class
+constexpr int SMEM_DOUBLES = 8 * CLS;      // 26880 doubles = 215040 bytes
+constexpr int MAX_ENTRIES = 216;           // 6^3 - 1 partners per cell at most
+constexpr int ROOT_SMEM_DOUBLES = NCOMP * NCELL;
+static_assert(ROOT_SMEM_DOUBLES <= SMEM_DOUBLES, "root staging fits");
+static_assert(RB % 16 == 12 || RB % 16 == 4, "row stride must keep 4x4 lane blocks conflict-free");
+
+// FP32-split layout: per cell 14 FP64 components (centre of mass / dx, mass,
+// scaled octupoles for L_c) and 20 FP32 components (scaled moments). Rows of
+// 6 cells: 84 doubles then 120 floats, padded to 148 doubles (= 4 mod 16:
+// conflict-free 8-byte loads per half-warp); the x stride of 890 doubles
+// makes the 32 lanes' 4-byte loads hit 32 distinct banks.
+constexpr int S_DCOMP = 14;
+constexpr int S_FCOMP = 20;
+constexpr int S_RB = 148;
+constexpr int S_FOFF = 2 * S_DCOMP * SUB_YZ;   // float offset of the FP32 part within a row
+constexpr int S_XS = 890;
+constexpr int S_CLS = (REG_X / 2) * S_XS;
+constexpr int S_SMEM_DOUBLES = 8 * S_CLS;      // 28480 doubles = 227840 bytes
+constexpr int SPLIT_CHUNK = 16;                // FP32 partial sums promoted to FP64 every 16 partners
+static_assert(S_RB >= S_DCOMP * SUB_YZ + S_FCOMP * SUB_YZ / 2, "split row fits");
+static_assert(S_RB % 16 == 4 || S_RB % 16 == 12, "split rows conflict-free for 8-byte loads");
+static_assert(S_XS >= SUB_YZ * S_RB && (S_XS % 16 == 2 || S_XS % 16 == 6 || S_XS % 16 == 10 || S_XS % 16 == 14),
+              "split x stride");
+static_assert(S_SMEM_DOUBLES * 8 <= 232448, "split layout fits the 227 KB shared-memory limit");
+
+// P2P layout: one leaf subgrid per CTA (512 threads, one cell each); the
+// mass region -2..9 per axis split by parity into 6^3 sub-lattices with rows
+// padded to 12 doubles (4x4 lane blocks conflict-free).
+constexpr int P_THREADS = 512;
+constexpr int P_REG = INX + 4;
+constexpr int P_SUB = 6;
+constexpr int P_RS = 12;
+constexpr int P_XS = 80;                    // >= 6 rows of 12; = 16 mod 32 for the FP32 copy
+constexpr int P_CLS = P_SUB * P_XS;
+constexpr int P_SMEM_DOUBLES = 8 * P_CLS;   // 3840 elements
+// Lane (i, j, k) = (l >> 4, (l >> 2) & 3, l & 3) reads element k + 12 j + 80 i:
+// distinct 8-byte slots per half-warp and distinct 4-byte banks per warp.
+static_assert(P_XS >= P_SUB * P_RS && P_RS % 16 == 12 && P_XS % 32 == 16, "P2P region strides");
+
+// Monopole constants {-1/r, x/r^3, y/r^3, z/r^3} per stencil offset (they do
+// not depend on theta), read warp-uniformly through the constant cache.
+__constant__ double c_four[FULL][4];
+
+// Entry flags
+constexpr int F_FAR = 1;    // phase-one offset: full multipole partner
+constexpr int F_NEAR = 2;   // monopole-only offset
+
+struct Tables {
+    const int2* entries;     // [8][MAX_ENTRIES]: x = smem delta, y = packed offset/flags/stencil index
+    const int* count;        // [8]
+    const int2* entries_fast;   // same entries, full-multipole (far) offsets first
+    const int* count_far;       // [8] number of far offsets
+    const int4* entries_split;  // far-first entries for the split layout: x = double delta, y = packed, z = float delta
+    const int2* entries_p2p;    // stencil-order entries for the P2P layout: x = smem delta, y = stencil index
+    const int4* entries_ws;     // far-first entries for the warp-specialised split layout: x = float2 delta,
+                                // y = double2 delta, z = packed
+    const double* four;      // [FULL][4] monopole constants
+    const uint8_t* phase;    // [FULL] inner_stencil_masks (true outside the stencil)
+    const int* p2m_start;    // [512][28]: per cell, start of the entries of raw direction r in p2m_list
+    const uint16_t* p2m_list;   // partner cell index (in its neighbour) of every entry, grouped by direction
+    const int* p2m_perm_start;  // [28]: start of raw direction r in p2m_perm
+    const uint16_t* p2m_perm;   // per direction, the cells with partners there, most partners first
+    const int16_t* p2m_slot;    // [27][512]: position of a cell in its direction's p2m_perm list, -1 if absent
+    const double4* p2p_four;    // [8][MAX_ENTRIES]: monopole constants of entries_p2p (zeros past the count)
+};
+
+__device__ __forceinline__ int entry_sx(int y) { return (y & 15) - 8; }
+__device__ __forceinline__ int entry_sy(int y) { return ((y >> 4) & 15) - 8; }
+__device__ __forceinline__ int entry_sz(int y) { return ((y >> 8) & 15) - 8; }
+__device__ __forceinline__ int entry_flags(int y) { return (y >> 12) & 3; }
+__device__ __forceinline__ int entry_sidx(int y) { return (y >> 16) & 2047; }
+
+// Raw direction (0..26, 13 = centre) of absolute cell coordinates a in [-8, 15].
+__device__ __forceinline__ int raw_dir(int ax, int ay, int az) {
+    return ((ax >> 3) + 1) + 3 * ((ay >> 3) + 1) + 9 * ((az >> 3) + 1);
+}
+
+enum : int { PREC_EXACT = OTFMM_FP64_EXACT, PREC_FAST = OTFMM_FP64, PREC_SPLIT = OTFMM_FP32_SPLIT };
+
+// Scaling folded into staged moments by the fast form.
+template <int PREC>
+__device__ __forceinline__ double stage_scale(int q) {
+    if (PREC == PREC_FAST) {
+        if (q >= 4 && q < 10) return factor_of(q) / 2.0;
+        if (q >= 10 && q < 20) return factor_of(q) / 6.0;
+    }
+    return 1.0;
+}
+
+__device__ __forceinline__ int region_addr(int ax, int ay, int az, int x0) {
+    const int rx = ax - x0 + 2, ry = ay + 2, rz = az + 2;
+    const int cls = ((ax & 1) << 2) | ((ay & 1) << 1) | (az & 1);
+    return cls * CLS + (rx >> 1) * XS + (ry >> 1) * RB + (rz >> 1);
+}
+
+struct ItemInfo {
+    int subgrid, kind;
+    int nb[26];
+    double dx, xbase[3];
+};
+
+
+// ---------------------------------------------------------------- kernels
+// Device-side work lists, filled by classify_kernel: item indices per kind
+// and the counters the persistent launches take their tiles from.
+enum : int { WL_M2L = 0, WL_LEAF = 1, WL_P2M = 2, WL_M2L_NEXT = 3, WL_P2M_NEXT = 4, WL_ROOT = 5, WL_COUNTERS = 8 };
+struct WorkLists {
+    int* m2l;      // refined, non-root items
+    int* root;     // level-0 items
+    int* leaf;     // leaf items
+    int* p2m;      // leaf items with a refined neighbour
+    int* counts;   // WL_* counters
+};
+
+struct BatchArgs {
+    const double* M;
+    const double* com;
+    const double* mon;
+    const uint8_t* is_leaf;
+    int n_sub;
+    const otfmm_work_item* items;
+    int n_items;
+    double* L;
+    double* Lc;
+    Tables t;
+    int* err;
+    WorkLists wl;
+    int p2m_lanes;   // fast-form P2M: at most this many lanes share one cell's entries (1..16, power of two)
+};
+
+__device__ __forceinline__ bool item_valid(const BatchArgs& a, const otfmm_work_item& w) {
+    bool b = (w.subgrid < 0 || w.subgrid >= a.n_sub || w.kind < 0 || w.kind > 2 || !(w.dx > 0.0));
+    for (int d = 0; d < 26; ++d) b |= (w.neighbors[d] < -1 || w.neighbors[d] >= a.n_sub);
+    if (!b && w.kind != OTFMM_KIND_M2L_ROOT) b |= (a.is_leaf[w.subgrid] != 0) != (w.kind == OTFMM_KIND_LEAF);
+    return !b;
+}
+
+// One thread per work item: validates it (a malformed item raises the error
+// flag and is dropped before anything reads with its fields) and appends it
+// to the list of its kind.
+__global__ void classify_kernel(BatchArgs a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n_items) return;
+    const otfmm_work_item& w = a.items[i];
+    if (!item_valid(a, w)) {
+        atomicOr(a.err, 1);
+        return;
+    }
+    if (w.kind == OTFMM_KIND_M2L) {
+        a.wl.m2l[atomicAdd(a.wl.counts + WL_M2L, 1)] = i;
+    } else if (w.kind == OTFMM_KIND_M2L_ROOT) {
+        a.wl.root[atomicAdd(a.wl.counts + WL_ROOT, 1)] = i;
+    } else {
+        a.wl.leaf[atomicAdd(a.wl.counts + WL_LEAF, 1)] = i;
+        bool refined_nb = false;
+        for (int d = 0; d < 26; ++d) refined_nb |= (w.neighbors[d] >= 0 && !a.is_leaf[w.neighbors[d]]);
+        if (refined_nb) a.wl.p2m[atomicAdd(a.wl.counts + WL_P2M, 1)] = i;
+    }
+}
+
+// Copies an item (already validated by classify_kernel) into shared memory.
+__device__ __forceinline__ void load_item(const BatchArgs& a, int item_idx, ItemInfo& it) {
+    if (threadIdx.x == 0) {
+        const otfmm_work_item& w = a.items[item_idx];
+        it.subgrid = w.subgrid;
+        it.kind = w.kind;
+        it.dx = w.dx;
+        for (int q = 0; q < 3; ++q) it.xbase[q] = w.xbase[q];
+        for (int d = 0; d < 26; ++d) it.nb[d] = w.neighbors[d];
+    }
+    __syncthreads();
+}
+
+}   // namespace otfmm

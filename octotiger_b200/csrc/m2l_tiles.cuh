@@ -1,0 +1,864 @@
+// Multipole (M2L) tiles of refined subgrids: halo staging into shared memory,
+// the FP64 exact / fast tile sweeps, the FP32-split forms (single-role and
+// warp-specialised), the root tile, and the persistent batched kernels.
+// Part of libotfmm.so; included once, in order, by otfmm.cu (one translation unit).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "../../include/otfmm.h"
+#include "pair_math.cuh"
+#include "layout.cuh"
+
+namespace otfmm {
+
+// ---------------------------------------------------------------- staging
+// Gathers the tile region from the subgrid pool
+// (restates multipole update_input, octotiger/multipole_interactions/legacy/
+// multipole_interaction_interface.hpp:88-281, for full-size neighbour payloads;
+// leaf tiles follow monopole update_input + update_neighbor_input,
+// octotiger/monopole_interactions/legacy/monopole_interaction_interface.hpp:64-143,
+// p2m_interaction_interface.hpp:102-160).
+template <int PREC>
+__device__ void stage_region_pool(double* sm, const ItemInfo& it, int x0, bool leaf_tile, const double* __restrict__ M,
+                                  const double* __restrict__ com, const double* __restrict__ mon,
+                                  const uint8_t* __restrict__ is_leaf) {
+    for (int r = threadIdx.x; r < REG_CELLS; r += blockDim.x) {
+        const int rx = r / (REG_YZ * REG_YZ), ry = (r / REG_YZ) % REG_YZ, rz = r % REG_YZ;
+        const int ax = x0 - 2 + rx, ay = ry - 2, az = rz - 2;
+        const int raw = raw_dir(ax, ay, az);
+        const bool centre = (raw == 13);
+        const int src = centre ? it.subgrid : it.nb[raw < 13 ? raw : raw - 1];
+        const int lx = ax & 7, ly = ay & 7, lz = az & 7;
+        const int u = lx * 64 + ly * 8 + lz;
+        const int base = region_addr(ax, ay, az, x0);
+        double v[NCOMP];
+        if (src < 0) {
+#pragma unroll
+            for (int q = 0; q < NCOMP; ++q) v[q] = 0.0;
+        } else {
+            const bool use_mon = centre ? leaf_tile : (is_leaf[src] != 0);
+            if (use_mon) {
+                v[0] = mon[(size_t)src * NCELL + u];
+#pragma unroll
+                for (int q = 1; q < 20; ++q) v[q] = 0.0;
+                if (centre) {
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) v[20 + a] = com[((size_t)src * 3 + a) * NCELL + u];
+                } else {
+                    // cell centre: i*dx + xbase - INX*dx with i the padded index (:221-234)
+                    const int ip[3] = {ax + INX, ay + INX, az + INX};
+#pragma unroll
+                    for (int a = 0; a < 3; ++a)
+                        v[20 + a] = __dsub_rn(__dadd_rn(__dmul_rn((double)ip[a], it.dx), it.xbase[a]),
+                                              __dmul_rn((double)INX, it.dx));
+                }
+            } else {
+#pragma unroll
+                for (int q = 0; q < 20; ++q) v[q] = M[((size_t)src * 20 + q) * NCELL + u] * stage_scale<PREC>(q);
+#pragma unroll
+                for (int a = 0; a < 3; ++a) v[20 + a] = com[((size_t)src * 3 + a) * NCELL + u];
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < NCOMP; ++q) sm[base + q * SUB_YZ] = v[q];
+    }
+}
+
+// Same region from the reference's 18^3 SoA buffers. m0 holds mon + M0, the
+// value phase-one offsets use (:270-283 of kokkos_kernel.hpp).
+template <int PREC>
+__device__ void stage_region_soa(double* sm, int x0, const double* __restrict__ mon, const double* __restrict__ M,
+                                 const double* __restrict__ com) {
+    for (int r = threadIdx.x; r < REG_CELLS; r += blockDim.x) {
+        const int rx = r / (REG_YZ * REG_YZ), ry = (r / REG_YZ) % REG_YZ, rz = r % REG_YZ;
+        const int ax = x0 - 2 + rx, ay = ry - 2, az = rz - 2;
+        const int f = (ax + INX - PAD_OFF) * PSTRIDE * PSTRIDE + (ay + INX - PAD_OFF) * PSTRIDE + (az + INX - PAD_OFF);
+        const int base = region_addr(ax, ay, az, x0);
+        sm[base] = __dadd_rn(mon[f], M[f]) * stage_scale<PREC>(0);
+#pragma unroll
+        for (int q = 1; q < 20; ++q) sm[base + q * SUB_YZ] = M[q * CL + f] * stage_scale<PREC>(q);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) sm[base + (20 + a) * SUB_YZ] = com[a * CL + f];
+    }
+}
+
+// ---------------------------------------------------------------- compute
+struct CellMap {
+    int p, i, j, k, cx, cy, cz, lane_off, own;
+};
+__device__ __forceinline__ CellMap cell_map(int x0) {
+    CellMap c;
+    const int lane = threadIdx.x & 31;
+    c.p = threadIdx.x >> 5;
+    c.i = lane >> 4;
+    c.j = (lane >> 2) & 3;
+    c.k = lane & 3;
+    c.cx = x0 + ((c.p >> 2) & 1) + 2 * c.i;
+    c.cy = ((c.p >> 1) & 1) + 2 * c.j;
+    c.cz = (c.p & 1) + 2 * c.k;
+    c.lane_off = c.i * XS + c.j * RB + c.k;
+    c.own = c.p * CLS + (c.i + 1) * XS + (c.j + 1) * RB + (c.k + 1);
+    return c;
+}
+
+struct OutPtr {
+    double* L;
+    double* Lc;
+    int stride;   // component stride
+    bool pool;    // pool outputs: L_c is written (zeros) for DRHODT too
+};
+
+template <bool RHO>
+__device__ __forceinline__ void write_lc(const OutPtr& out, int cf, const double corr[3]) {
+    if (RHO || out.pool) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) out.Lc[a * out.stride + cf] = RHO ? corr[a] : 0.0;
+    }
+}
+
+// M2L over the staged region. near_mon != nullptr: monopole-only offsets read
+// the partner mass from that 18^3 buffer (SoA path); else from the region for
+// leaf-neighbour partners (bit set in monomask, indexed by raw direction).
+template <int PREC, bool RHO>
+__device__ void m2l_tile(const double* sm, int x0, const Tables& t, uint32_t monomask, const double* near_mon,
+                         OutPtr out) {
+    const CellMap c = cell_map(x0);
+    double X[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) X[a] = sm[c.own + (20 + a) * SUB_YZ];
+    double acc[20], corr[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int q = 0; q < 20; ++q) acc[q] = 0.0;
+    const int n = t.count[c.p];
+    const int2* ent = t.entries + c.p * MAX_ENTRIES;
+    if (PREC == PREC_EXACT) {
+        double mc[20];
+#pragma unroll
+        for (int q = 0; q < 20; ++q) mc[q] = sm[c.own + q * SUB_YZ];
+        for (int e = 0; e < n; ++e) {
+            const int2 en = __ldg(ent + e);
+            const int pb = en.x + c.lane_off;
+            double Y[3], mp[20];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) Y[a] = sm[pb + (20 + a) * SUB_YZ];
+            if (entry_flags(en.y) & F_FAR) {
+#pragma unroll
+                for (int q = 0; q < 20; ++q) mp[q] = sm[pb + q * SUB_YZ];
+            } else {
+                const int ax = c.cx + entry_sx(en.y), ay = c.cy + entry_sy(en.y), az = c.cz + entry_sz(en.y);
+                double m0;
+                if (near_mon) {
+                    m0 = near_mon[(ax + INX - PAD_OFF) * PSTRIDE * PSTRIDE + (ay + INX - PAD_OFF) * PSTRIDE +
+                                  (az + INX - PAD_OFF)];
+                } else {
+                    if (!((monomask >> raw_dir(ax, ay, az)) & 1u)) continue;   // contributes exactly zero
+                    m0 = sm[pb];
+                }
+                mp[0] = m0;
+#pragma unroll
+                for (int q = 1; q < 20; ++q) mp[q] = 0.0;
+            }
+            exact_m2l_pair<RHO>(X, Y, mp, mc, acc, corr);
+        }
+    } else {
+        const double inv_m0 = 1.0 / sm[c.own];
+        double mc_oct[10];
+#pragma unroll
+        for (int o = 0; o < 10; ++o) mc_oct[o] = sm[c.own + (10 + o) * SUB_YZ];
+        const int nfar = t.count_far[c.p];
+        const int2* entf = t.entries_fast + c.p * MAX_ENTRIES;
+        // full-multipole partners: branch-free, two pairs in flight
+#pragma unroll 2
+        for (int e = 0; e < nfar; ++e) {
+            const int pb = __ldg(&entf[e].x) + c.lane_off;
+            double Y[3], mp[20];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) Y[a] = sm[pb + (20 + a) * SUB_YZ];
+#pragma unroll
+            for (int q = 0; q < 20; ++q) mp[q] = sm[pb + q * SUB_YZ];
+            fast_m2l_pair<RHO>(X, Y, mp, mc_oct, inv_m0, acc, corr);
+        }
+        // monopole-only offsets: only leaf-neighbour partners contribute
+#pragma unroll 1
+        for (int e = nfar; e < n; ++e) {
+            const int2 en = __ldg(entf + e);
+            const int pb = en.x + c.lane_off;
+            const int ax = c.cx + entry_sx(en.y), ay = c.cy + entry_sy(en.y), az = c.cz + entry_sz(en.y);
+            double m0;
+            if (near_mon) {
+                m0 = near_mon[(ax + INX - PAD_OFF) * PSTRIDE * PSTRIDE + (ay + INX - PAD_OFF) * PSTRIDE +
+                              (az + INX - PAD_OFF)];
+            } else {
+                if (!((monomask >> raw_dir(ax, ay, az)) & 1u)) continue;
+                m0 = sm[pb];
+            }
+            double Y[3];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) Y[a] = sm[pb + (20 + a) * SUB_YZ];
+            fast_m2l_mass_pair<RHO>(X, Y, m0, mc_oct, inv_m0, acc, corr);
+        }
+    }
+    const int cf = c.cx * 64 + c.cy * 8 + c.cz;
+#pragma unroll
+    for (int q = 0; q < 20; ++q) out.L[q * out.stride + cf] = acc[q];
+    write_lc<RHO>(out, cf, corr);
+}
+
+// Split staging from the pool: same sources as stage_region_pool, values in
+// units of dx (inv_dx = 1/dx), multinomial factors folded in.
+__device__ void stage_region_split(double* sm, const ItemInfo& it, int x0, double inv_dx, const double* __restrict__ M,
+                                   const double* __restrict__ com, const double* __restrict__ mon,
+                                   const uint8_t* __restrict__ is_leaf) {
+    float* smf = reinterpret_cast<float*>(sm);
+    const double inv2 = inv_dx * inv_dx, inv3 = inv2 * inv_dx;
+    for (int r = threadIdx.x; r < REG_CELLS; r += blockDim.x) {
+        const int rx = r / (REG_YZ * REG_YZ), ry = (r / REG_YZ) % REG_YZ, rz = r % REG_YZ;
+        const int ax = x0 - 2 + rx, ay = ry - 2, az = rz - 2;
+        const int raw = raw_dir(ax, ay, az);
+        const bool centre = (raw == 13);
+        const int src = centre ? it.subgrid : it.nb[raw < 13 ? raw : raw - 1];
+        const int u = (ax & 7) * 64 + (ay & 7) * 8 + (az & 7);
+        const int cls = ((ax & 1) << 2) | ((ay & 1) << 1) | (az & 1);
+        const int row = cls * S_CLS + (rx >> 1) * S_XS + (ry >> 1) * S_RB;
+        const int zp = rz >> 1;
+        double m[20], c[3];
+        if (src < 0) {
+#pragma unroll
+            for (int q = 0; q < 20; ++q) m[q] = 0.0;
+#pragma unroll
+            for (int a = 0; a < 3; ++a) c[a] = 0.0;
+        } else if (!centre && is_leaf[src]) {
+            m[0] = mon[(size_t)src * NCELL + u];
+#pragma unroll
+            for (int q = 1; q < 20; ++q) m[q] = 0.0;
+            const int ip[3] = {ax + INX, ay + INX, az + INX};
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+                c[a] = __dsub_rn(__dadd_rn(__dmul_rn((double)ip[a], it.dx), it.xbase[a]), __dmul_rn((double)INX, it.dx));
+        } else {
+#pragma unroll
+            for (int q = 0; q < 20; ++q) m[q] = M[((size_t)src * 20 + q) * NCELL + u];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) c[a] = com[((size_t)src * 3 + a) * NCELL + u];
+        }
+#pragma unroll
+        for (int q = 1; q < 4; ++q) m[q] *= inv_dx;
+#pragma unroll
+        for (int q = 4; q < 10; ++q) m[q] *= (factor_of(q) / 2.0) * inv2;
+#pragma unroll
+        for (int q = 10; q < 20; ++q) m[q] *= (factor_of(q) / 6.0) * inv3;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) sm[row + a * SUB_YZ + zp] = c[a] * inv_dx;
+        sm[row + 3 * SUB_YZ + zp] = m[0];
+#pragma unroll
+        for (int o = 0; o < 10; ++o) sm[row + (4 + o) * SUB_YZ + zp] = m[10 + o];
+#pragma unroll
+        for (int q = 0; q < 20; ++q) smf[2 * row + S_FOFF + q * SUB_YZ + zp] = (float)m[q];
+    }
+}
+
+// M2L over the split-staged region: FP32 tensor and contraction with FP64
+// chunk sums, FP64 centre-of-mass differences, derivative factors and L_c.
+template <bool RHO>
+__device__ void m2l_tile_split(const double* sm, int x0, const Tables& t, uint32_t monomask, double inv_dx,
+                               OutPtr out) {
+    const float* smf = reinterpret_cast<const float*>(sm);
+    const CellMap c = cell_map(x0);
+    const int lane_d = c.i * S_XS + c.j * S_RB + c.k;
+    const int lane_f = 2 * (c.i * S_XS + c.j * S_RB) + c.k;
+    const int own = c.p * S_CLS + (c.i + 1) * S_XS + (c.j + 1) * S_RB + (c.k + 1);
+    double X[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) X[a] = sm[own + a * SUB_YZ];
+    const double inv_m0 = 1.0 / sm[own + 3 * SUB_YZ];
+    double mc_oct[10];
+#pragma unroll
+    for (int o = 0; o < 10; ++o) mc_oct[o] = sm[own + (4 + o) * SUB_YZ];
+    double acc[20], corr[3] = {0.0, 0.0, 0.0};
+    float accf[20];
+#pragma unroll
+    for (int q = 0; q < 20; ++q) {
+        acc[q] = 0.0;
+        accf[q] = 0.0f;
+    }
+    const int n = t.count[c.p];
+    const int nfar = t.count_far[c.p];
+    const int4* ent = t.entries_split + c.p * MAX_ENTRIES;
+#pragma unroll 1
+    for (int e0 = 0; e0 < nfar; e0 += SPLIT_CHUNK) {
+        const int e1 = min(e0 + SPLIT_CHUNK, nfar);
+#pragma unroll 2
+        for (int e = e0; e < e1; ++e) {
+            const int4 en = __ldg(ent + e);
+            const int pd = en.x + lane_d, pf = en.z + lane_f;
+            double Y[3], mp_oct[10];
+            float mpf[20];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) Y[a] = sm[pd + a * SUB_YZ];
+            const double m0 = sm[pd + 3 * SUB_YZ];
+            if (RHO) {
+#pragma unroll
+                for (int o = 0; o < 10; ++o) mp_oct[o] = sm[pd + (4 + o) * SUB_YZ];
+            }
+#pragma unroll
+            for (int q = 0; q < 20; ++q) mpf[q] = smf[pf + q * SUB_YZ];
+            split_m2l_pair<RHO>(X, Y, mpf, m0, mp_oct, mc_oct, inv_m0, accf, corr);
+        }
+#pragma unroll
+        for (int q = 0; q < 20; ++q) {
+            acc[q] += (double)accf[q];
+            accf[q] = 0.0f;
+        }
+    }
+    // monopole-only offsets (leaf-neighbour partners), FP64 in dx units
+#pragma unroll 1
+    for (int e = nfar; e < n; ++e) {
+        const int4 en = __ldg(ent + e);
+        const int ax = c.cx + entry_sx(en.y), ay = c.cy + entry_sy(en.y), az = c.cz + entry_sz(en.y);
+        if (!((monomask >> raw_dir(ax, ay, az)) & 1u)) continue;
+        const int pd = en.x + lane_d;
+        double Y[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) Y[a] = sm[pd + a * SUB_YZ];
+        fast_m2l_mass_pair<RHO>(X, Y, sm[pd + 3 * SUB_YZ], mc_oct, inv_m0, acc, corr);
+    }
+    // back to physical units: L_(n) = L'_(n) dx^-(n+1), L_c = L_c' dx^-2
+    const double s1 = inv_dx, s2 = s1 * inv_dx, s3 = s2 * inv_dx, s4 = s3 * inv_dx;
+    const int cf = c.cx * 64 + c.cy * 8 + c.cz;
+#pragma unroll
+    for (int q = 0; q < 20; ++q) out.L[q * out.stride + cf] = acc[q] * (q == 0 ? s1 : q < 4 ? s2 : q < 10 ? s3 : s4);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) corr[a] *= s2;
+    write_lc<RHO>(out, cf, corr);
+}
+
+// ------------------------------------------------ FP32 split, warp-specialised
+// RHO multipole tiles with 16 warps on one staged region. Warps 0-7
+// ("contraction warps") build each pair's derivative tensor in FP32 from the
+// FP64 centre-of-mass difference and contract it with the FP32 partner
+// moments, promoting FP32 partial sums to FP64 every CHUNK partners; warps
+// 8-15 ("correction warps") compute the angular-momentum correction L_c of
+// the same pairs entirely in FP64. Warp w serves the 32 target cells of
+// parity class w & 7 in either role, so the FP64 pipe (correction warps) and
+// the FP32 pipe (contraction warps) work side by side on every SM.
+// Shared memory per parity class (4 x 6 x 6 sub-lattice), rows of 6 z-cells:
+//   FP32 part: pairs (M0,M1) .. (M18,M19) as float2, [10 pairs][6 z] = 60 float2 per row;
+//   FP64 part: (Px,Py) (Pz,m0) (O0,O1) .. (O8,O9) as double2, [7][6 z] = 42 per row.
+// P = (centre of mass - xbase) / dx, moments in units of dx with the multinomial
+// factors folded in (exact rescaling for dx = 2^-k). Lane l of a warp serves
+// sub-lattice cell (i, j, k) = ((l >> 2) & 1, l >> 3, l & 3): a half-warp
+// (16 lanes: k, i, two j) reads float2 at offsets k + {0, 8, 12, 4} mod 16
+// (x stride 360, row stride 60), a quarter-warp (8 lanes: k, i) reads double2
+// at k + {0, 4} mod 8 (x stride 252): both without bank conflicts. The stencil
+// table follows the two parts: per parity class and entry, the float2 and
+// double2 partner deltas packed as 16 + 16 bits.
+constexpr int WS_THREADS = 512;
+constexpr int WA_ROW = 10 * SUB_YZ;            // 60 float2
+constexpr int WA_XS = SUB_YZ * WA_ROW;
+constexpr int WA_CLS = (REG_X / 2) * WA_XS;
+constexpr int WB_ROW = 7 * SUB_YZ;             // 42 double2
+constexpr int WB_XS = SUB_YZ * WB_ROW;
+constexpr int WB_CLS = (REG_X / 2) * WB_XS;
+constexpr int WS_A_BYTES = 8 * WA_CLS * 8;
+constexpr int WS_B_BYTES = 8 * WB_CLS * 16;
+constexpr int WS_TABLE_BYTES = 8 * MAX_ENTRIES * 4;
+constexpr int WS_SMEM_BYTES = WS_A_BYTES + WS_B_BYTES + WS_TABLE_BYTES;   // 92160 + 129024 + 6912 = 228096
+static_assert(WA_ROW % 16 == 12 && WA_XS % 16 == 8, "float2 half-warps (k, i, j pair) conflict-free");
+static_assert(WB_XS % 8 == 4, "double2 quarter-warps (k, i) conflict-free");
+static_assert(8 * WA_CLS < 65536 && 8 * WB_CLS < 65536, "deltas fit 16 bits");
+static_assert(WS_SMEM_BYTES + 256 <= 232448, "warp-specialised layout fits the 227 KB shared-memory limit");
+static_assert(ROOT_SMEM_DOUBLES * 8 <= WS_A_BYTES + WS_B_BYTES, "root staging leaves the stencil table intact");
+// Smallest squared distance (in dx^2) the FP32 derivative tensor accepts; it
+// keeps d3 ~ r^-7 finite in FP32. Cells of one grid have distinct centres of
+// mass at least ~0.2 dx apart; the FP64 forms clamp at 1e-20 like the reference.
+constexpr float WS_R2_MIN = 1.0e-6f;
+
+__device__ void stage_region_ws(float2* sa, double2* sb, const ItemInfo& it, int x0, double inv_dx,
+                                const double* __restrict__ M, const double* __restrict__ com,
+                                const double* __restrict__ mon, const uint8_t* __restrict__ is_leaf) {
+    const double inv2 = inv_dx * inv_dx, inv3 = inv2 * inv_dx;
+    for (int r = threadIdx.x; r < REG_CELLS; r += blockDim.x) {
+        const int rx = r / (REG_YZ * REG_YZ), ry = (r / REG_YZ) % REG_YZ, rz = r % REG_YZ;
+        const int ax = x0 - 2 + rx, ay = ry - 2, az = rz - 2;
+        const int raw = raw_dir(ax, ay, az);
+        const bool centre = (raw == 13);
+        const int src = centre ? it.subgrid : it.nb[raw < 13 ? raw : raw - 1];
+        const int u = (ax & 7) * 64 + (ay & 7) * 8 + (az & 7);
+        double m[20], P[3];
+        if (src < 0) {
+            // empty direction: zero moments at the cell's own centre (never at a
+            // target's centre of mass, so the pair stays finite)
+#pragma unroll
+            for (int q = 0; q < 20; ++q) m[q] = 0.0;
+            P[0] = ax;
+            P[1] = ay;
+            P[2] = az;
+        } else if (!centre && is_leaf[src]) {
+            m[0] = mon[(size_t)src * NCELL + u];
+#pragma unroll
+            for (int q = 1; q < 20; ++q) m[q] = 0.0;
+            // leaf cell centre i*dx + xbase - INX*dx (monopole_interaction_interface.hpp:221-234)
+            const int ip[3] = {ax + INX, ay + INX, az + INX};
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                const double c = __dsub_rn(__dadd_rn(__dmul_rn((double)ip[a], it.dx), it.xbase[a]),
+                                           __dmul_rn((double)INX, it.dx));
+                P[a] = (c - it.xbase[a]) * inv_dx;
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < 20; ++q) m[q] = M[((size_t)src * 20 + q) * NCELL + u];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) P[a] = (com[((size_t)src * 3 + a) * NCELL + u] - it.xbase[a]) * inv_dx;
+        }
+#pragma unroll
+        for (int q = 1; q < 4; ++q) m[q] *= inv_dx;
+#pragma unroll
+        for (int q = 4; q < 10; ++q) m[q] *= (factor_of(q) / 2.0) * inv2;
+#pragma unroll
+        for (int q = 10; q < 20; ++q) m[q] *= (factor_of(q) / 6.0) * inv3;
+        const int cls = ((ax & 1) << 2) | ((ay & 1) << 1) | (az & 1);
+        const int ua = cls * WA_CLS + (rx >> 1) * WA_XS + (ry >> 1) * WA_ROW + (rz >> 1);
+        const int ub = cls * WB_CLS + (rx >> 1) * WB_XS + (ry >> 1) * WB_ROW + (rz >> 1);
+#pragma unroll
+        for (int q = 0; q < 10; ++q) sa[ua + q * SUB_YZ] = make_float2((float)m[2 * q], (float)m[2 * q + 1]);
+        sb[ub] = make_double2(P[0], P[1]);
+        sb[ub + SUB_YZ] = make_double2(P[2], m[0]);
+#pragma unroll
+        for (int o = 0; o < 5; ++o) sb[ub + (2 + o) * SUB_YZ] = make_double2(m[10 + 2 * o], m[11 + 2 * o]);
+    }
+}
+
+// FP32 derivative tensor and contraction of one pair (dX in units of dx).
+// 1/r: hardware estimate plus one Newton step with an FMA residual
+// (within about one FP32 ulp).
+__device__ __forceinline__ void ws_contract_pair(const float dX[3], const float m[20], float acc[20]) {
+    const float r2 = fmaxf(fmaf(dX[0], dX[0], fmaf(dX[1], dX[1], dX[2] * dX[2])), WS_R2_MIN);
+    const float y0 = rsqrtf(r2);
+    const float h = fmaf(-r2 * y0, y0, 1.0f);
+    const float rs = fmaf(0.5f * y0, h, y0);
+    const float r2inv = rs * rs;
+    const float d1 = rs * r2inv;
+    const float d2 = -3.0f * d1 * r2inv;
+    const float d3 = -5.0f * d2 * r2inv;
+    float D[20];
+    d_tensor<float>(dX, -rs, d1, d2, d3, D);
+    fast_low_terms<float>(m, D, acc, false);
+    fast_high_terms<float>(m, D, acc);
+}
+
+// Same contraction with packed FP32 FMAs (two products per instruction; on
+// sm_100 these co-issue with the FP64 pipe far better than scalar FMAs).
+// Accumulator pairs: A[k] = (L_2k, L_2k+1) for k = 0..9; A[10] = L0 quadrupole
+// part, A[11] = L0 octupole part (subtracted), A[12..14] = L1..L3 quadrupole
+// parts, each as two partial sums. The derivative tensor is used as its
+// natural pairs (D_2k, D_2k+1) plus the five pairs the quadrupole/dipole terms
+// of L2, L3 and L4..L9 need: (D11,D13) (D14,D16) (D17,D18) (D12,D14) (D15,D17).
+constexpr int WS_PACKED_ACC = 15;
+__device__ __forceinline__ void ws_contract_pair_packed(const float dX[3], const float2 mm[10],
+                                                        float2 A[WS_PACKED_ACC]) {
+    const float r2 = fmaxf(fmaf(dX[0], dX[0], fmaf(dX[1], dX[1], dX[2] * dX[2])), WS_R2_MIN);
+    const float y0 = rsqrtf(r2);
+    const float h = fmaf(-r2 * y0, y0, 1.0f);
+    const float rs = fmaf(0.5f * y0, h, y0);
+    const float r2inv = rs * rs;
+    const float d1 = rs * r2inv;
+    const float d2 = -3.0f * d1 * r2inv;
+    const float d3 = -5.0f * d2 * r2inv;
+    float D[20];
+    d_tensor<float>(dX, -rs, d1, d2, d3, D);
+    float2 P[10];
+#pragma unroll
+    for (int k = 0; k < 10; ++k) P[k] = make_float2(D[2 * k], D[2 * k + 1]);
+    const float2 Q1 = make_float2(D[11], D[13]), Q2 = make_float2(D[14], D[16]), Q3 = make_float2(D[17], D[18]);
+    const float2 R1 = make_float2(D[12], D[14]), R2 = make_float2(D[15], D[17]);
+    const float2 b0 = make_float2(mm[0].x, mm[0].x);
+    const float2 n1 = make_float2(-mm[0].y, -mm[0].y), n2 = make_float2(-mm[1].x, -mm[1].x),
+                 n3 = make_float2(-mm[1].y, -mm[1].y);
+    // monopole: L0..L19 += M0 D0..D19
+#pragma unroll
+    for (int k = 0; k < 10; ++k) A[k] = __ffma2_rn(b0, P[k], A[k]);
+    // dipole part of L4..L9: -= M_(1+a) D[quad_axis(q, a)]
+    A[2] = __ffma2_rn(n1, P[5], A[2]);
+    A[3] = __ffma2_rn(n1, P[6], A[3]);
+    A[4] = __ffma2_rn(n1, P[7], A[4]);
+    A[2] = __ffma2_rn(n2, Q1, A[2]);
+    A[3] = __ffma2_rn(n2, Q2, A[3]);
+    A[4] = __ffma2_rn(n2, Q3, A[4]);
+    A[2] = __ffma2_rn(n3, R1, A[2]);
+    A[3] = __ffma2_rn(n3, R2, A[3]);
+    A[4] = __ffma2_rn(n3, P[9], A[4]);
+    // quadrupole part of L0 and L1..L3
+#pragma unroll
+    for (int q = 0; q < 3; ++q) A[10] = __ffma2_rn(mm[2 + q], P[2 + q], A[10]);
+    A[12] = __ffma2_rn(mm[2], P[5], A[12]);
+    A[12] = __ffma2_rn(mm[3], P[6], A[12]);
+    A[12] = __ffma2_rn(mm[4], P[7], A[12]);
+    A[13] = __ffma2_rn(mm[2], Q1, A[13]);
+    A[13] = __ffma2_rn(mm[3], Q2, A[13]);
+    A[13] = __ffma2_rn(mm[4], Q3, A[13]);
+    A[14] = __ffma2_rn(mm[2], R1, A[14]);
+    A[14] = __ffma2_rn(mm[3], R2, A[14]);
+    A[14] = __ffma2_rn(mm[4], P[9], A[14]);
+    // octupole part of L0 (subtracted when the pairs are folded)
+#pragma unroll
+    for (int o = 0; o < 5; ++o) A[11] = __ffma2_rn(mm[5 + o], P[5 + o], A[11]);
+}
+
+// Folds the packed accumulators into the FP64 sums of L0..L19 and clears them.
+__device__ __forceinline__ void ws_fold_packed(float2 A[WS_PACKED_ACC], double acc[20]) {
+    acc[0] += (double)((A[0].x + (A[10].x + A[10].y)) - (A[11].x + A[11].y));
+    acc[1] += (double)(A[0].y + (A[12].x + A[12].y));
+    acc[2] += (double)(A[1].x + (A[13].x + A[13].y));
+    acc[3] += (double)(A[1].y + (A[14].x + A[14].y));
+#pragma unroll
+    for (int k = 2; k < 10; ++k) {
+        acc[2 * k] += (double)A[k].x;
+        acc[2 * k + 1] += (double)A[k].y;
+    }
+#pragma unroll
+    for (int k = 0; k < WS_PACKED_ACC; ++k) A[k] = make_float2(0.0f, 0.0f);
+}
+
+// Partner with mass only (monopole-only entries, leaf-neighbour partners).
+__device__ __forceinline__ void ws_contract_mass(const float dX[3], float m0, float acc[20]) {
+    const float r2 = fmaxf(fmaf(dX[0], dX[0], fmaf(dX[1], dX[1], dX[2] * dX[2])), WS_R2_MIN);
+    const float y0 = rsqrtf(r2);
+    const float h = fmaf(-r2 * y0, y0, 1.0f);
+    const float rs = fmaf(0.5f * y0, h, y0);
+    const float r2inv = rs * rs;
+    const float d1 = rs * r2inv;
+    const float d2 = -3.0f * d1 * r2inv;
+    const float d3 = -5.0f * d2 * r2inv;
+    float D[20];
+    d_tensor<float>(dX, -rs, d1, d2, d3, D);
+#pragma unroll
+    for (int q = 0; q < 20; ++q) acc[q] = fmaf(m0, D[q], acc[q]);
+}
+
+// FP64 angular-momentum correction of one pair: g = O_p - O_c m_p / m_c
+// against the fourth-order slice (compute_kernel_templates.hpp:232-334).
+__device__ __forceinline__ void ws_correction_pair(const double dX[3], double m0p, const double op[10],
+                                                   const double mc_oct[10], double inv_m0, double Lc[3]) {
+    FastDerivs f;
+    f.X00 = dX[0] * dX[0];
+    f.X11 = dX[1] * dX[1];
+    f.X22 = dX[2] * dX[2];
+    f.X01 = dX[0] * dX[1];
+    f.X02 = dX[0] * dX[2];
+    f.X12 = dX[1] * dX[2];
+    const double r2 = fmax(f.X00 + f.X11 + f.X22, 1.0e-20);
+    const double y = (double)rsqrtf((float)r2);
+    const double rs = y * fma(-0.5 * r2 * y, y, 1.5);   // one Newton step: ~1e-14 relative
+    const double r2inv = rs * rs;
+    const double d1 = rs * r2inv;
+    f.d2 = -3.0 * d1 * r2inv;
+    f.d3 = -5.0 * f.d2 * r2inv;
+    const double n0 = m0p * inv_m0;
+    double g[10];
+#pragma unroll
+    for (int o = 0; o < 10; ++o) g[o] = fma(-mc_oct[o], n0, op[o]);
+    fast_upper_correction(f, g, Lc);
+}
+
+// Lane -> sub-lattice cell of the warp's parity class (see the layout above).
+struct WsLane {
+    int i, j, k;
+};
+__device__ __forceinline__ WsLane ws_lane() {
+    const int lane = threadIdx.x & 31;
+    return WsLane{(lane >> 2) & 1, lane >> 3, lane & 3};
+}
+
+template <int CHUNK, bool PACKED>
+__device__ void ws_contraction_warp(const float2* sa, const double2* sb, const unsigned* s_ent, int x0, int p,
+                                    const Tables& t, uint32_t monomask, double inv_dx, const OutPtr& out) {
+    const WsLane l = ws_lane();
+    const int lane_a = l.i * WA_XS + l.j * WA_ROW + l.k;
+    const int lane_b = l.i * WB_XS + l.j * WB_ROW + l.k;
+    const int own_b = p * WB_CLS + WB_XS + WB_ROW + 1 + lane_b;
+    const double2 o0 = sb[own_b], o1 = sb[own_b + SUB_YZ];
+    const double Pc0 = o0.x, Pc1 = o0.y, Pc2 = o1.x;
+    double acc[20];
+    float accf[20];
+#pragma unroll
+    for (int q = 0; q < 20; ++q) {
+        acc[q] = 0.0;
+        accf[q] = 0.0f;
+    }
+    const int n = t.count[p], nfar = t.count_far[p];
+    const unsigned* ent = s_ent + p * MAX_ENTRIES;
+    if (PACKED) {
+        float2 A[WS_PACKED_ACC];
+#pragma unroll
+        for (int k = 0; k < WS_PACKED_ACC; ++k) A[k] = make_float2(0.0f, 0.0f);
+#pragma unroll 1
+        for (int e0 = 0; e0 < nfar; e0 += CHUNK) {
+            const int e1 = min(e0 + CHUNK, nfar);
+#pragma unroll 2
+            for (int e = e0; e < e1; ++e) {
+                const unsigned en = ent[e];
+                const double2* pb = sb + (en >> 16) + lane_b;
+                const double2 q0 = pb[0], q1 = pb[SUB_YZ];
+                const float dX[3] = {(float)(Pc0 - q0.x), (float)(Pc1 - q0.y), (float)(Pc2 - q1.x)};
+                const float2* pa = sa + (en & 0xffffu) + lane_a;
+                float2 mm[10];
+#pragma unroll
+                for (int q = 0; q < 10; ++q) mm[q] = pa[q * SUB_YZ];
+                ws_contract_pair_packed(dX, mm, A);
+            }
+            ws_fold_packed(A, acc);
+        }
+    } else {
+#pragma unroll 1
+        for (int e0 = 0; e0 < nfar; e0 += CHUNK) {
+            const int e1 = min(e0 + CHUNK, nfar);
+#pragma unroll 2
+            for (int e = e0; e < e1; ++e) {
+                const unsigned en = ent[e];
+                const double2* pb = sb + (en >> 16) + lane_b;
+                const double2 q0 = pb[0], q1 = pb[SUB_YZ];
+                const float dX[3] = {(float)(Pc0 - q0.x), (float)(Pc1 - q0.y), (float)(Pc2 - q1.x)};
+                const float2* pa = sa + (en & 0xffffu) + lane_a;
+                float m[20];
+#pragma unroll
+                for (int q = 0; q < 10; ++q) {
+                    const float2 v = pa[q * SUB_YZ];
+                    m[2 * q] = v.x;
+                    m[2 * q + 1] = v.y;
+                }
+                ws_contract_pair(dX, m, accf);
+            }
+#pragma unroll
+            for (int q = 0; q < 20; ++q) {
+                acc[q] += (double)accf[q];
+                accf[q] = 0.0f;
+            }
+        }
+    }
+    const int cx = x0 + ((p >> 2) & 1) + 2 * l.i, cy = ((p >> 1) & 1) + 2 * l.j, cz = (p & 1) + 2 * l.k;
+    if (monomask) {
+        // monopole-only offsets: only leaf-neighbour partners contribute
+        const int4* gent = t.entries_ws + p * MAX_ENTRIES;
+#pragma unroll 1
+        for (int e = nfar; e < n; ++e) {
+            const int4 en = __ldg(gent + e);
+            const int ax = cx + entry_sx(en.z), ay = cy + entry_sy(en.z), az = cz + entry_sz(en.z);
+            if (!((monomask >> raw_dir(ax, ay, az)) & 1u)) continue;
+            const double2 q0 = sb[en.y + lane_b], q1 = sb[en.y + lane_b + SUB_YZ];
+            const float dX[3] = {(float)(Pc0 - q0.x), (float)(Pc1 - q0.y), (float)(Pc2 - q1.x)};
+            ws_contract_mass(dX, sa[en.x + lane_a].x, accf);
+        }
+#pragma unroll
+        for (int q = 0; q < 20; ++q) acc[q] += (double)accf[q];
+    }
+    // back to physical units: L_(n) = L'_(n) dx^-(n+1)
+    const double s1 = inv_dx, s2 = s1 * inv_dx, s3 = s2 * inv_dx, s4 = s3 * inv_dx;
+    const int cf = cx * 64 + cy * 8 + cz;
+#pragma unroll
+    for (int q = 0; q < 20; ++q) out.L[q * out.stride + cf] = acc[q] * (q == 0 ? s1 : q < 4 ? s2 : q < 10 ? s3 : s4);
+}
+
+__device__ void ws_correction_warp(const double2* sb, const unsigned* s_ent, int x0, int p, const Tables& t,
+                                   uint32_t monomask, double inv_dx, const OutPtr& out) {
+    const WsLane l = ws_lane();
+    const int lane_b = l.i * WB_XS + l.j * WB_ROW + l.k;
+    const int own_b = p * WB_CLS + WB_XS + WB_ROW + 1 + lane_b;
+    const double2 o0 = sb[own_b], o1 = sb[own_b + SUB_YZ];
+    const double Pc0 = o0.x, Pc1 = o0.y, Pc2 = o1.x;
+    const double inv_m0 = 1.0 / o1.y;
+    double mc_oct[10];
+#pragma unroll
+    for (int o = 0; o < 5; ++o) {
+        const double2 v = sb[own_b + (2 + o) * SUB_YZ];
+        mc_oct[2 * o] = v.x;
+        mc_oct[2 * o + 1] = v.y;
+    }
+    double corr[3] = {0.0, 0.0, 0.0};
+    const int n = t.count[p], nfar = t.count_far[p];
+    const unsigned* ent = s_ent + p * MAX_ENTRIES;
+#pragma unroll 2
+    for (int e = 0; e < nfar; ++e) {
+        const double2* pb = sb + (ent[e] >> 16) + lane_b;
+        const double2 q0 = pb[0], q1 = pb[SUB_YZ];
+        const double dX[3] = {Pc0 - q0.x, Pc1 - q0.y, Pc2 - q1.x};
+        double op[10];
+#pragma unroll
+        for (int o = 0; o < 5; ++o) {
+            const double2 v = pb[(2 + o) * SUB_YZ];
+            op[2 * o] = v.x;
+            op[2 * o + 1] = v.y;
+        }
+        ws_correction_pair(dX, q1.y, op, mc_oct, inv_m0, corr);
+    }
+    const int cx = x0 + ((p >> 2) & 1) + 2 * l.i, cy = ((p >> 1) & 1) + 2 * l.j, cz = (p & 1) + 2 * l.k;
+    if (monomask) {
+        const int4* gent = t.entries_ws + p * MAX_ENTRIES;
+#pragma unroll 1
+        for (int e = nfar; e < n; ++e) {
+            const int4 en = __ldg(gent + e);
+            const int ax = cx + entry_sx(en.z), ay = cy + entry_sy(en.z), az = cz + entry_sz(en.z);
+            if (!((monomask >> raw_dir(ax, ay, az)) & 1u)) continue;
+            const int pb = en.y + lane_b;
+            const double2 q0 = sb[pb], q1 = sb[pb + SUB_YZ];
+            const double dX[3] = {Pc0 - q0.x, Pc1 - q0.y, Pc2 - q1.x};
+            double op[10];
+#pragma unroll
+            for (int o = 0; o < 10; ++o) op[o] = 0.0;   // leaf partners carry no octupole
+            ws_correction_pair(dX, q1.y, op, mc_oct, inv_m0, corr);
+        }
+    }
+    const double s2 = inv_dx * inv_dx;
+    const int cf = cx * 64 + cy * 8 + cz;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) out.Lc[a * out.stride + cf] = corr[a] * s2;
+}
+
+// Root node: partners are all own cells except the monopole-only stencil
+// offsets and the cell itself (multipole_kernel_root_*_impl).
+// Staged layout: sm[q * 512 + cell].
+template <int PREC, bool RHO>
+__device__ void root_tile(const double* sm, int x0, const Tables& t, OutPtr out) {
+    const CellMap c = cell_map(x0);
+    const int cu = c.cx * 64 + c.cy * 8 + c.cz;
+    double X[3], acc[20], corr[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) X[a] = sm[(20 + a) * NCELL + cu];
+#pragma unroll
+    for (int q = 0; q < 20; ++q) acc[q] = 0.0;
+    double mc[20];
+#pragma unroll
+    for (int q = 0; q < 20; ++q) mc[q] = sm[q * NCELL + cu];
+    const double inv_m0 = 1.0 / mc[0];
+    for (int pu = 0; pu < NCELL; ++pu) {
+        const int sx = (pu >> 6) - c.cx, sy = ((pu >> 3) & 7) - c.cy, sz = (pu & 7) - c.cz;
+        if (abs(sx) <= SMAX && abs(sy) <= SMAX && abs(sz) <= SMAX) {
+            const int sidx = (sx + SMAX) * SINX * SINX + (sy + SMAX) * SINX + (sz + SMAX);
+            if (!__ldg(t.phase + sidx) || (sx == 0 && sy == 0 && sz == 0)) continue;
+        }
+        double Y[3], mp[20];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) Y[a] = sm[(20 + a) * NCELL + pu];
+#pragma unroll
+        for (int q = 0; q < 20; ++q) mp[q] = sm[q * NCELL + pu];
+        if (PREC == PREC_EXACT)
+            exact_m2l_pair<RHO>(X, Y, mp, mc, acc, corr);
+        else
+            fast_m2l_pair<RHO>(X, Y, mp, mc + 10, inv_m0, acc, corr);
+    }
+#pragma unroll
+    for (int q = 0; q < 20; ++q) out.L[q * out.stride + cu] = acc[q];
+    write_lc<RHO>(out, cu, corr);
+}
+
+
+// Multipole tiles (two per refined item), persistent: one CTA per SM takes
+// tiles from an atomic counter, root tiles (longest) first.
+template <int PREC, bool RHO>
+__global__ void __launch_bounds__(THREADS, 1) m2l_batch_kernel(BatchArgs a) {
+    extern __shared__ double sm[];
+    __shared__ ItemInfo it;
+    __shared__ int tile;
+    const int nroot = a.wl.counts[WL_ROOT], nm2l = a.wl.counts[WL_M2L];
+    const int total = 2 * (nroot + nm2l);
+    // the split form covers the multipole tiles; the root tile uses fast FP64
+    constexpr int P64 = (PREC == PREC_SPLIT) ? PREC_FAST : PREC;
+    for (;;) {
+        if (threadIdx.x == 0) tile = atomicAdd(a.wl.counts + WL_M2L_NEXT, 1);
+        __syncthreads();
+        const int t = tile;
+        if (t >= total) break;
+        const int item_idx = (t < 2 * nroot) ? a.wl.root[t >> 1] : a.wl.m2l[(t - 2 * nroot) >> 1];
+        load_item(a, item_idx, it);
+        const int x0 = TILE_X * (t & 1);
+        const size_t sub = (size_t)it.subgrid;
+        OutPtr out{a.L + sub * 20 * NCELL, a.Lc + sub * 3 * NCELL, NCELL, true};
+        if (it.kind == OTFMM_KIND_M2L_ROOT) {
+            for (int r = threadIdx.x; r < NCELL; r += blockDim.x)
+                for (int q = 0; q < NCOMP; ++q)
+                    sm[q * NCELL + r] = (q < 20) ? a.M[(sub * 20 + q) * NCELL + r] * stage_scale<P64>(q)
+                                                 : a.com[(sub * 3 + (q - 20)) * NCELL + r];
+            __syncthreads();
+            root_tile<P64, RHO>(sm, x0, a.t, out);
+        } else {
+            // leaf neighbours, indexed by raw direction (monopole-only offsets)
+            uint32_t monomask = 0;
+            for (int d = 0; d < 26; ++d) {
+                const int nb = it.nb[d];
+                if (nb >= 0 && a.is_leaf[nb]) monomask |= 1u << (d < 13 ? d : d + 1);
+            }
+            if (PREC == PREC_SPLIT) {
+                const double inv_dx = 1.0 / it.dx;
+                stage_region_split(sm, it, x0, inv_dx, a.M, a.com, a.mon, a.is_leaf);
+                __syncthreads();
+                m2l_tile_split<RHO>(sm, x0, a.t, monomask, inv_dx, out);
+            } else {
+                stage_region_pool<P64>(sm, it, x0, false, a.M, a.com, a.mon, a.is_leaf);
+                __syncthreads();
+                m2l_tile<P64, RHO>(sm, x0, a.t, monomask, nullptr, out);
+            }
+        }
+        __syncthreads();   // shared memory and `it` are reused by the next tile
+    }
+}
+
+// RHO multipole tiles in the FP32 split precision, warp-specialised (see
+// stage_region_ws): persistent over the same tile counter as m2l_batch_kernel,
+// 512 threads, one CTA per SM. The root tile runs the fast FP64 form on the
+// first 256 threads.
+template <int CHUNK, bool PACKED>
+__global__ void __launch_bounds__(WS_THREADS, 1) m2l_split_ws_kernel(BatchArgs a) {
+    extern __shared__ __align__(16) unsigned char ws_dyn[];
+    float2* sa = reinterpret_cast<float2*>(ws_dyn);
+    double2* sb = reinterpret_cast<double2*>(ws_dyn + WS_A_BYTES);
+    unsigned* s_ent = reinterpret_cast<unsigned*>(ws_dyn + WS_A_BYTES + WS_B_BYTES);
+    __shared__ ItemInfo it;
+    __shared__ int tile;
+    const int nroot = a.wl.counts[WL_ROOT], nm2l = a.wl.counts[WL_M2L];
+    const int total = 2 * (nroot + nm2l);
+    const int warp = threadIdx.x >> 5;
+    // far-first partner deltas of the 8 parity classes, resident for the whole launch
+    for (int e = threadIdx.x; e < 8 * MAX_ENTRIES; e += blockDim.x) {
+        const int4 en = a.t.entries_ws[e];
+        s_ent[e] = (unsigned)en.x | ((unsigned)en.y << 16);
+    }
+    for (;;) {
+        if (threadIdx.x == 0) tile = atomicAdd(a.wl.counts + WL_M2L_NEXT, 1);
+        __syncthreads();
+        const int t = tile;
+        if (t >= total) break;
+        const int item_idx = (t < 2 * nroot) ? a.wl.root[t >> 1] : a.wl.m2l[(t - 2 * nroot) >> 1];
+        load_item(a, item_idx, it);
+        const int x0 = TILE_X * (t & 1);
+        const size_t sub = (size_t)it.subgrid;
+        OutPtr out{a.L + sub * 20 * NCELL, a.Lc + sub * 3 * NCELL, NCELL, true};
+        if (it.kind == OTFMM_KIND_M2L_ROOT) {
+            double* sm = reinterpret_cast<double*>(ws_dyn);
+            for (int r = threadIdx.x; r < NCELL; r += blockDim.x)
+                for (int q = 0; q < NCOMP; ++q)
+                    sm[q * NCELL + r] = (q < 20) ? a.M[(sub * 20 + q) * NCELL + r] * stage_scale<PREC_FAST>(q)
+                                                 : a.com[(sub * 3 + (q - 20)) * NCELL + r];
+            __syncthreads();
+            if (threadIdx.x < THREADS) root_tile<PREC_FAST, true>(sm, x0, a.t, out);
+        } else {
+            uint32_t monomask = 0;
+            for (int d = 0; d < 26; ++d) {
+                const int nb = it.nb[d];
+                if (nb >= 0 && a.is_leaf[nb]) monomask |= 1u << (d < 13 ? d : d + 1);
+            }
+            const double inv_dx = 1.0 / it.dx;
+            stage_region_ws(sa, sb, it, x0, inv_dx, a.M, a.com, a.mon, a.is_leaf);
+            __syncthreads();
+            if (warp < 8)
+                ws_contraction_warp<CHUNK, PACKED>(sa, sb, s_ent, x0, warp, a.t, monomask, inv_dx, out);
+            else
+                ws_correction_warp(sb, s_ent, x0, warp & 7, a.t, monomask, inv_dx, out);
+        }
+        __syncthreads();   // shared memory and `it` are reused by the next tile
+    }
+}
+
+}   // namespace otfmm
