@@ -70,3 +70,44 @@ def test_create_rejects_small_theta_without_gpu():
     h = ctypes.c_void_p()
     assert lib.otfmm_create(0, 0.2, ctypes.byref(h)) == -2
     assert b"theta" in lib.otfmm_last_error()
+
+
+def test_entry_points_reject_missing_context_without_gpu():
+    """Every entry point that takes a context refuses a NULL one (and NULL
+    buffers) with OTFMM_ERR_INVALID before any device call."""
+    from octotiger_b200.otfmm import LIB_PATH, Tuning, load_library
+    if not LIB_PATH.exists():
+        pytest.fail("libotfmm.so not built")
+    lib = load_library()
+    null = None
+    inv = -1
+    assert lib.otfmm_batch(null, null, null, null, null, 1, null, 1, null, null, 0, 1, null) == inv
+    assert lib.otfmm_batch_host(null, null, null, null, null, 1, null, 1, null, null, 0, 1, null) == inv
+    assert lib.otfmm_batch_profile(null, null, null, null, null, 1, null, 1, null, null, 0, 1, null, null) == inv
+    assert lib.otfmm_autotune(null, null, null, null, null, 1, null, 1, null, null, 0, 1, 3, null, null) == inv
+    plan = ctypes.c_void_p()
+    assert lib.otfmm_plan_create(null, null, null, null, null, 1, null, 1, null, null, 0, 1,
+                                 ctypes.byref(plan)) == inv
+    assert lib.otfmm_plan_launch(null, null) == inv
+    assert lib.otfmm_plan_destroy(null) == 0
+    t = Tuning()
+    assert lib.otfmm_get_tuning(null, ctypes.byref(t)) == inv
+    assert lib.otfmm_set_tuning(null, ctypes.byref(t)) == inv
+    ls = (ctypes.c_int32 * 2)(0, 1)
+    assert lib.otfmm_upward(null, null, null, null, null, null, 1, null, ls, 1, 0, null) == inv
+    assert lib.otfmm_downward(null, null, null, null, 1, null, ls, 1, null, null, null, 1.0, 1, 0, null) == inv
+    stride = ctypes.c_int32()
+    assert lib.otfmm_stage_soa(null, null, null, null, null, 1, null, null, null, null, null) == inv
+    assert lib.otfmm_stage_p2m_soa(null, null, null, 1, 0, 0, null, null, ctypes.byref(stride), null) == inv
+    assert lib.otfmm_m2l_soa_host_noalloc(null, 1, null, null, null, null, null, 0, 0, 1, null) == inv
+    assert lib.otfmm_destroy(null) == 0
+    assert lib.otfmm_last_error() != b""
+
+
+def test_tree_records_reject_missing_parent():
+    from octotiger_b200.tree import tree_nodes
+    with pytest.raises(ValueError):
+        tree_nodes([0, 2], [[0, 0, 0], [1, 1, 1]])
+    nodes, ls = tree_nodes([0, 1, 1], [[0, 0, 0], [1, 0, 0], [0, 1, 1]])
+    assert list(ls) == [0, 1, 3]
+    assert list(nodes["parent"]) == [0 - 1, 0, 0] and sorted(nodes["octant"][1:]) == [1, 6]
