@@ -38,7 +38,8 @@ constexpr int RB = NCOMP * SUB_YZ + 2;     // 140 doubles per (x', y') row
 constexpr int XS = SUB_YZ * RB;            // 840
 constexpr int CLS = (REG_X / 2) * XS;      // 3360 doubles per parity class
 constexpr int SMEM_DOUBLES = 8 * CLS;      // 26880 doubles = 215040 bytes
-constexpr int MAX_ENTRIES = 216;           // 6^3 - 1 partners per cell at most
+constexpr int MAX_ENTRIES = 216;           // 6^3 - 1 partners per cell at most (coarse reach 1)
+constexpr int MAX_ENTRIES_R2 = 1000;       // partners per cell at most for theta >= 0.34 (coarse reach 2)
 constexpr int ROOT_SMEM_DOUBLES = NCOMP * NCELL;
 static_assert(ROOT_SMEM_DOUBLES <= SMEM_DOUBLES, "root staging fits");
 static_assert(RB % 16 == 12 || RB % 16 == 4, "row stride must keep 4x4 lane blocks conflict-free");
@@ -101,6 +102,7 @@ struct Tables {
     const uint16_t* p2m_perm;   // per direction, the cells with partners there, most partners first
     const int16_t* p2m_slot;    // [27][512]: position of a cell in its direction's p2m_perm list, -1 if absent
     const double4* p2p_four;    // [8][MAX_ENTRIES]: monopole constants of entries_p2p (zeros past the count)
+    const int2* entries_r2;     // [8][MAX_ENTRIES_R2]: stencil-order entries of any reach (y = packed)
 };
 
 __device__ __forceinline__ int entry_sx(int y) { return (y & 15) - 8; }

@@ -18,7 +18,8 @@
 //                    against refined neighbours;
 //   soa_kernels.cuh  per-subgrid entry points on the reference's SoA buffers and
 //                    their device-side staging;
-//   tree_kernels.cuh upward (M2M) and downward (L2L) passes.
+//   tree_kernels.cuh upward (M2M) and downward (L2L) passes;
+//   reach2_kernels.cuh opening angles below 0.5 (partners read from global memory).
 // The exact forms visit partners in the reference's stencil order with
 // explicitly rounded IEEE operations, so they are bit-identical to it.
 #include <cuda_runtime.h>
@@ -36,6 +37,7 @@
 #include "leaf_kernels.cuh"
 #include "m2l_tiles.cuh"
 #include "pair_math.cuh"
+#include "reach2_kernels.cuh"
 #include "soa_kernels.cuh"
 #include "tree_kernels.cuh"
 
@@ -156,11 +158,13 @@ int coarse_of(int i) { return ((i + INX) >> 1) - INX / 2; }
 
 // Per parity class: the partner offsets in stencil (x, y, z) order that pass
 // the per-cell coarse criterion dist^2 < 1/theta^2
-// (kokkos_kernel.hpp:241-256), packed with their shared-memory delta. False
-// when the stencil reaches further than one coarse cell (theta < 0.5).
-bool build_entries(const HostStencil& st, double theta, std::vector<int2>& entries, int counts[8], int& reach) {
+// (kokkos_kernel.hpp:241-256), packed with their shared-memory delta in the
+// tile layout (reach 1 only; 0 for reach 2). `stride` entries per class.
+// False when a class holds more than `stride` entries.
+bool build_entries(const HostStencil& st, double theta, int stride, std::vector<int2>& entries, int counts[8],
+                   int& reach) {
     const double trs = (1.0 / theta) * (1.0 / theta);
-    entries.assign(8 * MAX_ENTRIES, int2{0, 0});
+    entries.assign(8 * (size_t)stride, int2{0, 0});
     reach = 0;
     for (int p = 0; p < 8; ++p) {
         const int px = (p >> 2) & 1, py = (p >> 1) & 1, pz = p & 1;
@@ -175,13 +179,16 @@ bool build_entries(const HostStencil& st, double theta, std::vector<int2>& entri
                     const int c = coarse_of(pz + INX) - coarse_of(pz + INX + sz);
                     if (!(double(a * a + b * b + c * c) < trs)) continue;
                     reach = std::max({reach, std::abs(a), std::abs(b), std::abs(c)});
-                    if (reach > 1 || n >= MAX_ENTRIES) return false;
-                    const int qx = px + 2 + sx, qy = py + 2 + sy, qz = pz + 2 + sz;   // >= 0 for reach 1
-                    const int cls = (((px + sx) & 1) << 2) | (((py + sy) & 1) << 1) | ((pz + sz) & 1);
-                    const int delta = cls * CLS + (qx >> 1) * XS + (qy >> 1) * RB + (qz >> 1);
+                    if (n >= stride) return false;
+                    int delta = 0;
+                    if (std::abs(a) <= 1 && std::abs(b) <= 1 && std::abs(c) <= 1) {
+                        const int qx = px + 2 + sx, qy = py + 2 + sy, qz = pz + 2 + sz;   // >= 0 for reach 1
+                        const int cls = (((px + sx) & 1) << 2) | (((py + sy) & 1) << 1) | ((pz + sz) & 1);
+                        delta = cls * CLS + (qx >> 1) * XS + (qy >> 1) * RB + (qz >> 1);
+                    }
                     const int flags = st.phase[idx] ? F_FAR : F_NEAR;
                     const int packed = (sx + 8) | ((sy + 8) << 4) | ((sz + 8) << 8) | (flags << 12) | (idx << 16);
-                    entries[p * MAX_ENTRIES + n] = int2{delta, packed};
+                    entries[p * (size_t)stride + n] = int2{delta, packed};
                     ++n;
                 }
         counts[p] = n;
@@ -209,6 +216,7 @@ struct otfmm_context {
     int* d_p2m_perm_start = nullptr;
     uint16_t* d_p2m_perm = nullptr;
     int16_t* d_p2m_slot = nullptr;
+    int2* d_entries_r2 = nullptr;   // stencil-order entries, MAX_ENTRIES_R2 per class (any reach)
     int p2m_groups_max = 0;   // cells with partners summed over the 26 directions
     double4* d_p2p_four = nullptr;
     int counts_far[8] = {};
@@ -235,7 +243,7 @@ struct otfmm_context {
     std::mutex mu;
     Tables tables() const { return Tables{d_entries,    d_count, d_entries_fast, d_count_far, d_entries_split, d_entries_p2p,
                       d_entries_ws, d_four,  d_phase,        d_p2m_start,     d_p2m_list,    d_p2m_perm_start,
-                      d_p2m_perm,   d_p2m_slot,     d_p2p_four}; }
+                      d_p2m_perm,   d_p2m_slot,     d_p2p_four,      d_entries_r2}; }
 };
 
 namespace {
@@ -284,6 +292,10 @@ int ensure_attributes(int device) {
     rc = rc ? rc : set_smem(p2p_leaf_kernel<double, 0>, p2_smem_bytes<double>());
     rc = rc ? rc : set_smem(p2p_leaf_kernel<float, 32>, p2_smem_bytes<float>());
     rc = rc ? rc : set_smem(p2p_leaf_kernel<float, 16>, p2_smem_bytes<float>());
+    rc = rc ? rc : set_smem(m2l_r2_kernel<PREC_EXACT, true>, ROOT_SMEM_DOUBLES * 8);
+    rc = rc ? rc : set_smem(m2l_r2_kernel<PREC_EXACT, false>, ROOT_SMEM_DOUBLES * 8);
+    rc = rc ? rc : set_smem(m2l_r2_kernel<PREC_FAST, true>, ROOT_SMEM_DOUBLES * 8);
+    rc = rc ? rc : set_smem(m2l_r2_kernel<PREC_FAST, false>, ROOT_SMEM_DOUBLES * 8);
     rc = rc ? rc : set_smem(p2m_fast_kernel<true>, 7 * 8 * 6 * NCELL);
     rc = rc ? rc : set_smem(p2m_fast_kernel<false>, 7 * 8 * 6 * NCELL);
     rc = rc ? rc : set_smem(soa_m2l_kernel<PREC_EXACT, true, false>, bytes);
@@ -311,7 +323,7 @@ extern "C" {
 const char* otfmm_last_error(void) { return g_last_error.c_str(); }
 
 const char* otfmm_build_info(void) {
-    return "otfmm sm_100a; tiles of 4x8x8 cells, 256 threads, 215040 B (FP64) / 227840 B (FP32 split) shared memory; theta >= 0.5";
+    return "otfmm sm_100a; tiles of 4x8x8 cells; theta >= 0.5: shared-memory tiles (FP64 215040 B, FP32 split warp-specialised 228096 B); 0.34 <= theta < 0.5: global-memory sweeps";
 }
 
 int otfmm_create(int device, double theta, otfmm_context** out) {
@@ -329,18 +341,27 @@ int otfmm_create(int device, double theta, otfmm_context** out) {
         delete ctx;
         return fail(OTFMM_ERR_THETA, "stencil exceeds the compiled maximum width");
     }
-    // Per-parity offset lists in stencil order, filtered by the coarse criterion.
-    std::vector<int2> entries;
+    // Per-parity offset lists in stencil order, filtered by the coarse criterion:
+    // for theta >= 0.5 (coarse reach 1) in the tile layout, below that (reach 2)
+    // as the long lists of the global-memory kernels.
+    std::vector<int2> entries, entries_r2;
     int reach = 0;
-    if (!build_entries(ctx->st, theta, entries, ctx->counts, reach)) {
+    if (!build_entries(ctx->st, theta, MAX_ENTRIES_R2, entries_r2, ctx->counts, reach)) {
         delete ctx;
-        return fail(OTFMM_ERR_UNSUPPORTED, "theta < 0.5 (coarse reach 2) is not built into this library");
+        return fail(OTFMM_ERR_UNSUPPORTED, "stencil longer than the compiled maximum");
     }
     ctx->reach = reach;
+    if (reach <= 1) {
+        build_entries(ctx->st, theta, MAX_ENTRIES, entries, ctx->counts, reach);
+    } else {
+        // reach-1 tables stay empty; the tile kernels are not used
+        entries.assign(8 * MAX_ENTRIES, int2{0, 0});
+    }
     // P2P-layout table (stencil order)
     std::vector<int2> entries_p2p(8 * MAX_ENTRIES, int2{0, 0});
     std::vector<double4> p2p_four(8 * MAX_ENTRIES, double4{0.0, 0.0, 0.0, 0.0});
-    for (int p = 0; p < 8; ++p)
+    const int n_tile = (reach <= 1) ? 8 : 0;   // reach-1 (tile) tables only for theta >= 0.5
+    for (int p = 0; p < n_tile; ++p)
         for (int e = 0; e < ctx->counts[p]; ++e) {
             const int2 en = entries[p * MAX_ENTRIES + e];
             const int sx = (en.y & 15) - 8, sy = ((en.y >> 4) & 15) - 8, sz = ((en.y >> 8) & 15) - 8;
@@ -356,7 +377,7 @@ int otfmm_create(int device, double theta, otfmm_context** out) {
     std::vector<int4> entries_ws(8 * MAX_ENTRIES, int4{0, 0, 0, 0});
     // fast-form table: far offsets first (accumulation order is free there)
     std::vector<int2> entries_fast(entries.size(), int2{0, 0});
-    for (int p = 0; p < 8; ++p) {
+    for (int p = 0; p < n_tile; ++p) {
         int k = 0;
         for (int pass = 0; pass < 2; ++pass)
             for (int e = 0; e < ctx->counts[p]; ++e) {
@@ -381,7 +402,7 @@ int otfmm_create(int device, double theta, otfmm_context** out) {
     // the partner (stencil order inside a group), as partner cell indices
     std::vector<int> p2m_start(NCELL * 28, 0);
     std::vector<uint16_t> p2m_list;
-    p2m_list.reserve((size_t)NCELL * MAX_ENTRIES);
+    p2m_list.reserve((size_t)NCELL * MAX_ENTRIES_R2);
     for (int cu = 0; cu < NCELL; ++cu) {
         const int cx = cu >> 6, cy = (cu >> 3) & 7, cz = cu & 7;
         const int p = ((cx & 1) << 2) | ((cy & 1) << 1) | (cz & 1);
@@ -389,7 +410,7 @@ int otfmm_create(int device, double theta, otfmm_context** out) {
             p2m_start[cu * 28 + r] = (int)p2m_list.size();
             if (r == 13) continue;
             for (int e2 = 0; e2 < ctx->counts[p]; ++e2) {
-                const int y = entries[p * MAX_ENTRIES + e2].y;
+                const int y = entries_r2[p * (size_t)MAX_ENTRIES_R2 + e2].y;
                 const int ax = cx + (y & 15) - 8, ay = cy + ((y >> 4) & 15) - 8, az = cz + ((y >> 8) & 15) - 8;
                 const int raw = ((ax >> 3) + 1) + 3 * ((ay >> 3) + 1) + 9 * ((az >> 3) + 1);
                 if (raw == r) p2m_list.push_back((uint16_t)((ax & 7) * 64 + (ay & 7) * 8 + (az & 7)));
@@ -418,7 +439,10 @@ int otfmm_create(int device, double theta, otfmm_context** out) {
     ctx->p2m_groups_max = (int)p2m_perm.size();
     DeviceGuard g(device);
     cudaError_t e;
-    if ((e = cudaMalloc(&ctx->d_p2m_slot, sizeof(int16_t) * p2m_slot.size())) != cudaSuccess ||
+    if ((e = cudaMalloc(&ctx->d_entries_r2, sizeof(int2) * entries_r2.size())) != cudaSuccess ||
+        (e = cudaMemcpy(ctx->d_entries_r2, entries_r2.data(), sizeof(int2) * entries_r2.size(),
+                        cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMalloc(&ctx->d_p2m_slot, sizeof(int16_t) * p2m_slot.size())) != cudaSuccess ||
         (e = cudaMemcpy(ctx->d_p2m_slot, p2m_slot.data(), sizeof(int16_t) * p2m_slot.size(),
                         cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMalloc(&ctx->d_p2p_four, sizeof(double4) * p2p_four.size())) != cudaSuccess ||
@@ -490,6 +514,7 @@ int otfmm_destroy(otfmm_context* ctx) {
     cudaFree(ctx->d_p2m_perm);
     cudaFree(ctx->d_p2p_four);
     cudaFree(ctx->d_p2m_slot);
+    cudaFree(ctx->d_entries_r2);
     {
         auto& hp = ctx->hp;
         if (hp.ready) {
@@ -544,7 +569,15 @@ int otfmm_m2l_soa(otfmm_context* ctx, const double* mon, const double* M, const 
     const size_t bytes = SMEM_DOUBLES * sizeof(double);
     cudaStream_t s = (cudaStream_t)stream;
 #define OT_SOA(P, R, T) soa_m2l_kernel<P, R, T><<<2, THREADS, bytes, s>>>(a)
-    if (precision == OTFMM_FP64_EXACT) {
+    if (ctx->reach > 1 && !use_root_stencil) {
+        if (precision == OTFMM_FP64_EXACT) {
+            if (rho) soa_m2l_r2_kernel<PREC_EXACT, true><<<2, THREADS, 0, s>>>(a);
+            else soa_m2l_r2_kernel<PREC_EXACT, false><<<2, THREADS, 0, s>>>(a);
+        } else {
+            if (rho) soa_m2l_r2_kernel<PREC_FAST, true><<<2, THREADS, 0, s>>>(a);
+            else soa_m2l_r2_kernel<PREC_FAST, false><<<2, THREADS, 0, s>>>(a);
+        }
+    } else if (precision == OTFMM_FP64_EXACT) {
         if (use_root_stencil) { if (rho) OT_SOA(PREC_EXACT, true, true); else OT_SOA(PREC_EXACT, false, true); }
         else { if (rho) OT_SOA(PREC_EXACT, true, false); else OT_SOA(PREC_EXACT, false, false); }
     } else {
@@ -759,6 +792,31 @@ int enqueue_batch(otfmm_context* ctx, const double* pool_M, const double* pool_c
     classify_kernel<<<(n_items + 255) / 256, 256, 0, s>>>(a);
     mark(1);
     const dim3 tiles_grid(sms), p2p_grid(P2P_CTAS_PER_SM * sms), p2m_grid(std::min(n_items, 8 * sms));
+    if (ctx->reach > 1) {
+        // theta < 0.5: partners from global memory; the split precision runs the fast FP64 form
+        const size_t rbytes = ROOT_SMEM_DOUBLES * sizeof(double);
+        const dim3 leaf_grid(std::min(n_items, 8 * sms));
+        if (precision == OTFMM_FP64_EXACT) {
+            if (rho) m2l_r2_kernel<PREC_EXACT, true><<<4 * sms, THREADS, rbytes, s>>>(a);
+            else m2l_r2_kernel<PREC_EXACT, false><<<4 * sms, THREADS, rbytes, s>>>(a);
+            mark(2);
+            p2p_r2_kernel<PREC_EXACT><<<leaf_grid, P_THREADS, 0, s>>>(a);
+            mark(3);
+            if (rho) p2m_batch_kernel<PREC_EXACT, true><<<p2m_grid, P_THREADS, 0, s>>>(a);
+            else p2m_batch_kernel<PREC_EXACT, false><<<p2m_grid, P_THREADS, 0, s>>>(a);
+        } else {
+            if (rho) m2l_r2_kernel<PREC_FAST, true><<<4 * sms, THREADS, rbytes, s>>>(a);
+            else m2l_r2_kernel<PREC_FAST, false><<<4 * sms, THREADS, rbytes, s>>>(a);
+            mark(2);
+            p2p_r2_kernel<PREC_FAST><<<leaf_grid, P_THREADS, 0, s>>>(a);
+            mark(3);
+            if (rho) p2m_batch_kernel<PREC_FAST, true><<<p2m_grid, P_THREADS, 0, s>>>(a);
+            else p2m_batch_kernel<PREC_FAST, false><<<p2m_grid, P_THREADS, 0, s>>>(a);
+        }
+        mark(4);
+        OT_CUDA(cudaGetLastError());
+        return OTFMM_OK;
+    }
     if (precision == OTFMM_FP64_EXACT) {
         if (rho) m2l_batch_kernel<PREC_EXACT, true><<<tiles_grid, THREADS, bytes, s>>>(a);
         else m2l_batch_kernel<PREC_EXACT, false><<<tiles_grid, THREADS, bytes, s>>>(a);

@@ -1,0 +1,220 @@
+// Kernels for opening angles below 0.5 (coarse reach 2: partners up to five
+// cells away, theta >= 0.34). The halo of a tile no longer fits in shared
+// memory, so partners are read from global memory (L1/L2) in the reference's
+// stencil order:
+//   * m2l_r2_kernel: multipole tiles of refined items from the resident pool,
+//     each partner resolved the way update_input stages it
+//     (multipole_interaction_interface.hpp:88-281);
+//   * p2p_r2_kernel: P2P of leaves from the pool;
+//   * soa_m2l_r2_kernel: the per-subgrid entry point on the reference's 18^3
+//     SoA buffers.
+// Root tiles and P2M use the reach-independent kernels.
+// Part of libotfmm.so; included once, in order, by otfmm.cu (one translation unit).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "../../include/otfmm.h"
+#include "pair_math.cuh"
+#include "layout.cuh"
+#include "m2l_tiles.cuh"
+#include "soa_kernels.cuh"
+
+namespace otfmm {
+
+// Multipole tiles (half a subgrid, 256 threads; warp = parity class) of
+// refined and root items, persistent over the same tile counter as
+// m2l_batch_kernel. Root tiles stage their own cells in shared memory
+// (reach-independent root stencil).
+template <int PREC, bool RHO>
+__global__ void __launch_bounds__(THREADS, 1) m2l_r2_kernel(BatchArgs a) {
+    extern __shared__ double sm[];
+    __shared__ ItemInfo it;
+    __shared__ int tile;
+    const int nroot = a.wl.counts[WL_ROOT], nm2l = a.wl.counts[WL_M2L];
+    const int total = 2 * (nroot + nm2l);
+    for (;;) {
+        if (threadIdx.x == 0) tile = atomicAdd(a.wl.counts + WL_M2L_NEXT, 1);
+        __syncthreads();
+        const int t = tile;
+        if (t >= total) break;
+        const int item_idx = (t < 2 * nroot) ? a.wl.root[t >> 1] : a.wl.m2l[(t - 2 * nroot) >> 1];
+        load_item(a, item_idx, it);
+        const int x0 = TILE_X * (t & 1);
+        const size_t sub = (size_t)it.subgrid;
+        OutPtr out{a.L + sub * 20 * NCELL, a.Lc + sub * 3 * NCELL, NCELL, true};
+        if (it.kind == OTFMM_KIND_M2L_ROOT) {
+            for (int r = threadIdx.x; r < NCELL; r += blockDim.x)
+                for (int q = 0; q < NCOMP; ++q)
+                    sm[q * NCELL + r] = (q < 20) ? a.M[(sub * 20 + q) * NCELL + r] * stage_scale<PREC>(q)
+                                                 : a.com[(sub * 3 + (q - 20)) * NCELL + r];
+            __syncthreads();
+            root_tile<PREC, RHO>(sm, x0, a.t, out);
+        } else {
+            const CellMap c = cell_map(x0);
+            const int cu = c.cx * 64 + c.cy * 8 + c.cz;
+            double X[3], mc[20], acc[20], corr[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+            for (int q = 0; q < 3; ++q) X[q] = a.com[(sub * 3 + q) * NCELL + cu];
+#pragma unroll
+            for (int q = 0; q < 20; ++q) {
+                mc[q] = a.M[(sub * 20 + q) * NCELL + cu] * stage_scale<PREC>(q);
+                acc[q] = 0.0;
+            }
+            const double inv_m0 = 1.0 / mc[0];
+            const int n = a.t.count[c.p];
+            const int2* ent = a.t.entries_r2 + c.p * MAX_ENTRIES_R2;
+#pragma unroll 1
+            for (int e = 0; e < n; ++e) {
+                const int y = __ldg(&ent[e].y);
+                const bool far = (entry_flags(y) & F_FAR) != 0;
+                const int ax = c.cx + entry_sx(y), ay = c.cy + entry_sy(y), az = c.cz + entry_sz(y);
+                const int raw = raw_dir(ax, ay, az);
+                const int src = (raw == 13) ? it.subgrid : it.nb[raw < 13 ? raw : raw - 1];
+                const bool leaf = src >= 0 && raw != 13 && a.is_leaf[src];
+                // monopole-only offsets: only leaf partners carry mass (the staged
+                // mon is zero for multipole and empty cells)
+                if (!far && !leaf) continue;
+                const int u = (ax & 7) * 64 + (ay & 7) * 8 + (az & 7);
+                double Y[3], mp[20];
+                if (src < 0) {
+                    // empty direction: zero moments at the origin, as staged
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) Y[q] = 0.0;
+#pragma unroll
+                    for (int q = 0; q < 20; ++q) mp[q] = 0.0;
+                } else if (leaf) {
+                    const int ip[3] = {ax + INX, ay + INX, az + INX};
+#pragma unroll
+                    for (int q = 0; q < 3; ++q)
+                        Y[q] = __dsub_rn(__dadd_rn(__dmul_rn((double)ip[q], it.dx), it.xbase[q]),
+                                         __dmul_rn((double)INX, it.dx));
+                    mp[0] = __ldg(a.mon + (size_t)src * NCELL + u);
+#pragma unroll
+                    for (int q = 1; q < 20; ++q) mp[q] = 0.0;
+                } else {
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) Y[q] = __ldg(a.com + ((size_t)src * 3 + q) * NCELL + u);
+#pragma unroll
+                    for (int q = 0; q < 20; ++q)
+                        mp[q] = __ldg(a.M + ((size_t)src * 20 + q) * NCELL + u) * stage_scale<PREC>(q);
+                }
+                if (PREC == PREC_EXACT)
+                    exact_m2l_pair<RHO>(X, Y, mp, mc, acc, corr);
+                else
+                    fast_m2l_pair<RHO>(X, Y, mp, mc + 10, inv_m0, acc, corr);
+            }
+#pragma unroll
+            for (int q = 0; q < 20; ++q) out.L[q * out.stride + cu] = acc[q];
+            write_lc<RHO>(out, cu, corr);
+        }
+        __syncthreads();   // shared memory and `it` are reused by the next tile
+    }
+}
+
+// P2P of leaves: one CTA (512 threads) per leaf, grid stride; warp w serves
+// half of parity class w >> 1 (32 of its 64 cells), so the warp walks one
+// entry list and reads one constant per entry. Refined and empty neighbours
+// contribute zero mass, as staged by monopole update_input
+// (monopole_interaction_interface.hpp:64-143).
+template <int PREC>
+__global__ void __launch_bounds__(P_THREADS) p2p_r2_kernel(BatchArgs a) {
+    __shared__ ItemInfo it;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int p = w >> 1, q = lane + 32 * (w & 1);
+    const int cx = ((p >> 2) & 1) + 2 * (q >> 4), cy = ((p >> 1) & 1) + 2 * ((q >> 2) & 3), cz = (p & 1) + 2 * (q & 3);
+    const int cu = cx * 64 + cy * 8 + cz;
+    const int n = a.t.count[p];
+    const int2* ent = a.t.entries_r2 + p * MAX_ENTRIES_R2;
+    const int nleaf = a.wl.counts[WL_LEAF];
+    for (int kk = blockIdx.x; kk < nleaf; kk += gridDim.x) {
+        __syncthreads();   // `it` is reused
+        load_item(a, a.wl.leaf[kk], it);
+        const double dc0 = __ddiv_rn(1.0, it.dx), dc1 = __ddiv_rn(-1.0, it.dx);
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 4
+        for (int e = 0; e < n; ++e) {
+            const int y = __ldg(&ent[e].y);
+            const int ax = cx + entry_sx(y), ay = cy + entry_sy(y), az = cz + entry_sz(y);
+            const int raw = raw_dir(ax, ay, az);
+            const int src = (raw == 13) ? it.subgrid : it.nb[raw < 13 ? raw : raw - 1];
+            double m = 0.0;
+            if (src >= 0 && (raw == 13 || a.is_leaf[src]))
+                m = __ldg(a.mon + (size_t)src * NCELL + (ax & 7) * 64 + (ay & 7) * 8 + (az & 7));
+            const double* four = c_four[entry_sidx(y)];
+            if (PREC == PREC_EXACT) {
+                const double ms = __dmul_rn(m, dc0);
+                acc[0] = __dadd_rn(acc[0], __dmul_rn(four[0], ms));
+#pragma unroll
+                for (int c = 1; c < 4; ++c) acc[c] = __dadd_rn(acc[c], __dmul_rn(__dmul_rn(four[c], ms), dc1));
+            } else {
+                const double ms = m * dc0;
+                acc[0] = fma(four[0], ms, acc[0]);
+#pragma unroll
+                for (int c = 1; c < 4; ++c) acc[c] = fma(four[c], ms, acc[c]);
+            }
+        }
+        if (PREC != PREC_EXACT)
+#pragma unroll
+            for (int c = 1; c < 4; ++c) acc[c] *= dc1;
+        double* L = a.L + (size_t)it.subgrid * 20 * NCELL;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) L[c * NCELL + cu] = acc[c];
+    }
+}
+
+// Per-subgrid multipole sweep on the reference's SoA buffers (two tiles of
+// 4 x 8 x 8 cells): phase-one partners take mon + M0 and the higher moments,
+// monopole-only partners the mass alone (kokkos_kernel.hpp:241-283).
+template <int PREC, bool RHO>
+__global__ void __launch_bounds__(THREADS) soa_m2l_r2_kernel(SoaArgs a) {
+    const int x0 = TILE_X * blockIdx.x;
+    const CellMap c = cell_map(x0);
+    auto padded = [](int x, int y, int z) {
+        return (x + INX - PAD_OFF) * PSTRIDE * PSTRIDE + (y + INX - PAD_OFF) * PSTRIDE + (z + INX - PAD_OFF);
+    };
+    const int fc = padded(c.cx, c.cy, c.cz);
+    double X[3], mc[20], acc[20], corr[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int q = 0; q < 3; ++q) X[q] = a.com[q * CL + fc];
+#pragma unroll
+    for (int q = 0; q < 20; ++q) {
+        mc[q] = a.M[q * CL + fc] * stage_scale<PREC>(q);
+        acc[q] = 0.0;
+    }
+    const double inv_m0 = 1.0 / mc[0];
+    const int n = a.t.count[c.p];
+    const int2* ent = a.t.entries_r2 + c.p * MAX_ENTRIES_R2;
+#pragma unroll 1
+    for (int e = 0; e < n; ++e) {
+        const int y = __ldg(&ent[e].y);
+        const bool far = (entry_flags(y) & F_FAR) != 0;
+        const int f = padded(c.cx + entry_sx(y), c.cy + entry_sy(y), c.cz + entry_sz(y));
+        double Y[3], mp[20];
+        if (far) {
+            mp[0] = __dadd_rn(__ldg(a.mon + f), __ldg(a.M + f)) * stage_scale<PREC>(0);
+#pragma unroll
+            for (int q = 1; q < 20; ++q) mp[q] = __ldg(a.M + q * CL + f) * stage_scale<PREC>(q);
+        } else {
+            mp[0] = __ldg(a.mon + f);
+            if (mp[0] == 0.0) continue;   // no mass: contributes exactly zero
+#pragma unroll
+            for (int q = 1; q < 20; ++q) mp[q] = 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < 3; ++q) Y[q] = __ldg(a.com + q * CL + f);
+        if (PREC == PREC_EXACT)
+            exact_m2l_pair<RHO>(X, Y, mp, mc, acc, corr);
+        else
+            fast_m2l_pair<RHO>(X, Y, mp, mc + 10, inv_m0, acc, corr);
+    }
+    OutPtr out{a.L, a.Lc, CLU, false};
+    const int cf = c.cx * 64 + c.cy * 8 + c.cz;
+#pragma unroll
+    for (int q = 0; q < 20; ++q) out.L[q * out.stride + cf] = acc[q];
+    write_lc<RHO>(out, cf, corr);
+}
+
+}   // namespace otfmm
