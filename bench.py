@@ -53,14 +53,14 @@ PROFILED_TRAFFIC = {("uniform_level3", "fp32_split"): 61.0e6, ("uniform_level3",
 WORKLOADS = ("uniform_level3", "amr_polytrope", "amr_binary")
 
 
-def make_workload(name: str):
+def make_workload(name: str, theta: float = 0.5):
     if name == "uniform_level3":
-        return syn.uniform_level(3)
+        return syn.uniform_level(3, theta=theta)
     from octotiger_b200 import amr
     if name == "amr_polytrope":
-        return amr.polytrope_batch()
+        return amr.polytrope_batch(theta=theta)
     if name == "amr_binary":
-        return amr.binary_batch()
+        return amr.binary_batch(theta=theta)
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -192,7 +192,7 @@ def reference_arm(args) -> None:
     world, rank, _ = dist_setup()
     if rank != 0:
         return
-    batch = make_workload(args.workload)
+    batch = make_workload(args.workload, args.theta)
     solve = RHO if args.gsolve == "rho" else DRHODT
     from oracle.pyoracle import Oracle, RefMath, ref_library_path
     nthreads = os.cpu_count() or 1
@@ -237,7 +237,7 @@ def gpu_arm(args) -> None:
         pg = dist
     from octotiger_b200.otfmm import BatchSolver, Context, measure_fma_peaks, order_work_list
 
-    batch = make_workload(args.workload)
+    batch = make_workload(args.workload, args.theta)
     solve = RHO if args.gsolve == "rho" else DRHODT
     ctx = Context(local, batch.theta)
     counts = pair_counts(batch, ctx)
@@ -494,6 +494,7 @@ def main() -> None:
     ap.add_argument("--precision", default="fp32_split", choices=["fp32_split", "fp64", "fp64_exact"])
     ap.add_argument("--compare", nargs="*", default=["fp64", "fp64_exact"])
     ap.add_argument("--gsolve", default="rho", choices=["rho", "drhodt"])
+    ap.add_argument("--theta", type=float, default=0.5, help="opening angle (>= 0.34)")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-per-subgrid", action="store_true", help="skip the per-subgrid FP64 comparison")

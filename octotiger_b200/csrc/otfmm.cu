@@ -296,6 +296,8 @@ int ensure_attributes(int device) {
     rc = rc ? rc : set_smem(m2l_r2_kernel<PREC_EXACT, false>, ROOT_SMEM_DOUBLES * 8);
     rc = rc ? rc : set_smem(m2l_r2_kernel<PREC_FAST, true>, ROOT_SMEM_DOUBLES * 8);
     rc = rc ? rc : set_smem(m2l_r2_kernel<PREC_FAST, false>, ROOT_SMEM_DOUBLES * 8);
+    rc = rc ? rc : set_smem(p2p_r2_kernel<PREC_EXACT>, R2_SMEM_BYTES);
+    rc = rc ? rc : set_smem(p2p_r2_kernel<PREC_FAST>, R2_SMEM_BYTES);
     rc = rc ? rc : set_smem(p2m_fast_kernel<true>, 7 * 8 * 6 * NCELL);
     rc = rc ? rc : set_smem(p2m_fast_kernel<false>, 7 * 8 * 6 * NCELL);
     rc = rc ? rc : set_smem(soa_m2l_kernel<PREC_EXACT, true, false>, bytes);
@@ -800,7 +802,7 @@ int enqueue_batch(otfmm_context* ctx, const double* pool_M, const double* pool_c
             if (rho) m2l_r2_kernel<PREC_EXACT, true><<<4 * sms, THREADS, rbytes, s>>>(a);
             else m2l_r2_kernel<PREC_EXACT, false><<<4 * sms, THREADS, rbytes, s>>>(a);
             mark(2);
-            p2p_r2_kernel<PREC_EXACT><<<leaf_grid, P_THREADS, 0, s>>>(a);
+            p2p_r2_kernel<PREC_EXACT><<<leaf_grid, P_THREADS, R2_SMEM_BYTES, s>>>(a);
             mark(3);
             if (rho) p2m_batch_kernel<PREC_EXACT, true><<<p2m_grid, P_THREADS, 0, s>>>(a);
             else p2m_batch_kernel<PREC_EXACT, false><<<p2m_grid, P_THREADS, 0, s>>>(a);
@@ -808,7 +810,7 @@ int enqueue_batch(otfmm_context* ctx, const double* pool_M, const double* pool_c
             if (rho) m2l_r2_kernel<PREC_FAST, true><<<4 * sms, THREADS, rbytes, s>>>(a);
             else m2l_r2_kernel<PREC_FAST, false><<<4 * sms, THREADS, rbytes, s>>>(a);
             mark(2);
-            p2p_r2_kernel<PREC_FAST><<<leaf_grid, P_THREADS, 0, s>>>(a);
+            p2p_r2_kernel<PREC_FAST><<<leaf_grid, P_THREADS, R2_SMEM_BYTES, s>>>(a);
             mark(3);
             if (rho) p2m_batch_kernel<PREC_FAST, true><<<p2m_grid, P_THREADS, 0, s>>>(a);
             else p2m_batch_kernel<PREC_FAST, false><<<p2m_grid, P_THREADS, 0, s>>>(a);

@@ -114,35 +114,49 @@ __global__ void __launch_bounds__(THREADS, 1) m2l_r2_kernel(BatchArgs a) {
     }
 }
 
-// P2P of leaves: one CTA (512 threads) per leaf, grid stride; warp w serves
-// half of parity class w >> 1 (32 of its 64 cells), so the warp walks one
-// entry list and reads one constant per entry. Refined and empty neighbours
-// contribute zero mass, as staged by monopole update_input
-// (monopole_interaction_interface.hpp:64-143).
+// P2P of leaves: one CTA (512 threads) per leaf, grid stride. The leaf's
+// 18^3 mass halo (padding 5) is staged in shared memory first, refined and
+// empty neighbours as zero mass (monopole update_input,
+// monopole_interaction_interface.hpp:64-143); warp w then serves half of
+// parity class w >> 1 (32 of its 64 cells), so the warp walks one entry list
+// and reads one constant per entry.
+constexpr int R2_PAD = SMAX;                  // halo width
+constexpr int R2_REG = INX + 2 * R2_PAD;      // 18
+constexpr int R2_ROW = R2_REG + 1;            // z rows padded to 19 doubles
+constexpr int R2_PLANE = R2_REG * R2_ROW;
+constexpr int R2_SMEM_BYTES = R2_REG * R2_PLANE * 8;   // 49,248 bytes
 template <int PREC>
 __global__ void __launch_bounds__(P_THREADS) p2p_r2_kernel(BatchArgs a) {
+    extern __shared__ double pm[];
     __shared__ ItemInfo it;
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int p = w >> 1, q = lane + 32 * (w & 1);
     const int cx = ((p >> 2) & 1) + 2 * (q >> 4), cy = ((p >> 1) & 1) + 2 * ((q >> 2) & 3), cz = (p & 1) + 2 * (q & 3);
     const int cu = cx * 64 + cy * 8 + cz;
+    const int own = (cx + R2_PAD) * R2_PLANE + (cy + R2_PAD) * R2_ROW + (cz + R2_PAD);
     const int n = a.t.count[p];
     const int2* ent = a.t.entries_r2 + p * MAX_ENTRIES_R2;
     const int nleaf = a.wl.counts[WL_LEAF];
     for (int kk = blockIdx.x; kk < nleaf; kk += gridDim.x) {
-        __syncthreads();   // `it` is reused
+        __syncthreads();   // `it` and the halo are reused
         load_item(a, a.wl.leaf[kk], it);
+        for (int r = threadIdx.x; r < R2_REG * R2_REG * R2_REG; r += blockDim.x) {
+            const int ax = r / (R2_REG * R2_REG) - R2_PAD, ay = (r / R2_REG) % R2_REG - R2_PAD,
+                      az = r % R2_REG - R2_PAD;
+            const int raw = raw_dir(ax, ay, az);
+            const int src = (raw == 13) ? it.subgrid : it.nb[raw < 13 ? raw : raw - 1];
+            double m = 0.0;
+            if (src >= 0 && (raw == 13 || a.is_leaf[src]))
+                m = a.mon[(size_t)src * NCELL + (ax & 7) * 64 + (ay & 7) * 8 + (az & 7)];
+            pm[(ax + R2_PAD) * R2_PLANE + (ay + R2_PAD) * R2_ROW + (az + R2_PAD)] = m;
+        }
+        __syncthreads();
         const double dc0 = __ddiv_rn(1.0, it.dx), dc1 = __ddiv_rn(-1.0, it.dx);
         double acc[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll 4
         for (int e = 0; e < n; ++e) {
             const int y = __ldg(&ent[e].y);
-            const int ax = cx + entry_sx(y), ay = cy + entry_sy(y), az = cz + entry_sz(y);
-            const int raw = raw_dir(ax, ay, az);
-            const int src = (raw == 13) ? it.subgrid : it.nb[raw < 13 ? raw : raw - 1];
-            double m = 0.0;
-            if (src >= 0 && (raw == 13 || a.is_leaf[src]))
-                m = __ldg(a.mon + (size_t)src * NCELL + (ax & 7) * 64 + (ay & 7) * 8 + (az & 7));
+            const double m = pm[own + entry_sx(y) * R2_PLANE + entry_sy(y) * R2_ROW + entry_sz(y)];
             const double* four = c_four[entry_sidx(y)];
             if (PREC == PREC_EXACT) {
                 const double ms = __dmul_rn(m, dc0);
