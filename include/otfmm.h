@@ -90,7 +90,9 @@ typedef struct otfmm_context otfmm_context;
 /* Creates a context on `device` for opening angle theta (opts().theta,
  * src/options_processing.cpp:119; must be >= 0.34, :234-236). Builds the
  * multipole two-phase stencil and the monopole stencil with its constants and
- * uploads them. Replaces calculate_stencil + get_device_masks. */
+ * uploads them. Replaces calculate_stencil + get_device_masks. theta >= 0.5
+ * runs the shared-memory tile kernels, 0.34 <= theta < 0.5 (partners up to
+ * two coarse cells away) global-memory kernels of the same results. */
 int otfmm_create(int device, double theta, otfmm_context** out);
 int otfmm_destroy(otfmm_context* ctx);
 
