@@ -102,7 +102,9 @@ struct Tables {
     const uint16_t* p2m_perm;   // per direction, the cells with partners there, most partners first
     const int16_t* p2m_slot;    // [27][512]: position of a cell in its direction's p2m_perm list, -1 if absent
     const double4* p2p_four;    // [8][MAX_ENTRIES]: monopole constants of entries_p2p (zeros past the count)
-    const int2* entries_r2;     // [8][MAX_ENTRIES_R2]: stencil-order entries of any reach (y = packed)
+    const int2* entries_r2;     // [8][MAX_ENTRIES_R2]: stencil-order entries of any reach (x = plane delta,
+                                // y = packed)
+    const int* r2_sx_start;     // [8][12]: first entry of each sx = -5 .. 5 in entries_r2 (and the end)
 };
 
 __device__ __forceinline__ int entry_sx(int y) { return (y & 15) - 8; }

@@ -217,6 +217,7 @@ struct otfmm_context {
     uint16_t* d_p2m_perm = nullptr;
     int16_t* d_p2m_slot = nullptr;
     int2* d_entries_r2 = nullptr;   // stencil-order entries, MAX_ENTRIES_R2 per class (any reach)
+    int* d_r2_sx_start = nullptr;
     int p2m_groups_max = 0;   // cells with partners summed over the 26 directions
     double4* d_p2p_four = nullptr;
     int counts_far[8] = {};
@@ -243,7 +244,7 @@ struct otfmm_context {
     std::mutex mu;
     Tables tables() const { return Tables{d_entries,    d_count, d_entries_fast, d_count_far, d_entries_split, d_entries_p2p,
                       d_entries_ws, d_four,  d_phase,        d_p2m_start,     d_p2m_list,    d_p2m_perm_start,
-                      d_p2m_perm,   d_p2m_slot,     d_p2p_four,      d_entries_r2}; }
+                      d_p2m_perm,   d_p2m_slot,     d_p2p_four,      d_entries_r2,  d_r2_sx_start}; }
 };
 
 namespace {
@@ -292,10 +293,10 @@ int ensure_attributes(int device) {
     rc = rc ? rc : set_smem(p2p_leaf_kernel<double, 0>, p2_smem_bytes<double>());
     rc = rc ? rc : set_smem(p2p_leaf_kernel<float, 32>, p2_smem_bytes<float>());
     rc = rc ? rc : set_smem(p2p_leaf_kernel<float, 16>, p2_smem_bytes<float>());
-    rc = rc ? rc : set_smem(m2l_r2_kernel<PREC_EXACT, true>, ROOT_SMEM_DOUBLES * 8);
-    rc = rc ? rc : set_smem(m2l_r2_kernel<PREC_EXACT, false>, ROOT_SMEM_DOUBLES * 8);
-    rc = rc ? rc : set_smem(m2l_r2_kernel<PREC_FAST, true>, ROOT_SMEM_DOUBLES * 8);
-    rc = rc ? rc : set_smem(m2l_r2_kernel<PREC_FAST, false>, ROOT_SMEM_DOUBLES * 8);
+    rc = rc ? rc : set_smem(m2l_r2_kernel<PREC_EXACT, true>, PL_SMEM_BYTES);
+    rc = rc ? rc : set_smem(m2l_r2_kernel<PREC_EXACT, false>, PL_SMEM_BYTES);
+    rc = rc ? rc : set_smem(m2l_r2_kernel<PREC_FAST, true>, PL_SMEM_BYTES);
+    rc = rc ? rc : set_smem(m2l_r2_kernel<PREC_FAST, false>, PL_SMEM_BYTES);
     rc = rc ? rc : set_smem(p2p_r2_kernel<PREC_EXACT>, R2_SMEM_BYTES);
     rc = rc ? rc : set_smem(p2p_r2_kernel<PREC_FAST>, R2_SMEM_BYTES);
     rc = rc ? rc : set_smem(p2m_fast_kernel<true>, 7 * 8 * 6 * NCELL);
@@ -353,6 +354,22 @@ int otfmm_create(int device, double theta, otfmm_context** out) {
         return fail(OTFMM_ERR_UNSUPPORTED, "stencil longer than the compiled maximum");
     }
     ctx->reach = reach;
+    // plane delta of every long-list entry (reach-2 plane layout of m2l_r2_kernel)
+    // and where each sx starts in a class's list (the lists are sorted by sx)
+    std::vector<int> r2_sx_start(8 * 12, 0);
+    for (int p = 0; p < 8; ++p) {
+        const int py = (p >> 1) & 1, pz = p & 1;
+        int sx_prev = -SMAX;
+        r2_sx_start[p * 12] = 0;
+        for (int e = 0; e < ctx->counts[p]; ++e) {
+            int2& en = entries_r2[p * (size_t)MAX_ENTRIES_R2 + e];
+            const int sx = (en.y & 15) - 8, sy = ((en.y >> 4) & 15) - 8, sz = ((en.y >> 8) & 15) - 8;
+            const int cls = (((py + sy) & 1) << 1) | ((pz + sz) & 1);
+            en.x = cls * PL_CLS + ((py + sy + 4) >> 1) * PL_RS + ((pz + sz + 4) >> 1);
+            while (sx_prev < sx) r2_sx_start[p * 12 + (++sx_prev) + SMAX] = e;
+        }
+        while (sx_prev < SMAX + 1) r2_sx_start[p * 12 + (++sx_prev) + SMAX] = ctx->counts[p];
+    }
     if (reach <= 1) {
         build_entries(ctx->st, theta, MAX_ENTRIES, entries, ctx->counts, reach);
     } else {
@@ -441,7 +458,10 @@ int otfmm_create(int device, double theta, otfmm_context** out) {
     ctx->p2m_groups_max = (int)p2m_perm.size();
     DeviceGuard g(device);
     cudaError_t e;
-    if ((e = cudaMalloc(&ctx->d_entries_r2, sizeof(int2) * entries_r2.size())) != cudaSuccess ||
+    if ((e = cudaMalloc(&ctx->d_r2_sx_start, sizeof(int) * r2_sx_start.size())) != cudaSuccess ||
+        (e = cudaMemcpy(ctx->d_r2_sx_start, r2_sx_start.data(), sizeof(int) * r2_sx_start.size(),
+                        cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMalloc(&ctx->d_entries_r2, sizeof(int2) * entries_r2.size())) != cudaSuccess ||
         (e = cudaMemcpy(ctx->d_entries_r2, entries_r2.data(), sizeof(int2) * entries_r2.size(),
                         cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMalloc(&ctx->d_p2m_slot, sizeof(int16_t) * p2m_slot.size())) != cudaSuccess ||
@@ -517,6 +537,7 @@ int otfmm_destroy(otfmm_context* ctx) {
     cudaFree(ctx->d_p2p_four);
     cudaFree(ctx->d_p2m_slot);
     cudaFree(ctx->d_entries_r2);
+    cudaFree(ctx->d_r2_sx_start);
     {
         auto& hp = ctx->hp;
         if (hp.ready) {
@@ -796,7 +817,7 @@ int enqueue_batch(otfmm_context* ctx, const double* pool_M, const double* pool_c
     const dim3 tiles_grid(sms), p2p_grid(P2P_CTAS_PER_SM * sms), p2m_grid(std::min(n_items, 8 * sms));
     if (ctx->reach > 1) {
         // theta < 0.5: partners from global memory; the split precision runs the fast FP64 form
-        const size_t rbytes = ROOT_SMEM_DOUBLES * sizeof(double);
+        const size_t rbytes = PL_SMEM_BYTES;
         const dim3 leaf_grid(std::min(n_items, 8 * sms));
         if (precision == OTFMM_FP64_EXACT) {
             if (rho) m2l_r2_kernel<PREC_EXACT, true><<<4 * sms, THREADS, rbytes, s>>>(a);

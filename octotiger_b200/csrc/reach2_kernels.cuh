@@ -1,10 +1,9 @@
 // Kernels for opening angles below 0.5 (coarse reach 2: partners up to five
 // cells away, theta >= 0.34). The halo of a tile no longer fits in shared
-// memory, so partners are read from global memory (L1/L2) in the reference's
-// stencil order:
-//   * m2l_r2_kernel: multipole tiles of refined items from the resident pool,
-//     each partner resolved the way update_input stages it
-//     (multipole_interaction_interface.hpp:88-281);
+// memory as a whole; partners are staged plane by plane or read from the
+// buffers, in the reference's stencil order:
+//   * m2l_r2_kernel: multipole tiles of refined items, partner x-planes
+//     staged one by one in shared memory;
 //   * p2p_r2_kernel: P2P of leaves from the pool;
 //   * soa_m2l_r2_kernel: the per-subgrid entry point on the reference's 18^3
 //     SoA buffers.
@@ -26,8 +25,21 @@ namespace otfmm {
 
 // Multipole tiles (half a subgrid, 256 threads; warp = parity class) of
 // refined and root items, persistent over the same tile counter as
-// m2l_batch_kernel. Root tiles stage their own cells in shared memory
+// m2l_batch_kernel. A tile's partners lie in the 12 x-planes x0-4 .. x0+7 of
+// 16 x 16 cells (y, z in -4 .. 11); the planes are staged one after the other
+// in shared memory (what update_input stages at those positions:
+// multipole_interaction_interface.hpp:88-281) and every target cell walks the
+// entries of its parity class with sx = plane - cx. Increasing planes mean
+// increasing sx, and the entries of one sx are in stencil order, so each cell
+// accumulates in the reference's order. Root tiles stage their own cells
 // (reach-independent root stencil).
+constexpr int PL_RS = 12;                     // z' row: 8 cells + 4 pad (half-warps conflict-free)
+constexpr int PL_COMP = 8 * PL_RS;            // one component of one (y, z) parity class
+constexpr int PL_CLS = NCOMP * PL_COMP;       // 2208 doubles
+constexpr int PL_DOUBLES = 4 * PL_CLS;        // 8832 doubles = 70,656 bytes
+constexpr int PL_SMEM_BYTES = (ROOT_SMEM_DOUBLES > PL_DOUBLES ? ROOT_SMEM_DOUBLES : PL_DOUBLES) * 8;
+static_assert(PL_RS % 16 == 12, "plane rows keep (j, k) half-warps conflict-free");
+
 template <int PREC, bool RHO>
 __global__ void __launch_bounds__(THREADS, 1) m2l_r2_kernel(BatchArgs a) {
     extern __shared__ double sm[];
@@ -52,64 +64,99 @@ __global__ void __launch_bounds__(THREADS, 1) m2l_r2_kernel(BatchArgs a) {
                                                  : a.com[(sub * 3 + (q - 20)) * NCELL + r];
             __syncthreads();
             root_tile<PREC, RHO>(sm, x0, a.t, out);
-        } else {
-            const CellMap c = cell_map(x0);
-            const int cu = c.cx * 64 + c.cy * 8 + c.cz;
-            double X[3], mc[20], acc[20], corr[3] = {0.0, 0.0, 0.0};
+            __syncthreads();   // shared memory and `it` are reused by the next tile
+            continue;
+        }
+        uint32_t monomask = 0;   // leaf neighbours, by raw direction
+        for (int d = 0; d < 26; ++d) {
+            const int nb = it.nb[d];
+            if (nb >= 0 && a.is_leaf[nb]) monomask |= 1u << (d < 13 ? d : d + 1);
+        }
+        const CellMap c = cell_map(x0);
+        const int cu = c.cx * 64 + c.cy * 8 + c.cz;
+        const int lane_off = c.j * PL_RS + c.k;
+        double X[3], mc[20], acc[20], corr[3] = {0.0, 0.0, 0.0};
 #pragma unroll
-            for (int q = 0; q < 3; ++q) X[q] = a.com[(sub * 3 + q) * NCELL + cu];
+        for (int q = 0; q < 3; ++q) X[q] = a.com[(sub * 3 + q) * NCELL + cu];
 #pragma unroll
-            for (int q = 0; q < 20; ++q) {
-                mc[q] = a.M[(sub * 20 + q) * NCELL + cu] * stage_scale<PREC>(q);
-                acc[q] = 0.0;
-            }
-            const double inv_m0 = 1.0 / mc[0];
-            const int n = a.t.count[c.p];
-            const int2* ent = a.t.entries_r2 + c.p * MAX_ENTRIES_R2;
-#pragma unroll 1
-            for (int e = 0; e < n; ++e) {
-                const int y = __ldg(&ent[e].y);
-                const bool far = (entry_flags(y) & F_FAR) != 0;
-                const int ax = c.cx + entry_sx(y), ay = c.cy + entry_sy(y), az = c.cz + entry_sz(y);
+        for (int q = 0; q < 20; ++q) {
+            mc[q] = a.M[(sub * 20 + q) * NCELL + cu] * stage_scale<PREC>(q);
+            acc[q] = 0.0;
+        }
+        const double inv_m0 = 1.0 / mc[0];
+        const int2* ent = a.t.entries_r2 + c.p * MAX_ENTRIES_R2;
+        const int* sxs = a.t.r2_sx_start + c.p * 12;
+        for (int plane = x0 - 4; plane <= x0 + 7; ++plane) {
+            __syncthreads();   // the previous plane is consumed
+            {
+                // stage plane `plane`: one cell per thread
+                const int r = threadIdx.x;
+                const int ax = plane, ay = (r >> 4) - 4, az = (r & 15) - 4;
                 const int raw = raw_dir(ax, ay, az);
                 const int src = (raw == 13) ? it.subgrid : it.nb[raw < 13 ? raw : raw - 1];
-                const bool leaf = src >= 0 && raw != 13 && a.is_leaf[src];
-                // monopole-only offsets: only leaf partners carry mass (the staged
-                // mon is zero for multipole and empty cells)
-                if (!far && !leaf) continue;
                 const int u = (ax & 7) * 64 + (ay & 7) * 8 + (az & 7);
-                double Y[3], mp[20];
+                double v[NCOMP];
                 if (src < 0) {
-                    // empty direction: zero moments at the origin, as staged
 #pragma unroll
-                    for (int q = 0; q < 3; ++q) Y[q] = 0.0;
+                    for (int q = 0; q < NCOMP; ++q) v[q] = 0.0;
+                } else if (raw != 13 && a.is_leaf[src]) {
+                    v[0] = a.mon[(size_t)src * NCELL + u];
 #pragma unroll
-                    for (int q = 0; q < 20; ++q) mp[q] = 0.0;
-                } else if (leaf) {
+                    for (int q = 1; q < 20; ++q) v[q] = 0.0;
                     const int ip[3] = {ax + INX, ay + INX, az + INX};
 #pragma unroll
                     for (int q = 0; q < 3; ++q)
-                        Y[q] = __dsub_rn(__dadd_rn(__dmul_rn((double)ip[q], it.dx), it.xbase[q]),
-                                         __dmul_rn((double)INX, it.dx));
-                    mp[0] = __ldg(a.mon + (size_t)src * NCELL + u);
-#pragma unroll
-                    for (int q = 1; q < 20; ++q) mp[q] = 0.0;
+                        v[20 + q] = __dsub_rn(__dadd_rn(__dmul_rn((double)ip[q], it.dx), it.xbase[q]),
+                                              __dmul_rn((double)INX, it.dx));
                 } else {
 #pragma unroll
-                    for (int q = 0; q < 3; ++q) Y[q] = __ldg(a.com + ((size_t)src * 3 + q) * NCELL + u);
+                    for (int q = 0; q < 20; ++q) v[q] = a.M[((size_t)src * 20 + q) * NCELL + u] * stage_scale<PREC>(q);
 #pragma unroll
-                    for (int q = 0; q < 20; ++q)
-                        mp[q] = __ldg(a.M + ((size_t)src * 20 + q) * NCELL + u) * stage_scale<PREC>(q);
+                    for (int q = 0; q < 3; ++q) v[20 + q] = a.com[((size_t)src * 3 + q) * NCELL + u];
                 }
-                if (PREC == PREC_EXACT)
-                    exact_m2l_pair<RHO>(X, Y, mp, mc, acc, corr);
-                else
-                    fast_m2l_pair<RHO>(X, Y, mp, mc + 10, inv_m0, acc, corr);
-            }
+                const int base = (((ay & 1) << 1) | (az & 1)) * PL_CLS + ((ay + 4) >> 1) * PL_RS + ((az + 4) >> 1);
 #pragma unroll
-            for (int q = 0; q < 20; ++q) out.L[q * out.stride + cu] = acc[q];
-            write_lc<RHO>(out, cu, corr);
+                for (int q = 0; q < NCOMP; ++q) sm[base + q * PL_COMP] = v[q];
+            }
+            __syncthreads();
+            const int sx = plane - c.cx;
+            if (sx < -SMAX || sx > SMAX) continue;
+            const int e1 = sxs[sx + SMAX + 1];
+#pragma unroll 1
+            for (int e = sxs[sx + SMAX]; e < e1; ++e) {
+                const int2 en = __ldg(ent + e);
+                const int pb = en.x + lane_off;
+                double Y[3];
+#pragma unroll
+                for (int q = 0; q < 3; ++q) Y[q] = sm[pb + (20 + q) * PL_COMP];
+                if (entry_flags(en.y) & F_FAR) {
+                    double mp[20];
+#pragma unroll
+                    for (int q = 0; q < 20; ++q) mp[q] = sm[pb + q * PL_COMP];
+                    if (PREC == PREC_EXACT)
+                        exact_m2l_pair<RHO>(X, Y, mp, mc, acc, corr);
+                    else
+                        fast_m2l_pair<RHO>(X, Y, mp, mc + 10, inv_m0, acc, corr);
+                } else {
+                    // monopole-only offsets: only leaf partners carry mass
+                    const int ay = c.cy + entry_sy(en.y), az = c.cz + entry_sz(en.y);
+                    if (!((monomask >> raw_dir(plane, ay, az)) & 1u)) continue;
+                    const double m0 = sm[pb];
+                    if (PREC == PREC_EXACT) {
+                        double mp[20];
+                        mp[0] = m0;
+#pragma unroll
+                        for (int q = 1; q < 20; ++q) mp[q] = 0.0;
+                        exact_m2l_pair<RHO>(X, Y, mp, mc, acc, corr);
+                    } else {
+                        fast_m2l_mass_pair<RHO>(X, Y, m0, mc + 10, inv_m0, acc, corr);
+                    }
+                }
+            }
         }
+#pragma unroll
+        for (int q = 0; q < 20; ++q) out.L[q * out.stride + cu] = acc[q];
+        write_lc<RHO>(out, cu, corr);
         __syncthreads();   // shared memory and `it` are reused by the next tile
     }
 }
