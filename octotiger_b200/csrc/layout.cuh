@@ -105,6 +105,7 @@ struct Tables {
     const int2* entries_r2;     // [8][MAX_ENTRIES_R2]: stencil-order entries of any reach (x = plane delta,
                                 // y = packed)
     const int* r2_sx_start;     // [8][12]: first entry of each sx = -5 .. 5 in entries_r2 (and the end)
+    const double4* r2_four;     // [8][MAX_ENTRIES_R2]: monopole constants of the entries_r2 offsets
 };
 
 __device__ __forceinline__ int entry_sx(int y) { return (y & 15) - 8; }

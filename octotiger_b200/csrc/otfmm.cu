@@ -218,6 +218,7 @@ struct otfmm_context {
     int16_t* d_p2m_slot = nullptr;
     int2* d_entries_r2 = nullptr;   // stencil-order entries, MAX_ENTRIES_R2 per class (any reach)
     int* d_r2_sx_start = nullptr;
+    double4* d_r2_four = nullptr;
     int p2m_groups_max = 0;   // cells with partners summed over the 26 directions
     double4* d_p2p_four = nullptr;
     int counts_far[8] = {};
@@ -244,7 +245,7 @@ struct otfmm_context {
     std::mutex mu;
     Tables tables() const { return Tables{d_entries,    d_count, d_entries_fast, d_count_far, d_entries_split, d_entries_p2p,
                       d_entries_ws, d_four,  d_phase,        d_p2m_start,     d_p2m_list,    d_p2m_perm_start,
-                      d_p2m_perm,   d_p2m_slot,     d_p2p_four,      d_entries_r2,  d_r2_sx_start}; }
+                      d_p2m_perm,   d_p2m_slot,     d_p2p_four,      d_entries_r2,  d_r2_sx_start, d_r2_four}; }
 };
 
 namespace {
@@ -357,6 +358,7 @@ int otfmm_create(int device, double theta, otfmm_context** out) {
     // plane delta of every long-list entry (reach-2 plane layout of m2l_r2_kernel)
     // and where each sx starts in a class's list (the lists are sorted by sx)
     std::vector<int> r2_sx_start(8 * 12, 0);
+    std::vector<double4> r2_four(8 * (size_t)MAX_ENTRIES_R2, double4{0.0, 0.0, 0.0, 0.0});
     for (int p = 0; p < 8; ++p) {
         const int py = (p >> 1) & 1, pz = p & 1;
         int sx_prev = -SMAX;
@@ -367,6 +369,8 @@ int otfmm_create(int device, double theta, otfmm_context** out) {
             const int cls = (((py + sy) & 1) << 1) | ((pz + sz) & 1);
             en.x = cls * PL_CLS + ((py + sy + 4) >> 1) * PL_RS + ((pz + sz + 4) >> 1);
             while (sx_prev < sx) r2_sx_start[p * 12 + (++sx_prev) + SMAX] = e;
+            const double* f = ctx->st.four[(en.y >> 16) & 2047];
+            r2_four[p * (size_t)MAX_ENTRIES_R2 + e] = double4{f[0], f[1], f[2], f[3]};
         }
         while (sx_prev < SMAX + 1) r2_sx_start[p * 12 + (++sx_prev) + SMAX] = ctx->counts[p];
     }
@@ -458,7 +462,10 @@ int otfmm_create(int device, double theta, otfmm_context** out) {
     ctx->p2m_groups_max = (int)p2m_perm.size();
     DeviceGuard g(device);
     cudaError_t e;
-    if ((e = cudaMalloc(&ctx->d_r2_sx_start, sizeof(int) * r2_sx_start.size())) != cudaSuccess ||
+    if ((e = cudaMalloc(&ctx->d_r2_four, sizeof(double4) * r2_four.size())) != cudaSuccess ||
+        (e = cudaMemcpy(ctx->d_r2_four, r2_four.data(), sizeof(double4) * r2_four.size(),
+                        cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMalloc(&ctx->d_r2_sx_start, sizeof(int) * r2_sx_start.size())) != cudaSuccess ||
         (e = cudaMemcpy(ctx->d_r2_sx_start, r2_sx_start.data(), sizeof(int) * r2_sx_start.size(),
                         cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMalloc(&ctx->d_entries_r2, sizeof(int2) * entries_r2.size())) != cudaSuccess ||
@@ -538,6 +545,7 @@ int otfmm_destroy(otfmm_context* ctx) {
     cudaFree(ctx->d_p2m_slot);
     cudaFree(ctx->d_entries_r2);
     cudaFree(ctx->d_r2_sx_start);
+    cudaFree(ctx->d_r2_four);
     {
         auto& hp = ctx->hp;
         if (hp.ready) {
@@ -823,7 +831,7 @@ int enqueue_batch(otfmm_context* ctx, const double* pool_M, const double* pool_c
             if (rho) m2l_r2_kernel<PREC_EXACT, true><<<4 * sms, THREADS, rbytes, s>>>(a);
             else m2l_r2_kernel<PREC_EXACT, false><<<4 * sms, THREADS, rbytes, s>>>(a);
             mark(2);
-            p2p_r2_kernel<PREC_EXACT><<<leaf_grid, P_THREADS, R2_SMEM_BYTES, s>>>(a);
+            p2p_r2_kernel<PREC_EXACT><<<leaf_grid, 256, R2_SMEM_BYTES, s>>>(a);
             mark(3);
             if (rho) p2m_batch_kernel<PREC_EXACT, true><<<p2m_grid, P_THREADS, 0, s>>>(a);
             else p2m_batch_kernel<PREC_EXACT, false><<<p2m_grid, P_THREADS, 0, s>>>(a);
@@ -831,7 +839,7 @@ int enqueue_batch(otfmm_context* ctx, const double* pool_M, const double* pool_c
             if (rho) m2l_r2_kernel<PREC_FAST, true><<<4 * sms, THREADS, rbytes, s>>>(a);
             else m2l_r2_kernel<PREC_FAST, false><<<4 * sms, THREADS, rbytes, s>>>(a);
             mark(2);
-            p2p_r2_kernel<PREC_FAST><<<leaf_grid, P_THREADS, R2_SMEM_BYTES, s>>>(a);
+            p2p_r2_kernel<PREC_FAST><<<leaf_grid, 256, R2_SMEM_BYTES, s>>>(a);
             mark(3);
             if (rho) p2m_batch_kernel<PREC_FAST, true><<<p2m_grid, P_THREADS, 0, s>>>(a);
             else p2m_batch_kernel<PREC_FAST, false><<<p2m_grid, P_THREADS, 0, s>>>(a);

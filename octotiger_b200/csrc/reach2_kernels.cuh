@@ -164,25 +164,28 @@ __global__ void __launch_bounds__(THREADS, 1) m2l_r2_kernel(BatchArgs a) {
 // P2P of leaves: one CTA (512 threads) per leaf, grid stride. The leaf's
 // 18^3 mass halo (padding 5) is staged in shared memory first, refined and
 // empty neighbours as zero mass (monopole update_input,
-// monopole_interaction_interface.hpp:64-143); warp w then serves half of
-// parity class w >> 1 (32 of its 64 cells), so the warp walks one entry list
-// and reads one constant per entry.
+// monopole_interaction_interface.hpp:64-143); warp w then serves parity class
+// w (two cells per thread), so the warp walks one entry list and every entry's
+// constants serve two pairs.
 constexpr int R2_PAD = SMAX;                  // halo width
 constexpr int R2_REG = INX + 2 * R2_PAD;      // 18
 constexpr int R2_ROW = R2_REG + 1;            // z rows padded to 19 doubles
 constexpr int R2_PLANE = R2_REG * R2_ROW;
 constexpr int R2_SMEM_BYTES = R2_REG * R2_PLANE * 8;   // 49,248 bytes
 template <int PREC>
-__global__ void __launch_bounds__(P_THREADS) p2p_r2_kernel(BatchArgs a) {
+__global__ void __launch_bounds__(256) p2p_r2_kernel(BatchArgs a) {
     extern __shared__ double pm[];
     __shared__ ItemInfo it;
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int p = w >> 1, q = lane + 32 * (w & 1);
-    const int cx = ((p >> 2) & 1) + 2 * (q >> 4), cy = ((p >> 1) & 1) + 2 * ((q >> 2) & 3), cz = (p & 1) + 2 * (q & 3);
-    const int cu = cx * 64 + cy * 8 + cz;
-    const int own = (cx + R2_PAD) * R2_PLANE + (cy + R2_PAD) * R2_ROW + (cz + R2_PAD);
+    // warp = parity class, two cells per thread (sub-lattice x' = i and i + 2)
+    const int p = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i = lane >> 4, j = (lane >> 2) & 3, k = lane & 3;
+    const int cy = ((p >> 1) & 1) + 2 * j, cz = (p & 1) + 2 * k;
+    const int cxa = ((p >> 2) & 1) + 2 * i, cxb = cxa + 4;
+    const int own_a = (cxa + R2_PAD) * R2_PLANE + (cy + R2_PAD) * R2_ROW + (cz + R2_PAD);
+    constexpr int OFF_B = 4 * R2_PLANE;
     const int n = a.t.count[p];
     const int2* ent = a.t.entries_r2 + p * MAX_ENTRIES_R2;
+    const double4* four = a.t.r2_four + p * MAX_ENTRIES_R2;
     const int nleaf = a.wl.counts[WL_LEAF];
     for (int kk = blockIdx.x; kk < nleaf; kk += gridDim.x) {
         __syncthreads();   // `it` and the halo are reused
@@ -199,30 +202,48 @@ __global__ void __launch_bounds__(P_THREADS) p2p_r2_kernel(BatchArgs a) {
         }
         __syncthreads();
         const double dc0 = __ddiv_rn(1.0, it.dx), dc1 = __ddiv_rn(-1.0, it.dx);
-        double acc[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll 4
+        double ga[4] = {0.0, 0.0, 0.0, 0.0}, gb[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 2
         for (int e = 0; e < n; ++e) {
             const int y = __ldg(&ent[e].y);
-            const double m = pm[own + entry_sx(y) * R2_PLANE + entry_sy(y) * R2_ROW + entry_sz(y)];
-            const double* four = c_four[entry_sidx(y)];
+            const double4 f = four[e];
+            const int d = own_a + entry_sx(y) * R2_PLANE + entry_sy(y) * R2_ROW + entry_sz(y);
+            const double ma = pm[d], mb = pm[d + OFF_B];
             if (PREC == PREC_EXACT) {
-                const double ms = __dmul_rn(m, dc0);
-                acc[0] = __dadd_rn(acc[0], __dmul_rn(four[0], ms));
-#pragma unroll
-                for (int c = 1; c < 4; ++c) acc[c] = __dadd_rn(acc[c], __dmul_rn(__dmul_rn(four[c], ms), dc1));
+                const double sa = __dmul_rn(ma, dc0), sb = __dmul_rn(mb, dc0);
+                ga[0] = __dadd_rn(ga[0], __dmul_rn(f.x, sa));
+                ga[1] = __dadd_rn(ga[1], __dmul_rn(__dmul_rn(f.y, sa), dc1));
+                ga[2] = __dadd_rn(ga[2], __dmul_rn(__dmul_rn(f.z, sa), dc1));
+                ga[3] = __dadd_rn(ga[3], __dmul_rn(__dmul_rn(f.w, sa), dc1));
+                gb[0] = __dadd_rn(gb[0], __dmul_rn(f.x, sb));
+                gb[1] = __dadd_rn(gb[1], __dmul_rn(__dmul_rn(f.y, sb), dc1));
+                gb[2] = __dadd_rn(gb[2], __dmul_rn(__dmul_rn(f.z, sb), dc1));
+                gb[3] = __dadd_rn(gb[3], __dmul_rn(__dmul_rn(f.w, sb), dc1));
             } else {
-                const double ms = m * dc0;
-                acc[0] = fma(four[0], ms, acc[0]);
-#pragma unroll
-                for (int c = 1; c < 4; ++c) acc[c] = fma(four[c], ms, acc[c]);
+                const double sa = ma * dc0, sb = mb * dc0;
+                ga[0] = fma(f.x, sa, ga[0]);
+                ga[1] = fma(f.y, sa, ga[1]);
+                ga[2] = fma(f.z, sa, ga[2]);
+                ga[3] = fma(f.w, sa, ga[3]);
+                gb[0] = fma(f.x, sb, gb[0]);
+                gb[1] = fma(f.y, sb, gb[1]);
+                gb[2] = fma(f.z, sb, gb[2]);
+                gb[3] = fma(f.w, sb, gb[3]);
             }
         }
         if (PREC != PREC_EXACT)
 #pragma unroll
-            for (int c = 1; c < 4; ++c) acc[c] *= dc1;
+            for (int c = 1; c < 4; ++c) {
+                ga[c] *= dc1;
+                gb[c] *= dc1;
+            }
         double* L = a.L + (size_t)it.subgrid * 20 * NCELL;
+        const int cfa = cxa * 64 + cy * 8 + cz, cfb = cxb * 64 + cy * 8 + cz;
 #pragma unroll
-        for (int c = 0; c < 4; ++c) L[c * NCELL + cu] = acc[c];
+        for (int c = 0; c < 4; ++c) {
+            L[c * NCELL + cfa] = ga[c];
+            L[c * NCELL + cfb] = gb[c];
+        }
     }
 }
 
