@@ -50,10 +50,12 @@ PROFILED_TRAFFIC = {("uniform_level3", "fp32_split"): 61.0e6, ("uniform_level3",
                     ("amr_polytrope_l6", "fp32_split"): 78.6e6, ("amr_polytrope_l6", "fp64"): 77.4e6}
 
 
-WORKLOADS = ("uniform_level3", "amr_polytrope", "amr_binary")
+WORKLOADS = ("uniform_level3", "amr_polytrope", "amr_binary", "single_subgrid")
 
 
 def make_workload(name: str, theta: float = 0.5):
+    if name == "single_subgrid":
+        return syn.single_subgrid(theta=theta)
     if name == "uniform_level3":
         return syn.uniform_level(3, theta=theta)
     from octotiger_b200 import amr
