@@ -15,8 +15,15 @@
 // (octotiger/multipole_interactions/legacy/multipole_interaction_interface.hpp:88-281,
 //  octotiger/monopole_interactions/legacy/monopole_interaction_interface.hpp:64-143,
 //  octotiger/monopole_interactions/legacy/p2m_interaction_interface.hpp:102-160).
-// Neighbour payloads must be full size (512 cells); the compressed
-// ilist_n_bnd payloads of remote neighbours are expanded by the caller.
+// Neighbour payloads are full size (512 cells) or compressed the way
+// grid::get_gravity_boundary packs remote neighbours (src/grid_fmm.cpp:1805-1850):
+// element k of the payload is the neighbour's cell grid->get_ilist_n_bnd(dir)[k].second.
+// The overloads that take the grid (the reference's own argument lists) expand
+// compressed payloads as update_input does: the direction's halo band is reset
+// (zeros; leaf neighbours in the multipole staging keep their cell-centre
+// COMs), then the listed cells are filled. Without a grid a compressed payload
+// is an error (OTFMM_ERR_INVALID), as is a listed cell outside the halo band or
+// a list longer than its payload.
 //
 // Template parameters are Octo-Tiger's own types (multipole = taylor<4>,
 // expansion = taylor<4>, space_vector, neighbor_gravity_type with
@@ -28,11 +35,14 @@
 // misconfiguration (multipole_kernel_interface.cpp:107-158).
 #pragma once
 
+#include <algorithm>
 #include <array>
+#include <cstddef>
 #include <cstdio>
 #include <cstdlib>
 #include <iostream>
 #include <memory>
+#include <type_traits>
 #include <vector>
 
 #include "otfmm.h"
@@ -65,6 +75,39 @@ inline void padding_range(const int o[3], int s[3], int e[3], int p[3]) {
     }
 }
 
+inline bool in_band(const int o[3], int x, int y, int z) {
+    int s[3], e[3], p[3];
+    padding_range(o, s, e, p);
+    return x >= s[0] && x < e[0] && y >= s[1] && y < e[1] && z >= s[2] && z < e[2];
+}
+
+// Walks the cells of direction d's compressed payload of `payload_size`
+// elements: put(k, x, y, z) for payload element k and neighbour-local cell
+// (x, y, z) (flat_index_to_multiindex_not_padded, multiindex.hpp:82-91).
+// GridPtr is a pointer-like to Octo-Tiger's grid, or std::nullptr_t where the
+// caller has none.
+template <class GridPtr, class F>
+int expand_compressed(const GridPtr& grid, int d, size_t payload_size, F&& put) {
+    if constexpr (std::is_same_v<GridPtr, std::nullptr_t>) {
+        (void)grid, (void)d, (void)payload_size, (void)put;
+        return OTFMM_ERR_INVALID;
+    } else {
+        if (!grid) return OTFMM_ERR_INVALID;
+        int o[3];
+        dir_offsets(d, o);
+        size_t k = 0;
+        for (const auto& cell : grid->get_ilist_n_bnd(d)) {
+            const int u = static_cast<int>(cell.second);
+            if (k >= payload_size || u < 0 || u >= NCELL) return OTFMM_ERR_INVALID;
+            const int x = u / (INX * INX), y = (u / INX) % INX, z = u % INX;
+            if (!in_band(o, x, y, z)) return OTFMM_ERR_INVALID;
+            put(k, x, y, z);
+            ++k;
+        }
+        return OTFMM_OK;
+    }
+}
+
 // Host and device staging of one subgrid, reused across calls of a thread
 // (the reference recycles its buffers through CPPuddle).
 struct Staging {
@@ -76,10 +119,10 @@ inline Staging& thread_staging() {
     return s;
 }
 
-template <class Multipole, class SpaceVector, class Neighbor>
-void stage_multipole_input(const std::vector<Multipole>& M_ptr, const SpaceVector* com0,
-                           const std::vector<Neighbor>& neighbors, double dx, const std::array<double, 3>& xbase,
-                           bool is_root, Staging& st) {
+template <class Multipole, class SpaceVector, class Neighbor, class GridPtr = std::nullptr_t>
+int stage_multipole_input(const std::vector<Multipole>& M_ptr, const SpaceVector* com0,
+                          const std::vector<Neighbor>& neighbors, double dx, const std::array<double, 3>& xbase,
+                          bool is_root, Staging& st, const GridPtr& grid = nullptr) {
     std::fill(st.mon.begin(), st.mon.end(), 0.0);
     std::fill(st.M.begin(), st.M.end(), 0.0);
     std::fill(st.com.begin(), st.com.end(), 0.0);
@@ -90,19 +133,22 @@ void stage_multipole_input(const std::vector<Multipole>& M_ptr, const SpaceVecto
                 for (int c = 0; c < 20; ++c) st.M[c * CL + f] = M_ptr[u][c];
                 for (int c = 0; c < 3; ++c) st.com[c * CL + f] = com0[u][c];
             }
-    if (is_root) return;
+    if (is_root) return OTFMM_OK;
     for (int d = 0; d < 26; ++d) {
         const Neighbor& nb = neighbors[d];
         int o[3], s[3], e[3], p[3];
         dir_offsets(d, o);
         padding_range(o, s, e, p);
+        const bool full = nb.is_monopole ? (nb.data.m && nb.data.m->size() == NCELL)
+                                         : (nb.data.M && nb.data.M->size() == NCELL && nb.data.x &&
+                                            nb.data.x->size() == NCELL);
         for (int x = s[0]; x < e[0]; ++x)
             for (int y = s[1]; y < e[1]; ++y)
                 for (int z = s[2]; z < e[2]; ++z) {
                     const int ix = x + p[0], iy = y + p[1], iz = z + p[2];
                     const int f = flat_padded(ix, iy, iz), u = flat_inner(x, y, z);
                     if (!nb.is_monopole) {
-                        if (!nb.data.M) continue;   // empty direction: zeros
+                        if (!full) continue;   // empty direction or compressed payload: zeros first
                         for (int c = 0; c < 20; ++c) st.M[c * CL + f] = (*nb.data.M)[u][c];
                         for (int c = 0; c < 3; ++c) st.com[c * CL + f] = (*nb.data.x)[u][c];
                     } else {
@@ -110,16 +156,125 @@ void stage_multipole_input(const std::vector<Multipole>& M_ptr, const SpaceVecto
                         st.com[0 * CL + f] = ix * dx + xbase[0] - INX * dx;
                         st.com[1 * CL + f] = iy * dx + xbase[1] - INX * dx;
                         st.com[2 * CL + f] = iz * dx + xbase[2] - INX * dx;
-                        st.mon[f] = (*nb.data.m)[u];
+                        if (full) st.mon[f] = (*nb.data.m)[u];
                     }
                 }
+        if (full || (nb.is_monopole ? !nb.data.m : !nb.data.M)) continue;
+        int rc;
+        if (nb.is_monopole) {
+            const auto& m = *nb.data.m;
+            rc = expand_compressed(grid, d, m.size(), [&](size_t k, int x, int y, int z) {
+                st.mon[flat_padded(x + p[0], y + p[1], z + p[2])] = m[k];
+            });
+        } else {
+            const auto& nM = *nb.data.M;
+            const size_t n = nb.data.x ? std::min(nM.size(), nb.data.x->size()) : 0;
+            rc = expand_compressed(grid, d, n, [&](size_t k, int x, int y, int z) {
+                const int f = flat_padded(x + p[0], y + p[1], z + p[2]);
+                for (int c = 0; c < 20; ++c) st.M[c * CL + f] = nM[k][c];
+                for (int c = 0; c < 3; ++c) st.com[c * CL + f] = (*nb.data.x)[k][c];
+            });
+        }
+        if (rc != OTFMM_OK) return rc;
     }
+    return OTFMM_OK;
+}
+
+// monopole update_input (monopole_interaction_interface.hpp:64-143): the 18^3
+// mass buffer `mon` (ENTRIES) gets the own masses, leaf neighbours' masses and
+// zeros elsewhere.
+template <class Neighbor, class GridPtr = std::nullptr_t>
+int stage_monopole_input(const std::vector<double>& monopoles, const std::vector<Neighbor>& neighbors, double* mon,
+                         const GridPtr& grid = nullptr) {
+    std::fill(mon, mon + ENTRIES, 0.0);
+    for (int x = 0; x < INX; ++x)
+        for (int y = 0; y < INX; ++y)
+            for (int z = 0; z < INX; ++z) mon[flat_padded(x + INX, y + INX, z + INX)] = monopoles[flat_inner(x, y, z)];
+    for (int d = 0; d < 26; ++d) {
+        const Neighbor& nb = neighbors[d];
+        if (!nb.is_monopole || !nb.data.m) continue;
+        int o[3], s[3], e[3], p[3];
+        dir_offsets(d, o);
+        padding_range(o, s, e, p);
+        const auto& m = *nb.data.m;
+        if (m.size() == NCELL) {
+            for (int x = s[0]; x < e[0]; ++x)
+                for (int y = s[1]; y < e[1]; ++y)
+                    for (int z = s[2]; z < e[2]; ++z)
+                        mon[flat_padded(x + p[0], y + p[1], z + p[2])] = m[flat_inner(x, y, z)];
+        } else {
+            const int rc = expand_compressed(grid, d, m.size(), [&](size_t k, int x, int y, int z) {
+                mon[flat_padded(x + p[0], y + p[1], z + p[2])] = m[k];
+            });
+            if (rc != OTFMM_OK) return rc;
+        }
+    }
+    return OTFMM_OK;
+}
+
+// update_neighbor_input (p2m_interaction_interface.hpp:102-160): refined
+// neighbour d's slab of 8x8x5, 8x5x5 or 5x5x5 cells in its own SoA layout,
+// component stride *stride (cells + 19); nM / ncom hold 20 x 419 / 3 x 419.
+template <class Neighbor, class GridPtr = std::nullptr_t>
+int stage_p2m_slab(const Neighbor& nb, int d, double* nM, double* ncom, int* stride,
+                   const GridPtr& grid = nullptr) {
+    int o[3], s[3], e[3], sz[3];
+    dir_offsets(d, o);
+    for (int a = 0; a < 3; ++a) {
+        s[a] = (o[a] == -1) ? INX - SMAX : 0;
+        e[a] = (o[a] == 1) ? SMAX : INX;
+        sz[a] = e[a] - s[a];
+    }
+    const int st = sz[0] * sz[1] * sz[2] + 19;
+    *stride = st;
+    const auto& M = *nb.data.M;
+    const size_t n_x = nb.data.x ? nb.data.x->size() : 0;
+    std::fill(nM, nM + 20 * st, 0.0);
+    std::fill(ncom, ncom + 3 * st, 0.0);
+    if (M.size() == NCELL && n_x == NCELL) {
+        for (int x = s[0]; x < e[0]; ++x)
+            for (int y = s[1]; y < e[1]; ++y)
+                for (int z = s[2]; z < e[2]; ++z) {
+                    const int f = (x - s[0]) * (sz[1] * sz[2]) + (y - s[1]) * sz[2] + (z - s[2]);
+                    const int u = flat_inner(x, y, z);
+                    for (int c = 0; c < 20; ++c) nM[c * st + f] = M[u][c];
+                    for (int c = 0; c < 3; ++c) ncom[c * st + f] = (*nb.data.x)[u][c];
+                }
+        return OTFMM_OK;
+    }
+    // compressed payload: the listed cells over the zeros
+    return expand_compressed(grid, d, std::min(M.size(), n_x), [&](size_t k, int x, int y, int z) {
+        const int f = (x - s[0]) * (sz[1] * sz[2]) + (y - s[1]) * sz[2] + (z - s[2]);
+        for (int c = 0; c < 20; ++c) nM[c * st + f] = M[k][c];
+        for (int c = 0; c < 3; ++c) ncom[c * st + f] = (*nb.data.x)[k][c];
+    });
 }
 
 // multipole_kernel_interface(monopoles, M_ptr, com_ptr, neighbors, type, dx,
 // is_direction_empty, xbase, grid, use_root_stencil): L += result,
 // L_c = correction (RHO). `monopoles` is not read: a refined node's own cells
 // enter as multipoles (update_input sets their monopole slots to zero).
+template <class Multipole, class SpaceVector, class Neighbor, class Expansion, class GridPtr>
+int multipole_kernel_impl(otfmm_context* ctx, const std::vector<Multipole>& M_ptr,
+                          const std::vector<std::shared_ptr<std::vector<SpaceVector>>>& com_ptr,
+                          const std::vector<Neighbor>& neighbors, int type, double dx, std::array<double, 3> xbase,
+                          std::vector<Expansion>& L, std::vector<SpaceVector>& L_c, bool use_root_stencil,
+                          int precision, const GridPtr& grid) {
+    Staging& st = thread_staging();
+    int rc = stage_multipole_input(M_ptr, com_ptr[0]->data(), neighbors, dx, xbase, use_root_stencil, st, grid);
+    if (rc != OTFMM_OK) return rc;
+    rc = otfmm_m2l_soa_host(ctx, use_root_stencil ? nullptr : st.mon.data(), st.M.data(), st.com.data(),
+                            st.L.data(), st.Lc.data(), type, use_root_stencil ? 1 : 0, precision);
+    if (rc != OTFMM_OK) return rc;
+    for (int c = 0; c < 20; ++c)
+        for (int u = 0; u < NCELL; ++u) L[u][c] += st.L[c * CLU + u];
+    if (type == OTFMM_RHO)
+        for (int c = 0; c < 3; ++c)
+            for (int u = 0; u < NCELL; ++u) L_c[u][c] = st.Lc[c * CLU + u];
+    return OTFMM_OK;
+}
+
+// L and L_c passed explicitly; every neighbour payload full size.
 template <class Multipole, class SpaceVector, class Neighbor, class Expansion>
 int multipole_kernel_interface(otfmm_context* ctx, const std::vector<double>& /*monopoles*/,
                                const std::vector<Multipole>& M_ptr,
@@ -128,17 +283,23 @@ int multipole_kernel_interface(otfmm_context* ctx, const std::vector<double>& /*
                                const std::array<bool, 26>& /*is_direction_empty*/, std::array<double, 3> xbase,
                                std::vector<Expansion>& L, std::vector<SpaceVector>& L_c, bool use_root_stencil,
                                int precision = OTFMM_FP64) {
-    Staging& st = thread_staging();
-    stage_multipole_input(M_ptr, com_ptr[0]->data(), neighbors, dx, xbase, use_root_stencil, st);
-    const int rc = otfmm_m2l_soa_host(ctx, use_root_stencil ? nullptr : st.mon.data(), st.M.data(), st.com.data(),
-                                      st.L.data(), st.Lc.data(), type, use_root_stencil ? 1 : 0, precision);
-    if (rc != OTFMM_OK) return rc;
-    for (int c = 0; c < 20; ++c)
-        for (int u = 0; u < NCELL; ++u) L[u][c] += st.L[c * CLU + u];
-    if (type == OTFMM_RHO)
-        for (int c = 0; c < 3; ++c)
-            for (int u = 0; u < NCELL; ++u) L_c[u][c] = st.Lc[c * CLU + u];
-    return OTFMM_OK;
+    return multipole_kernel_impl(ctx, M_ptr, com_ptr, neighbors, type, dx, xbase, L, L_c, use_root_stencil,
+                                 precision, nullptr);
+}
+
+// The reference's argument list (multipole_kernel_interface.hpp:18-22): the
+// result goes to grid->get_L() / grid->get_L_c(), compressed payloads are
+// expanded with grid->get_ilist_n_bnd(dir).
+template <class Multipole, class SpaceVector, class Neighbor, class GridPtr>
+int multipole_kernel_interface(otfmm_context* ctx, const std::vector<double>& /*monopoles*/,
+                               const std::vector<Multipole>& M_ptr,
+                               const std::vector<std::shared_ptr<std::vector<SpaceVector>>>& com_ptr,
+                               const std::vector<Neighbor>& neighbors, int type, double dx,
+                               const std::array<bool, 26>& /*is_direction_empty*/, std::array<double, 3> xbase,
+                               const GridPtr& grid, bool use_root_stencil, int precision = OTFMM_FP64) {
+    if (!grid) return OTFMM_ERR_INVALID;
+    return multipole_kernel_impl(ctx, M_ptr, com_ptr, neighbors, type, dx, xbase, grid->get_L(), grid->get_L_c(),
+                                 use_root_stencil, precision, grid);
 }
 
 template <class Multipole, class SpaceVector, class Neighbor, class Expansion>
@@ -161,13 +322,12 @@ void multipole_kernel_interface_or_abort(otfmm_context* ctx, const std::vector<d
 // is_direction_empty, grid, contains_multipole_neighbor): L[0..3] += P2P (+ P2M),
 // L_c = P2M correction when a neighbour is refined (RHO). Device staging is
 // allocated once per thread.
-template <class SpaceVector, class Neighbor, class Expansion>
-int monopole_kernel_interface(otfmm_context* ctx, const std::vector<double>& monopoles,
-                              const std::vector<std::shared_ptr<std::vector<SpaceVector>>>& com_ptr,
-                              const std::vector<Neighbor>& neighbors, int type, double dx,
-                              const std::array<bool, 26>& /*is_direction_empty*/, std::vector<Expansion>& L,
-                              std::vector<SpaceVector>& L_c, bool contains_multipole_neighbor,
-                              int precision = OTFMM_FP64) {
+template <class SpaceVector, class Neighbor, class Expansion, class GridPtr>
+int monopole_kernel_impl(otfmm_context* ctx, const std::vector<double>& monopoles,
+                         const std::vector<std::shared_ptr<std::vector<SpaceVector>>>& com_ptr,
+                         const std::vector<Neighbor>& neighbors, int type, double dx, std::vector<Expansion>& L,
+                         std::vector<SpaceVector>& L_c, bool contains_multipole_neighbor, int precision,
+                         const GridPtr& grid) {
     struct Dev {
         double* buf = nullptr;
         ~Dev() { if (buf) otfmm_device_free(buf); }
@@ -186,23 +346,9 @@ int monopole_kernel_interface(otfmm_context* ctx, const std::vector<double>& mon
     double* d_icom = d_Lc + n_Lc;
     double* d_nM = d_icom + n_icom;
     double* d_ncom = d_nM + n_nM;
-    // monopole update_input: own masses, leaf neighbours' masses, zeros else
-    std::vector<double> mon(ENTRIES, 0.0);
-    for (int x = 0; x < INX; ++x)
-        for (int y = 0; y < INX; ++y)
-            for (int z = 0; z < INX; ++z) mon[flat_padded(x + INX, y + INX, z + INX)] = monopoles[flat_inner(x, y, z)];
-    for (int d = 0; d < 26; ++d) {
-        const Neighbor& nb = neighbors[d];
-        if (!nb.is_monopole || !nb.data.m) continue;
-        int o[3], s[3], e[3], p[3];
-        dir_offsets(d, o);
-        padding_range(o, s, e, p);
-        for (int x = s[0]; x < e[0]; ++x)
-            for (int y = s[1]; y < e[1]; ++y)
-                for (int z = s[2]; z < e[2]; ++z)
-                    mon[flat_padded(x + p[0], y + p[1], z + p[2])] = (*nb.data.m)[flat_inner(x, y, z)];
-    }
-    int rc = otfmm_copy_to_device(ctx, d_mon, mon.data(), sizeof(double) * ENTRIES);
+    std::vector<double> mon(ENTRIES);
+    int rc = stage_monopole_input(monopoles, neighbors, mon.data(), grid);
+    if (rc == OTFMM_OK) rc = otfmm_copy_to_device(ctx, d_mon, mon.data(), sizeof(double) * ENTRIES);
     if (rc == OTFMM_OK) rc = otfmm_p2p_soa(ctx, d_mon, dx, d_L4, precision == OTFMM_FP64_EXACT ? OTFMM_FP64_EXACT : OTFMM_FP64, nullptr);
     if (rc != OTFMM_OK) return rc;
     bool any_p2m = false;
@@ -216,23 +362,9 @@ int monopole_kernel_interface(otfmm_context* ctx, const std::vector<double>& mon
         for (int d = 0; d < 26; ++d) {
             const Neighbor& nb = neighbors[d];
             if (nb.is_monopole || !nb.data.M) continue;
-            // update_neighbor_input: the refined neighbour's slab, own SoA stride
-            int o[3], s[3], e[3], sz[3];
-            dir_offsets(d, o);
-            for (int a = 0; a < 3; ++a) {
-                s[a] = (o[a] == -1) ? INX - SMAX : 0;
-                e[a] = (o[a] == 1) ? SMAX : INX;
-                sz[a] = e[a] - s[a];
-            }
-            const int stride = sz[0] * sz[1] * sz[2] + 19;
-            for (int x = s[0]; x < e[0]; ++x)
-                for (int y = s[1]; y < e[1]; ++y)
-                    for (int z = s[2]; z < e[2]; ++z) {
-                        const int f = (x - s[0]) * (sz[1] * sz[2]) + (y - s[1]) * sz[2] + (z - s[2]);
-                        const int u = flat_inner(x, y, z);
-                        for (int c = 0; c < 20; ++c) nM[c * stride + f] = (*nb.data.M)[u][c];
-                        for (int c = 0; c < 3; ++c) ncom[c * stride + f] = (*nb.data.x)[u][c];
-                    }
+            int stride = 0;
+            rc = stage_p2m_slab(nb, d, nM.data(), ncom.data(), &stride, grid);
+            if (rc != OTFMM_OK) return rc;
             rc = otfmm_copy_to_device(ctx, d_nM, nM.data(), sizeof(double) * 20 * stride);
             if (rc == OTFMM_OK) rc = otfmm_copy_to_device(ctx, d_ncom, ncom.data(), sizeof(double) * 3 * stride);
             if (rc == OTFMM_OK)
@@ -252,6 +384,32 @@ int monopole_kernel_interface(otfmm_context* ctx, const std::vector<double>& mon
         for (int c = 0; c < 3; ++c)
             for (int u = 0; u < NCELL; ++u) L_c[u][c] = st.Lc[c * CLU + u];
     return OTFMM_OK;
+}
+
+// L and L_c passed explicitly; every neighbour payload full size.
+template <class SpaceVector, class Neighbor, class Expansion>
+int monopole_kernel_interface(otfmm_context* ctx, const std::vector<double>& monopoles,
+                              const std::vector<std::shared_ptr<std::vector<SpaceVector>>>& com_ptr,
+                              const std::vector<Neighbor>& neighbors, int type, double dx,
+                              const std::array<bool, 26>& /*is_direction_empty*/, std::vector<Expansion>& L,
+                              std::vector<SpaceVector>& L_c, bool contains_multipole_neighbor,
+                              int precision = OTFMM_FP64) {
+    return monopole_kernel_impl(ctx, monopoles, com_ptr, neighbors, type, dx, L, L_c, contains_multipole_neighbor,
+                                precision, nullptr);
+}
+
+// The reference's argument list (monopole_kernel_interface.hpp:19-23): the
+// result goes to grid->get_L() / grid->get_L_c(), compressed payloads are
+// expanded with grid->get_ilist_n_bnd(dir).
+template <class SpaceVector, class Neighbor, class GridPtr>
+int monopole_kernel_interface(otfmm_context* ctx, const std::vector<double>& monopoles,
+                              const std::vector<std::shared_ptr<std::vector<SpaceVector>>>& com_ptr,
+                              const std::vector<Neighbor>& neighbors, int type, double dx,
+                              const std::array<bool, 26>& /*is_direction_empty*/, const GridPtr& grid,
+                              bool contains_multipole_neighbor, int precision = OTFMM_FP64) {
+    if (!grid) return OTFMM_ERR_INVALID;
+    return monopole_kernel_impl(ctx, monopoles, com_ptr, neighbors, type, dx, grid->get_L(), grid->get_L_c(),
+                                contains_multipole_neighbor, precision, grid);
 }
 
 }   // namespace otfmm_octotiger

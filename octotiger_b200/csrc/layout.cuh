@@ -106,6 +106,9 @@ struct Tables {
                                 // y = packed)
     const int* r2_sx_start;     // [8][12]: first entry of each sx = -5 .. 5 in entries_r2 (and the end)
     const double4* r2_four;     // [8][MAX_ENTRIES_R2]: monopole constants of the entries_r2 offsets
+    const double4* p2p_box;     // [8][216]: per parity, monopole constants over the 6^3 partner box (box
+                                // position (i, j, k) = offset + 2 + parity), zero off the stencil and at the cell
+    const double4* p2p_cube;    // [343]: monopole constants of the offsets -3..3 per axis, zero at the centre
 };
 
 __device__ __forceinline__ int entry_sx(int y) { return (y & 15) - 8; }
@@ -141,6 +144,8 @@ struct ItemInfo {
     int subgrid, kind;
     int nb[26];
     double dx, xbase[3];
+    uint32_t leafmask;   // raw directions (13 = centre, never set) whose neighbour is a leaf
+    uint32_t nbmask;     // raw directions with a neighbour
 };
 
 
@@ -202,15 +207,32 @@ __global__ void classify_kernel(BatchArgs a) {
     }
 }
 
-// Copies an item (already validated by classify_kernel) into shared memory.
+// Raw-direction bit mask (bit 13, the centre, left out) of 26 per-direction flags.
+__device__ __forceinline__ uint32_t raw_bits(uint32_t dirbits) {
+    return (dirbits & 0x1fffu) | ((dirbits >> 13) << 14);
+}
+
+// Copies an item (already validated by classify_kernel) into shared memory:
+// the first warp, one lane per direction, with the leaf / neighbour masks.
 __device__ __forceinline__ void load_item(const BatchArgs& a, int item_idx, ItemInfo& it) {
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
         const otfmm_work_item& w = a.items[item_idx];
-        it.subgrid = w.subgrid;
-        it.kind = w.kind;
-        it.dx = w.dx;
-        for (int q = 0; q < 3; ++q) it.xbase[q] = w.xbase[q];
-        for (int d = 0; d < 26; ++d) it.nb[d] = w.neighbors[d];
+        int nb = -1;
+        if (lane < 26) {
+            nb = w.neighbors[lane];
+            it.nb[lane] = nb;
+        }
+        const bool leaf = nb >= 0 && a.is_leaf[nb] != 0;
+        const uint32_t lb = __ballot_sync(0xffffffffu, leaf), eb = __ballot_sync(0xffffffffu, nb >= 0);
+        if (lane == 0) {
+            it.subgrid = w.subgrid;
+            it.kind = w.kind;
+            it.dx = w.dx;
+            for (int q = 0; q < 3; ++q) it.xbase[q] = w.xbase[q];
+            it.leafmask = raw_bits(lb);
+            it.nbmask = raw_bits(eb);
+        }
     }
     __syncthreads();
 }

@@ -65,7 +65,7 @@ __global__ void __launch_bounds__(P2P_THREADS, P2P_CTAS_PER_SM) p2p_batch_kernel
             const int raw = raw_dir(ax, ay, az);
             const int src = (raw == 13) ? it.subgrid : it.nb[raw < 13 ? raw : raw - 1];
             double m = 0.0;
-            if (src >= 0 && (raw == 13 || a.is_leaf[src]))
+            if (raw == 13 || ((it.leafmask >> raw) & 1u))
                 m = a.mon[(size_t)src * NCELL + (ax & 7) * 64 + (ay & 7) * 8 + (az & 7)];
             if (PREC != PREC_EXACT) m *= dc0;   // 1/dx folded into the staged mass
             const int cls = ((ax & 1) << 2) | ((ay & 1) << 1) | (az & 1);
@@ -259,6 +259,196 @@ __global__ void __launch_bounds__(P2_THREADS, 1) p2p_leaf_kernel(BatchArgs a) {
     }
 }
 
+// Leaf items, P2P over the partner box (fast FP64 form T = double; FP32 split
+// form T = float, FP32 partial sums promoted to FP64 every ROWS partner rows of
+// 6). With a stencil of coarse reach 1 the partners of a cell are the cells of
+// the 3x3x3 coarse cells around its own, a 6x6x6 box shared by the 8 cells of a
+// coarse cell. One CTA of 128 threads per leaf (grid stride over the leaves):
+// warp w takes the cells of x/y parity (w >> 1, w & 1); lane (Cx, Cy, c) the
+// four cells (2 Cx + px, 2 Cy + py, z), z in {2c, 2c + 1, 2c + 4, 2c + 5}.
+// A partner mass read from shared memory serves two of them (the two cells of
+// a coarse cell), a monopole constant (one warp-uniform read) two as well (the
+// two cells of one parity). FULL: every parity has the whole box in its stencil
+// and the constants come from the 7^3 table of offsets; otherwise from the
+// per-parity box tables, zero where an offset is off the stencil.
+template <class T>
+struct BoxLayout;
+template <>
+struct BoxLayout<float> {   // float2 reads: the 16 lanes of a half-warp hit distinct 8-byte slots
+    static constexpr int RYS = 18, RXS = 216;
+    using V2 = float2;
+};
+template <>
+struct BoxLayout<double> {   // double2 reads: the 8 lanes of a quarter-warp hit distinct 16-byte slots
+    static constexpr int RYS = 14, RXS = 168;
+    using V2 = double2;
+};
+constexpr int BOX_THREADS = 128;
+constexpr int BOX_CUBE = 343;
+constexpr int BOX_CELLS = 216;
+template <class T, bool FULL>
+constexpr int box_smem_bytes() {
+    return (FULL ? BOX_CUBE : 8 * BOX_CELLS) * (int)sizeof(typename P2Vec<T>::type) +
+           P_REG * BoxLayout<T>::RXS * (int)sizeof(T);
+}
+static_assert(11 * BoxLayout<float>::RYS + 12 <= BoxLayout<float>::RXS &&
+                  11 * BoxLayout<double>::RYS + 12 <= BoxLayout<double>::RXS,
+              "box region rows fit their planes");
+
+__device__ __forceinline__ float box_fma(float x, float y, float z) { return fmaf(x, y, z); }
+__device__ __forceinline__ double box_fma(double x, double y, double z) { return fma(x, y, z); }
+
+template <class T, bool FULL, int ROWS>
+__global__ void __launch_bounds__(BOX_THREADS, 4) p2p_box_kernel(BatchArgs a) {
+    using V4 = typename P2Vec<T>::type;
+    using V2 = typename BoxLayout<T>::V2;
+    constexpr int RYS = BoxLayout<T>::RYS, RXS = BoxLayout<T>::RXS;
+    constexpr int NT = FULL ? BOX_CUBE : 8 * BOX_CELLS;
+    extern __shared__ __align__(16) unsigned char bx_dyn[];
+    V4* s_four = reinterpret_cast<V4*>(bx_dyn);
+    T* reg = reinterpret_cast<T*>(bx_dyn + NT * sizeof(V4));
+    __shared__ ItemInfo it;
+    const int nleaf = a.wl.counts[WL_LEAF];
+    if (blockIdx.x >= nleaf) return;   // uniform for the block
+    const double4* src4 = FULL ? a.t.p2p_cube : a.t.p2p_box;
+    for (int e = threadIdx.x; e < NT; e += BOX_THREADS) {
+        const double4 f = src4[e];
+        s_four[e] = V4{(T)f.x, (T)f.y, (T)f.z, (T)f.w};
+    }
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int px = w >> 1, py = w & 1;
+    const int c = lane & 1, Cy = (lane >> 1) & 3, Cx = lane >> 3;
+    // constants of the cells of z parity 0 (qa) and 1 (qb) for box row (i, j):
+    // FULL: qa[k] = cube[base(i, j) + k + 1], qb[k] = cube[base(i, j) + k]
+    const V4* tab_a = FULL ? s_four + (1 - px) * 49 + (1 - py) * 7 : s_four + (4 * px + 2 * py) * BOX_CELLS;
+    const V4* tab_b = FULL ? tab_a : tab_a + BOX_CELLS;
+    const int lane_off = (2 * Cx) * RXS + (2 * Cy) * RYS + 2 * c;
+    for (int kk = blockIdx.x; kk < nleaf; kk += gridDim.x) {
+        __syncthreads();   // the previous leaf is done with `reg` and `it`
+        load_item(a, a.wl.leaf[kk], it);
+        const double dc0 = 1.0 / it.dx;
+        const uint32_t lm = it.leafmask | (1u << 13);   // the leaf itself and its leaf neighbours
+        const size_t own = (size_t)it.subgrid;
+        // masses / dx of the cells -2..9 per axis (the leaf and its leaf neighbours;
+        // zeros elsewhere), seven loads of a thread in flight at a time
+        constexpr int NR = P_REG * P_REG * P_REG, NB = 7;
+#pragma unroll 1
+        for (int r0 = 0; r0 < NR; r0 += NB * BOX_THREADS) {
+            double v[NB];
+#pragma unroll
+            for (int t = 0; t < NB; ++t) {
+                const int r = r0 + threadIdx.x + t * BOX_THREADS;
+                v[t] = 0.0;
+                if (r < NR) {
+                    const int ax = r / (P_REG * P_REG) - 2, ay = (r / P_REG) % P_REG - 2, az = r % P_REG - 2;
+                    const int raw = raw_dir(ax, ay, az);
+                    if ((lm >> raw) & 1u) {
+                        const size_t src = (raw == 13) ? own : (size_t)it.nb[raw < 13 ? raw : raw - 1];
+                        v[t] = __ldg(a.mon + src * NCELL + (ax & 7) * 64 + (ay & 7) * 8 + (az & 7));
+                    }
+                }
+            }
+#pragma unroll
+            for (int t = 0; t < NB; ++t) {
+                const int r = r0 + threadIdx.x + t * BOX_THREADS;
+                if (r < NR) {
+                    const int rx = r / (P_REG * P_REG), ry = (r / P_REG) % P_REG, rz = r % P_REG;
+                    reg[rx * RXS + ry * RYS + rz] = (T)(v[t] * dc0);
+                }
+            }
+        }
+        __syncthreads();
+        double g[4][4];
+        T f[4][4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                g[u][q] = 0.0;
+                f[u][q] = (T)0;
+            }
+#pragma unroll 1
+        for (int i = 0; i < 6; ++i) {
+#pragma unroll
+            for (int j = 0; j < 6; ++j) {
+                // partner masses of box row (i, j): m[k] for cells 2c, 2c + 1 and m[k + 4] for 2c + 4, 2c + 5
+                const T* row = reg + lane_off + i * RXS + j * RYS;
+                T m[10];
+#pragma unroll
+                for (int h = 0; h < 5; ++h) {
+                    const V2 v = *reinterpret_cast<const V2*>(row + 2 * h);
+                    m[2 * h] = v.x;
+                    m[2 * h + 1] = v.y;
+                }
+                const int b = FULL ? i * 49 + j * 7 : (i * 6 + j) * 6;
+                V4 qa[6], qb[6];
+                if (FULL) {
+                    V4 q7[7];
+#pragma unroll
+                    for (int k = 0; k < 7; ++k) q7[k] = tab_a[b + k];
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) {
+                        qa[k] = q7[k + 1];
+                        qb[k] = q7[k];
+                    }
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) {
+                        qa[k] = tab_a[b + k];
+                        qb[k] = tab_b[b + k];
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < 6; ++k) {
+                    const T mA = m[k], mC = m[k + 4];
+                    f[0][0] = box_fma(qa[k].x, mA, f[0][0]);
+                    f[0][1] = box_fma(qa[k].y, mA, f[0][1]);
+                    f[0][2] = box_fma(qa[k].z, mA, f[0][2]);
+                    f[0][3] = box_fma(qa[k].w, mA, f[0][3]);
+                    f[1][0] = box_fma(qb[k].x, mA, f[1][0]);
+                    f[1][1] = box_fma(qb[k].y, mA, f[1][1]);
+                    f[1][2] = box_fma(qb[k].z, mA, f[1][2]);
+                    f[1][3] = box_fma(qb[k].w, mA, f[1][3]);
+                    f[2][0] = box_fma(qa[k].x, mC, f[2][0]);
+                    f[2][1] = box_fma(qa[k].y, mC, f[2][1]);
+                    f[2][2] = box_fma(qa[k].z, mC, f[2][2]);
+                    f[2][3] = box_fma(qa[k].w, mC, f[2][3]);
+                    f[3][0] = box_fma(qb[k].x, mC, f[3][0]);
+                    f[3][1] = box_fma(qb[k].y, mC, f[3][1]);
+                    f[3][2] = box_fma(qb[k].z, mC, f[3][2]);
+                    f[3][3] = box_fma(qb[k].w, mC, f[3][3]);
+                }
+                if constexpr (sizeof(T) == 4) {
+                    if ((j % ROWS) != ROWS - 1) continue;
+#pragma unroll
+                    for (int u = 0; u < 4; ++u)
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            g[u][q] += (double)f[u][q];
+                            f[u][q] = (T)0;
+                        }
+                }
+            }
+        }
+        if constexpr (sizeof(T) == 8) {
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) g[u][q] = (double)f[u][q];
+        }
+        const double dc1 = -dc0;
+        double* L = a.L + (size_t)it.subgrid * 20 * NCELL;
+        const int cxy = (2 * Cx + px) * 64 + (2 * Cy + py) * 8;
+        const int zc[4] = {2 * c, 2 * c + 1, 2 * c + 4, 2 * c + 5};
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            L[cxy + zc[u]] = g[u][0];
+#pragma unroll
+            for (int q = 1; q < 4; ++q) L[q * NCELL + cxy + zc[u]] = g[u][q] * dc1;
+        }
+    }
+}
+
 // Leaf items with refined neighbours: P2M (p2m_kernel_impl_rho / _non_rho,
 // monopole kokkos_kernel.hpp:517-942) after P2P: one CTA per leaf of the P2M
 // work list (grid stride). The refined directions are taken one after the
@@ -279,11 +469,7 @@ __global__ void __launch_bounds__(P_THREADS) p2m_batch_kernel(BatchArgs a) {
     for (int kk = blockIdx.x; kk < np2m; kk += gridDim.x) {
         __syncthreads();   // `it` and s_acc are reused
         load_item(a, a.wl.p2m[kk], it);
-        uint32_t refmask = 0;
-        for (int d = 0; d < 26; ++d) {
-            const int nb = it.nb[d];
-            if (nb >= 0 && !a.is_leaf[nb]) refmask |= 1u << (d < 13 ? d : d + 1);
-        }
+        const uint32_t refmask = it.nbmask & ~it.leafmask;
         const size_t sub = (size_t)it.subgrid;
         double* L = a.L + sub * 20 * NCELL;
         double* Lc = a.Lc + sub * 3 * NCELL;
@@ -383,10 +569,10 @@ __global__ void __launch_bounds__(P_THREADS) p2m_fast_kernel(BatchArgs a) {
         load_item(a, a.wl.p2m[kk], it);
         if (threadIdx.x == 0) {
             int n = 0, cum = 0;
+            const uint32_t refmask = it.nbmask & ~it.leafmask;
             for (int d = 0; d < 26; ++d) {
-                const int nb = it.nb[d];
-                if (nb >= 0 && !a.is_leaf[nb]) {
-                    const int r = d < 13 ? d : d + 1;
+                const int r = d < 13 ? d : d + 1;
+                if ((refmask >> r) & 1u) {
                     s_dir[n] = r;
                     s_cum[n] = cum;
                     cum += (a.t.p2m_perm_start[r + 1] - a.t.p2m_perm_start[r]) * F;

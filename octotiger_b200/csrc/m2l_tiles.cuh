@@ -39,7 +39,7 @@ __device__ void stage_region_pool(double* sm, const ItemInfo& it, int x0, bool l
 #pragma unroll
             for (int q = 0; q < NCOMP; ++q) v[q] = 0.0;
         } else {
-            const bool use_mon = centre ? leaf_tile : (is_leaf[src] != 0);
+            const bool use_mon = centre ? leaf_tile : ((it.leafmask >> raw) & 1u) != 0;
             if (use_mon) {
                 v[0] = mon[(size_t)src * NCELL + u];
 #pragma unroll
@@ -230,7 +230,7 @@ __device__ void stage_region_split(double* sm, const ItemInfo& it, int x0, doubl
             for (int q = 0; q < 20; ++q) m[q] = 0.0;
 #pragma unroll
             for (int a = 0; a < 3; ++a) c[a] = 0.0;
-        } else if (!centre && is_leaf[src]) {
+        } else if (!centre && ((it.leafmask >> raw) & 1u)) {
             m[0] = mon[(size_t)src * NCELL + u];
 #pragma unroll
             for (int q = 1; q < 20; ++q) m[q] = 0.0;
@@ -396,7 +396,7 @@ __device__ void stage_region_ws(float2* sa, double2* sb, const ItemInfo& it, int
             P[0] = ax;
             P[1] = ay;
             P[2] = az;
-        } else if (!centre && is_leaf[src]) {
+        } else if (!centre && ((it.leafmask >> raw) & 1u)) {
             m[0] = mon[(size_t)src * NCELL + u];
 #pragma unroll
             for (int q = 1; q < 20; ++q) m[q] = 0.0;
@@ -785,11 +785,7 @@ __global__ void __launch_bounds__(THREADS, 1) m2l_batch_kernel(BatchArgs a) {
             root_tile<P64, RHO>(sm, x0, a.t, out);
         } else {
             // leaf neighbours, indexed by raw direction (monopole-only offsets)
-            uint32_t monomask = 0;
-            for (int d = 0; d < 26; ++d) {
-                const int nb = it.nb[d];
-                if (nb >= 0 && a.is_leaf[nb]) monomask |= 1u << (d < 13 ? d : d + 1);
-            }
+            const uint32_t monomask = it.leafmask;
             if (PREC == PREC_SPLIT) {
                 const double inv_dx = 1.0 / it.dx;
                 stage_region_split(sm, it, x0, inv_dx, a.M, a.com, a.mon, a.is_leaf);
@@ -844,11 +840,7 @@ __global__ void __launch_bounds__(WS_THREADS, 1) m2l_split_ws_kernel(BatchArgs a
             __syncthreads();
             if (threadIdx.x < THREADS) root_tile<PREC_FAST, true>(sm, x0, a.t, out);
         } else {
-            uint32_t monomask = 0;
-            for (int d = 0; d < 26; ++d) {
-                const int nb = it.nb[d];
-                if (nb >= 0 && a.is_leaf[nb]) monomask |= 1u << (d < 13 ? d : d + 1);
-            }
+            const uint32_t monomask = it.leafmask;
             const double inv_dx = 1.0 / it.dx;
             stage_region_ws(sa, sb, it, x0, inv_dx, a.M, a.com, a.mon, a.is_leaf);
             __syncthreads();

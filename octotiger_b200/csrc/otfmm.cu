@@ -221,6 +221,10 @@ struct otfmm_context {
     double4* d_r2_four = nullptr;
     int p2m_groups_max = 0;   // cells with partners summed over the 26 directions
     double4* d_p2p_four = nullptr;
+    double4* d_p2p_box = nullptr;    // [8][216] per-parity box constants
+    double4* d_p2p_cube = nullptr;   // [343] constants of the offsets -3..3
+    bool p2p_full_box = false;       // every parity's stencil is its whole 6^3 box
+    int box_grid[6] = {};            // resident CTAs of the box P2P kernels (all SMs)
     int counts_far[8] = {};
     double* d_four = nullptr;
     uint8_t* d_phase = nullptr;
@@ -228,7 +232,7 @@ struct otfmm_context {
     double* d_soa_scratch = nullptr;   // host-buffer path staging
     int* d_lists = nullptr;            // batched work lists (grown on demand)
     int list_capacity = 0;
-    otfmm_tuning tuning = {OTFMM_SPLIT_WARP_SPECIALISED, 16, 32, 16};
+    otfmm_tuning tuning = {OTFMM_SPLIT_WARP_SPECIALISED, 16, 32, 16, OTFMM_P2P_BOX};
     // otfmm_batch_host: device copies of the pool, work list and outputs, a
     // pinned host copy of the reordered work list, two copy streams and events
     struct HostPath {
@@ -245,7 +249,8 @@ struct otfmm_context {
     std::mutex mu;
     Tables tables() const { return Tables{d_entries,    d_count, d_entries_fast, d_count_far, d_entries_split, d_entries_p2p,
                       d_entries_ws, d_four,  d_phase,        d_p2m_start,     d_p2m_list,    d_p2m_perm_start,
-                      d_p2m_perm,   d_p2m_slot,     d_p2p_four,      d_entries_r2,  d_r2_sx_start, d_r2_four}; }
+                      d_p2m_perm,   d_p2m_slot,     d_p2p_four,      d_entries_r2,  d_r2_sx_start, d_r2_four,
+                      d_p2p_box,    d_p2p_cube}; }
 };
 
 namespace {
@@ -294,6 +299,12 @@ int ensure_attributes(int device) {
     rc = rc ? rc : set_smem(p2p_leaf_kernel<double, 0>, p2_smem_bytes<double>());
     rc = rc ? rc : set_smem(p2p_leaf_kernel<float, 32>, p2_smem_bytes<float>());
     rc = rc ? rc : set_smem(p2p_leaf_kernel<float, 16>, p2_smem_bytes<float>());
+    rc = rc ? rc : set_smem(p2p_box_kernel<double, true, 6>, box_smem_bytes<double, true>());
+    rc = rc ? rc : set_smem(p2p_box_kernel<double, false, 6>, box_smem_bytes<double, false>());
+    rc = rc ? rc : set_smem(p2p_box_kernel<float, true, 3>, box_smem_bytes<float, true>());
+    rc = rc ? rc : set_smem(p2p_box_kernel<float, true, 6>, box_smem_bytes<float, true>());
+    rc = rc ? rc : set_smem(p2p_box_kernel<float, false, 3>, box_smem_bytes<float, false>());
+    rc = rc ? rc : set_smem(p2p_box_kernel<float, false, 6>, box_smem_bytes<float, false>());
     rc = rc ? rc : set_smem(m2l_r2_kernel<PREC_EXACT, true>, PL_SMEM_BYTES);
     rc = rc ? rc : set_smem(m2l_r2_kernel<PREC_EXACT, false>, PL_SMEM_BYTES);
     rc = rc ? rc : set_smem(m2l_r2_kernel<PREC_FAST, true>, PL_SMEM_BYTES);
@@ -318,6 +329,28 @@ int check_precision(int precision, bool batched = false) {
     if (precision == OTFMM_FP64_EXACT || precision == OTFMM_FP64) return OTFMM_OK;
     if (precision == OTFMM_FP32_SPLIT && batched) return OTFMM_OK;
     return fail(OTFMM_ERR_UNSUPPORTED, "precision not available for this entry point (FP32 split is batched only)");
+}
+
+// Grid of the box P2P kernels: as many CTAs as are resident on all SMs at once
+// (the kernels stride over the leaves).
+int box_occupancy(otfmm_context* ctx) {
+    int sms = 0;
+    OT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+    int per_sm[6] = {};
+    OT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[0], p2p_box_kernel<double, true, 6>, BOX_THREADS,
+                                                          box_smem_bytes<double, true>()));
+    OT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1], p2p_box_kernel<double, false, 6>, BOX_THREADS,
+                                                          box_smem_bytes<double, false>()));
+    OT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[2], p2p_box_kernel<float, true, 3>, BOX_THREADS,
+                                                          box_smem_bytes<float, true>()));
+    OT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[3], p2p_box_kernel<float, true, 6>, BOX_THREADS,
+                                                          box_smem_bytes<float, true>()));
+    OT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[4], p2p_box_kernel<float, false, 3>, BOX_THREADS,
+                                                          box_smem_bytes<float, false>()));
+    OT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[5], p2p_box_kernel<float, false, 6>, BOX_THREADS,
+                                                          box_smem_bytes<float, false>()));
+    for (int v = 0; v < 6; ++v) ctx->box_grid[v] = std::max(1, per_sm[v]) * sms;
+    return OTFMM_OK;
 }
 
 }   // namespace
@@ -395,6 +428,33 @@ int otfmm_create(int device, double theta, otfmm_context** out) {
             const double* f = ctx->st.four[(en.y >> 16) & 2047];
             p2p_four[p * MAX_ENTRIES + e] = double4{f[0], f[1], f[2], f[3]};
         }
+    // box-form P2P tables: per parity the 6^3 partner box (zeros off the
+    // stencil and at the cell itself), and the 7^3 offset cube when every
+    // parity's stencil is its whole box
+    std::vector<double4> p2p_box(8 * 216, double4{0.0, 0.0, 0.0, 0.0});
+    std::vector<double4> p2p_cube(343, double4{0.0, 0.0, 0.0, 0.0});
+    ctx->p2p_full_box = (n_tile == 8);
+    for (int p = 0; p < n_tile; ++p) {
+        const int px = (p >> 2) & 1, py = (p >> 1) & 1, pz = p & 1;
+        int in_box = 0;
+        for (int e = 0; e < ctx->counts[p]; ++e) {
+            const int2 en = entries[p * MAX_ENTRIES + e];
+            const int sx = (en.y & 15) - 8, sy = ((en.y >> 4) & 15) - 8, sz = ((en.y >> 8) & 15) - 8;
+            const int bi = sx + 2 + px, bj = sy + 2 + py, bk = sz + 2 + pz;
+            if (bi < 0 || bi > 5 || bj < 0 || bj > 5 || bk < 0 || bk > 5) continue;   // reach 1 keeps every entry in the box
+            ++in_box;
+            const double* f = ctx->st.four[(en.y >> 16) & 2047];
+            p2p_box[p * 216 + (bi * 6 + bj) * 6 + bk] = double4{f[0], f[1], f[2], f[3]};
+        }
+        if (in_box != ctx->counts[p] || in_box != 215) ctx->p2p_full_box = false;
+    }
+    for (int sx = -3; sx <= 3; ++sx)
+        for (int sy = -3; sy <= 3; ++sy)
+            for (int sz = -3; sz <= 3; ++sz) {
+                if (sx == 0 && sy == 0 && sz == 0) continue;
+                const double* f = ctx->st.four[(sx + SMAX) * SINX * SINX + (sy + SMAX) * SINX + (sz + SMAX)];
+                p2p_cube[(sx + 3) * 49 + (sy + 3) * 7 + (sz + 3)] = double4{f[0], f[1], f[2], f[3]};
+            }
     // split-layout table (far first, like the fast one)
     std::vector<int4> entries_split(8 * MAX_ENTRIES, int4{0, 0, 0, 0});
     std::vector<int4> entries_ws(8 * MAX_ENTRIES, int4{0, 0, 0, 0});
@@ -474,6 +534,12 @@ int otfmm_create(int device, double theta, otfmm_context** out) {
         (e = cudaMalloc(&ctx->d_p2m_slot, sizeof(int16_t) * p2m_slot.size())) != cudaSuccess ||
         (e = cudaMemcpy(ctx->d_p2m_slot, p2m_slot.data(), sizeof(int16_t) * p2m_slot.size(),
                         cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMalloc(&ctx->d_p2p_box, sizeof(double4) * p2p_box.size())) != cudaSuccess ||
+        (e = cudaMemcpy(ctx->d_p2p_box, p2p_box.data(), sizeof(double4) * p2p_box.size(),
+                        cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMalloc(&ctx->d_p2p_cube, sizeof(double4) * p2p_cube.size())) != cudaSuccess ||
+        (e = cudaMemcpy(ctx->d_p2p_cube, p2p_cube.data(), sizeof(double4) * p2p_cube.size(),
+                        cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMalloc(&ctx->d_p2p_four, sizeof(double4) * p2p_four.size())) != cudaSuccess ||
         (e = cudaMemcpy(ctx->d_p2p_four, p2p_four.data(), sizeof(double4) * p2p_four.size(),
                         cudaMemcpyHostToDevice)) != cudaSuccess ||
@@ -519,7 +585,8 @@ int otfmm_create(int device, double theta, otfmm_context** out) {
         otfmm_destroy(ctx);
         return cuda_fail(e, "otfmm_create");
     }
-    const int rc = ensure_attributes(device);
+    int rc = ensure_attributes(device);
+    if (rc == OTFMM_OK) rc = box_occupancy(ctx);
     if (rc != OTFMM_OK) {
         otfmm_destroy(ctx);
         return rc;
@@ -542,6 +609,8 @@ int otfmm_destroy(otfmm_context* ctx) {
     cudaFree(ctx->d_p2m_perm_start);
     cudaFree(ctx->d_p2m_perm);
     cudaFree(ctx->d_p2p_four);
+    cudaFree(ctx->d_p2p_box);
+    cudaFree(ctx->d_p2p_cube);
     cudaFree(ctx->d_p2m_slot);
     cudaFree(ctx->d_entries_r2);
     cudaFree(ctx->d_r2_sx_start);
@@ -783,6 +852,7 @@ int check_tuning(const otfmm_tuning& t) {
     if (t.split_m2l_chunk != 8 && t.split_m2l_chunk != 16) return fail(OTFMM_ERR_INVALID, "split M2L chunk must be 8 or 16");
     if (t.split_p2p_chunk != 16 && t.split_p2p_chunk != 32) return fail(OTFMM_ERR_INVALID, "split P2P chunk must be 16 or 32");
     if (t.p2m_lanes != 4 && t.p2m_lanes != 8 && t.p2m_lanes != 16) return fail(OTFMM_ERR_INVALID, "P2M lanes must be 4, 8 or 16");
+    if (t.p2p_form != OTFMM_P2P_BOX && t.p2p_form != OTFMM_P2P_STENCIL) return fail(OTFMM_ERR_INVALID, "unknown P2P form");
     return OTFMM_OK;
 }
 
@@ -874,13 +944,30 @@ int enqueue_batch(otfmm_context* ctx, const double* pool_M, const double* pool_c
                 m2l_batch_kernel<PREC_SPLIT, false><<<tiles_grid, THREADS, sbytes, s>>>(a);
             }
             mark(2);
-            if (tu.split_p2p_chunk == 16) p2p_leaf_kernel<float, 16><<<sms, P2_THREADS, p2_smem_bytes<float>(), s>>>(a);
-            else p2p_leaf_kernel<float, 32><<<sms, P2_THREADS, p2_smem_bytes<float>(), s>>>(a);
+            if (tu.p2p_form == OTFMM_P2P_BOX) {
+                const bool full = ctx->p2p_full_box;
+                if (tu.split_p2p_chunk == 16) {
+                    if (full) p2p_box_kernel<float, true, 3><<<ctx->box_grid[2], BOX_THREADS, box_smem_bytes<float, true>(), s>>>(a);
+                    else p2p_box_kernel<float, false, 3><<<ctx->box_grid[4], BOX_THREADS, box_smem_bytes<float, false>(), s>>>(a);
+                } else {
+                    if (full) p2p_box_kernel<float, true, 6><<<ctx->box_grid[3], BOX_THREADS, box_smem_bytes<float, true>(), s>>>(a);
+                    else p2p_box_kernel<float, false, 6><<<ctx->box_grid[5], BOX_THREADS, box_smem_bytes<float, false>(), s>>>(a);
+                }
+            } else if (tu.split_p2p_chunk == 16) {
+                p2p_leaf_kernel<float, 16><<<sms, P2_THREADS, p2_smem_bytes<float>(), s>>>(a);
+            } else {
+                p2p_leaf_kernel<float, 32><<<sms, P2_THREADS, p2_smem_bytes<float>(), s>>>(a);
+            }
         } else {
             if (rho) m2l_batch_kernel<PREC_FAST, true><<<tiles_grid, THREADS, bytes, s>>>(a);
             else m2l_batch_kernel<PREC_FAST, false><<<tiles_grid, THREADS, bytes, s>>>(a);
             mark(2);
-            p2p_leaf_kernel<double, 0><<<sms, P2_THREADS, p2_smem_bytes<double>(), s>>>(a);
+            if (tu.p2p_form == OTFMM_P2P_BOX) {
+                if (ctx->p2p_full_box) p2p_box_kernel<double, true, 6><<<ctx->box_grid[0], BOX_THREADS, box_smem_bytes<double, true>(), s>>>(a);
+                else p2p_box_kernel<double, false, 6><<<ctx->box_grid[1], BOX_THREADS, box_smem_bytes<double, false>(), s>>>(a);
+            } else {
+                p2p_leaf_kernel<double, 0><<<sms, P2_THREADS, p2_smem_bytes<double>(), s>>>(a);
+            }
         }
         mark(3);
         const size_t part_bytes = sizeof(double) * 7 * (size_t)ctx->p2m_groups_max;
@@ -1274,16 +1361,18 @@ int otfmm_autotune(otfmm_context* ctx, const double* pool_M, const double* pool_
     rc = time_of(best, tbest);
     const int forms[3] = {OTFMM_SPLIT_WARP_SPECIALISED_PACKED, OTFMM_SPLIT_WARP_SPECIALISED, OTFMM_SPLIT_SINGLE_ROLE};
     const int m2l_chunks[2] = {8, 16}, p2p_chunks[2] = {16, 32}, lanes[3] = {4, 8, 16};
+    const int p2p_forms[2] = {OTFMM_P2P_BOX, OTFMM_P2P_STENCIL};
     const bool split = (precision == OTFMM_FP32_SPLIT), fast = (precision != OTFMM_FP64_EXACT);
-    for (int dim = 0; dim < 4 && rc == OTFMM_OK; ++dim) {
+    for (int dim = 0; dim < 5 && rc == OTFMM_OK; ++dim) {
         const int nvar = (dim == 3 || dim == 0) ? 3 : 2;
-        if ((dim < 3 && !split) || (dim == 3 && !fast)) continue;
+        if ((dim < 3 && !split) || (dim >= 3 && !fast)) continue;
         for (int v = 0; v < nvar && rc == OTFMM_OK; ++v) {
             otfmm_tuning tu = best;
             if (dim == 0) tu.split_m2l_form = forms[v];
             if (dim == 1) tu.split_m2l_chunk = m2l_chunks[v];
             if (dim == 2) tu.split_p2p_chunk = p2p_chunks[v];
             if (dim == 3) tu.p2m_lanes = lanes[v];
+            if (dim == 4) tu.p2p_form = p2p_forms[v];
             if (std::memcmp(&tu, &best, sizeof tu) == 0) continue;
             float t = 0.f;
             rc = time_of(tu, t);

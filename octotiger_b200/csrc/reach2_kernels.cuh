@@ -67,11 +67,7 @@ __global__ void __launch_bounds__(THREADS, 1) m2l_r2_kernel(BatchArgs a) {
             __syncthreads();   // shared memory and `it` are reused by the next tile
             continue;
         }
-        uint32_t monomask = 0;   // leaf neighbours, by raw direction
-        for (int d = 0; d < 26; ++d) {
-            const int nb = it.nb[d];
-            if (nb >= 0 && a.is_leaf[nb]) monomask |= 1u << (d < 13 ? d : d + 1);
-        }
+        const uint32_t monomask = it.leafmask;   // leaf neighbours, by raw direction
         const CellMap c = cell_map(x0);
         const int cu = c.cx * 64 + c.cy * 8 + c.cz;
         const int lane_off = c.j * PL_RS + c.k;
@@ -99,7 +95,7 @@ __global__ void __launch_bounds__(THREADS, 1) m2l_r2_kernel(BatchArgs a) {
                 if (src < 0) {
 #pragma unroll
                     for (int q = 0; q < NCOMP; ++q) v[q] = 0.0;
-                } else if (raw != 13 && a.is_leaf[src]) {
+                } else if ((it.leafmask >> raw) & 1u) {
                     v[0] = a.mon[(size_t)src * NCELL + u];
 #pragma unroll
                     for (int q = 1; q < 20; ++q) v[q] = 0.0;
@@ -196,7 +192,7 @@ __global__ void __launch_bounds__(256) p2p_r2_kernel(BatchArgs a) {
             const int raw = raw_dir(ax, ay, az);
             const int src = (raw == 13) ? it.subgrid : it.nb[raw < 13 ? raw : raw - 1];
             double m = 0.0;
-            if (src >= 0 && (raw == 13 || a.is_leaf[src]))
+            if (raw == 13 || ((it.leafmask >> raw) & 1u))
                 m = a.mon[(size_t)src * NCELL + (ax & 7) * 64 + (ay & 7) * 8 + (az & 7)];
             pm[(ax + R2_PAD) * R2_PLANE + (ay + R2_PAD) * R2_ROW + (az + R2_PAD)] = m;
         }

@@ -27,7 +27,7 @@ def adapter_bin(tmp_path_factory):
     return out
 
 
-def run_adapter(adapter_bin, tmp_path, b, solve, precision):
+def run_adapter(adapter_bin, tmp_path, b, solve, precision, mode=0, expect_rc=0):
     it = b.items[0]
     p = b.pool
     inp = tmp_path / "in.bin"
@@ -41,7 +41,10 @@ def run_adapter(adapter_bin, tmp_path, b, solve, precision):
         p.mon.tofile(f)
         p.is_leaf.tofile(f)
     outp = tmp_path / "out.bin"
-    subprocess.run([str(adapter_bin), str(inp), str(outp), str(precision), str(b.theta)], check=True)
+    r = subprocess.run([str(adapter_bin), str(inp), str(outp), str(precision), str(b.theta), str(mode)])
+    assert r.returncode == expect_rc
+    if expect_rc != 0:
+        return None
     raw = np.fromfile(outp, np.float64)
     return raw[:512 * 20].reshape(512, 20).T, raw[512 * 20:].reshape(512, 3).T
 
@@ -65,3 +68,27 @@ def test_adapter_exact_matches_oracle(adapter_bin, tmp_path, oracle, name, solve
     np.testing.assert_array_equal(L[:ncomp], Lo[s][:ncomp])
     if solve == RHO:
         np.testing.assert_array_equal(Lc, Lco[s])
+
+
+NEIGHBOURED = ("refined_mixed", "leaf_p2m")
+
+
+@pytest.mark.parametrize("solve", [RHO, DRHODT])
+@pytest.mark.parametrize("name", NEIGHBOURED)
+def test_adapter_compressed_payloads(adapter_bin, tmp_path, oracle, name, solve):
+    """Remote neighbours' compressed payloads (grid::get_gravity_boundary packs
+    the cells of grid::get_ilist_n_bnd(dir)) through the overloads that take the
+    grid: the whole band listed gives the full-size result bit for bit; a list
+    with cells left out gives the result of full payloads with those cells
+    zeroed; without a grid the compressed payloads are rejected."""
+    b = CASES[name]()
+    full = run_adapter(adapter_bin, tmp_path, b, solve, 0, mode=0)
+    whole = run_adapter(adapter_bin, tmp_path, b, solve, 0, mode=1)
+    subset = run_adapter(adapter_bin, tmp_path, b, solve, 0, mode=2)
+    zeroed = run_adapter(adapter_bin, tmp_path, b, solve, 0, mode=3)
+    for a, c in zip(whole, full):
+        np.testing.assert_array_equal(a, c)
+    for a, c in zip(subset, zeroed):
+        np.testing.assert_array_equal(a, c)
+    assert not np.array_equal(subset[0], full[0])
+    run_adapter(adapter_bin, tmp_path, b, solve, 0, mode=4, expect_rc=7)
