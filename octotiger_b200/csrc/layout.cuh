@@ -109,6 +109,14 @@ struct Tables {
     const double4* p2p_box;     // [8][216]: per parity, monopole constants over the 6^3 partner box (box
                                 // position (i, j, k) = offset + 2 + parity), zero off the stencil and at the cell
     const double4* p2p_cube;    // [343]: monopole constants of the offsets -3..3 per axis, zero at the centre
+    // P2M by coarse cell (reach 1): the 8 cells of a coarse cell share their partners in a direction
+    const int* pc_unit_start;   // [28]: first unit (4 coarse cells) of raw direction r
+    const int16_t* pc_coarse;   // [units][4]: coarse cell (x 16 + y 4 + z) of each unit slot, -1 past the end
+    const int2* pc_range;       // [27][64]: partner range in pc_list of coarse cell C in direction r
+    const uint16_t* pc_list;    // partner cells as indices into the direction's slab (see pc_slab_shape),
+                                // stencil order of the coarse cell's first cell
+    const int16_t* pc_slot;     // [27][64]: slot of coarse cell C among direction r's units, -1 if none
+    const int* pc_parts;        // [27]: parts each unit's partner lists of direction r are cut in
 };
 
 __device__ __forceinline__ int entry_sx(int y) { return (y & 15) - 8; }
@@ -152,7 +160,16 @@ struct ItemInfo {
 // ---------------------------------------------------------------- kernels
 // Device-side work lists, filled by classify_kernel: item indices per kind
 // and the counters the persistent launches take their tiles from.
-enum : int { WL_M2L = 0, WL_LEAF = 1, WL_P2M = 2, WL_M2L_NEXT = 3, WL_P2M_NEXT = 4, WL_ROOT = 5, WL_COUNTERS = 8 };
+enum : int {
+    WL_M2L = 0,
+    WL_LEAF = 1,
+    WL_P2M = 2,
+    WL_M2L_NEXT = 3,
+    WL_P2M_NEXT = 4,
+    WL_ROOT = 5,
+    WL_LEAF_NEXT = 6,
+    WL_COUNTERS = 8
+};
 struct WorkLists {
     int* m2l;      // refined, non-root items
     int* root;     // level-0 items

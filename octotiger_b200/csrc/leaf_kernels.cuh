@@ -263,7 +263,7 @@ __global__ void __launch_bounds__(P2_THREADS, 1) p2p_leaf_kernel(BatchArgs a) {
 // form T = float, FP32 partial sums promoted to FP64 every ROWS partner rows of
 // 6). With a stencil of coarse reach 1 the partners of a cell are the cells of
 // the 3x3x3 coarse cells around its own, a 6x6x6 box shared by the 8 cells of a
-// coarse cell. One CTA of 128 threads per leaf (grid stride over the leaves):
+// coarse cell. One CTA of 128 threads per leaf (CTAs take leaves from an atomic counter):
 // warp w takes the cells of x/y parity (w >> 1, w & 1); lane (Cx, Cy, c) the
 // four cells (2 Cx + px, 2 Cy + py, z), z in {2c, 2c + 1, 2c + 4, 2c + 5}.
 // A partner mass read from shared memory serves two of them (the two cells of
@@ -323,8 +323,13 @@ __global__ void __launch_bounds__(BOX_THREADS, 4) p2p_box_kernel(BatchArgs a) {
     const V4* tab_a = FULL ? s_four + (1 - px) * 49 + (1 - py) * 7 : s_four + (4 * px + 2 * py) * BOX_CELLS;
     const V4* tab_b = FULL ? tab_a : tab_a + BOX_CELLS;
     const int lane_off = (2 * Cx) * RXS + (2 * Cy) * RYS + 2 * c;
-    for (int kk = blockIdx.x; kk < nleaf; kk += gridDim.x) {
+    __shared__ int s_next;
+    for (;;) {
         __syncthreads();   // the previous leaf is done with `reg` and `it`
+        if (threadIdx.x == 0) s_next = atomicAdd(a.wl.counts + WL_LEAF_NEXT, 1);
+        __syncthreads();
+        const int kk = s_next;
+        if (kk >= nleaf) break;
         load_item(a, a.wl.leaf[kk], it);
         const double dc0 = 1.0 / it.dx;
         const uint32_t lm = it.leafmask | (1u << 13);   // the leaf itself and its leaf neighbours
@@ -548,8 +553,175 @@ __global__ void __launch_bounds__(P_THREADS) p2m_batch_kernel(BatchArgs a) {
     }
 }
 
+// Fast-form P2M by coarse cell (reach 1). The partners of a leaf cell in a
+// refined neighbour are the neighbour's cells inside the 3x3x3 coarse cells
+// around the cell's coarse cell, one list shared by the 8 cells of a coarse
+// cell, all inside the neighbour's slab next to the leaf (2 cells deep across
+// each shared face). Per leaf the refined directions are taken in rounds (in
+// raw-direction order, as many as fit the shared-memory budget): the round's
+// slabs are staged in shared memory (scaled moments and centres of mass), then
+// its units - 4 coarse cells of one direction - go to the warps, one lane per
+// cell (lane = 8 x slot + cell of the coarse cell), so the 8 lanes of a coarse
+// cell read each partner together. A direction's partner lists are cut in
+// parts of at most PC_PART partners (the same number of parts for all its
+// units), so that face units (72 partners) and corner units (8) make work
+// items of similar length. Each (item, cell) partial goes to shared memory; at
+// the end of the round every cell adds the round's partials to L (and L_c) in
+// direction, then part order. One CTA per leaf of the P2M work list (taken
+// from an atomic counter).
+constexpr int PC_THREADS = 256;
+constexpr int PC_PART = 24;               // partners of one work item (a unit's list is cut in parts)
+constexpr int PC_ROUND_ITEMS = 24;        // partials of one round: 24 x 32 x 7 doubles
+constexpr int PC_ROUND_CELLS = 320;       // staged slab cells of one round: 23 doubles each
+constexpr int PC_SMEM_BYTES = (PC_ROUND_ITEMS * 32 * 7 + 23 * PC_ROUND_CELLS) * 8;
+__device__ __forceinline__ void pc_slab_shape(int r, int lo[3], int n[3]) {
+    const int o[3] = {r % 3 - 1, (r / 3) % 3 - 1, r / 9 - 1};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        lo[d] = (o[d] == -1) ? INX - 2 : 0;
+        n[d] = (o[d] == 0) ? INX : 2;
+    }
+}
+
+template <bool RHO>
+__global__ void __launch_bounds__(PC_THREADS, 2) p2m_coarse_kernel(BatchArgs a) {
+    extern __shared__ double s_pc[];
+    double* part = s_pc;                              // [round items][32 lanes][7]: L0..L3, L_c x, y, z
+    double* slab = s_pc + PC_ROUND_ITEMS * 32 * 7;    // [23][PC_ROUND_CELLS]: 20 scaled moments, centre of mass
+    __shared__ ItemInfo it;
+    __shared__ int s_next, s_nr;
+    __shared__ int8_t s_rdir[27];                     // the round's directions, in order
+    __shared__ int s_rcell[28], s_ritem[28];          // their first slab cell / work item in the round
+    const int np2m = a.wl.counts[WL_P2M];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    for (;;) {
+        __syncthreads();   // `it` and the round tables are reused
+        if (threadIdx.x == 0) s_next = atomicAdd(a.wl.counts + WL_P2M_NEXT, 1);
+        __syncthreads();
+        const int kk = s_next;
+        if (kk >= np2m) break;
+        load_item(a, a.wl.p2m[kk], it);
+        const uint32_t refmask = it.nbmask & ~it.leafmask;
+        const size_t sub = (size_t)it.subgrid;
+        double* L = a.L + sub * 20 * NCELL;
+        double* Lc = a.Lc + sub * 3 * NCELL;
+        bool first_round = true;
+        for (int r0 = 0; r0 < 27;) {
+            if (threadIdx.x == 0) {
+                // the next round: directions from r0 on while slabs and units fit
+                int n = 0, cells = 0, items = 0, r = r0;
+                for (; r < 27; ++r) {
+                    if (!((refmask >> r) & 1u)) continue;
+                    int lo[3], sz[3];
+                    pc_slab_shape(r, lo, sz);
+                    const int c = sz[0] * sz[1] * sz[2];
+                    const int w = (a.t.pc_unit_start[r + 1] - a.t.pc_unit_start[r]) * a.t.pc_parts[r];
+                    if (n > 0 && (cells + c > PC_ROUND_CELLS || items + w > PC_ROUND_ITEMS)) break;
+                    s_rdir[n] = (int8_t)r;
+                    s_rcell[n] = cells;
+                    s_ritem[n] = items;
+                    cells += c;
+                    items += w;
+                    ++n;
+                }
+                s_rcell[n] = cells;
+                s_ritem[n] = items;
+                s_nr = n;
+                s_next = r;   // where the following round starts
+            }
+            __syncthreads();
+            const int nr = s_nr;
+            r0 = s_next;
+            // stage the round's slabs
+            for (int t = threadIdx.x; t < s_rcell[nr]; t += blockDim.x) {
+                int k = 0;
+                while (s_rcell[k + 1] <= t) ++k;
+                const int r = s_rdir[k], idx = t - s_rcell[k];
+                int lo[3], sz[3];
+                pc_slab_shape(r, lo, sz);
+                const int x = lo[0] + idx / (sz[1] * sz[2]), y = lo[1] + (idx / sz[2]) % sz[1], z = lo[2] + idx % sz[2];
+                const int u = x * 64 + y * 8 + z;
+                const size_t nb = (size_t)it.nb[r < 13 ? r : r - 1];
+#pragma unroll
+                for (int c = 0; c < 20; ++c)
+                    slab[c * PC_ROUND_CELLS + t] = __ldg(a.M + (nb * 20 + c) * NCELL + u) * stage_scale<PREC_FAST>(c);
+#pragma unroll
+                for (int q = 0; q < 3; ++q) slab[(20 + q) * PC_ROUND_CELLS + t] = __ldg(a.com + (nb * 3 + q) * NCELL + u);
+            }
+            __syncthreads();
+            // the round's work items: (unit, part) of each direction
+            for (int wi = warp; wi < s_ritem[nr]; wi += nwarps) {
+                int k = 0;
+                while (s_ritem[k + 1] <= wi) ++k;
+                const int r = s_rdir[k], np = a.t.pc_parts[r];
+                const int unit = (wi - s_ritem[k]) / np, pt = (wi - s_ritem[k]) % np;
+                const int slot = 4 * unit + (lane >> 3), ci = lane & 7;
+                const int C = __ldg(a.t.pc_coarse + 4 * a.t.pc_unit_start[r] + slot);
+                double acc[4] = {0.0, 0.0, 0.0, 0.0}, corr[3] = {0.0, 0.0, 0.0};
+                if (C >= 0) {
+                    const int cu = (2 * (C >> 4) + (ci & 1)) * 64 + (2 * ((C >> 2) & 3) + ((ci >> 1) & 1)) * 8 +
+                                   (2 * (C & 3) + (ci >> 2));
+                    double X[3];
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) X[q] = __ldg(a.com + (sub * 3 + q) * NCELL + cu);
+                    const int2 be = __ldg(a.t.pc_range + r * 64 + C);
+                    const double* sl = slab + s_rcell[k];
+                    const int q1 = min(be.y, be.x + (pt + 1) * PC_PART);
+#pragma unroll 1
+                    for (int q = be.x + pt * PC_PART; q < q1; ++q) {
+                        const int v = __ldg(a.t.pc_list + q);
+                        double Y[3], mp[20];
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) Y[c] = sl[(20 + c) * PC_ROUND_CELLS + v];
+#pragma unroll
+                        for (int c = 0; c < 20; ++c) mp[c] = sl[c * PC_ROUND_CELLS + v];
+                        fast_p2m_pair<RHO>(X, Y, mp, acc, corr);
+                    }
+                }
+                double* pp = part + ((size_t)wi * 32 + lane) * 7;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) pp[q] = acc[q];
+#pragma unroll
+                for (int q = 0; q < 3; ++q) pp[4 + q] = corr[q];
+            }
+            __syncthreads();
+            // every cell adds the round's partials in direction, then part order
+            for (int cu = threadIdx.x; cu < NCELL; cu += blockDim.x) {
+                const int cx = cu >> 6, cy = (cu >> 3) & 7, cz = cu & 7;
+                const int C = (cx >> 1) * 16 + (cy >> 1) * 4 + (cz >> 1);
+                const int ci = (cx & 1) | ((cy & 1) << 1) | ((cz & 1) << 2);
+                double acc[4], corr[3];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) acc[q] = L[q * NCELL + cu];
+#pragma unroll
+                for (int q = 0; q < 3; ++q) corr[q] = first_round ? 0.0 : Lc[q * NCELL + cu];
+                for (int k = 0; k < nr; ++k) {
+                    const int sl = __ldg(a.t.pc_slot + s_rdir[k] * 64 + C);
+                    if (sl < 0) continue;
+                    const int np = a.t.pc_parts[s_rdir[k]];
+                    for (int pt = 0; pt < np; ++pt) {
+                        const double* pp =
+                            part + ((size_t)(s_ritem[k] + (sl >> 2) * np + pt) * 32 + (sl & 3) * 8 + ci) * 7;
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) acc[q] += pp[q];
+#pragma unroll
+                        for (int q = 0; q < 3; ++q) corr[q] += pp[4 + q];
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < 4; ++q) L[q * NCELL + cu] = acc[q];
+#pragma unroll
+                for (int q = 0; q < 3; ++q) Lc[q * NCELL + cu] = RHO ? corr[q] : 0.0;
+            }
+            first_round = false;
+            __syncthreads();   // partials, slabs and the round tables are reused
+            if (nr == 0) break;
+        }
+    }
+}
+
 // Fast-form P2M with every refined direction of a leaf in flight at once:
-// one CTA per leaf of the P2M work list (grid stride). The work of a leaf is
+// one CTA per leaf of the P2M work list (taken from an atomic counter). The work of a leaf is
 // the list of (direction, cell, lane) slots of its refined directions, F lanes
 // per cell (F = the tuning's P2M lane count), walked in rounds of the CTA's
 // threads; the F lanes of a cell sum their partners' contributions in a fixed
@@ -562,10 +734,15 @@ __global__ void __launch_bounds__(P_THREADS) p2m_fast_kernel(BatchArgs a) {
     __shared__ ItemInfo it;
     __shared__ int s_dir[27], s_cum[28];
     __shared__ int s_ndir;
+    __shared__ int s_next;
     const int F = a.p2m_lanes;
     const int np2m = a.wl.counts[WL_P2M];
-    for (int kk = blockIdx.x; kk < np2m; kk += gridDim.x) {
+    for (;;) {
         __syncthreads();   // `it`, the direction list and s_part are reused
+        if (threadIdx.x == 0) s_next = atomicAdd(a.wl.counts + WL_P2M_NEXT, 1);
+        __syncthreads();
+        const int kk = s_next;
+        if (kk >= np2m) break;
         load_item(a, a.wl.p2m[kk], it);
         if (threadIdx.x == 0) {
             int n = 0, cum = 0;

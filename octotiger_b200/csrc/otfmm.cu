@@ -224,7 +224,20 @@ struct otfmm_context {
     double4* d_p2p_box = nullptr;    // [8][216] per-parity box constants
     double4* d_p2p_cube = nullptr;   // [343] constants of the offsets -3..3
     bool p2p_full_box = false;       // every parity's stencil is its whole 6^3 box
+    int* d_pc_unit_start = nullptr;  // coarse-cell P2M tables (reach 1)
+    int16_t* d_pc_coarse = nullptr;
+    int2* d_pc_range = nullptr;
+    uint16_t* d_pc_list = nullptr;
+    int16_t* d_pc_slot = nullptr;
+    int* d_pc_parts = nullptr;
+    int pc_units = 0;                // units over all 26 directions
+    bool pc_ok = false;              // the 8 cells of every coarse cell share their partners
     int box_grid[6] = {};            // resident CTAs of the box P2P kernels (all SMs)
+    // leaf kernels of a batched solve run on `aux`, forked after the
+    // classification and joined before the solve ends, so that they fill the
+    // SMs the multipole tiles leave idle
+    cudaStream_t aux = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int counts_far[8] = {};
     double* d_four = nullptr;
     uint8_t* d_phase = nullptr;
@@ -232,7 +245,7 @@ struct otfmm_context {
     double* d_soa_scratch = nullptr;   // host-buffer path staging
     int* d_lists = nullptr;            // batched work lists (grown on demand)
     int list_capacity = 0;
-    otfmm_tuning tuning = {OTFMM_SPLIT_WARP_SPECIALISED, 16, 32, 16, OTFMM_P2P_BOX};
+    otfmm_tuning tuning = {OTFMM_SPLIT_WARP_SPECIALISED, 16, 32, 4, OTFMM_P2P_BOX, OTFMM_P2M_LANES};
     // otfmm_batch_host: device copies of the pool, work list and outputs, a
     // pinned host copy of the reordered work list, two copy streams and events
     struct HostPath {
@@ -250,7 +263,8 @@ struct otfmm_context {
     Tables tables() const { return Tables{d_entries,    d_count, d_entries_fast, d_count_far, d_entries_split, d_entries_p2p,
                       d_entries_ws, d_four,  d_phase,        d_p2m_start,     d_p2m_list,    d_p2m_perm_start,
                       d_p2m_perm,   d_p2m_slot,     d_p2p_four,      d_entries_r2,  d_r2_sx_start, d_r2_four,
-                      d_p2p_box,    d_p2p_cube}; }
+                      d_p2p_box,    d_p2p_cube,     d_pc_unit_start, d_pc_coarse,  d_pc_range,    d_pc_list,
+                      d_pc_slot,    d_pc_parts}; }
 };
 
 namespace {
@@ -311,6 +325,8 @@ int ensure_attributes(int device) {
     rc = rc ? rc : set_smem(m2l_r2_kernel<PREC_FAST, false>, PL_SMEM_BYTES);
     rc = rc ? rc : set_smem(p2p_r2_kernel<PREC_EXACT>, R2_SMEM_BYTES);
     rc = rc ? rc : set_smem(p2p_r2_kernel<PREC_FAST>, R2_SMEM_BYTES);
+    rc = rc ? rc : set_smem(p2m_coarse_kernel<true>, PC_SMEM_BYTES);
+    rc = rc ? rc : set_smem(p2m_coarse_kernel<false>, PC_SMEM_BYTES);
     rc = rc ? rc : set_smem(p2m_fast_kernel<true>, 7 * 8 * 6 * NCELL);
     rc = rc ? rc : set_smem(p2m_fast_kernel<false>, 7 * 8 * 6 * NCELL);
     rc = rc ? rc : set_smem(soa_m2l_kernel<PREC_EXACT, true, false>, bytes);
@@ -520,6 +536,65 @@ int otfmm_create(int device, double theta, otfmm_context** out) {
         for (int t = p2m_perm_start[r]; t < p2m_perm_start[r + 1]; ++t)
             p2m_slot[r * NCELL + p2m_perm[t]] = (int16_t)(t - p2m_perm_start[r]);
     ctx->p2m_groups_max = (int)p2m_perm.size();
+    // P2M by coarse cell (reach 1): per direction, the coarse cells with
+    // partners there (4 per unit) and their shared partner list
+    std::vector<int> pc_unit_start(28, 0);
+    std::vector<int16_t> pc_coarse;
+    std::vector<int2> pc_range(27 * 64, int2{0, 0});
+    std::vector<uint16_t> pc_list;
+    std::vector<int16_t> pc_slot(27 * 64, -1);
+    ctx->pc_ok = (ctx->reach <= 1);
+    for (int r = 0; r < 27 && ctx->pc_ok; ++r) {
+        pc_unit_start[r] = (int)pc_coarse.size() / 4;
+        int nslot = 0;
+        for (int C = 0; C < 64 && r != 13; ++C) {
+            const int Cx = C >> 4, Cy = (C >> 2) & 3, Cz = C & 3;
+            std::vector<uint16_t> first;
+            for (int ci = 0; ci < 8; ++ci) {
+                const int cu = (2 * Cx + (ci & 1)) * 64 + (2 * Cy + ((ci >> 1) & 1)) * 8 + (2 * Cz + (ci >> 2));
+                std::vector<uint16_t> l(p2m_list.begin() + p2m_start[cu * 28 + r],
+                                        p2m_list.begin() + p2m_start[cu * 28 + r + 1]);
+                if (ci == 0) {
+                    first = l;
+                } else {
+                    std::vector<uint16_t> a0 = first, a1 = l;
+                    std::sort(a0.begin(), a0.end());
+                    std::sort(a1.begin(), a1.end());
+                    if (a0 != a1) ctx->pc_ok = false;
+                }
+            }
+            if (first.empty()) continue;
+            // partner cells as indices into the direction's slab (the cells 2 deep
+            // across each shared face, whole rows along the others)
+            const int o[3] = {r % 3 - 1, (r / 3) % 3 - 1, r / 9 - 1};
+            int lo[3], n[3];
+            for (int d = 0; d < 3; ++d) {
+                lo[d] = (o[d] == -1) ? INX - 2 : 0;
+                n[d] = (o[d] == 0) ? INX : 2;
+            }
+            pc_range[r * 64 + C] = int2{(int)pc_list.size(), (int)(pc_list.size() + first.size())};
+            for (uint16_t u : first) {
+                const int x = (u >> 6) - lo[0], y = ((u >> 3) & 7) - lo[1], z = (u & 7) - lo[2];
+                if (x < 0 || x >= n[0] || y < 0 || y >= n[1] || z < 0 || z >= n[2]) ctx->pc_ok = false;
+                pc_list.push_back((uint16_t)((x * n[1] + y) * n[2] + z));
+            }
+            pc_slot[r * 64 + C] = (int16_t)nslot++;
+            pc_coarse.push_back((int16_t)C);
+        }
+        while (pc_coarse.size() % 4) pc_coarse.push_back(-1);
+    }
+    pc_unit_start[27] = (int)pc_coarse.size() / 4;
+    ctx->pc_units = pc_unit_start[27];
+    // parts per unit of each direction: its longest partner list cut in PC_PART pieces
+    std::vector<int> pc_parts(27, 1);
+    for (int r = 0; r < 27; ++r) {
+        int longest = 0;
+        for (int C = 0; C < 64; ++C) longest = std::max(longest, pc_range[r * 64 + C].y - pc_range[r * 64 + C].x);
+        pc_parts[r] = std::max(1, (longest + PC_PART - 1) / PC_PART);
+        if ((pc_unit_start[r + 1] - pc_unit_start[r]) * pc_parts[r] > PC_ROUND_ITEMS) ctx->pc_ok = false;
+    }
+    if (pc_coarse.empty()) pc_coarse.assign(4, -1);
+    if (pc_list.empty()) pc_list.assign(1, 0);
     DeviceGuard g(device);
     cudaError_t e;
     if ((e = cudaMalloc(&ctx->d_r2_four, sizeof(double4) * r2_four.size())) != cudaSuccess ||
@@ -533,6 +608,24 @@ int otfmm_create(int device, double theta, otfmm_context** out) {
                         cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMalloc(&ctx->d_p2m_slot, sizeof(int16_t) * p2m_slot.size())) != cudaSuccess ||
         (e = cudaMemcpy(ctx->d_p2m_slot, p2m_slot.data(), sizeof(int16_t) * p2m_slot.size(),
+                        cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMalloc(&ctx->d_pc_unit_start, sizeof(int) * pc_unit_start.size())) != cudaSuccess ||
+        (e = cudaMemcpy(ctx->d_pc_unit_start, pc_unit_start.data(), sizeof(int) * pc_unit_start.size(),
+                        cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMalloc(&ctx->d_pc_coarse, sizeof(int16_t) * pc_coarse.size())) != cudaSuccess ||
+        (e = cudaMemcpy(ctx->d_pc_coarse, pc_coarse.data(), sizeof(int16_t) * pc_coarse.size(),
+                        cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMalloc(&ctx->d_pc_range, sizeof(int2) * pc_range.size())) != cudaSuccess ||
+        (e = cudaMemcpy(ctx->d_pc_range, pc_range.data(), sizeof(int2) * pc_range.size(),
+                        cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMalloc(&ctx->d_pc_list, sizeof(uint16_t) * pc_list.size())) != cudaSuccess ||
+        (e = cudaMemcpy(ctx->d_pc_list, pc_list.data(), sizeof(uint16_t) * pc_list.size(),
+                        cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMalloc(&ctx->d_pc_parts, sizeof(int) * pc_parts.size())) != cudaSuccess ||
+        (e = cudaMemcpy(ctx->d_pc_parts, pc_parts.data(), sizeof(int) * pc_parts.size(),
+                        cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMalloc(&ctx->d_pc_slot, sizeof(int16_t) * pc_slot.size())) != cudaSuccess ||
+        (e = cudaMemcpy(ctx->d_pc_slot, pc_slot.data(), sizeof(int16_t) * pc_slot.size(),
                         cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMalloc(&ctx->d_p2p_box, sizeof(double4) * p2p_box.size())) != cudaSuccess ||
         (e = cudaMemcpy(ctx->d_p2p_box, p2p_box.data(), sizeof(double4) * p2p_box.size(),
@@ -585,6 +678,12 @@ int otfmm_create(int device, double theta, otfmm_context** out) {
         otfmm_destroy(ctx);
         return cuda_fail(e, "otfmm_create");
     }
+    if ((e = cudaStreamCreateWithFlags(&ctx->aux, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming)) != cudaSuccess) {
+        otfmm_destroy(ctx);
+        return cuda_fail(e, "otfmm_create");
+    }
     int rc = ensure_attributes(device);
     if (rc == OTFMM_OK) rc = box_occupancy(ctx);
     if (rc != OTFMM_OK) {
@@ -611,6 +710,18 @@ int otfmm_destroy(otfmm_context* ctx) {
     cudaFree(ctx->d_p2p_four);
     cudaFree(ctx->d_p2p_box);
     cudaFree(ctx->d_p2p_cube);
+    cudaFree(ctx->d_pc_unit_start);
+    cudaFree(ctx->d_pc_coarse);
+    cudaFree(ctx->d_pc_range);
+    cudaFree(ctx->d_pc_list);
+    cudaFree(ctx->d_pc_slot);
+    cudaFree(ctx->d_pc_parts);
+    if (ctx->aux) {
+        cudaStreamSynchronize(ctx->aux);
+        cudaStreamDestroy(ctx->aux);
+    }
+    if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+    if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
     cudaFree(ctx->d_p2m_slot);
     cudaFree(ctx->d_entries_r2);
     cudaFree(ctx->d_r2_sx_start);
@@ -853,6 +964,7 @@ int check_tuning(const otfmm_tuning& t) {
     if (t.split_p2p_chunk != 16 && t.split_p2p_chunk != 32) return fail(OTFMM_ERR_INVALID, "split P2P chunk must be 16 or 32");
     if (t.p2m_lanes != 4 && t.p2m_lanes != 8 && t.p2m_lanes != 16) return fail(OTFMM_ERR_INVALID, "P2M lanes must be 4, 8 or 16");
     if (t.p2p_form != OTFMM_P2P_BOX && t.p2p_form != OTFMM_P2P_STENCIL) return fail(OTFMM_ERR_INVALID, "unknown P2P form");
+    if (t.p2m_form != OTFMM_P2M_COARSE && t.p2m_form != OTFMM_P2M_LANES) return fail(OTFMM_ERR_INVALID, "unknown P2M form");
     return OTFMM_OK;
 }
 
@@ -918,14 +1030,24 @@ int enqueue_batch(otfmm_context* ctx, const double* pool_M, const double* pool_c
         OT_CUDA(cudaGetLastError());
         return OTFMM_OK;
     }
+    // The leaf kernels (P2P, then P2M: the reference's order) write other
+    // subgrids than the tiles, so outside profiling they run on the context's
+    // aux stream beside the tiles and start on SMs as the tile CTAs retire.
+    const bool fork = (marks == nullptr);
+    cudaStream_t ls = s;
+    if (fork) {
+        OT_CUDA(cudaEventRecord(ctx->ev_fork, s));
+        OT_CUDA(cudaStreamWaitEvent(ctx->aux, ctx->ev_fork, 0));
+        ls = ctx->aux;
+    }
     if (precision == OTFMM_FP64_EXACT) {
         if (rho) m2l_batch_kernel<PREC_EXACT, true><<<tiles_grid, THREADS, bytes, s>>>(a);
         else m2l_batch_kernel<PREC_EXACT, false><<<tiles_grid, THREADS, bytes, s>>>(a);
         mark(2);
-        p2p_batch_kernel<PREC_EXACT><<<p2p_grid, P2P_THREADS, P2P_SMEM_BYTES, s>>>(a);
+        p2p_batch_kernel<PREC_EXACT><<<p2p_grid, P2P_THREADS, P2P_SMEM_BYTES, ls>>>(a);
         mark(3);
-        if (rho) p2m_batch_kernel<PREC_EXACT, true><<<p2m_grid, P_THREADS, 0, s>>>(a);
-        else p2m_batch_kernel<PREC_EXACT, false><<<p2m_grid, P_THREADS, 0, s>>>(a);
+        if (rho) p2m_batch_kernel<PREC_EXACT, true><<<p2m_grid, P_THREADS, 0, ls>>>(a);
+        else p2m_batch_kernel<PREC_EXACT, false><<<p2m_grid, P_THREADS, 0, ls>>>(a);
     } else {
         if (precision == OTFMM_FP32_SPLIT) {
             const size_t sbytes = S_SMEM_DOUBLES * sizeof(double);
@@ -947,32 +1069,41 @@ int enqueue_batch(otfmm_context* ctx, const double* pool_M, const double* pool_c
             if (tu.p2p_form == OTFMM_P2P_BOX) {
                 const bool full = ctx->p2p_full_box;
                 if (tu.split_p2p_chunk == 16) {
-                    if (full) p2p_box_kernel<float, true, 3><<<ctx->box_grid[2], BOX_THREADS, box_smem_bytes<float, true>(), s>>>(a);
-                    else p2p_box_kernel<float, false, 3><<<ctx->box_grid[4], BOX_THREADS, box_smem_bytes<float, false>(), s>>>(a);
+                    if (full) p2p_box_kernel<float, true, 3><<<ctx->box_grid[2], BOX_THREADS, box_smem_bytes<float, true>(), ls>>>(a);
+                    else p2p_box_kernel<float, false, 3><<<ctx->box_grid[4], BOX_THREADS, box_smem_bytes<float, false>(), ls>>>(a);
                 } else {
-                    if (full) p2p_box_kernel<float, true, 6><<<ctx->box_grid[3], BOX_THREADS, box_smem_bytes<float, true>(), s>>>(a);
-                    else p2p_box_kernel<float, false, 6><<<ctx->box_grid[5], BOX_THREADS, box_smem_bytes<float, false>(), s>>>(a);
+                    if (full) p2p_box_kernel<float, true, 6><<<ctx->box_grid[3], BOX_THREADS, box_smem_bytes<float, true>(), ls>>>(a);
+                    else p2p_box_kernel<float, false, 6><<<ctx->box_grid[5], BOX_THREADS, box_smem_bytes<float, false>(), ls>>>(a);
                 }
             } else if (tu.split_p2p_chunk == 16) {
-                p2p_leaf_kernel<float, 16><<<sms, P2_THREADS, p2_smem_bytes<float>(), s>>>(a);
+                p2p_leaf_kernel<float, 16><<<sms, P2_THREADS, p2_smem_bytes<float>(), ls>>>(a);
             } else {
-                p2p_leaf_kernel<float, 32><<<sms, P2_THREADS, p2_smem_bytes<float>(), s>>>(a);
+                p2p_leaf_kernel<float, 32><<<sms, P2_THREADS, p2_smem_bytes<float>(), ls>>>(a);
             }
         } else {
             if (rho) m2l_batch_kernel<PREC_FAST, true><<<tiles_grid, THREADS, bytes, s>>>(a);
             else m2l_batch_kernel<PREC_FAST, false><<<tiles_grid, THREADS, bytes, s>>>(a);
             mark(2);
             if (tu.p2p_form == OTFMM_P2P_BOX) {
-                if (ctx->p2p_full_box) p2p_box_kernel<double, true, 6><<<ctx->box_grid[0], BOX_THREADS, box_smem_bytes<double, true>(), s>>>(a);
-                else p2p_box_kernel<double, false, 6><<<ctx->box_grid[1], BOX_THREADS, box_smem_bytes<double, false>(), s>>>(a);
+                if (ctx->p2p_full_box) p2p_box_kernel<double, true, 6><<<ctx->box_grid[0], BOX_THREADS, box_smem_bytes<double, true>(), ls>>>(a);
+                else p2p_box_kernel<double, false, 6><<<ctx->box_grid[1], BOX_THREADS, box_smem_bytes<double, false>(), ls>>>(a);
             } else {
-                p2p_leaf_kernel<double, 0><<<sms, P2_THREADS, p2_smem_bytes<double>(), s>>>(a);
+                p2p_leaf_kernel<double, 0><<<sms, P2_THREADS, p2_smem_bytes<double>(), ls>>>(a);
             }
         }
         mark(3);
-        const size_t part_bytes = sizeof(double) * 7 * (size_t)ctx->p2m_groups_max;
-        if (rho) p2m_fast_kernel<true><<<p2m_grid, P_THREADS, part_bytes, s>>>(a);
-        else p2m_fast_kernel<false><<<p2m_grid, P_THREADS, part_bytes, s>>>(a);
+        if (tu.p2m_form == OTFMM_P2M_COARSE && ctx->pc_ok) {
+            if (rho) p2m_coarse_kernel<true><<<p2m_grid, PC_THREADS, PC_SMEM_BYTES, ls>>>(a);
+            else p2m_coarse_kernel<false><<<p2m_grid, PC_THREADS, PC_SMEM_BYTES, ls>>>(a);
+        } else {
+            const size_t part_bytes = sizeof(double) * 7 * (size_t)ctx->p2m_groups_max;
+            if (rho) p2m_fast_kernel<true><<<p2m_grid, P_THREADS, part_bytes, ls>>>(a);
+            else p2m_fast_kernel<false><<<p2m_grid, P_THREADS, part_bytes, ls>>>(a);
+        }
+    }
+    if (fork) {
+        OT_CUDA(cudaEventRecord(ctx->ev_join, ls));
+        OT_CUDA(cudaStreamWaitEvent(s, ctx->ev_join, 0));
     }
     mark(4);
     OT_CUDA(cudaGetLastError());
@@ -1361,9 +1492,9 @@ int otfmm_autotune(otfmm_context* ctx, const double* pool_M, const double* pool_
     rc = time_of(best, tbest);
     const int forms[3] = {OTFMM_SPLIT_WARP_SPECIALISED_PACKED, OTFMM_SPLIT_WARP_SPECIALISED, OTFMM_SPLIT_SINGLE_ROLE};
     const int m2l_chunks[2] = {8, 16}, p2p_chunks[2] = {16, 32}, lanes[3] = {4, 8, 16};
-    const int p2p_forms[2] = {OTFMM_P2P_BOX, OTFMM_P2P_STENCIL};
+    const int p2p_forms[2] = {OTFMM_P2P_BOX, OTFMM_P2P_STENCIL}, p2m_forms[2] = {OTFMM_P2M_LANES, OTFMM_P2M_COARSE};
     const bool split = (precision == OTFMM_FP32_SPLIT), fast = (precision != OTFMM_FP64_EXACT);
-    for (int dim = 0; dim < 5 && rc == OTFMM_OK; ++dim) {
+    for (int dim = 0; dim < 6 && rc == OTFMM_OK; ++dim) {
         const int nvar = (dim == 3 || dim == 0) ? 3 : 2;
         if ((dim < 3 && !split) || (dim >= 3 && !fast)) continue;
         for (int v = 0; v < nvar && rc == OTFMM_OK; ++v) {
@@ -1373,6 +1504,7 @@ int otfmm_autotune(otfmm_context* ctx, const double* pool_M, const double* pool_
             if (dim == 2) tu.split_p2p_chunk = p2p_chunks[v];
             if (dim == 3) tu.p2m_lanes = lanes[v];
             if (dim == 4) tu.p2p_form = p2p_forms[v];
+            if (dim == 5) tu.p2m_form = p2m_forms[v];
             if (std::memcmp(&tu, &best, sizeof tu) == 0) continue;
             float t = 0.f;
             rc = time_of(tu, t);

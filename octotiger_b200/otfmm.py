@@ -36,17 +36,20 @@ _lib = None
 SPLIT_WARP_SPECIALISED, SPLIT_SINGLE_ROLE, SPLIT_WARP_SPECIALISED_PACKED = 0, 1, 2
 SPLIT_FORMS = {0: "warp_specialised", 1: "single_role", 2: "warp_specialised_packed"}
 P2P_FORMS = {0: "box", 1: "stencil"}
+P2M_FORMS = {0: "coarse", 1: "lanes"}
 
 
 class Tuning(ctypes.Structure):
     """otfmm_tuning: the kernel variants of the batched solve."""
     _fields_ = [("split_m2l_form", ctypes.c_int32), ("split_m2l_chunk", ctypes.c_int32),
-                ("split_p2p_chunk", ctypes.c_int32), ("p2m_lanes", ctypes.c_int32), ("p2p_form", ctypes.c_int32)]
+                ("split_p2p_chunk", ctypes.c_int32), ("p2m_lanes", ctypes.c_int32), ("p2p_form", ctypes.c_int32),
+                ("p2m_form", ctypes.c_int32)]
 
     def as_dict(self) -> dict:
         return {"split_m2l_form": SPLIT_FORMS.get(self.split_m2l_form, str(self.split_m2l_form)),
                 "split_m2l_chunk": self.split_m2l_chunk, "split_p2p_chunk": self.split_p2p_chunk,
-                "p2m_lanes": self.p2m_lanes, "p2p_form": P2P_FORMS.get(self.p2p_form, str(self.p2p_form))}
+                "p2m_lanes": self.p2m_lanes, "p2p_form": P2P_FORMS.get(self.p2p_form, str(self.p2p_form)),
+                "p2m_form": P2M_FORMS.get(self.p2m_form, str(self.p2m_form))}
 
 
 class OtfmmError(RuntimeError):

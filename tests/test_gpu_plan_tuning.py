@@ -60,6 +60,7 @@ def test_plan_replays_batch(ctx, precision, solve):
 
 VARIANTS = list(itertools.product([0, 1, 2], [8, 16], [16, 32], [4, 8, 16]))
 P2P_FORMS = (0, 1)   # OTFMM_P2P_BOX, OTFMM_P2P_STENCIL
+P2M_FORMS = (0, 1)   # OTFMM_P2M_COARSE, OTFMM_P2M_LANES
 
 
 @pytest.mark.parametrize("form,m2l_chunk,p2p_chunk,lanes", VARIANTS)
@@ -69,7 +70,7 @@ def test_every_variant_within_tolerance(ctx, oracle, form, m2l_chunk, p2p_chunk,
     Lo, Lco = oracle.batch(0.5, b.pool, b.items, rho=True)
     keep = ctx.get_tuning()
     try:
-        ctx.set_tuning(Tuning(form, m2l_chunk, p2p_chunk, lanes))
+        ctx.set_tuning(Tuning(form, m2l_chunk, p2p_chunk, lanes, 0, 1))
         s = BatchSolver(ctx, b.pool, b.items)
         s.run(RHO, "fp32_split")
         L, Lc = s.results()
@@ -84,10 +85,10 @@ def test_every_variant_within_tolerance(ctx, oracle, form, m2l_chunk, p2p_chunk,
 
 
 @pytest.mark.parametrize("theta", [0.5, 0.7])
-@pytest.mark.parametrize("p2p_form", P2P_FORMS)
+@pytest.mark.parametrize("p2p_form,p2m_form", list(itertools.product(P2P_FORMS, P2M_FORMS)))
 @pytest.mark.parametrize("precision,p2p_chunk", [("fp64", 32), ("fp32_split", 16), ("fp32_split", 32)])
-def test_p2p_forms_within_tolerance(oracle, theta, p2p_form, precision, p2p_chunk):
-    """Both leaf P2P forms, with the partner box full (theta = 0.5: every
+def test_leaf_forms_within_tolerance(oracle, theta, p2p_form, p2m_form, precision, p2p_chunk):
+    """The leaf P2P and P2M forms, with the partner box full (theta = 0.5: every
     parity's stencil is its whole 6^3 box, one table of offsets) and partial
     (theta = 0.7: the coarse corners drop out, per-parity masked tables)."""
     from octotiger_b200.otfmm import BatchSolver, Context, Tuning
@@ -95,7 +96,7 @@ def test_p2p_forms_within_tolerance(oracle, theta, p2p_form, precision, p2p_chun
     Lo, Lco = oracle.batch(theta, b.pool, b.items, rho=True)
     c = Context(0, theta)
     try:
-        c.set_tuning(Tuning(0, 16, p2p_chunk, 16, p2p_form))
+        c.set_tuning(Tuning(0, 16, p2p_chunk, 8, p2p_form, p2m_form))
         s = BatchSolver(c, b.pool, b.items)
         s.run(RHO, precision)
         L, Lc = s.results()
@@ -117,7 +118,7 @@ def test_autotune_keeps_an_allowed_variant(ctx, oracle):
         s = BatchSolver(ctx, b.pool, b.items)
         t = s.autotune(RHO, "fp32_split", repeats=2)
         assert (t.split_m2l_form, t.split_m2l_chunk, t.split_p2p_chunk, t.p2m_lanes) in VARIANTS
-        assert t.p2p_form in P2P_FORMS
+        assert t.p2p_form in P2P_FORMS and t.p2m_form in P2M_FORMS
         got = ctx.get_tuning()
         assert got.as_dict() == t.as_dict()
         s.run(RHO, "fp32_split")
@@ -132,7 +133,7 @@ def test_invalid_variants_rejected(ctx):
     from octotiger_b200.otfmm import OtfmmError, Tuning
     keep = ctx.get_tuning()
     for bad in (Tuning(3, 16, 32, 16), Tuning(0, 12, 32, 16), Tuning(0, 16, 8, 16), Tuning(0, 16, 32, 3),
-                Tuning(0, 16, 32, 16, 2)):
+                Tuning(0, 16, 32, 16, 2), Tuning(0, 16, 32, 16, 0, 2)):
         with pytest.raises(OtfmmError):
             ctx.set_tuning(bad)
     assert ctx.get_tuning().as_dict() == keep.as_dict()
