@@ -295,8 +295,22 @@ static_assert(11 * BoxLayout<float>::RYS + 12 <= BoxLayout<float>::RXS &&
                   11 * BoxLayout<double>::RYS + 12 <= BoxLayout<double>::RXS,
               "box region rows fit their planes");
 
-__device__ __forceinline__ float box_fma(float x, float y, float z) { return fmaf(x, y, z); }
-__device__ __forceinline__ double box_fma(double x, double y, double z) { return fma(x, y, z); }
+// f[0..3] += q * m: FP32 as two packed FMAs (x, y) and (z, w); FP64 as four.
+__device__ __forceinline__ void box_fma4(const float4& q, float m, float f[4]) {
+    const float2 mm = make_float2(m, m);
+    const float2 lo = __ffma2_rn(make_float2(q.x, q.y), mm, make_float2(f[0], f[1]));
+    const float2 hi = __ffma2_rn(make_float2(q.z, q.w), mm, make_float2(f[2], f[3]));
+    f[0] = lo.x;
+    f[1] = lo.y;
+    f[2] = hi.x;
+    f[3] = hi.y;
+}
+__device__ __forceinline__ void box_fma4(const double4& q, double m, double f[4]) {
+    f[0] = fma(q.x, m, f[0]);
+    f[1] = fma(q.y, m, f[1]);
+    f[2] = fma(q.z, m, f[2]);
+    f[3] = fma(q.w, m, f[3]);
+}
 
 template <class T, bool FULL, int ROWS>
 __global__ void __launch_bounds__(BOX_THREADS, 4) p2p_box_kernel(BatchArgs a) {
@@ -406,22 +420,10 @@ __global__ void __launch_bounds__(BOX_THREADS, 4) p2p_box_kernel(BatchArgs a) {
 #pragma unroll
                 for (int k = 0; k < 6; ++k) {
                     const T mA = m[k], mC = m[k + 4];
-                    f[0][0] = box_fma(qa[k].x, mA, f[0][0]);
-                    f[0][1] = box_fma(qa[k].y, mA, f[0][1]);
-                    f[0][2] = box_fma(qa[k].z, mA, f[0][2]);
-                    f[0][3] = box_fma(qa[k].w, mA, f[0][3]);
-                    f[1][0] = box_fma(qb[k].x, mA, f[1][0]);
-                    f[1][1] = box_fma(qb[k].y, mA, f[1][1]);
-                    f[1][2] = box_fma(qb[k].z, mA, f[1][2]);
-                    f[1][3] = box_fma(qb[k].w, mA, f[1][3]);
-                    f[2][0] = box_fma(qa[k].x, mC, f[2][0]);
-                    f[2][1] = box_fma(qa[k].y, mC, f[2][1]);
-                    f[2][2] = box_fma(qa[k].z, mC, f[2][2]);
-                    f[2][3] = box_fma(qa[k].w, mC, f[2][3]);
-                    f[3][0] = box_fma(qb[k].x, mC, f[3][0]);
-                    f[3][1] = box_fma(qb[k].y, mC, f[3][1]);
-                    f[3][2] = box_fma(qb[k].z, mC, f[3][2]);
-                    f[3][3] = box_fma(qb[k].w, mC, f[3][3]);
+                    box_fma4(qa[k], mA, f[0]);
+                    box_fma4(qb[k], mA, f[1]);
+                    box_fma4(qa[k], mC, f[2]);
+                    box_fma4(qb[k], mC, f[3]);
                 }
                 if constexpr (sizeof(T) == 4) {
                     if ((j % ROWS) != ROWS - 1) continue;
