@@ -125,11 +125,21 @@ def _solve_errors(oracle, theta):
     pos = com[leaf].transpose(0, 2, 1).reshape(-1, 3)
     mass = pool.mon[leaf].reshape(-1)
     pick = np.random.default_rng(3).choice(len(pos), 400, replace=False)
-    d = pos[pick, None, :] - pos[None, :, :]
-    r = np.sqrt((d ** 2).sum(-1))
-    r[np.arange(len(pick)), pick] = np.inf
-    phi = -(mass[None, :] / r).sum(1)
-    g = -(mass[None, :, None] * d / r[..., None] ** 3).sum(1)
+    phi = np.empty(len(pick))
+    g = np.empty((len(pick), 3))
+    pt = np.ascontiguousarray(pos.T)   # [3][N]
+    d = np.empty((3, len(pos)))
+    r2 = np.empty(len(pos))
+    w = np.empty(len(pos))
+    for t, c in enumerate(pick):   # one target at a time, buffers reused
+        np.subtract(pos[c][:, None], pt, out=d)   # x_target - x_j
+        np.einsum("kn,kn->n", d, d, out=r2)
+        r2[c] = np.inf
+        np.sqrt(r2, out=w)
+        np.divide(mass, w, out=w)                 # m / r
+        phi[t] = -w.sum()
+        np.divide(w, r2, out=w)                   # m / r^3
+        g[t] = -(d @ w)
     Gl = G[leaf].transpose(0, 2, 1).reshape(-1, 4)[pick]
     return np.abs(Gl[:, 0] - phi).max() / np.abs(phi).max(), np.abs(Gl[:, 1:] - g).max() / np.abs(g).max()
 
