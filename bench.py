@@ -349,10 +349,15 @@ def gpu_arm(args) -> None:
     pin = {k: torch.from_numpy(getattr(batch.pool, k)).pin_memory() for k in ("M", "com", "mon", "is_leaf")}
     items_h = order_work_list(batch.items)
     items_pin = torch.from_numpy(items_h.view(np.uint8).reshape(-1).copy()).pin_memory()
-    L_pin = torch.empty(solver.L.shape, dtype=torch.float64).pin_memory()
-    Lc_pin = torch.empty(solver.Lc.shape, dtype=torch.float64).pin_memory()
-    h2d = sum(t.numel() * t.element_size() for t in pin.values()) + items_pin.numel()
-    d2h = L_pin.numel() * 8 + Lc_pin.numel() * 8
+    # zeroed once, as node_server::compute_fmm zeroes L before the kernels: the
+    # call writes every result but leaves the leaves' L4..L19 (no kernel writes them)
+    L_pin = torch.zeros(solver.L.shape, dtype=torch.float64).pin_memory()
+    Lc_pin = torch.zeros(solver.Lc.shape, dtype=torch.float64).pin_memory()
+    # bytes the call uploads: the moments of refined subgrids only (no kernel reads a leaf's moments)
+    m_bytes = int((batch.pool.is_leaf == 0).sum()) * 20 * 512 * 8
+    h2d = m_bytes + sum(pin[k].numel() * pin[k].element_size() for k in ("com", "mon", "is_leaf")) + items_pin.numel()
+    n_leaf = int((batch.pool.is_leaf == 1).sum())
+    d2h = L_pin.numel() * 8 - n_leaf * 16 * 512 * 8 + Lc_pin.numel() * 8
 
     def e2e_step():
         ctx.batch_host(pin["M"], pin["com"], pin["mon"], pin["is_leaf"], batch.pool.n, items_pin, len(items_h),
@@ -373,6 +378,13 @@ def gpu_arm(args) -> None:
         e1.synchronize()
         e2e_ms += e0.elapsed_time(e1)
     ctx.batch_status()
+    # the host results equal the resident-pool solve's (outside the timed region)
+    plans[args.precision].launch(stream)
+    torch.cuda.synchronize()
+    leaf = torch.from_numpy(batch.pool.is_leaf == 1)
+    Ld = solver.L.cpu()
+    e2e_matches = bool(torch.equal(L_pin[~leaf], Ld[~leaf]) and torch.equal(L_pin[leaf, :4], Ld[leaf, :4])
+                       and torch.equal(Lc_pin, solver.Lc.cpu()))
     if pg:
         t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
@@ -469,7 +481,8 @@ def gpu_arm(args) -> None:
         "ratios": {"vs_batched_fp64": (value / world / others["fp64"]["value"]) if "fp64" in others else None,
                    "vs_per_subgrid_fp64": (value / world / per_subgrid["value"]) if per_subgrid else None},
         "accuracy_vs_fp64_exact": accuracy,
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                "matches_device_solve": e2e_matches},
         "gpu_launches": 4 * args.steps,
         "roofline": roof,
         "clocks": clk.summary(),

@@ -246,11 +246,14 @@ int otfmm_plan_status(otfmm_plan* plan, void* stream);
 int otfmm_plan_destroy(otfmm_plan* plan);
 
 /* Batched solve from host buffers (pinned memory lets the copies overlap):
- * pool and work list as for otfmm_batch but in host memory; writes the whole
- * of the host outputs L[n][20][512] and L_c[n][3][512]: the solve's results,
- * zeros elsewhere (node_server::compute_fmm zeroes L / L_c before the
- * reference's kernels, src/node_server.cpp:701-705). The pool is uploaded in
- * chunks of consecutive subgrids; each work item runs once the records it
+ * pool and work list as for otfmm_batch but in host memory; writes the host
+ * outputs L[n][20][512] and L_c[n][3][512]: the solve's results, zeros where
+ * it computes nothing, as node_server::compute_fmm zeroes L / L_c before the
+ * reference's kernels (src/node_server.cpp:701-705) - except L[4..19] of leaf
+ * subgrids, which no kernel writes (the reference's monopole kernels output
+ * L[0..3] and L_c) and which are left as the caller set them. The pool is uploaded in
+ * chunks of consecutive subgrids (the moments of refined subgrids only: leaves
+ * enter the kernels as masses at their cell centres); each work item runs once the records it
  * reads have arrived and each output range is copied back once final, on two
  * copy streams, so uploads, kernels and downloads overlap when neighbours have
  * nearby pool indices. Device copies live in the context (grown on demand).

@@ -23,8 +23,7 @@ namespace otfmm {
 // p2m_interaction_interface.hpp:102-160).
 template <int PREC>
 __device__ void stage_region_pool(double* sm, const ItemInfo& it, int x0, bool leaf_tile, const double* __restrict__ M,
-                                  const double* __restrict__ com, const double* __restrict__ mon,
-                                  const uint8_t* __restrict__ is_leaf) {
+                                  const double* __restrict__ com, const double* __restrict__ mon) {
     for (int r = threadIdx.x; r < REG_CELLS; r += blockDim.x) {
         const int rx = r / (REG_YZ * REG_YZ), ry = (r / REG_YZ) % REG_YZ, rz = r % REG_YZ;
         const int ax = x0 - 2 + rx, ay = ry - 2, az = rz - 2;
@@ -210,8 +209,7 @@ __device__ void m2l_tile(const double* sm, int x0, const Tables& t, uint32_t mon
 // Split staging from the pool: same sources as stage_region_pool, values in
 // units of dx (inv_dx = 1/dx), multinomial factors folded in.
 __device__ void stage_region_split(double* sm, const ItemInfo& it, int x0, double inv_dx, const double* __restrict__ M,
-                                   const double* __restrict__ com, const double* __restrict__ mon,
-                                   const uint8_t* __restrict__ is_leaf) {
+                                   const double* __restrict__ com, const double* __restrict__ mon) {
     float* smf = reinterpret_cast<float*>(sm);
     const double inv2 = inv_dx * inv_dx, inv3 = inv2 * inv_dx;
     for (int r = threadIdx.x; r < REG_CELLS; r += blockDim.x) {
@@ -378,7 +376,7 @@ constexpr float WS_R2_MIN = 1.0e-6f;
 
 __device__ void stage_region_ws(float2* sa, double2* sb, const ItemInfo& it, int x0, double inv_dx,
                                 const double* __restrict__ M, const double* __restrict__ com,
-                                const double* __restrict__ mon, const uint8_t* __restrict__ is_leaf) {
+                                const double* __restrict__ mon) {
     const double inv2 = inv_dx * inv_dx, inv3 = inv2 * inv_dx;
     for (int r = threadIdx.x; r < REG_CELLS; r += blockDim.x) {
         const int rx = r / (REG_YZ * REG_YZ), ry = (r / REG_YZ) % REG_YZ, rz = r % REG_YZ;
@@ -788,11 +786,11 @@ __global__ void __launch_bounds__(THREADS, 1) m2l_batch_kernel(BatchArgs a) {
             const uint32_t monomask = it.leafmask;
             if (PREC == PREC_SPLIT) {
                 const double inv_dx = 1.0 / it.dx;
-                stage_region_split(sm, it, x0, inv_dx, a.M, a.com, a.mon, a.is_leaf);
+                stage_region_split(sm, it, x0, inv_dx, a.M, a.com, a.mon);
                 __syncthreads();
                 m2l_tile_split<RHO>(sm, x0, a.t, monomask, inv_dx, out);
             } else {
-                stage_region_pool<P64>(sm, it, x0, false, a.M, a.com, a.mon, a.is_leaf);
+                stage_region_pool<P64>(sm, it, x0, false, a.M, a.com, a.mon);
                 __syncthreads();
                 m2l_tile<P64, RHO>(sm, x0, a.t, monomask, nullptr, out);
             }
@@ -842,7 +840,7 @@ __global__ void __launch_bounds__(WS_THREADS, 1) m2l_split_ws_kernel(BatchArgs a
         } else {
             const uint32_t monomask = it.leafmask;
             const double inv_dx = 1.0 / it.dx;
-            stage_region_ws(sa, sb, it, x0, inv_dx, a.M, a.com, a.mon, a.is_leaf);
+            stage_region_ws(sa, sb, it, x0, inv_dx, a.M, a.com, a.mon);
             __syncthreads();
             if (warp < 8)
                 ws_contraction_warp<CHUNK, PACKED>(sa, sb, s_ent, x0, warp, a.t, monomask, inv_dx, out);

@@ -1333,8 +1333,19 @@ int otfmm_batch_host(otfmm_context* ctx, const double* pool_M, const double* poo
                             cudaMemcpyHostToDevice, hp.h2d));
     for (int k = 0; k < K; ++k) {
         const size_t a = bnd[k], n = bnd[k + 1] - bnd[k];
-        OT_CUDA(cudaMemcpyAsync(hp.M + a * 20 * NCELL, pool_M + a * 20 * NCELL, n * 20 * cell, cudaMemcpyHostToDevice,
-                                hp.h2d));
+        // moments of refined subgrids only (runs of consecutive ones): no kernel
+        // reads a leaf's moments, leaves enter as masses at their cell centres
+        for (size_t i = a; i < a + n;) {
+            if (pool_is_leaf[i]) {
+                ++i;
+                continue;
+            }
+            size_t j = i + 1;
+            while (j < a + n && !pool_is_leaf[j]) ++j;
+            OT_CUDA(cudaMemcpyAsync(hp.M + i * 20 * NCELL, pool_M + i * 20 * NCELL, (j - i) * 20 * cell,
+                                    cudaMemcpyHostToDevice, hp.h2d));
+            i = j;
+        }
         OT_CUDA(cudaMemcpyAsync(hp.com + a * 3 * NCELL, pool_com + a * 3 * NCELL, n * 3 * cell,
                                 cudaMemcpyHostToDevice, hp.h2d));
         OT_CUDA(cudaMemcpyAsync(hp.mon + a * NCELL, pool_mon + a * NCELL, n * cell, cudaMemcpyHostToDevice, hp.h2d));
@@ -1359,8 +1370,20 @@ int otfmm_batch_host(otfmm_context* ctx, const double* pool_M, const double* poo
     for (int k = 0; k < K; ++k) {
         OT_CUDA(cudaStreamWaitEvent(hp.d2h, ev_comp[need[k]], 0));
         const size_t a = bnd[k], n = bnd[k + 1] - bnd[k];
-        OT_CUDA(cudaMemcpyAsync(L + a * 20 * NCELL, hp.L + a * 20 * NCELL, n * 20 * cell, cudaMemcpyDeviceToHost,
-                                hp.d2h));
+        // L of refined subgrids whole; of leaves the monopole kernels' L0..L3
+        // (their L4..L19 stay as the caller set them), runs of consecutive ones
+        for (size_t i = a; i < a + n;) {
+            const uint8_t leaf = pool_is_leaf[i];
+            size_t j = i + 1;
+            while (j < a + n && pool_is_leaf[j] == leaf) ++j;
+            if (leaf)
+                OT_CUDA(cudaMemcpy2DAsync(L + i * 20 * NCELL, 20 * cell, hp.L + i * 20 * NCELL, 20 * cell, 4 * cell,
+                                          j - i, cudaMemcpyDeviceToHost, hp.d2h));
+            else
+                OT_CUDA(cudaMemcpyAsync(L + i * 20 * NCELL, hp.L + i * 20 * NCELL, (j - i) * 20 * cell,
+                                        cudaMemcpyDeviceToHost, hp.d2h));
+            i = j;
+        }
         OT_CUDA(cudaMemcpyAsync(L_c + a * 3 * NCELL, hp.Lc + a * 3 * NCELL, n * 3 * cell, cudaMemcpyDeviceToHost,
                                 hp.d2h));
         OT_CUDA(cudaEventRecord(ev_d2h[k], hp.d2h));
