@@ -112,3 +112,27 @@ def test_whole_gravity_solve(ctx, oracle, tree, precision):
     err_phi = np.abs(G[leaf, 0] - eG[leaf, 0]).max() / np.abs(eG[leaf, 0]).max()
     err_g = np.abs(G[leaf, 1:] - eG[leaf, 1:]).max() / np.abs(eG[leaf, 1:]).max()
     assert err_phi <= tol_phi and err_g <= tol_g, (err_phi, err_g)
+
+
+@pytest.mark.parametrize("precision", ["fp64_exact", "fp64", "fp32_split"])
+def test_device_solve_of_uniform_sphere(ctx, oracle, precision):
+    """The whole device solve of a uniform sphere (the analogue of the
+    reference's `sphere` gravity scenario): its potential and acceleration
+    against the analytic ones within the bounds the oracle meets, and equal to
+    the oracle's solve with the exact form."""
+    from octotiger_b200.otfmm import GravitySolver
+    sys.path.insert(0, str(Path(__file__).resolve().parent))
+    from sphere_case import analytic_errors, sphere_batch
+    b = sphere_batch(max_level=4)
+    nodes, ls = batch_tree(b)
+    gs = GravitySolver(ctx, b.pool, b.items, nodes, ls, gconst=1.0, correct_am_grav=True)
+    gs.run(RHO, precision)
+    L, Lc, G = gs.results()
+    M, com, c1 = oracle.upward(b.pool, nodes, ls, rho=True)
+    e_phi, l1_phi, e_g = analytic_errors(SubgridPool(M=M, com=com, mon=b.pool.mon, is_leaf=b.pool.is_leaf), com, G)
+    assert e_phi < 3e-3 and l1_phi < 1e-3 and e_g < 3e-2, (e_phi, l1_phi, e_g)
+    if precision == "fp64_exact":
+        pool = SubgridPool(M=M, com=com, mon=b.pool.mon, is_leaf=b.pool.is_leaf)
+        Lo, Lco = oracle.batch(b.theta, pool, b.items, rho=True)
+        _, _, eG = oracle.downward(com, pool.is_leaf, c1, nodes, ls, Lo, Lco, gconst=1.0, correct_am=True, rho=True)
+        np.testing.assert_array_equal(G, eG)
