@@ -84,21 +84,22 @@ def test_every_variant_within_tolerance(ctx, oracle, form, m2l_chunk, p2p_chunk,
         ctx.set_tuning(keep)
 
 
+@pytest.mark.parametrize("solve", [RHO, DRHODT])
 @pytest.mark.parametrize("theta", [0.5, 0.7])
 @pytest.mark.parametrize("p2p_form,p2m_form", list(itertools.product(P2P_FORMS, P2M_FORMS)))
 @pytest.mark.parametrize("precision,p2p_chunk", [("fp64", 32), ("fp32_split", 16), ("fp32_split", 32)])
-def test_leaf_forms_within_tolerance(oracle, theta, p2p_form, p2m_form, precision, p2p_chunk):
+def test_leaf_forms_within_tolerance(oracle, solve, theta, p2p_form, p2m_form, precision, p2p_chunk):
     """The leaf P2P and P2M forms, with the partner box full (theta = 0.5: every
     parity's stencil is its whole 6^3 box, one table of offsets) and partial
     (theta = 0.7: the coarse corners drop out, per-parity masked tables)."""
     from octotiger_b200.otfmm import BatchSolver, Context, Tuning
     b = amr_small()
-    Lo, Lco = oracle.batch(theta, b.pool, b.items, rho=True)
+    Lo, Lco = oracle.batch(theta, b.pool, b.items, rho=(solve == RHO))
     c = Context(0, theta)
     try:
         c.set_tuning(Tuning(0, 16, p2p_chunk, 8, p2p_form, p2m_form))
         s = BatchSolver(c, b.pool, b.items)
-        s.run(RHO, precision)
+        s.run(solve, precision)
         L, Lc = s.results()
         e = scaled(L, Lo)
         if precision == "fp64":
