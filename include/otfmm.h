@@ -180,7 +180,9 @@ int otfmm_stage_p2m_soa(otfmm_context* ctx, const double* pool_M, const double* 
  * same entries. Enqueues a classification kernel that builds device-side work
  * lists, then persistent launches for the multipole tiles of refined items,
  * P2P of the leaves and P2M of leaves with refined neighbours (the reference's
- * P2P-then-P2M order). Work-list storage lives in the context and grows (a
+ * P2P-then-P2M order); the two leaf launches run on the context's second
+ * stream, forked from `stream` after the classification and joined back into
+ * it, so that they use the SMs the tiles leave idle. Work-list storage lives in the context and grows (a
  * device allocation) when a larger work list arrives. Asynchronous; work items
  * are validated on the device and a bad one is reported by otfmm_batch_status
  * (its outputs are left unwritten). Every subgrid may appear in at most one
