@@ -752,24 +752,76 @@ __device__ void root_tile(const double* sm, int x0, const Tables& t, OutPtr out)
     write_lc<RHO>(out, cu, corr);
 }
 
+// Root items in the fast forms: ROOT_UNITS_FAST units of 32 target cells, the
+// partners of a cell spread over F = blockDim.x / 32 lanes (every F-th partner
+// in cell order) and the F partial sums added in a fixed butterfly order, so a
+// root solve spreads over 16 CTAs instead of two. The exact form keeps two
+// tiles with one lane per cell (the reference's partner order).
+constexpr int ROOT_UNITS_FAST = 16;
+template <int PREC>
+constexpr int root_units() {
+    return PREC == PREC_EXACT ? 2 : ROOT_UNITS_FAST;
+}
+
+template <bool RHO, int F>
+__device__ void root_unit_fast(const double* sm, int unit, const Tables& t, OutPtr out) {
+    static_assert(32 % F == 0 && NCELL / ROOT_UNITS_FAST == 32, "F lanes per cell, 32 cells per unit");
+    const int f = threadIdx.x % F, cu = unit * 32 + threadIdx.x / F;
+    const int cx = cu >> 6, cy = (cu >> 3) & 7, cz = cu & 7;
+    double X[3], acc[20], corr[3] = {0.0, 0.0, 0.0}, mc[20];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) X[a] = sm[(20 + a) * NCELL + cu];
+#pragma unroll
+    for (int q = 0; q < 20; ++q) {
+        acc[q] = 0.0;
+        mc[q] = sm[q * NCELL + cu];
+    }
+    const double inv_m0 = 1.0 / mc[0];
+    for (int pu = f; pu < NCELL; pu += F) {
+        const int sx = (pu >> 6) - cx, sy = ((pu >> 3) & 7) - cy, sz = (pu & 7) - cz;
+        if (abs(sx) <= SMAX && abs(sy) <= SMAX && abs(sz) <= SMAX) {
+            const int sidx = (sx + SMAX) * SINX * SINX + (sy + SMAX) * SINX + (sz + SMAX);
+            if (!__ldg(t.phase + sidx) || (sx == 0 && sy == 0 && sz == 0)) continue;
+        }
+        double Y[3], mp[20];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) Y[a] = sm[(20 + a) * NCELL + pu];
+#pragma unroll
+        for (int q = 0; q < 20; ++q) mp[q] = sm[q * NCELL + pu];
+        fast_m2l_pair<RHO>(X, Y, mp, mc + 10, inv_m0, acc, corr);
+    }
+#pragma unroll
+    for (int o = F / 2; o > 0; o >>= 1) {
+#pragma unroll
+        for (int q = 0; q < 20; ++q) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) corr[a] += __shfl_xor_sync(0xffffffffu, corr[a], o);
+    }
+    if (f == 0) {
+#pragma unroll
+        for (int q = 0; q < 20; ++q) out.L[q * out.stride + cu] = acc[q];
+        write_lc<RHO>(out, cu, corr);
+    }
+}
 
 // Multipole tiles (two per refined item), persistent: one CTA per SM takes
-// tiles from an atomic counter, root tiles (longest) first.
+// tiles from an atomic counter, root units (longest) first.
 template <int PREC, bool RHO>
 __global__ void __launch_bounds__(THREADS, 1) m2l_batch_kernel(BatchArgs a) {
     extern __shared__ double sm[];
     __shared__ ItemInfo it;
     __shared__ int tile;
-    const int nroot = a.wl.counts[WL_ROOT], nm2l = a.wl.counts[WL_M2L];
-    const int total = 2 * (nroot + nm2l);
-    // the split form covers the multipole tiles; the root tile uses fast FP64
+    // the split form covers the multipole tiles; the root uses fast FP64
     constexpr int P64 = (PREC == PREC_SPLIT) ? PREC_FAST : PREC;
+    constexpr int RU = root_units<P64>();
+    const int nroot = a.wl.counts[WL_ROOT], nm2l = a.wl.counts[WL_M2L];
+    const int total = RU * nroot + 2 * nm2l;
     for (;;) {
         if (threadIdx.x == 0) tile = atomicAdd(a.wl.counts + WL_M2L_NEXT, 1);
         __syncthreads();
         const int t = tile;
         if (t >= total) break;
-        const int item_idx = (t < 2 * nroot) ? a.wl.root[t >> 1] : a.wl.m2l[(t - 2 * nroot) >> 1];
+        const int item_idx = (t < RU * nroot) ? a.wl.root[t / RU] : a.wl.m2l[(t - RU * nroot) >> 1];
         load_item(a, item_idx, it);
         const int x0 = TILE_X * (t & 1);
         const size_t sub = (size_t)it.subgrid;
@@ -780,7 +832,10 @@ __global__ void __launch_bounds__(THREADS, 1) m2l_batch_kernel(BatchArgs a) {
                     sm[q * NCELL + r] = (q < 20) ? a.M[(sub * 20 + q) * NCELL + r] * stage_scale<P64>(q)
                                                  : a.com[(sub * 3 + (q - 20)) * NCELL + r];
             __syncthreads();
-            root_tile<P64, RHO>(sm, x0, a.t, out);
+            if (P64 == PREC_EXACT)
+                root_tile<P64, RHO>(sm, x0, a.t, out);
+            else
+                root_unit_fast<RHO, THREADS / 32>(sm, t % RU, a.t, out);
         } else {
             // leaf neighbours, indexed by raw direction (monopole-only offsets)
             const uint32_t monomask = it.leafmask;
@@ -801,8 +856,8 @@ __global__ void __launch_bounds__(THREADS, 1) m2l_batch_kernel(BatchArgs a) {
 
 // RHO multipole tiles in the FP32 split precision, warp-specialised (see
 // stage_region_ws): persistent over the same tile counter as m2l_batch_kernel,
-// 512 threads, one CTA per SM. The root tile runs the fast FP64 form on the
-// first 256 threads.
+// 512 threads, one CTA per SM. Root items run the fast FP64 form in 16 units
+// of 32 cells (16 lanes per cell).
 template <int CHUNK, bool PACKED>
 __global__ void __launch_bounds__(WS_THREADS, 1) m2l_split_ws_kernel(BatchArgs a) {
     extern __shared__ __align__(16) unsigned char ws_dyn[];
@@ -812,7 +867,7 @@ __global__ void __launch_bounds__(WS_THREADS, 1) m2l_split_ws_kernel(BatchArgs a
     __shared__ ItemInfo it;
     __shared__ int tile;
     const int nroot = a.wl.counts[WL_ROOT], nm2l = a.wl.counts[WL_M2L];
-    const int total = 2 * (nroot + nm2l);
+    const int total = ROOT_UNITS_FAST * nroot + 2 * nm2l;
     const int warp = threadIdx.x >> 5;
     // far-first partner deltas of the 8 parity classes, resident for the whole launch
     for (int e = threadIdx.x; e < 8 * MAX_ENTRIES; e += blockDim.x) {
@@ -824,7 +879,8 @@ __global__ void __launch_bounds__(WS_THREADS, 1) m2l_split_ws_kernel(BatchArgs a
         __syncthreads();
         const int t = tile;
         if (t >= total) break;
-        const int item_idx = (t < 2 * nroot) ? a.wl.root[t >> 1] : a.wl.m2l[(t - 2 * nroot) >> 1];
+        const int item_idx = (t < ROOT_UNITS_FAST * nroot) ? a.wl.root[t / ROOT_UNITS_FAST]
+                                                            : a.wl.m2l[(t - ROOT_UNITS_FAST * nroot) >> 1];
         load_item(a, item_idx, it);
         const int x0 = TILE_X * (t & 1);
         const size_t sub = (size_t)it.subgrid;
@@ -836,7 +892,7 @@ __global__ void __launch_bounds__(WS_THREADS, 1) m2l_split_ws_kernel(BatchArgs a
                     sm[q * NCELL + r] = (q < 20) ? a.M[(sub * 20 + q) * NCELL + r] * stage_scale<PREC_FAST>(q)
                                                  : a.com[(sub * 3 + (q - 20)) * NCELL + r];
             __syncthreads();
-            if (threadIdx.x < THREADS) root_tile<PREC_FAST, true>(sm, x0, a.t, out);
+            root_unit_fast<true, WS_THREADS / 32>(sm, t % ROOT_UNITS_FAST, a.t, out);
         } else {
             const uint32_t monomask = it.leafmask;
             const double inv_dx = 1.0 / it.dx;

@@ -45,14 +45,15 @@ __global__ void __launch_bounds__(THREADS, 1) m2l_r2_kernel(BatchArgs a) {
     extern __shared__ double sm[];
     __shared__ ItemInfo it;
     __shared__ int tile;
+    constexpr int RU = root_units<PREC>();
     const int nroot = a.wl.counts[WL_ROOT], nm2l = a.wl.counts[WL_M2L];
-    const int total = 2 * (nroot + nm2l);
+    const int total = RU * nroot + 2 * nm2l;
     for (;;) {
         if (threadIdx.x == 0) tile = atomicAdd(a.wl.counts + WL_M2L_NEXT, 1);
         __syncthreads();
         const int t = tile;
         if (t >= total) break;
-        const int item_idx = (t < 2 * nroot) ? a.wl.root[t >> 1] : a.wl.m2l[(t - 2 * nroot) >> 1];
+        const int item_idx = (t < RU * nroot) ? a.wl.root[t / RU] : a.wl.m2l[(t - RU * nroot) >> 1];
         load_item(a, item_idx, it);
         const int x0 = TILE_X * (t & 1);
         const size_t sub = (size_t)it.subgrid;
@@ -63,7 +64,10 @@ __global__ void __launch_bounds__(THREADS, 1) m2l_r2_kernel(BatchArgs a) {
                     sm[q * NCELL + r] = (q < 20) ? a.M[(sub * 20 + q) * NCELL + r] * stage_scale<PREC>(q)
                                                  : a.com[(sub * 3 + (q - 20)) * NCELL + r];
             __syncthreads();
-            root_tile<PREC, RHO>(sm, x0, a.t, out);
+            if (PREC == PREC_EXACT)
+                root_tile<PREC, RHO>(sm, x0, a.t, out);
+            else
+                root_unit_fast<RHO, THREADS / 32>(sm, t % RU, a.t, out);
             __syncthreads();   // shared memory and `it` are reused by the next tile
             continue;
         }
