@@ -780,7 +780,7 @@ __global__ void __launch_bounds__(P_THREADS) p2m_fast_kernel(BatchArgs a) {
 #pragma unroll
                 for (int q = 0; q < 3; ++q) X[q] = __ldg(a.com + (sub * 3 + q) * NCELL + cu);
                 const int beg = __ldg(a.t.p2m_start + cu * 28 + r), end = __ldg(a.t.p2m_start + cu * 28 + r + 1);
-#pragma unroll 1
+#pragma unroll 2
                 for (int q = beg + f; q < end; q += F) {
                     const int u = __ldg(a.t.p2m_list + q);
                     double Y[3], mp[20];
