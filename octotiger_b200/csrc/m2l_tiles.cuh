@@ -433,6 +433,7 @@ __device__ void stage_region_ws(float2* sa, double2* sb, const ItemInfo& it, int
 // FP32 derivative tensor and contraction of one pair (dX in units of dx).
 // 1/r: hardware estimate plus one Newton step with an FMA residual
 // (within about one FP32 ulp).
+template <bool DIPOLE>
 __device__ __forceinline__ void ws_contract_pair(const float dX[3], const float m[20], float acc[20]) {
     const float r2 = fmaxf(fmaf(dX[0], dX[0], fmaf(dX[1], dX[1], dX[2] * dX[2])), WS_R2_MIN);
     const float y0 = rsqrtf(r2);
@@ -444,7 +445,7 @@ __device__ __forceinline__ void ws_contract_pair(const float dX[3], const float 
     const float d3 = -5.0f * d2 * r2inv;
     float D[20];
     d_tensor<float>(dX, -rs, d1, d2, d3, D);
-    fast_low_terms<float>(m, D, acc, false);
+    fast_low_terms<float>(m, D, acc, DIPOLE);
     fast_high_terms<float>(m, D, acc);
 }
 
@@ -571,16 +572,20 @@ __device__ __forceinline__ WsLane ws_lane() {
     return WsLane{(lane >> 2) & 1, lane >> 3, lane & 3};
 }
 
-template <int CHUNK, bool PACKED>
-__device__ void ws_contraction_warp(const float2* sa, const double2* sb, const unsigned* s_ent, int x0, int p,
-                                    const Tables& t, uint32_t monomask, double inv_dx, const OutPtr& out) {
+// The contraction of one parity class over far entries [e_beg, e_end) of its
+// list, plus the monopole-only entries when `mono`, into acc (FP64 sums of the
+// FP32 chunk sums, in units of dx). DIPOLE: the partner dipole terms of L0..L3
+// (the d(rho)/dt solve).
+template <int CHUNK, bool PACKED, bool DIPOLE>
+__device__ void ws_contraction_acc(const float2* sa, const double2* sb, const unsigned* s_ent, int x0, int p,
+                                   const Tables& t, uint32_t monomask, int e_beg, int e_end, bool mono,
+                                   double acc[20]) {
     const WsLane l = ws_lane();
     const int lane_a = l.i * WA_XS + l.j * WA_ROW + l.k;
     const int lane_b = l.i * WB_XS + l.j * WB_ROW + l.k;
     const int own_b = p * WB_CLS + WB_XS + WB_ROW + 1 + lane_b;
     const double2 o0 = sb[own_b], o1 = sb[own_b + SUB_YZ];
     const double Pc0 = o0.x, Pc1 = o0.y, Pc2 = o1.x;
-    double acc[20];
     float accf[20];
 #pragma unroll
     for (int q = 0; q < 20; ++q) {
@@ -594,8 +599,8 @@ __device__ void ws_contraction_warp(const float2* sa, const double2* sb, const u
 #pragma unroll
         for (int k = 0; k < WS_PACKED_ACC; ++k) A[k] = make_float2(0.0f, 0.0f);
 #pragma unroll 1
-        for (int e0 = 0; e0 < nfar; e0 += CHUNK) {
-            const int e1 = min(e0 + CHUNK, nfar);
+        for (int e0 = e_beg; e0 < e_end; e0 += CHUNK) {
+            const int e1 = min(e0 + CHUNK, e_end);
 #pragma unroll 2
             for (int e = e0; e < e1; ++e) {
                 const unsigned en = ent[e];
@@ -612,8 +617,8 @@ __device__ void ws_contraction_warp(const float2* sa, const double2* sb, const u
         }
     } else {
 #pragma unroll 1
-        for (int e0 = 0; e0 < nfar; e0 += CHUNK) {
-            const int e1 = min(e0 + CHUNK, nfar);
+        for (int e0 = e_beg; e0 < e_end; e0 += CHUNK) {
+            const int e1 = min(e0 + CHUNK, e_end);
 #pragma unroll 2
             for (int e = e0; e < e1; ++e) {
                 const unsigned en = ent[e];
@@ -628,7 +633,7 @@ __device__ void ws_contraction_warp(const float2* sa, const double2* sb, const u
                     m[2 * q] = v.x;
                     m[2 * q + 1] = v.y;
                 }
-                ws_contract_pair(dX, m, accf);
+                ws_contract_pair<DIPOLE>(dX, m, accf);
             }
 #pragma unroll
             for (int q = 0; q < 20; ++q) {
@@ -638,7 +643,7 @@ __device__ void ws_contraction_warp(const float2* sa, const double2* sb, const u
         }
     }
     const int cx = x0 + ((p >> 2) & 1) + 2 * l.i, cy = ((p >> 1) & 1) + 2 * l.j, cz = (p & 1) + 2 * l.k;
-    if (monomask) {
+    if (mono && monomask) {
         // monopole-only offsets: only leaf-neighbour partners contribute
         const int4* gent = t.entries_ws + p * MAX_ENTRIES;
 #pragma unroll 1
@@ -653,7 +658,13 @@ __device__ void ws_contraction_warp(const float2* sa, const double2* sb, const u
 #pragma unroll
         for (int q = 0; q < 20; ++q) acc[q] += (double)accf[q];
     }
-    // back to physical units: L_(n) = L'_(n) dx^-(n+1)
+}
+
+// L of the warp's cells from the contraction sums: back to physical units,
+// L_(n) = L'_(n) dx^-(n+1).
+__device__ __forceinline__ void ws_write_l(const double acc[20], int x0, int p, double inv_dx, const OutPtr& out) {
+    const WsLane l = ws_lane();
+    const int cx = x0 + ((p >> 2) & 1) + 2 * l.i, cy = ((p >> 1) & 1) + 2 * l.j, cz = (p & 1) + 2 * l.k;
     const double s1 = inv_dx, s2 = s1 * inv_dx, s3 = s2 * inv_dx, s4 = s3 * inv_dx;
     const int cf = cx * 64 + cy * 8 + cz;
 #pragma unroll
@@ -854,11 +865,12 @@ __global__ void __launch_bounds__(THREADS, 1) m2l_batch_kernel(BatchArgs a) {
     }
 }
 
-// RHO multipole tiles in the FP32 split precision, warp-specialised (see
-// stage_region_ws): persistent over the same tile counter as m2l_batch_kernel,
+// Multipole tiles in the FP32 split precision, warp-specialised (see
+// stage_region_ws); the d(rho)/dt solve, which has no L_c, gives all 16 warps
+// to the contraction: persistent over the same tile counter as m2l_batch_kernel,
 // 512 threads, one CTA per SM. Root items run the fast FP64 form in 16 units
 // of 32 cells (16 lanes per cell).
-template <int CHUNK, bool PACKED>
+template <int CHUNK, bool PACKED, bool RHO>
 __global__ void __launch_bounds__(WS_THREADS, 1) m2l_split_ws_kernel(BatchArgs a) {
     extern __shared__ __align__(16) unsigned char ws_dyn[];
     float2* sa = reinterpret_cast<float2*>(ws_dyn);
@@ -892,16 +904,48 @@ __global__ void __launch_bounds__(WS_THREADS, 1) m2l_split_ws_kernel(BatchArgs a
                     sm[q * NCELL + r] = (q < 20) ? a.M[(sub * 20 + q) * NCELL + r] * stage_scale<PREC_FAST>(q)
                                                  : a.com[(sub * 3 + (q - 20)) * NCELL + r];
             __syncthreads();
-            root_unit_fast<true, WS_THREADS / 32>(sm, t % ROOT_UNITS_FAST, a.t, out);
+            root_unit_fast<RHO, WS_THREADS / 32>(sm, t % ROOT_UNITS_FAST, a.t, out);
         } else {
             const uint32_t monomask = it.leafmask;
             const double inv_dx = 1.0 / it.dx;
             stage_region_ws(sa, sb, it, x0, inv_dx, a.M, a.com, a.mon);
             __syncthreads();
-            if (warp < 8)
-                ws_contraction_warp<CHUNK, PACKED>(sa, sb, s_ent, x0, warp, a.t, monomask, inv_dx, out);
-            else
-                ws_correction_warp(sb, s_ent, x0, warp & 7, a.t, monomask, inv_dx, out);
+            if (RHO) {
+                if (warp < 8) {
+                    double acc[20];
+                    ws_contraction_acc<CHUNK, PACKED, false>(sa, sb, s_ent, x0, warp, a.t, monomask, 0,
+                                                             a.t.count_far[warp], true, acc);
+                    ws_write_l(acc, x0, warp, inv_dx, out);
+                } else {
+                    ws_correction_warp(sb, s_ent, x0, warp & 7, a.t, monomask, inv_dx, out);
+                }
+            } else {
+                // d(rho)/dt: no L_c, so all 16 warps contract, the far entries of a
+                // parity class in two halves (the second with the monopole-only
+                // entries), added in a fixed order through shared memory
+                const int p = warp & 7, half = warp >> 3, nfar = a.t.count_far[p], mid = nfar / 2;
+                double acc[20];
+                ws_contraction_acc<CHUNK, false, true>(sa, sb, s_ent, x0, p, a.t, monomask, half ? mid : 0,
+                                                       half ? nfar : mid, half == 1, acc);
+                __syncthreads();   // the region is read; its first 40 KB take the second halves' sums
+                double* part = reinterpret_cast<double*>(ws_dyn);
+                const int slot = p * 32 + (threadIdx.x & 31);
+                if (half) {
+#pragma unroll
+                    for (int q = 0; q < 20; ++q) part[q * THREADS + slot] = acc[q];
+                }
+                __syncthreads();
+                if (!half) {
+#pragma unroll
+                    for (int q = 0; q < 20; ++q) acc[q] += part[q * THREADS + slot];
+                    ws_write_l(acc, x0, p, inv_dx, out);
+                    const WsLane l = ws_lane();
+                    const int cf = (x0 + ((p >> 2) & 1) + 2 * l.i) * 64 + (((p >> 1) & 1) + 2 * l.j) * 8 +
+                                   ((p & 1) + 2 * l.k);
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) out.Lc[c * out.stride + cf] = 0.0;
+                }
+            }
         }
         __syncthreads();   // shared memory and `it` are reused by the next tile
     }

@@ -304,10 +304,12 @@ int ensure_attributes(int device) {
     rc = rc ? rc : set_smem(m2l_batch_kernel<PREC_FAST, false>, bytes);
     rc = rc ? rc : set_smem(m2l_batch_kernel<PREC_SPLIT, true>, S_SMEM_DOUBLES * (int)sizeof(double));
     rc = rc ? rc : set_smem(m2l_batch_kernel<PREC_SPLIT, false>, S_SMEM_DOUBLES * (int)sizeof(double));
-    rc = rc ? rc : set_smem(m2l_split_ws_kernel<16, false>, WS_SMEM_BYTES);
-    rc = rc ? rc : set_smem(m2l_split_ws_kernel<8, false>, WS_SMEM_BYTES);
-    rc = rc ? rc : set_smem(m2l_split_ws_kernel<16, true>, WS_SMEM_BYTES);
-    rc = rc ? rc : set_smem(m2l_split_ws_kernel<8, true>, WS_SMEM_BYTES);
+    rc = rc ? rc : set_smem(m2l_split_ws_kernel<16, false, true>, WS_SMEM_BYTES);
+    rc = rc ? rc : set_smem(m2l_split_ws_kernel<8, false, true>, WS_SMEM_BYTES);
+    rc = rc ? rc : set_smem(m2l_split_ws_kernel<16, true, true>, WS_SMEM_BYTES);
+    rc = rc ? rc : set_smem(m2l_split_ws_kernel<8, true, true>, WS_SMEM_BYTES);
+    rc = rc ? rc : set_smem(m2l_split_ws_kernel<16, false, false>, WS_SMEM_BYTES);
+    rc = rc ? rc : set_smem(m2l_split_ws_kernel<8, false, false>, WS_SMEM_BYTES);
     rc = rc ? rc : set_smem(p2p_batch_kernel<PREC_EXACT>, P2P_SMEM_BYTES);
     rc = rc ? rc : set_smem(p2p_batch_kernel<PREC_FAST>, P2P_SMEM_BYTES);
     rc = rc ? rc : set_smem(p2p_leaf_kernel<double, 0>, p2_smem_bytes<double>());
@@ -1054,12 +1056,16 @@ int enqueue_batch(otfmm_context* ctx, const double* pool_M, const double* pool_c
             if (rho && tu.split_m2l_form != OTFMM_SPLIT_SINGLE_ROLE) {
                 const bool packed = (tu.split_m2l_form == OTFMM_SPLIT_WARP_SPECIALISED_PACKED);
                 if (tu.split_m2l_chunk == 8) {
-                    if (packed) m2l_split_ws_kernel<8, true><<<tiles_grid, WS_THREADS, WS_SMEM_BYTES, s>>>(a);
-                    else m2l_split_ws_kernel<8, false><<<tiles_grid, WS_THREADS, WS_SMEM_BYTES, s>>>(a);
+                    if (packed) m2l_split_ws_kernel<8, true, true><<<tiles_grid, WS_THREADS, WS_SMEM_BYTES, s>>>(a);
+                    else m2l_split_ws_kernel<8, false, true><<<tiles_grid, WS_THREADS, WS_SMEM_BYTES, s>>>(a);
                 } else {
-                    if (packed) m2l_split_ws_kernel<16, true><<<tiles_grid, WS_THREADS, WS_SMEM_BYTES, s>>>(a);
-                    else m2l_split_ws_kernel<16, false><<<tiles_grid, WS_THREADS, WS_SMEM_BYTES, s>>>(a);
+                    if (packed) m2l_split_ws_kernel<16, true, true><<<tiles_grid, WS_THREADS, WS_SMEM_BYTES, s>>>(a);
+                    else m2l_split_ws_kernel<16, false, true><<<tiles_grid, WS_THREADS, WS_SMEM_BYTES, s>>>(a);
                 }
+            } else if (tu.split_m2l_form != OTFMM_SPLIT_SINGLE_ROLE) {
+                // d(rho)/dt: all warps contract (the packed form is a RHO variant)
+                if (tu.split_m2l_chunk == 8) m2l_split_ws_kernel<8, false, false><<<tiles_grid, WS_THREADS, WS_SMEM_BYTES, s>>>(a);
+                else m2l_split_ws_kernel<16, false, false><<<tiles_grid, WS_THREADS, WS_SMEM_BYTES, s>>>(a);
             } else if (rho) {
                 m2l_batch_kernel<PREC_SPLIT, true><<<tiles_grid, THREADS, sbytes, s>>>(a);
             } else {
