@@ -353,9 +353,12 @@ def gpu_arm(args) -> None:
     # call writes every result but leaves the leaves' L4..L19 (no kernel writes them)
     L_pin = torch.zeros(solver.L.shape, dtype=torch.float64).pin_memory()
     Lc_pin = torch.zeros(solver.Lc.shape, dtype=torch.float64).pin_memory()
-    # bytes the call uploads: the moments of refined subgrids only (no kernel reads a leaf's moments)
-    m_bytes = int((batch.pool.is_leaf == 0).sum()) * 20 * 512 * 8
-    h2d = m_bytes + sum(pin[k].numel() * pin[k].element_size() for k in ("com", "mon", "is_leaf")) + items_pin.numel()
+    # bytes the call uploads: the moments of refined subgrids, the masses of the pool
+    # chunks holding leaves (all of it unless no subgrid is a leaf), every centre of mass
+    n_ref = int((batch.pool.is_leaf == 0).sum())
+    mon_bytes = pin["mon"].numel() * 8 if n_ref < batch.pool.n else 0
+    h2d = (n_ref * 20 * 512 * 8 + mon_bytes + sum(pin[k].numel() * pin[k].element_size() for k in ("com", "is_leaf"))
+           + items_pin.numel())
     n_leaf = int((batch.pool.is_leaf == 1).sum())
     d2h = L_pin.numel() * 8 - n_leaf * 16 * 512 * 8 + Lc_pin.numel() * 8
 

@@ -254,8 +254,8 @@ int otfmm_plan_destroy(otfmm_plan* plan);
  * reference's kernels (src/node_server.cpp:701-705) - except L[4..19] of leaf
  * subgrids, which no kernel writes (the reference's monopole kernels output
  * L[0..3] and L_c) and which are left as the caller set them. The pool is uploaded in
- * chunks of consecutive subgrids (the moments of refined subgrids only: leaves
- * enter the kernels as masses at their cell centres); each work item runs once the records it
+ * chunks of consecutive subgrids (the moments of refined subgrids, the masses
+ * of chunks with leaves and every centre of mass: what the kernels read); each work item runs once the records it
  * reads have arrived and each output range is copied back once final, on two
  * copy streams, so uploads, kernels and downloads overlap when neighbours have
  * nearby pool indices. Device copies live in the context (grown on demand).

@@ -1339,10 +1339,13 @@ int otfmm_batch_host(otfmm_context* ctx, const double* pool_M, const double* poo
                             cudaMemcpyHostToDevice, hp.h2d));
     for (int k = 0; k < K; ++k) {
         const size_t a = bnd[k], n = bnd[k + 1] - bnd[k];
-        // moments of refined subgrids only (runs of consecutive ones): no kernel
-        // reads a leaf's moments, leaves enter as masses at their cell centres
+        // the moments of refined subgrids (runs of consecutive ones) and the masses
+        // of a chunk with leaves (one copy): the kernels read nothing else (a leaf
+        // enters as masses at its cell centres, a refined subgrid as moments)
+        bool any_leaf = false;
         for (size_t i = a; i < a + n;) {
             if (pool_is_leaf[i]) {
+                any_leaf = true;
                 ++i;
                 continue;
             }
@@ -1352,9 +1355,10 @@ int otfmm_batch_host(otfmm_context* ctx, const double* pool_M, const double* poo
                                     cudaMemcpyHostToDevice, hp.h2d));
             i = j;
         }
+        if (any_leaf)
+            OT_CUDA(cudaMemcpyAsync(hp.mon + a * NCELL, pool_mon + a * NCELL, n * cell, cudaMemcpyHostToDevice, hp.h2d));
         OT_CUDA(cudaMemcpyAsync(hp.com + a * 3 * NCELL, pool_com + a * 3 * NCELL, n * 3 * cell,
                                 cudaMemcpyHostToDevice, hp.h2d));
-        OT_CUDA(cudaMemcpyAsync(hp.mon + a * NCELL, pool_mon + a * NCELL, n * cell, cudaMemcpyHostToDevice, hp.h2d));
         OT_CUDA(cudaEventRecord(ev_h2d[k], hp.h2d));
     }
     OT_CUDA(cudaEventRecord(ev_items, hp.h2d));
