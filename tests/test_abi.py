@@ -111,3 +111,44 @@ def test_tree_records_reject_missing_parent():
     nodes, ls = tree_nodes([0, 1, 1], [[0, 0, 0], [1, 0, 0], [0, 1, 1]])
     assert list(ls) == [0, 1, 3]
     assert list(nodes["parent"]) == [0 - 1, 0, 0] and sorted(nodes["octant"][1:]) == [1, 6]
+
+
+def test_struct_layouts_match_header(tmp_path):
+    """Sizes and field offsets of the C structs of include/otfmm.h, from a
+    probe compiled against the header, equal the Python side's (numpy dtypes
+    of the work item and tree node, ctypes otfmm_tuning)."""
+    import subprocess
+    from octotiger_b200.otfmm import Tuning
+    from octotiger_b200.tree import TREE_NODE_DTYPE
+    src = tmp_path / "layout_probe.c"
+    src.write_text(r"""
+#include <stddef.h>
+#include <stdio.h>
+#include "otfmm.h"
+#define F(T, f) printf(#T " " #f " %zu\n", offsetof(T, f))
+int main(void) {
+    printf("otfmm_work_item size %zu\n", sizeof(otfmm_work_item));
+    F(otfmm_work_item, subgrid); F(otfmm_work_item, kind); F(otfmm_work_item, neighbors);
+    F(otfmm_work_item, dx); F(otfmm_work_item, xbase);
+    printf("otfmm_tree_node size %zu\n", sizeof(otfmm_tree_node));
+    F(otfmm_tree_node, subgrid); F(otfmm_tree_node, parent); F(otfmm_tree_node, octant);
+    F(otfmm_tree_node, dx); F(otfmm_tree_node, xbase);
+    printf("otfmm_tuning size %zu\n", sizeof(otfmm_tuning));
+    F(otfmm_tuning, split_m2l_form); F(otfmm_tuning, split_m2l_chunk); F(otfmm_tuning, split_p2p_chunk);
+    F(otfmm_tuning, p2m_lanes); F(otfmm_tuning, p2p_form); F(otfmm_tuning, p2m_form);
+    return 0;
+}
+""")
+    exe = tmp_path / "layout_probe"
+    subprocess.run(["gcc", "-std=c11", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    got = {}
+    for line in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.splitlines():
+        t, f, v = line.split()
+        got[(t, f)] = int(v)
+    for t, dt in (("otfmm_work_item", WORK_ITEM_DTYPE), ("otfmm_tree_node", TREE_NODE_DTYPE)):
+        assert got[(t, "size")] == dt.itemsize, t
+        for f in ("subgrid", "dx", "xbase") + (("kind", "neighbors") if t == "otfmm_work_item" else ("parent", "octant")):
+            assert got[(t, f)] == dt.fields[f][1], (t, f)
+    assert got[("otfmm_tuning", "size")] == ctypes.sizeof(Tuning)
+    for name, _ in Tuning._fields_:
+        assert got[("otfmm_tuning", name)] == getattr(Tuning, name).offset, name
