@@ -342,10 +342,10 @@ def gpu_arm(args) -> None:
         torch.cuda.synchronize()
         accuracy = accuracy_report(solver.L, solver.Lc, Le, Lce)
 
-    # end to end through the library's host-buffer entry point: pool and work
-    # list in pinned host memory, L and L_c back into pinned host memory, all
-    # copies inside the timed region (otfmm_batch_host pipelines them with the
-    # kernels in chunks of the pool)
+    # end to end through the library's host-buffer path: pool and work list in
+    # pinned host memory, L and L_c back into pinned host memory, all copies
+    # inside the timed region (otfmm_batch_host pipelines them with the kernels
+    # in chunks of the pool)
     pin = {k: torch.from_numpy(getattr(batch.pool, k)).pin_memory() for k in ("M", "com", "mon", "is_leaf")}
     items_h = order_work_list(batch.items)
     items_pin = torch.from_numpy(items_h.view(np.uint8).reshape(-1).copy()).pin_memory()

@@ -243,6 +243,17 @@ typedef struct otfmm_plan otfmm_plan;
 int otfmm_plan_create(otfmm_context* ctx, const double* pool_M, const double* pool_com, const double* pool_mon,
                       const uint8_t* pool_is_leaf, int32_t n_subgrids, const otfmm_work_item* items, int32_t n_items,
                       double* L, double* L_c, int gsolve_type, int precision, otfmm_plan** out);
+/* A plan of otfmm_batch_host: the whole host-buffer solve (chunked uploads,
+ * kernels, downloads) captured once for fixed pinned host buffers and work
+ * list, replayed by otfmm_plan_launch with one graph launch; every launch reads
+ * the host inputs' current contents and writes the host outputs (same contract
+ * as otfmm_batch_host). It uses the context's host-path buffers: an
+ * otfmm_batch_host call after it was made invalidates it (its launch then
+ * returns OTFMM_ERR_INVALID). No counterpart in the reference. */
+int otfmm_plan_create_host(otfmm_context* ctx, const double* pool_M, const double* pool_com, const double* pool_mon,
+                           const uint8_t* pool_is_leaf, int32_t n_subgrids, const otfmm_work_item* items,
+                           int32_t n_items, double* L, double* L_c, int gsolve_type, int precision,
+                           otfmm_plan** out);
 int otfmm_plan_launch(otfmm_plan* plan, void* stream);
 int otfmm_plan_status(otfmm_plan* plan, void* stream);
 int otfmm_plan_destroy(otfmm_plan* plan);

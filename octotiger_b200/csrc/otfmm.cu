@@ -257,6 +257,7 @@ struct otfmm_context {
         cudaStream_t h2d = nullptr, d2h = nullptr;
         cudaEvent_t ev[3 * 16 + 4] = {};
         bool ready = false;
+        long long gen = 0;   // calls so far (a host-buffer plan replays only the call it captured)
         std::mutex mu;   // one host-path call at a time per context
     } hp;
     std::mutex mu;
@@ -1138,6 +1139,8 @@ struct otfmm_plan {
     cudaGraphExec_t exec = nullptr;
     int* lists = nullptr;
     int* err = nullptr;
+    bool host = false;      // captured otfmm_batch_host: uses the context's host-path buffers
+    long long host_gen = 0; // ... as the captured call left them
 };
 
 extern "C" {
@@ -1253,6 +1256,7 @@ int otfmm_batch_host(otfmm_context* ctx, const double* pool_M, const double* poo
     cudaStream_t s = (cudaStream_t)stream;
     auto& hp = ctx->hp;
     std::lock_guard<std::mutex> lock(hp.mu);
+    ++hp.gen;
     if (!hp.ready) {
         OT_CUDA(cudaStreamCreateWithFlags(&hp.h2d, cudaStreamNonBlocking));
         OT_CUDA(cudaStreamCreateWithFlags(&hp.d2h, cudaStreamNonBlocking));
@@ -1458,8 +1462,59 @@ int otfmm_plan_create(otfmm_context* ctx, const double* pool_M, const double* po
     return OTFMM_OK;
 }
 
+int otfmm_plan_create_host(otfmm_context* ctx, const double* pool_M, const double* pool_com, const double* pool_mon,
+                           const uint8_t* pool_is_leaf, int32_t n_subgrids, const otfmm_work_item* items,
+                           int32_t n_items, double* L, double* L_c, int gsolve_type, int precision,
+                           otfmm_plan** out) {
+    if (!out) return fail(OTFMM_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    int rc = check_batch_args(ctx, pool_M, pool_com, pool_mon, pool_is_leaf, n_subgrids, items, n_items, L, L_c,
+                              gsolve_type, precision);
+    if (rc) return rc;
+    if (n_items == 0) return fail(OTFMM_ERR_INVALID, "empty work list");
+    DeviceGuard g(ctx->device);
+    cudaStream_t cs = nullptr;
+    OT_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    // one call outside the capture grows the context's buffers and work lists
+    rc = otfmm_batch_host(ctx, pool_M, pool_com, pool_mon, pool_is_leaf, n_subgrids, items, n_items, L, L_c,
+                          gsolve_type, precision, cs);
+    cudaError_t e = cudaStreamSynchronize(cs);
+    if (rc == OTFMM_OK && e != cudaSuccess) rc = cuda_fail(e, "otfmm_plan_create_host");
+    if (rc == OTFMM_OK && (e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeRelaxed)) != cudaSuccess)
+        rc = cuda_fail(e, "cudaStreamBeginCapture");
+    auto* plan = new otfmm_plan();
+    plan->ctx = ctx;
+    plan->host = true;
+    if (rc == OTFMM_OK) {
+        rc = otfmm_batch_host(ctx, pool_M, pool_com, pool_mon, pool_is_leaf, n_subgrids, items, n_items, L, L_c,
+                              gsolve_type, precision, cs);
+        cudaGraph_t graph = nullptr;
+        e = cudaStreamEndCapture(cs, &graph);
+        plan->graph = graph;
+        if (rc == OTFMM_OK && e != cudaSuccess) rc = cuda_fail(e, "cudaStreamEndCapture (host buffers must be pinned)");
+        if (rc == OTFMM_OK && (e = cudaGraphInstantiate(&plan->exec, plan->graph, 0)) != cudaSuccess)
+            rc = cuda_fail(e, "cudaGraphInstantiate");
+    }
+    // events recorded inside the capture are back to plain records for later eager calls
+    for (auto& ev : ctx->hp.ev) cudaEventRecord(ev, cs);
+    cudaEventRecord(ctx->ev_fork, cs);
+    cudaEventRecord(ctx->ev_join, cs);
+    cudaStreamSynchronize(cs);
+    cudaStreamDestroy(cs);
+    if (rc != OTFMM_OK) {
+        const std::string msg = g_last_error;
+        otfmm_plan_destroy(plan);
+        return fail(rc, msg);
+    }
+    plan->host_gen = ctx->hp.gen;
+    *out = plan;
+    return OTFMM_OK;
+}
+
 int otfmm_plan_launch(otfmm_plan* plan, void* stream) {
     if (!plan || !plan->exec) return fail(OTFMM_ERR_INVALID, "NULL plan");
+    if (plan->host && plan->host_gen != plan->ctx->hp.gen)
+        return fail(OTFMM_ERR_INVALID, "an otfmm_batch_host call since the plan was made changed the context's buffers");
     DeviceGuard g(plan->ctx->device);
     OT_CUDA(cudaGraphLaunch(plan->exec, (cudaStream_t)stream));
     return OTFMM_OK;
@@ -1469,7 +1524,8 @@ int otfmm_plan_status(otfmm_plan* plan, void* stream) {
     if (!plan) return fail(OTFMM_ERR_INVALID, "NULL plan");
     DeviceGuard g(plan->ctx->device);
     int h = 0;
-    OT_CUDA(cudaMemcpyAsync(&h, plan->err, sizeof(int), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    OT_CUDA(cudaMemcpyAsync(&h, plan->host ? plan->ctx->d_err : plan->err, sizeof(int), cudaMemcpyDeviceToHost,
+                            (cudaStream_t)stream));
     OT_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
     if (h) return fail(OTFMM_ERR_DEVICE, "a work item failed validation on the device");
     return OTFMM_OK;

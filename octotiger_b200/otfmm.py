@@ -82,6 +82,8 @@ def load_library(path: Path = LIB_PATH) -> ctypes.CDLL:
                                        ctypes.POINTER(Tuning), vp]
         lib.otfmm_plan_create.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int32, vp, ctypes.c_int32, vp, vp, i, i,
                                           ctypes.POINTER(vp)]
+        lib.otfmm_plan_create_host.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int32, vp, ctypes.c_int32, vp, vp, i,
+                                               i, ctypes.POINTER(vp)]
         lib.otfmm_plan_launch.argtypes = [vp, vp]
         lib.otfmm_upward.argtypes = [vp, vp, vp, vp, vp, vp, ctypes.c_int32, vp, vp, ctypes.c_int32, i, vp]
         lib.otfmm_downward.argtypes = [vp, vp, vp, vp, ctypes.c_int32, vp, vp, ctypes.c_int32, vp, vp, vp, dp, i, i,
@@ -242,20 +244,17 @@ class Context:
         """Batched solve from host buffers (numpy arrays or pinned CPU torch
         tensors): pipelined uploads, kernels and downloads; L / Lc are
         complete once `stream` has finished."""
-        def hp(a):
-            if a is None:
-                return None
-            if hasattr(a, "data_ptr"):
-                if a.is_cuda:
-                    raise ValueError("batch_host takes host buffers")
-                return ctypes.c_void_p(a.data_ptr())
-            if not a.flags.c_contiguous:
-                raise ValueError("host buffers must be C-contiguous")
-            return ctypes.c_void_p(a.ctypes.data)
+        hp = _host_ptr
         _check(load_library().otfmm_batch_host(self.handle, hp(M), hp(com), hp(mon), hp(is_leaf),
                                                ctypes.c_int32(n_subgrids), hp(items), ctypes.c_int32(n_items),
                                                hp(L), hp(Lc), int(gsolve_type), precision_code(precision),
                                                _stream(stream)))
+
+    def plan_host(self, M, com, mon, is_leaf, n_subgrids: int, items, n_items: int, L, Lc, gsolve_type=RHO,
+                  precision=FP64) -> "Plan":
+        """batch_host captured once for these pinned host buffers (see
+        otfmm_plan_create_host); launch() replays the whole host-buffer solve."""
+        return Plan.from_host(self, M, com, mon, is_leaf, n_subgrids, items, n_items, L, Lc, gsolve_type, precision)
 
     def upward(self, dev: "DevicePool", com1, nodes_dev, level_start: np.ndarray, gsolve_type=RHO,
                stream=None) -> None:
@@ -421,8 +420,36 @@ class GravitySolver:
         return self.batch.L.cpu().numpy(), self.batch.Lc.cpu().numpy(), self.G.cpu().numpy()
 
 
+def _host_ptr(a):
+    """Pointer of a host buffer (numpy array or CPU torch tensor)."""
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        if a.is_cuda:
+            raise ValueError("host buffers expected")
+        return ctypes.c_void_p(a.data_ptr())
+    if not a.flags.c_contiguous:
+        raise ValueError("host buffers must be C-contiguous")
+    return ctypes.c_void_p(a.ctypes.data)
+
+
 class Plan:
     """A batched solve captured into a CUDA graph; launch() replays it."""
+
+    @classmethod
+    def from_host(cls, ctx: Context, M, com, mon, is_leaf, n_subgrids: int, items, n_items: int, L, Lc,
+                  gsolve_type=RHO, precision=FP64) -> "Plan":
+        self = cls.__new__(cls)
+        self.ctx = ctx
+        self._keep = (M, com, mon, is_leaf, items, L, Lc)   # the graph binds these host pointers
+        hp = _host_ptr
+        h = ctypes.c_void_p()
+        _check(load_library().otfmm_plan_create_host(ctx.handle, hp(M), hp(com), hp(mon), hp(is_leaf),
+                                                     ctypes.c_int32(n_subgrids), hp(items), ctypes.c_int32(n_items),
+                                                     hp(L), hp(Lc), int(gsolve_type), precision_code(precision),
+                                                     ctypes.byref(h)))
+        self.handle = h
+        return self
 
     def __init__(self, ctx: Context, dev: DevicePool, items_dev, n_items: int, L, Lc, gsolve_type=RHO,
                  precision=FP64):

@@ -190,3 +190,40 @@ def test_batch_host_matches_device_batch(ctx, precision, pinned):
         np.testing.assert_array_equal(Lh[leaf, :4], L0[leaf, :4])
         assert np.isnan(Lh[leaf, 4:]).all()
         np.testing.assert_array_equal(Lch, Lc0)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32_split"])
+def test_host_plan_replays_batch_host(ctx, precision):
+    """otfmm_plan_create_host: the host-buffer solve captured once replays
+    with the results of the device batch (each launch reads the current host
+    inputs); an otfmm_batch_host call afterwards invalidates it."""
+    import torch
+    from octotiger_b200.otfmm import BatchSolver, OtfmmError, order_work_list
+    b = amr_small()
+    s = BatchSolver(ctx, b.pool, b.items)
+    s.run(RHO, precision)
+    L0, Lc0 = s.results()
+    n = b.pool.n
+    items = order_work_list(b.items)
+    arrs = {k: torch.from_numpy(getattr(b.pool, k)).pin_memory() for k in ("M", "com", "mon", "is_leaf")}
+    it = torch.from_numpy(items.view(np.uint8).reshape(-1).copy()).pin_memory()
+    L = torch.zeros((n, 20, 512), dtype=torch.float64).pin_memory()
+    Lc = torch.zeros((n, 3, 512), dtype=torch.float64).pin_memory()
+    plan = ctx.plan_host(arrs["M"], arrs["com"], arrs["mon"], arrs["is_leaf"], n, it, len(items), L, Lc, RHO,
+                         precision)
+    leaf = b.pool.is_leaf == 1
+    for _ in range(2):
+        L.fill_(np.nan)
+        Lc.fill_(np.nan)
+        L[torch.from_numpy(leaf)] = 0.0   # the caller zeroes L (leaves' L4..L19 are not written)
+        plan.launch()
+        torch.cuda.synchronize()
+        plan.status()
+        np.testing.assert_array_equal(L.numpy()[~leaf], L0[~leaf])
+        np.testing.assert_array_equal(L.numpy()[leaf, :4], L0[leaf, :4])
+        np.testing.assert_array_equal(Lc.numpy(), Lc0)
+    ctx.batch_host(arrs["M"], arrs["com"], arrs["mon"], arrs["is_leaf"], n, it, len(items), L, Lc, RHO, precision)
+    torch.cuda.synchronize()
+    with pytest.raises(OtfmmError):
+        plan.launch()
+    plan.close()
