@@ -247,9 +247,10 @@ int otfmm_plan_create(otfmm_context* ctx, const double* pool_M, const double* po
  * kernels, downloads) captured once for fixed pinned host buffers and work
  * list, replayed by otfmm_plan_launch with one graph launch; every launch reads
  * the host inputs' current contents and writes the host outputs (same contract
- * as otfmm_batch_host). It uses the context's host-path buffers: an
- * otfmm_batch_host call after it was made invalidates it (its launch then
- * returns OTFMM_ERR_INVALID). No counterpart in the reference. */
+ * as otfmm_batch_host). It uses the context's host-path buffers and work
+ * lists: an otfmm_batch_host call after it was made, or a solve of the context
+ * with more work items, invalidates it (its launch then returns
+ * OTFMM_ERR_INVALID). No counterpart in the reference. */
 int otfmm_plan_create_host(otfmm_context* ctx, const double* pool_M, const double* pool_com, const double* pool_mon,
                            const uint8_t* pool_is_leaf, int32_t n_subgrids, const otfmm_work_item* items,
                            int32_t n_items, double* L, double* L_c, int gsolve_type, int precision,

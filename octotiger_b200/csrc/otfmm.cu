@@ -1141,6 +1141,7 @@ struct otfmm_plan {
     int* err = nullptr;
     bool host = false;      // captured otfmm_batch_host: uses the context's host-path buffers
     long long host_gen = 0; // ... as the captured call left them
+    int* host_lists = nullptr;   // ... and its work-list storage (regrown by a larger solve)
 };
 
 extern "C" {
@@ -1507,14 +1508,15 @@ int otfmm_plan_create_host(otfmm_context* ctx, const double* pool_M, const doubl
         return fail(rc, msg);
     }
     plan->host_gen = ctx->hp.gen;
+    plan->host_lists = ctx->d_lists;
     *out = plan;
     return OTFMM_OK;
 }
 
 int otfmm_plan_launch(otfmm_plan* plan, void* stream) {
     if (!plan || !plan->exec) return fail(OTFMM_ERR_INVALID, "NULL plan");
-    if (plan->host && plan->host_gen != plan->ctx->hp.gen)
-        return fail(OTFMM_ERR_INVALID, "an otfmm_batch_host call since the plan was made changed the context's buffers");
+    if (plan->host && (plan->host_gen != plan->ctx->hp.gen || plan->host_lists != plan->ctx->d_lists))
+        return fail(OTFMM_ERR_INVALID, "the context's host-path buffers or work lists changed since the plan was made");
     DeviceGuard g(plan->ctx->device);
     OT_CUDA(cudaGraphLaunch(plan->exec, (cudaStream_t)stream));
     return OTFMM_OK;
