@@ -432,7 +432,13 @@ __device__ void stage_region_ws(float2* sa, double2* sb, const ItemInfo& it, int
 
 // FP32 derivative tensor and contraction of one pair (dX in units of dx).
 // 1/r: hardware estimate plus one Newton step with an FMA residual
-// (within about one FP32 ulp).
+// (within about one FP32 ulp). The monopole part m0 D_k of all 20 components
+// goes first, as 10 packed FMAs on the pairs (D_2k, D_2k+1) that the tensor
+// and the accumulators already hold side by side (no register moves); the
+// remaining terms are the scalar FMAs of fast_low_terms / fast_high_terms.
+// Same terms as those two, summed in another order (the d(rho)/dt tiles,
+// where every warp contracts, run 4% faster; the RHO tiles are bound by
+// their FP64 warps).
 template <bool DIPOLE>
 __device__ __forceinline__ void ws_contract_pair(const float dX[3], const float m[20], float acc[20]) {
     const float r2 = fmaxf(fmaf(dX[0], dX[0], fmaf(dX[1], dX[1], dX[2] * dX[2])), WS_R2_MIN);
@@ -445,8 +451,33 @@ __device__ __forceinline__ void ws_contract_pair(const float dX[3], const float 
     const float d3 = -5.0f * d2 * r2inv;
     float D[20];
     d_tensor<float>(dX, -rs, d1, d2, d3, D);
-    fast_low_terms<float>(m, D, acc, DIPOLE);
-    fast_high_terms<float>(m, D, acc);
+    const float2 m00 = make_float2(m[0], m[0]);
+#pragma unroll
+    for (int k = 0; k < 10; ++k) {
+        const float2 r = __ffma2_rn(make_float2(D[2 * k], D[2 * k + 1]), m00, make_float2(acc[2 * k], acc[2 * k + 1]));
+        acc[2 * k] = r.x;
+        acc[2 * k + 1] = r.y;
+    }
+    if (DIPOLE) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            acc[0] = fmaf(-m[1 + a], D[1 + a], acc[0]);
+#pragma unroll
+            for (int b = 0; b < 3; ++b) acc[1 + a] = fmaf(-m[1 + a], D[quad_row(a, b)], acc[1 + a]);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+        acc[0] = fmaf(m[4 + q], D[4 + q], acc[0]);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) acc[1 + a] = fmaf(m[4 + q], D[quad_axis(q, a)], acc[1 + a]);
+    }
+#pragma unroll
+    for (int k = 10; k < 20; ++k) acc[0] = fmaf(-m[k], D[k], acc[0]);
+#pragma unroll
+    for (int q = 0; q < 6; ++q)
+#pragma unroll
+        for (int a = 0; a < 3; ++a) acc[4 + q] = fmaf(-m[1 + a], D[quad_axis(q, a)], acc[4 + q]);
 }
 
 // Same contraction with packed FP32 FMAs (two products per instruction; on
