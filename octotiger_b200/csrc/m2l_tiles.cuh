@@ -374,6 +374,11 @@ static_assert(ROOT_SMEM_DOUBLES * 8 <= WS_A_BYTES + WS_B_BYTES, "root staging le
 // mass at least ~0.2 dx apart; the FP64 forms clamp at 1e-20 like the reference.
 constexpr float WS_R2_MIN = 1.0e-6f;
 
+// Sign of moment k in the FP32 staging of the warp-specialised tiles: the
+// contraction subtracts the dipole (k = 1..3) and octupole (k = 10..19) terms,
+// so their staged copies are negated and every term becomes a plain FMA.
+__host__ __device__ constexpr double ws_moment_sign(int k) { return ((k >= 1 && k <= 3) || k >= 10) ? -1.0 : 1.0; }
+
 __device__ void stage_region_ws(float2* sa, double2* sb, const ItemInfo& it, int x0, double inv_dx,
                                 const double* __restrict__ M, const double* __restrict__ com,
                                 const double* __restrict__ mon) {
@@ -421,8 +426,11 @@ __device__ void stage_region_ws(float2* sa, double2* sb, const ItemInfo& it, int
         const int cls = ((ax & 1) << 2) | ((ay & 1) << 1) | (az & 1);
         const int ua = cls * WA_CLS + (rx >> 1) * WA_XS + (ry >> 1) * WA_ROW + (rz >> 1);
         const int ub = cls * WB_CLS + (rx >> 1) * WB_XS + (ry >> 1) * WB_ROW + (rz >> 1);
+        // the FP32 copy carries the sign of the terms: dipoles and octupoles negated
 #pragma unroll
-        for (int q = 0; q < 10; ++q) sa[ua + q * SUB_YZ] = make_float2((float)m[2 * q], (float)m[2 * q + 1]);
+        for (int q = 0; q < 10; ++q)
+            sa[ua + q * SUB_YZ] = make_float2((float)(ws_moment_sign(2 * q) * m[2 * q]),
+                                              (float)(ws_moment_sign(2 * q + 1) * m[2 * q + 1]));
         sb[ub] = make_double2(P[0], P[1]);
         sb[ub + SUB_YZ] = make_double2(P[2], m[0]);
 #pragma unroll
@@ -432,15 +440,15 @@ __device__ void stage_region_ws(float2* sa, double2* sb, const ItemInfo& it, int
 
 // FP32 derivative tensor and contraction of one pair (dX in units of dx).
 // 1/r: hardware estimate plus one Newton step with an FMA residual
-// (within about one FP32 ulp). The monopole part m0 D_k of all 20 components
-// goes first, as 10 packed FMAs on the pairs (D_2k, D_2k+1) that the tensor
-// and the accumulators already hold side by side (no register moves); the
-// remaining terms are the scalar FMAs of fast_low_terms / fast_high_terms.
-// Same terms as those two, summed in another order (the d(rho)/dt tiles,
-// where every warp contracts, run 4% faster; the RHO tiles are bound by
-// their FP64 warps).
+// (within about one FP32 ulp). m holds the staged moments, dipoles and
+// octupoles negated (ws_moment_sign), so every term is an FMA. The terms of
+// fast_low_terms / fast_high_terms in another order: L0 is the dot product of
+// all moments with the tensor, 10 packed FMAs (__ffma2_rn) on the pairs
+// (m_2k, m_2k+1) and (D_2k, D_2k+1) that sit side by side in registers anyway,
+// with its second partial sum in *ext; the monopole part of L2..L19 likewise
+// on the pairs (acc_2k, acc_2k+1); the rest are scalar FMAs.
 template <bool DIPOLE>
-__device__ __forceinline__ void ws_contract_pair(const float dX[3], const float m[20], float acc[20]) {
+__device__ __forceinline__ void ws_contract_pair(const float dX[3], const float m[20], float acc[20], float* ext) {
     const float r2 = fmaxf(fmaf(dX[0], dX[0], fmaf(dX[1], dX[1], dX[2] * dX[2])), WS_R2_MIN);
     const float y0 = rsqrtf(r2);
     const float h = fmaf(-r2 * y0, y0, 1.0f);
@@ -451,39 +459,45 @@ __device__ __forceinline__ void ws_contract_pair(const float dX[3], const float 
     const float d3 = -5.0f * d2 * r2inv;
     float D[20];
     d_tensor<float>(dX, -rs, d1, d2, d3, D);
+    float2 a0 = make_float2(acc[0], *ext);
+    if (DIPOLE) {
+        a0 = __ffma2_rn(make_float2(m[0], m[1]), make_float2(D[0], D[1]), a0);
+        a0 = __ffma2_rn(make_float2(m[2], m[3]), make_float2(D[2], D[3]), a0);
+    } else {
+        a0.x = fmaf(m[0], D[0], a0.x);
+    }
+#pragma unroll
+    for (int k = 2; k < 10; ++k) a0 = __ffma2_rn(make_float2(m[2 * k], m[2 * k + 1]), make_float2(D[2 * k], D[2 * k + 1]), a0);
+    acc[0] = a0.x;
+    *ext = a0.y;
+    acc[1] = fmaf(m[0], D[1], acc[1]);
     const float2 m00 = make_float2(m[0], m[0]);
 #pragma unroll
-    for (int k = 0; k < 10; ++k) {
+    for (int k = 1; k < 10; ++k) {
         const float2 r = __ffma2_rn(make_float2(D[2 * k], D[2 * k + 1]), m00, make_float2(acc[2 * k], acc[2 * k + 1]));
         acc[2 * k] = r.x;
         acc[2 * k + 1] = r.y;
     }
     if (DIPOLE) {
 #pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            acc[0] = fmaf(-m[1 + a], D[1 + a], acc[0]);
+        for (int a = 0; a < 3; ++a)
 #pragma unroll
-            for (int b = 0; b < 3; ++b) acc[1 + a] = fmaf(-m[1 + a], D[quad_row(a, b)], acc[1 + a]);
-        }
+            for (int b = 0; b < 3; ++b) acc[1 + a] = fmaf(m[1 + a], D[quad_row(a, b)], acc[1 + a]);
     }
-#pragma unroll
-    for (int q = 0; q < 6; ++q) {
-        acc[0] = fmaf(m[4 + q], D[4 + q], acc[0]);
-#pragma unroll
-        for (int a = 0; a < 3; ++a) acc[1 + a] = fmaf(m[4 + q], D[quad_axis(q, a)], acc[1 + a]);
-    }
-#pragma unroll
-    for (int k = 10; k < 20; ++k) acc[0] = fmaf(-m[k], D[k], acc[0]);
 #pragma unroll
     for (int q = 0; q < 6; ++q)
 #pragma unroll
-        for (int a = 0; a < 3; ++a) acc[4 + q] = fmaf(-m[1 + a], D[quad_axis(q, a)], acc[4 + q]);
+        for (int a = 0; a < 3; ++a) acc[1 + a] = fmaf(m[4 + q], D[quad_axis(q, a)], acc[1 + a]);
+#pragma unroll
+    for (int q = 0; q < 6; ++q)
+#pragma unroll
+        for (int a = 0; a < 3; ++a) acc[4 + q] = fmaf(m[1 + a], D[quad_axis(q, a)], acc[4 + q]);
 }
 
 // Same contraction with packed FP32 FMAs (two products per instruction; on
 // sm_100 these co-issue with the FP64 pipe far better than scalar FMAs).
 // Accumulator pairs: A[k] = (L_2k, L_2k+1) for k = 0..9; A[10] = L0 quadrupole
-// part, A[11] = L0 octupole part (subtracted), A[12..14] = L1..L3 quadrupole
+// part, A[11] = L0 octupole part, A[12..14] = L1..L3 quadrupole
 // parts, each as two partial sums. The derivative tensor is used as its
 // natural pairs (D_2k, D_2k+1) plus the five pairs the quadrupole/dipole terms
 // of L2, L3 and L4..L9 need: (D11,D13) (D14,D16) (D17,D18) (D12,D14) (D15,D17).
@@ -506,8 +520,9 @@ __device__ __forceinline__ void ws_contract_pair_packed(const float dX[3], const
     const float2 Q1 = make_float2(D[11], D[13]), Q2 = make_float2(D[14], D[16]), Q3 = make_float2(D[17], D[18]);
     const float2 R1 = make_float2(D[12], D[14]), R2 = make_float2(D[15], D[17]);
     const float2 b0 = make_float2(mm[0].x, mm[0].x);
-    const float2 n1 = make_float2(-mm[0].y, -mm[0].y), n2 = make_float2(-mm[1].x, -mm[1].x),
-                 n3 = make_float2(-mm[1].y, -mm[1].y);
+    // staged dipoles carry their minus sign (ws_moment_sign)
+    const float2 n1 = make_float2(mm[0].y, mm[0].y), n2 = make_float2(mm[1].x, mm[1].x),
+                 n3 = make_float2(mm[1].y, mm[1].y);
     // monopole: L0..L19 += M0 D0..D19
 #pragma unroll
     for (int k = 0; k < 10; ++k) A[k] = __ffma2_rn(b0, P[k], A[k]);
@@ -533,14 +548,14 @@ __device__ __forceinline__ void ws_contract_pair_packed(const float dX[3], const
     A[14] = __ffma2_rn(mm[2], R1, A[14]);
     A[14] = __ffma2_rn(mm[3], R2, A[14]);
     A[14] = __ffma2_rn(mm[4], P[9], A[14]);
-    // octupole part of L0 (subtracted when the pairs are folded)
+    // octupole part of L0 (staged octupoles carry their minus sign)
 #pragma unroll
     for (int o = 0; o < 5; ++o) A[11] = __ffma2_rn(mm[5 + o], P[5 + o], A[11]);
 }
 
 // Folds the packed accumulators into the FP64 sums of L0..L19 and clears them.
 __device__ __forceinline__ void ws_fold_packed(float2 A[WS_PACKED_ACC], double acc[20]) {
-    acc[0] += (double)((A[0].x + (A[10].x + A[10].y)) - (A[11].x + A[11].y));
+    acc[0] += (double)((A[0].x + (A[10].x + A[10].y)) + (A[11].x + A[11].y));
     acc[1] += (double)(A[0].y + (A[12].x + A[12].y));
     acc[2] += (double)(A[1].x + (A[13].x + A[13].y));
     acc[3] += (double)(A[1].y + (A[14].x + A[14].y));
@@ -617,7 +632,7 @@ __device__ void ws_contraction_acc(const float2* sa, const double2* sb, const un
     const int own_b = p * WB_CLS + WB_XS + WB_ROW + 1 + lane_b;
     const double2 o0 = sb[own_b], o1 = sb[own_b + SUB_YZ];
     const double Pc0 = o0.x, Pc1 = o0.y, Pc2 = o1.x;
-    float accf[20];
+    float accf[20], ext = 0.0f;
 #pragma unroll
     for (int q = 0; q < 20; ++q) {
         acc[q] = 0.0;
@@ -664,8 +679,10 @@ __device__ void ws_contraction_acc(const float2* sa, const double2* sb, const un
                     m[2 * q] = v.x;
                     m[2 * q + 1] = v.y;
                 }
-                ws_contract_pair<DIPOLE>(dX, m, accf);
+                ws_contract_pair<DIPOLE>(dX, m, accf, &ext);
             }
+            accf[0] += ext;
+            ext = 0.0f;
 #pragma unroll
             for (int q = 0; q < 20; ++q) {
                 acc[q] += (double)accf[q];
