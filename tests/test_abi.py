@@ -61,6 +61,24 @@ def test_work_list_validation_rejects_bad_items():
         validate_work_list(dup, b.pool.n)
 
 
+def test_work_list_order_puts_multipole_items_first():
+    """order_work_list: refined and root items before leaves, each group in
+    its input order, every item kept once."""
+    from octotiger_b200 import amr
+    from octotiger_b200.otfmm import order_work_list
+    b = amr.polytrope_batch(max_level=4)
+    items = b.items[::-1].copy()   # leaves and multipole items interleaved differently
+    out = order_work_list(items)
+    assert len(out) == len(items) and out.flags["C_CONTIGUOUS"]
+    kinds = out["kind"]
+    n_multi = int((items["kind"] != 2).sum())
+    assert (kinds[:n_multi] != 2).all() and (kinds[n_multi:] == 2).all()
+    for group in (items[items["kind"] != 2], items[items["kind"] == 2]):
+        got = out[np.isin(out["subgrid"], group["subgrid"])]
+        np.testing.assert_array_equal(got["subgrid"], group["subgrid"])
+    assert sorted(out["subgrid"].tolist()) == sorted(items["subgrid"].tolist())
+
+
 def test_create_rejects_small_theta_without_gpu():
     """theta below 0.34 is rejected before any device call."""
     from octotiger_b200.otfmm import LIB_PATH, load_library
