@@ -46,10 +46,14 @@ def test_small_amr_batch_kinds():
     assert any(has_refined_nb) and any(has_empty)
 
 
-def test_small_amr_oracle_matches_reference_math(oracle, refmath):
-    b = amr.polytrope_batch(radius=0.05, max_level=5)
+@pytest.mark.parametrize("theta", [0.5, 0.34])
+def test_small_amr_oracle_matches_reference_math(oracle, refmath, theta):
+    """A ragged AMR work list (refined, root and leaf items, P2M at the
+    refinement boundaries) at the default opening angle and at 0.34, whose
+    partners reach two coarse cells."""
+    b = amr.polytrope_batch(radius=0.05, max_level=5, theta=theta)
     for rho in (True, False):
-        L, Lc = oracle.batch(0.5, b.pool, b.items, rho=rho)
-        L2, Lc2 = refmath.batch(0.5, b.pool, b.items, rho=rho)
+        L, Lc = oracle.batch(theta, b.pool, b.items, rho=rho)
+        L2, Lc2 = refmath.batch(theta, b.pool, b.items, rho=rho)
         np.testing.assert_array_equal(L, L2)
         np.testing.assert_array_equal(Lc, Lc2)

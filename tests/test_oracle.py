@@ -60,20 +60,23 @@ def test_oracle_matches_golden(oracle, name):
     np.testing.assert_array_equal(Lc[s], GOLDEN[f"{name}/Lc"])
 
 
+@pytest.mark.parametrize("theta", [0.34, 0.5, 0.7, 1.0])
 @pytest.mark.parametrize("simd", [False, True])
 @pytest.mark.parametrize("rho", [True, False])
-def test_oracle_matches_reference_math_soa(oracle, refmath, rho, simd):
+def test_oracle_matches_reference_math_soa(oracle, refmath, rho, simd, theta):
+    """Every supported stencil: theta 0.34 (partners up to two coarse cells
+    away), 0.5, and the smaller stencils of 0.7 and 1.0."""
     b = syn.single_subgrid(seed=7, leaf_dirs=(3, 9, 21), empty_dirs=(11,))
     mon, M, com = oracle.stage_m2l(b.pool, b.items[0])
     for root in (False, True):
-        L, Lc = oracle.m2l_soa(0.5, mon, M, com, rho=rho, root=root)
-        L2, Lc2 = refmath.m2l_soa(0.5, mon, M, com, rho=rho, root=root, simd=simd)
+        L, Lc = oracle.m2l_soa(theta, mon, M, com, rho=rho, root=root)
+        L2, Lc2 = refmath.m2l_soa(theta, mon, M, com, rho=rho, root=root, simd=simd)
         np.testing.assert_array_equal(L, L2)
         np.testing.assert_array_equal(Lc, Lc2)
     bl = syn.single_subgrid(seed=8, leaf_centre=True, leaf_dirs=(0, 1, 2, 13, 24))
     mon = oracle.stage_p2p(bl.pool, bl.items[0])
-    np.testing.assert_array_equal(oracle.p2p_soa(0.5, mon, 1 / 64),
-                                  refmath.p2p_soa(0.5, mon, 1 / 64, simd=simd))
+    np.testing.assert_array_equal(oracle.p2p_soa(theta, mon, 1 / 64),
+                                  refmath.p2p_soa(theta, mon, 1 / 64, simd=simd))
     icom = np.zeros(3 * COMPONENT_LENGTH_UNPADDED)
     icom.reshape(3, -1)[:, :NCELL] = bl.pool.com[0]
     for d in (3, 12, 25):   # refined neighbours of the leaf
@@ -84,7 +87,7 @@ def test_oracle_matches_reference_math_soa(oracle, refmath, rho, simd):
             L4 = np.arange(4 * COMPONENT_LENGTH_UNPADDED, dtype=np.float64) * 1e-3
             Lc = np.zeros(3 * COMPONENT_LENGTH_UNPADDED)
             kw = {} if impl is oracle else {"simd": simd}
-            impl.p2m_dir(0.5, d, nM, ncom, stride, icom, L4, Lc, rho=rho, reset=True, **kw)
+            impl.p2m_dir(theta, d, nM, ncom, stride, icom, L4, Lc, rho=rho, reset=True, **kw)
             outs.append((L4, Lc))
         np.testing.assert_array_equal(outs[0][0], outs[1][0])
         np.testing.assert_array_equal(outs[0][1], outs[1][1])
