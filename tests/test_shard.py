@@ -1,4 +1,4 @@
-"""Multi-rank sharding of a work list, on the CPU with world-size-2 gloo ranks:
+"""Multi-rank sharding of a work list, on the CPU with gloo ranks (world sizes 2 and 3):
 partition coverage and balance, halo exchange of remote neighbour records, and
 a sharded solve (oracle as the per-rank compute) equal to the global one."""
 from __future__ import annotations
@@ -77,11 +77,14 @@ def _worker(rank, world, port, result_path):
         dist.destroy_process_group()
 
 
-def test_sharded_solve_equals_global(tmp_path):
+@pytest.mark.parametrize("world", [2, 3])
+def test_sharded_solve_equals_global(tmp_path, world):
+    """World sizes 2 and 3 (uneven parts, a rank whose neighbours live on
+    both others)."""
     import torch.multiprocessing as mp
 
     from oracle.pyoracle import Oracle
-    world, port = 2, _free_port()
+    port = _free_port()
     res = str(tmp_path / "res")
     mp.start_processes(_worker, args=(world, port, res), nprocs=world, start_method="spawn", join=True)
     b = _small_amr()
