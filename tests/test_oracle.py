@@ -180,3 +180,28 @@ def test_angular_correction_cancels_pairwise(oracle):
     total = weighted.sum(axis=1)
     scale = np.abs(weighted).sum(axis=1)
     assert (np.abs(total) <= 1e-12 * scale).all(), (total, scale)
+
+
+@pytest.mark.parametrize("rho", [True, False])
+def test_zero_mass_cells_match_reference_math(oracle, refmath, rho):
+    """Cells whose multipoles are all zero (a massless target and massless
+    partners): the RHO correction divides by the target's mass, so the
+    reference's arithmetic gives non-finite L_c there; the oracle reproduces
+    every value, non-finite ones included, bit for bit."""
+    b = syn.single_subgrid(seed=17)
+    s = int(b.items[0]["subgrid"])
+    cells = [0, 77, 300, 511]
+    b.pool.M[s][:, cells] = 0.0
+    nb = int(b.items[0]["neighbors"][4])
+    b.pool.M[nb][:, [5, 6, 7]] = 0.0
+    mon, M, com = oracle.stage_m2l(b.pool, b.items[0])
+    L, Lc = oracle.m2l_soa(0.5, mon, M, com, rho=rho, root=False)
+    L2, Lc2 = refmath.m2l_soa(0.5, mon, M, com, rho=rho, root=False, simd=False)
+    np.testing.assert_array_equal(L, L2)
+    np.testing.assert_array_equal(Lc, Lc2)
+    if rho:
+        assert not np.isfinite(Lc).all() and np.isfinite(L).all()
+    Lb, Lcb = oracle.batch(0.5, b.pool, b.items, rho=rho, nthreads=2)
+    Lb2, Lcb2 = refmath.batch(0.5, b.pool, b.items, rho=rho)
+    np.testing.assert_array_equal(Lb, Lb2)
+    np.testing.assert_array_equal(Lcb, Lcb2)
