@@ -205,3 +205,12 @@ def test_zero_mass_cells_match_reference_math(oracle, refmath, rho):
     Lb2, Lcb2 = refmath.batch(0.5, b.pool, b.items, rho=rho)
     np.testing.assert_array_equal(Lb, Lb2)
     np.testing.assert_array_equal(Lcb, Lcb2)
+    # a leaf target with massless cells: P2P and the P2M of its refined neighbours
+    bl = syn.single_subgrid(seed=18, leaf_centre=True, leaf_dirs=tuple(range(0, 26, 3)))
+    sl = int(bl.items[0]["subgrid"])
+    bl.pool.mon[sl][cells] = 0.0
+    bl.pool.M[sl][:, cells] = 0.0
+    Lb, Lcb = oracle.batch(0.5, bl.pool, bl.items, rho=rho, nthreads=2)
+    Lb2, Lcb2 = refmath.batch(0.5, bl.pool, bl.items, rho=rho)
+    np.testing.assert_array_equal(Lb, Lb2)
+    np.testing.assert_array_equal(Lcb, Lcb2)
