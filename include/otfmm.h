@@ -272,7 +272,10 @@ int otfmm_plan_destroy(otfmm_plan* plan);
  * copy streams, so uploads, kernels and downloads overlap when neighbours have
  * nearby pool indices. Device copies live in the context (grown on demand).
  * Asynchronous: the outputs are valid once `stream` has completed; a later
- * call waits for the earlier call's uploads. Work items are re-validated on the
+ * call waits for the earlier call's uploads. Calls of one context share its
+ * device copies: consecutive calls on the same stream run in order, calls on
+ * different streams must not overlap on the GPU (wait for the earlier call's
+ * stream first, or use distinct contexts). Work items are re-validated on the
  * device (otfmm_batch_status). No counterpart in the reference. */
 int otfmm_batch_host(otfmm_context* ctx, const double* pool_M, const double* pool_com, const double* pool_mon,
                      const uint8_t* pool_is_leaf, int32_t n_subgrids, const otfmm_work_item* items, int32_t n_items,

@@ -243,7 +243,8 @@ class Context:
                    precision=FP64, stream=None) -> None:
         """Batched solve from host buffers (numpy arrays or pinned CPU torch
         tensors): pipelined uploads, kernels and downloads; L / Lc are
-        complete once `stream` has finished."""
+        complete once `stream` has finished. Calls of one context on
+        different streams must not overlap (they share its device copies)."""
         hp = _host_ptr
         _check(load_library().otfmm_batch_host(self.handle, hp(M), hp(com), hp(mon), hp(is_leaf),
                                                ctypes.c_int32(n_subgrids), hp(items), ctypes.c_int32(n_items),
