@@ -1,7 +1,11 @@
 """Benchmark of the FMM cell-interaction kernels (one JSON line on rank 0).
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
-                    [--workload uniform_level3|amr_polytrope] [--precision fp32_split|fp64|fp64_exact]
+                    [--workload amr_polytrope|uniform_level3|amr_binary|single_subgrid]
+                    [--precision fp32_split|fp64|fp64_exact]
+
+The default workload is the ragged AMR batch (n = 1.5 polytrope refined to
+levels 3-6: multipole, P2P and P2M work items in one solve).
 
 A step is one gravity solve's interaction work list (every work item of the
 workload) through one batched launch. ``value`` = cell-interactions / s with the
@@ -451,6 +455,8 @@ def gpu_arm(args) -> None:
     fp64_peak, fp32_peak = measure_fma_peaks(local)
     peak = fp32_peak if args.precision == "fp32_split" else fp64_peak
     traffic = PROFILED_TRAFFIC.get((batch.name, args.precision))
+    traffic_note = None if traffic else (f"no ncu capture of the {args.precision} tile kernel on the {batch.name} "
+                                          "workload is recorded in PROFILED_TRAFFIC")
     roof = {"bound": "fp64_fma" if args.precision != "fp32_split" else "fp32_fma", "achieved": achieved,
             "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
             "kernel": "multipole tiles (m2l)", "flops_per_launch": flops_m2l,
@@ -460,7 +466,7 @@ def gpu_arm(args) -> None:
             "peak_source": "measured in this run: register-resident FMA loop (otfmm_measure_fma_peaks); "
                            "MEASURED_PEAKS.json has no FP64/FP32 figure",
             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of the same kernel "
-                              "on this workload (tuned variant)" if traffic else None,
+                              "on this workload (tuned variant)" if traffic else traffic_note,
             "fp64_peak_tflops": fp64_peak, "fp32_peak_tflops": fp32_peak}
 
     line = {
@@ -508,7 +514,7 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="uniform_level3", choices=list(WORKLOADS))
+    ap.add_argument("--workload", default="amr_polytrope", choices=list(WORKLOADS))
     ap.add_argument("--precision", default="fp32_split", choices=["fp32_split", "fp64", "fp64_exact"])
     ap.add_argument("--compare", nargs="*", default=["fp64", "fp64_exact"])
     ap.add_argument("--gsolve", default="rho", choices=["rho", "drhodt"])
@@ -519,6 +525,18 @@ def main() -> None:
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.gpus != world:
+        if "WORLD_SIZE" in os.environ:
+            raise SystemExit(f"bench.py: --gpus {args.gpus} but WORLD_SIZE={world}")
+        # not under a launcher: start one process per GPU ourselves
+        import socket
+        with socket.socket() as sk:
+            sk.bind(("127.0.0.1", 0))
+            port = sk.getsockname()[1]
+        cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+               "--master-addr=127.0.0.1", f"--master-port={port}", str(Path(__file__).resolve()), *sys.argv[1:]]
+        raise SystemExit(subprocess.run(cmd).returncode)
     if args.impl == "reference":
         reference_arm(args)
     else:

@@ -127,9 +127,13 @@ int otfmm_m2l_soa_host(otfmm_context* ctx, const double* mon, const double* M, c
  * synchronisation of cudaMalloc/cudaFree, or HPX tasks on a hot path where the
  * reference uses recycled buffers. The first call on a device looks up the
  * array's device address (cudaGetSymbolAddress) and should come before any
- * stream capture. Larger n_subgrids is rejected (OTFMM_ERR_INVALID). All calls
+ * stream capture. With CUDA's lazy module loading the library's device code,
+ * and the array with it, is placed on a device when the library is first used
+ * there, so make that first call at set-up time, before the code that must not
+ * allocate runs. Larger n_subgrids is rejected (OTFMM_ERR_INVALID). All calls
  * share the one array: calls that overlap on the GPU would race, so calls
- * from this library are serialised and each waits for its stream. */
+ * from this library are serialised and each waits for its stream before it
+ * returns, on error returns too. */
 #define OTFMM_NOALLOC_MAX_SUBGRIDS 4
 int otfmm_m2l_soa_host_noalloc(otfmm_context* ctx, int32_t n_subgrids, const double* mon, const double* M,
                                const double* com, double* L, double* L_c, int gsolve_type, int use_root_stencil,

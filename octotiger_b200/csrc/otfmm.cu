@@ -830,8 +830,9 @@ int otfmm_m2l_soa_host(otfmm_context* ctx, const double* mon, const double* M, c
 // from the static g_noalloc_scratch array. Its device address is looked up
 // once per device (cudaGetSymbolAddress, on the first call on that device,
 // which should therefore come before any stream capture); later calls reuse
-// it. The array is shared by every call: calls are serialised here, and each
-// call clears the output staging it reads back.
+// it. The array is shared by every call: calls are serialised here, each call
+// clears the output staging it reads back, and each waits for its stream
+// before it returns, on error returns too.
 int otfmm_m2l_soa_host_noalloc(otfmm_context* ctx, int32_t n_subgrids, const double* mon, const double* M,
                                const double* com, double* L, double* L_c, int gsolve_type, int use_root_stencil,
                                int precision, void* stream) {
@@ -857,25 +858,36 @@ int otfmm_m2l_soa_host_noalloc(otfmm_context* ctx, int32_t n_subgrids, const dou
         scratch_ptr[ctx->device] = ptr;
     }
     cudaStream_t s = (cudaStream_t)stream;
-    for (int i = 0; i < n_subgrids; ++i) {
-        double* d_mon = scratch_ptr[ctx->device] + i * NOALLOC_SLOT;
-        double* d_M = d_mon + ENTRIES;
-        double* d_com = d_M + 20 * (size_t)CL;
-        double* d_L = d_com + 3 * (size_t)CL;
-        double* d_Lc = d_L + 20 * (size_t)CLU;
-        if (!use_root_stencil)
-            OT_CUDA(cudaMemcpyAsync(d_mon, mon + (size_t)i * ENTRIES, sizeof(double) * ENTRIES, cudaMemcpyHostToDevice, s));
-        OT_CUDA(cudaMemcpyAsync(d_M, M + (size_t)i * 20 * CL, sizeof(double) * 20 * CL, cudaMemcpyHostToDevice, s));
-        OT_CUDA(cudaMemcpyAsync(d_com, com + (size_t)i * 3 * CL, sizeof(double) * 3 * CL, cudaMemcpyHostToDevice, s));
-        OT_CUDA(cudaMemsetAsync(d_L, 0, sizeof(double) * 23 * CLU, s));
-        rc = otfmm_m2l_soa(ctx, use_root_stencil ? nullptr : d_mon, d_M, d_com, d_L, d_Lc, gsolve_type,
-                           use_root_stencil, precision, stream);
-        if (rc) return rc;
-        OT_CUDA(cudaMemcpyAsync(L + (size_t)i * 20 * CLU, d_L, sizeof(double) * 20 * CLU, cudaMemcpyDeviceToHost, s));
-        if (rho)
-            OT_CUDA(cudaMemcpyAsync(L_c + (size_t)i * 3 * CLU, d_Lc, sizeof(double) * 3 * CLU, cudaMemcpyDeviceToHost, s));
-    }
-    OT_CUDA(cudaStreamSynchronize(s));
+    // Everything is enqueued inside `enqueue`; whatever it returns, the stream
+    // is drained before the lock is released, so no copy or kernel of this call
+    // can still touch the shared array when the next call starts.
+    auto enqueue = [&]() -> int {
+        for (int i = 0; i < n_subgrids; ++i) {
+            double* d_mon = scratch_ptr[ctx->device] + i * NOALLOC_SLOT;
+            double* d_M = d_mon + ENTRIES;
+            double* d_com = d_M + 20 * (size_t)CL;
+            double* d_L = d_com + 3 * (size_t)CL;
+            double* d_Lc = d_L + 20 * (size_t)CLU;
+            if (!use_root_stencil)
+                OT_CUDA(cudaMemcpyAsync(d_mon, mon + (size_t)i * ENTRIES, sizeof(double) * ENTRIES,
+                                        cudaMemcpyHostToDevice, s));
+            OT_CUDA(cudaMemcpyAsync(d_M, M + (size_t)i * 20 * CL, sizeof(double) * 20 * CL, cudaMemcpyHostToDevice, s));
+            OT_CUDA(cudaMemcpyAsync(d_com, com + (size_t)i * 3 * CL, sizeof(double) * 3 * CL, cudaMemcpyHostToDevice, s));
+            OT_CUDA(cudaMemsetAsync(d_L, 0, sizeof(double) * 23 * CLU, s));
+            const int r = otfmm_m2l_soa(ctx, use_root_stencil ? nullptr : d_mon, d_M, d_com, d_L, d_Lc, gsolve_type,
+                                        use_root_stencil, precision, stream);
+            if (r) return r;
+            OT_CUDA(cudaMemcpyAsync(L + (size_t)i * 20 * CLU, d_L, sizeof(double) * 20 * CLU, cudaMemcpyDeviceToHost, s));
+            if (rho)
+                OT_CUDA(cudaMemcpyAsync(L_c + (size_t)i * 3 * CLU, d_Lc, sizeof(double) * 3 * CLU,
+                                        cudaMemcpyDeviceToHost, s));
+        }
+        return OTFMM_OK;
+    };
+    rc = enqueue();
+    const cudaError_t drained = cudaStreamSynchronize(s);
+    if (rc) return rc;   // the first error wins; the stream is drained either way
+    if (drained != cudaSuccess) return cuda_fail(drained, "cudaStreamSynchronize");
     return OTFMM_OK;
 }
 

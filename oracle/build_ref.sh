@@ -2,8 +2,9 @@
 # TEST INFRASTRUCTURE ONLY. Compiles the reference's own kernel arithmetic
 # (header templates + stencil generators, included in place from the
 # Octo-Tiger source tree) around oracle/ref_driver.cpp into oracle/_ref/.
-# Needs the reference tree (default /root/reference); outputs go only to
-# oracle/_ref/. Two builds: AVX-512 (8 SIMD lanes, the reference's host
+# Needs the reference tree: $OCTOTIGER_REFERENCE, else the recipe's default
+# location below; exits with status 3 when neither holds it. Outputs go only
+# to oracle/_ref/. Two builds: AVX-512 (8 SIMD lanes, the reference's host
 # AVX-512 configuration) and AVX2 (4 lanes) for hosts without AVX-512.
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"

@@ -7,7 +7,9 @@ otfmm_m2l_soa_host_noalloc serves them from a static device array. This test
 calls it twice in a row through the C ABI and checks each result against the
 allocating host-buffer entry point otfmm_m2l_soa_host (bit-identical for the
 exact form, 1e-12 for the fast form, the tolerances of the other GPU tests),
-and that a batch larger than the array is refused.
+that the exact form also equals the oracle bit for bit, that a call made after
+a warm-up call leaves the device's free memory unchanged, and that a batch
+larger than the array is refused.
 """
 from __future__ import annotations
 
@@ -41,6 +43,9 @@ def test_noalloc_matches_allocating_entry_point(oracle):
             Lr, Lcr = ctx.m2l_soa_host(mon[i], M[i], com[i], RHO, False, "fp64_exact")
             np.testing.assert_array_equal(_cells(L[i], 20), _cells(Lr, 20))
             np.testing.assert_array_equal(_cells(Lc[i], 3), _cells(Lcr, 3))
+            Lo, Lco = oracle.m2l_soa(0.5, mon[i], M[i], com[i], rho=True, root=False)
+            np.testing.assert_array_equal(_cells(L[i], 20), _cells(Lo, 20))
+            np.testing.assert_array_equal(_cells(Lc[i], 3), _cells(Lco, 3))
         # call 2 right after: the root stencil, DRHODT, fast FP64
         r = syn.root_subgrid(seed=63)
         _, Mr, comr = oracle.stage_m2l(r.pool, r.items[0])
@@ -49,6 +54,17 @@ def test_noalloc_matches_allocating_entry_point(oracle):
         got, ref = _cells(L2[0], 20), _cells(Lr2, 20)
         scale = np.abs(ref).max(axis=1)
         assert (np.abs(got - ref).max(axis=1) <= 1e-12 * scale).all()
+        # the call allocates nothing: the device's free memory is the same
+        # before and after a call that follows a warm-up call
+        import torch
+        ctx.m2l_soa_host_noalloc(mon, M, com, RHO, False, "fp64")   # warm-up: loads this kernel
+        free0, _ = torch.cuda.mem_get_info(0)
+        L3, _ = ctx.m2l_soa_host_noalloc(mon, M, com, RHO, False, "fp64")
+        free1, _ = torch.cuda.mem_get_info(0)
+        assert free1 == free0, (free0, free1)
+        Lf, _ = ctx.m2l_soa_host(mon[1], M[1], com[1], RHO, False, "fp64")
+        scale = np.abs(_cells(Lf, 20)).max(axis=1)
+        assert (np.abs(_cells(L3[1], 20) - _cells(Lf, 20)).max(axis=1) <= 1e-12 * scale).all()
         # more subgrids than the static array holds: refused, nothing run
         with pytest.raises(OtfmmError) as e:
             ctx.m2l_soa_host_noalloc(np.zeros((5, mon.shape[1])), np.zeros((5, M.shape[1])),
