@@ -508,6 +508,91 @@ def gpu_arm(args) -> None:
         pg.destroy_process_group()
 
 
+def sharded_arm(args) -> None:
+    """The solve partitioned over the ranks (one GPU each): Morton ranges of
+    the work list, each rank's own records uploaded and the remote neighbour
+    records fetched once per solve over NCCL into the rank's own memory
+    (octotiger_b200.shard.sharded_problem, the function the gloo tests run),
+    then the rank's batched solve replayed from its CUDA graph. Total work is
+    fixed as N grows (strong scaling); time = max over ranks."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    from octotiger_b200 import shard
+    from octotiger_b200.otfmm import BatchSolver, Context
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        dist.init_process_group("gloo", store=dist.HashStore(), rank=0, world_size=1)
+    batch = make_workload(args.workload, args.theta)
+    solve = RHO if args.gsolve == "rho" else DRHODT
+    ctx = Context(local, batch.theta)
+    counts = pair_counts(batch, ctx)
+    dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    lp = shard.sharded_problem(batch, rank, world, dist, device=dev if world > 1 else None)
+    torch.cuda.synchronize()
+    exch_s = time.perf_counter() - t0
+    solver = BatchSolver.from_device(ctx, lp.pool, lp.items) if world > 1 else BatchSolver(ctx, lp.pool, lp.items)
+    is_leaf_local = lp.pool.is_leaf.cpu().numpy() if world > 1 else lp.pool.is_leaf
+    local_pairs, _ = ctx.count_pairs(is_leaf_local, lp.items)
+    tuned = solver.autotune(solve, args.precision, repeats=3)
+    plan = solver.plan(solve, args.precision)
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    for _ in range(args.warmup):
+        plan.launch()
+    plan.status()
+    dist.barrier()
+    torch.cuda.synchronize()
+    total_ms = 0.0
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            plan.launch()
+            e1.record(stream)
+            e1.synchronize()
+            total_ms += e0.elapsed_time(e1)
+    plan.status()
+    dist.barrier()
+    t = torch.tensor([total_ms, exch_s, float(local_pairs)], dtype=torch.float64, device=dev if world > 1 else "cpu")
+    mx, sm = t.clone(), t.clone()
+    dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+    dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+    total_ms, exch_s, pairs_sum = float(mx[0]), float(mx[1]), int(sm[2])
+    value = counts["total"] * args.steps / (total_ms * 1e-3)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "dtype": "f64" if args.precision != "fp32_split" else "f32+f64", "data": "synthetic (seeded generator)",
+        "config": {"workload": batch.name, "n_subgrids": batch.pool.n, "pairs_per_step": counts["total"],
+                   "pairs_over_ranks": pairs_sum, "theta": batch.theta, "gsolve": args.gsolve,
+                   "precision": args.precision, "l2": "flushed (256 MiB write) before every timed step",
+                   "parallelism": f"{world} shards (Morton ranges of the work list, remote neighbour records "
+                                  "exchanged once per solve)",
+                   "tuning": tuned.as_dict()},
+        "exchange_s_max_over_ranks": exch_s,
+        "gpu_launches": 4 * args.steps,
+        "clocks": clk.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    plan.close()
+    del solver
+    ctx.close()
+    dist.barrier()
+    dist.destroy_process_group()
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -522,6 +607,8 @@ def main() -> None:
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-per-subgrid", action="store_true", help="skip the per-subgrid FP64 comparison")
+    ap.add_argument("--sharded", action="store_true",
+                    help="partition one solve over the ranks (strong scaling) instead of one replica per rank")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -539,6 +626,8 @@ def main() -> None:
         raise SystemExit(subprocess.run(cmd).returncode)
     if args.impl == "reference":
         reference_arm(args)
+    elif args.sharded:
+        sharded_arm(args)
     else:
         gpu_arm(args)
 

@@ -999,4 +999,403 @@ __global__ void __launch_bounds__(WS_THREADS, 1) m2l_split_ws_kernel(BatchArgs a
     }
 }
 
+
+// ------------------------------------------------ FP32 split, fused (RHO)
+// Every thread serves one target cell and computes, for each of its pairs,
+// the FP64 geometry and angular-momentum correction L_c and the FP32
+// derivative tensor and D.M contraction in one instruction stream. On sm_100
+// an FP64 FMA and FP32 work issued from the same warp run side by side (the
+// FP32 instructions fill the issue slots the FP64 pipe leaves), whereas warps
+// that hold only FP64 work are starved by warps that hold only FP32 work; so
+// both precisions share every warp here.
+// Shared memory per parity class (4 x 6 x 6 sub-lattice):
+//   FP32 part: float4 (Q0,Q1,Q2,Q3) (Q4,Q5,-O0,-O1) (-O2,-O3,-O4,-O5)
+//     (-O6,-O7,-O8,-O9) (quadrupoles Q, octupoles O in units of dx with the
+//     multinomial factors folded in, octupoles negated so that L0 is a plain
+//     dot product), rows [4][6 z] = 24 float4, x stride 148 float4;
+//   FP64 part: the double2 rows of the warp-specialised layout:
+//     (Px,Py) (Pz,m0) (O0,O1) .. (O8,O9), P = (centre of mass - xbase) / dx.
+// Lane l serves sub-lattice cell (i, j, k) = ((l >> 2) & 1, l >> 3, l & 3): a
+// quarter-warp (8 lanes: k, i) reads float4 at k + 4 i and double2 at k + 4 i
+// modulo 8 sixteen-byte slots (x strides 148 and 252): no bank conflicts.
+constexpr int FZ_THREADS = 256;
+constexpr int FZ_ROW = 4 * SUB_YZ;            // 24 float4
+constexpr int FZ_XS = SUB_YZ * FZ_ROW + 4;    // 148 float4
+constexpr int FZ_CLS = (REG_X / 2) * FZ_XS;   // 592 float4
+constexpr int FZ_A_BYTES = 8 * FZ_CLS * 16;
+constexpr int FZ_SMEM_BYTES = FZ_A_BYTES + WS_B_BYTES + WS_TABLE_BYTES;   // 75776 + 129024 + 6912 = 211712
+static_assert(FZ_XS % 8 == 4 && WB_XS % 8 == 4, "quarter-warps (k, i) read distinct 16-byte slots");
+static_assert(8 * FZ_CLS < 65536, "float4 deltas fit 16 bits");
+static_assert(FZ_SMEM_BYTES + 256 <= 232448, "fused layout fits the 227 KB shared-memory limit");
+static_assert(ROOT_SMEM_DOUBLES * 8 <= FZ_A_BYTES + WS_B_BYTES, "root staging leaves the stencil table intact");
+
+__device__ void stage_region_fz(float4* sf, double2* sb, const ItemInfo& it, int x0, double inv_dx,
+                                const double* __restrict__ M, const double* __restrict__ com,
+                                const double* __restrict__ mon) {
+    const double inv2 = inv_dx * inv_dx, inv3 = inv2 * inv_dx;
+    for (int r = threadIdx.x; r < REG_CELLS; r += blockDim.x) {
+        const int rx = r / (REG_YZ * REG_YZ), ry = (r / REG_YZ) % REG_YZ, rz = r % REG_YZ;
+        const int ax = x0 - 2 + rx, ay = ry - 2, az = rz - 2;
+        const int raw = raw_dir(ax, ay, az);
+        const bool centre = (raw == 13);
+        const int src = centre ? it.subgrid : it.nb[raw < 13 ? raw : raw - 1];
+        const int u = (ax & 7) * 64 + (ay & 7) * 8 + (az & 7);
+        double m0, q[6], o[10], P[3];
+        if (src < 0) {
+            // empty direction: zero moments at the cell's own centre (never at a
+            // target's centre of mass, so the pair stays finite)
+            m0 = 0.0;
+#pragma unroll
+            for (int k = 0; k < 6; ++k) q[k] = 0.0;
+#pragma unroll
+            for (int k = 0; k < 10; ++k) o[k] = 0.0;
+            P[0] = ax;
+            P[1] = ay;
+            P[2] = az;
+        } else if (!centre && ((it.leafmask >> raw) & 1u)) {
+            m0 = mon[(size_t)src * NCELL + u];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) q[k] = 0.0;
+#pragma unroll
+            for (int k = 0; k < 10; ++k) o[k] = 0.0;
+            // leaf cell centre i*dx + xbase - INX*dx (monopole_interaction_interface.hpp:221-234)
+            const int ip[3] = {ax + INX, ay + INX, az + INX};
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                const double c = __dsub_rn(__dadd_rn(__dmul_rn((double)ip[a], it.dx), it.xbase[a]),
+                                           __dmul_rn((double)INX, it.dx));
+                P[a] = (c - it.xbase[a]) * inv_dx;
+            }
+        } else {
+            const double* Ms = M + (size_t)src * 20 * NCELL + u;
+            m0 = Ms[0];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) q[k] = Ms[(4 + k) * NCELL] * ((factor_of(4 + k) / 2.0) * inv2);
+#pragma unroll
+            for (int k = 0; k < 10; ++k) o[k] = Ms[(10 + k) * NCELL] * ((factor_of(10 + k) / 6.0) * inv3);
+#pragma unroll
+            for (int a = 0; a < 3; ++a) P[a] = (com[((size_t)src * 3 + a) * NCELL + u] - it.xbase[a]) * inv_dx;
+        }
+        const int cls = ((ax & 1) << 2) | ((ay & 1) << 1) | (az & 1);
+        const int ua = cls * FZ_CLS + (rx >> 1) * FZ_XS + (ry >> 1) * FZ_ROW + (rz >> 1);
+        const int ub = cls * WB_CLS + (rx >> 1) * WB_XS + (ry >> 1) * WB_ROW + (rz >> 1);
+        sf[ua] = make_float4((float)q[0], (float)q[1], (float)q[2], (float)q[3]);
+        sf[ua + SUB_YZ] = make_float4((float)q[4], (float)q[5], (float)-o[0], (float)-o[1]);
+        sf[ua + 2 * SUB_YZ] = make_float4((float)-o[2], (float)-o[3], (float)-o[4], (float)-o[5]);
+        sf[ua + 3 * SUB_YZ] = make_float4((float)-o[6], (float)-o[7], (float)-o[8], (float)-o[9]);
+        sb[ub] = make_double2(P[0], P[1]);
+        sb[ub + SUB_YZ] = make_double2(P[2], m0);
+#pragma unroll
+        for (int k = 0; k < 5; ++k) sb[ub + (2 + k) * SUB_YZ] = make_double2(o[2 * k], o[2 * k + 1]);
+    }
+}
+
+// The FP32 half of a fused pair: derivative tensor and contraction with the
+// partner's FP32 moments (RHO terms: monopole, quadrupole and octupole parts;
+// the partner dipole does not enter), into the FP32 chunk sums acc (L0's
+// second partial sum in *ext). 1/r comes in as rsf.
+__device__ __forceinline__ void fz_contract(const float dXf[3], float rsf, float m0, const float4 f0, const float4 f1,
+                                            const float4 f2, const float4 f3, float acc[20], float* ext) {
+    const float r2invf = rsf * rsf;
+    const float d1 = rsf * r2invf;
+    const float d2 = -3.0f * d1 * r2invf;
+    const float d3 = -5.0f * d2 * r2invf;
+    float D[20];
+    d_tensor<float>(dXf, -rsf, d1, d2, d3, D);
+    // L0 = m0 D0 + sum Q_q D_(4+q) - sum O_o D_(10+o): a packed dot product
+    float2 a0 = make_float2(fmaf(m0, D[0], acc[0]), *ext);
+    a0 = __ffma2_rn(make_float2(f0.x, f0.y), make_float2(D[4], D[5]), a0);
+    a0 = __ffma2_rn(make_float2(f0.z, f0.w), make_float2(D[6], D[7]), a0);
+    a0 = __ffma2_rn(make_float2(f1.x, f1.y), make_float2(D[8], D[9]), a0);
+    a0 = __ffma2_rn(make_float2(f1.z, f1.w), make_float2(D[10], D[11]), a0);
+    a0 = __ffma2_rn(make_float2(f2.x, f2.y), make_float2(D[12], D[13]), a0);
+    a0 = __ffma2_rn(make_float2(f2.z, f2.w), make_float2(D[14], D[15]), a0);
+    a0 = __ffma2_rn(make_float2(f3.x, f3.y), make_float2(D[16], D[17]), a0);
+    a0 = __ffma2_rn(make_float2(f3.z, f3.w), make_float2(D[18], D[19]), a0);
+    acc[0] = a0.x;
+    *ext = a0.y;
+    // monopole part of L1..L19
+    acc[1] = fmaf(m0, D[1], acc[1]);
+    const float2 mm = make_float2(m0, m0);
+#pragma unroll
+    for (int k = 1; k < 10; ++k) {
+        const float2 r = __ffma2_rn(make_float2(D[2 * k], D[2 * k + 1]), mm, make_float2(acc[2 * k], acc[2 * k + 1]));
+        acc[2 * k] = r.x;
+        acc[2 * k + 1] = r.y;
+    }
+    // quadrupole part of L1..L3
+    const float Q[6] = {f0.x, f0.y, f0.z, f0.w, f1.x, f1.y};
+#pragma unroll
+    for (int q = 0; q < 6; ++q)
+#pragma unroll
+        for (int a = 0; a < 3; ++a) acc[1 + a] = fmaf(Q[q], D[quad_axis(q, a)], acc[1 + a]);
+}
+
+// Geometry of a pair for both precisions from dX (units of dx, FP64): the FP32
+// copy dXf, 1/r as an FP32 estimate refined by one FP32 Newton step (rsf,
+// r^2 floored at 1e-6 dx^2 for the FP32 tensor, which no pair of distinct
+// cells reaches) and by one FP64 Newton step from it (~1e-14 relative), the
+// products X_ab, d2 = -3 r^-5 and d3 = 15 r^-7 in FP64. The FP32 side does not
+// wait for the FP64 refinement.
+__device__ __forceinline__ void fz_geometry(const double dX[3], float dXf[3], FastDerivs& f, float* rsf) {
+    dXf[0] = (float)dX[0];
+    dXf[1] = (float)dX[1];
+    dXf[2] = (float)dX[2];
+    const float r2f = fmaxf(fmaf(dXf[0], dXf[0], fmaf(dXf[1], dXf[1], dXf[2] * dXf[2])), WS_R2_MIN);
+    const float y0 = rsqrtf(r2f);
+    const float h = fmaf(-r2f * y0, y0, 1.0f);
+    *rsf = fmaf(0.5f * y0, h, y0);
+    f.X00 = dX[0] * dX[0];
+    f.X11 = dX[1] * dX[1];
+    f.X22 = dX[2] * dX[2];
+    f.X01 = dX[0] * dX[1];
+    f.X02 = dX[0] * dX[2];
+    f.X12 = dX[1] * dX[2];
+    const double r2 = fmax(f.X00 + f.X11 + f.X22, 1.0e-20);
+    const double y = (double)*rsf;
+    const double rs = y * fma(-0.5 * r2 * y, y, 1.5);
+    const double r2inv = rs * rs;
+    const double m3 = -3.0 * r2inv, m5 = -5.0 * r2inv;
+    const double d1 = rs * r2inv;
+    f.d2 = d1 * m3;
+    f.d3 = f.d2 * m5;
+}
+
+// L_c -= sum_o h_o U_o. (fourth-order slice, compute_kernel_templates.hpp:232-334)
+// with each output's ten terms in two interleaved partial sums.
+__device__ __forceinline__ void fz_upper(const FastDerivs& f, const double h[10], double Lc[3]) {
+    const double d2 = f.d2, d3 = f.d3;
+    const double e01 = d3 * f.X01, e02 = d3 * f.X02, e12 = d3 * f.X12;
+    const double d3_6 = 6.0 * d3, d2_3 = 3.0 * d2;
+    double U[15];
+    U[0] = fma(d3_6, f.X00, d2_3);
+    U[1] = 3.0 * e01;
+    U[2] = 3.0 * e02;
+    U[3] = fma(d3, f.X00 + f.X11, d2);
+    U[4] = e12;
+    U[5] = fma(d3, f.X00 + f.X22, d2);
+    U[6] = U[1];
+    U[7] = e02;
+    U[8] = e01;
+    U[9] = U[2];
+    U[10] = fma(d3_6, f.X11, d2_3);
+    U[11] = 3.0 * e12;
+    U[12] = fma(d3, f.X11 + f.X22, d2);
+    U[13] = U[11];
+    U[14] = fma(d3_6, f.X22, d2_3);
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        double t = Lc[j], t1 = -h[1] * U[upper_idx(1, j)];
+#pragma unroll
+        for (int o = 0; o < 10; o += 2) t = fma(-h[o], U[upper_idx(o, j)], t);
+#pragma unroll
+        for (int o = 3; o < 10; o += 2) t1 = fma(-h[o], U[upper_idx(o, j)], t1);
+        Lc[j] = t + t1;
+    }
+}
+
+// L_c of a cell, split as L_c = -sum_p O_p . U(d_p) + (O_c / m_c) . sum_p m_p U(d_p)
+// (compute_kernel_templates.hpp:228-334 with g = O_p - O_c m_p / m_c expanded):
+// per pair the partner part goes into La (even pairs) / Lb (odd pairs), and
+// the mass-weighted geometry into V = sum m_p d2, W_ab = sum m_p d3 X_ab; the
+// target part is formed once per cell from V, W (fz_finish_lc). Both parts are
+// FP64 sums, so their difference keeps ~1e-16 of their size.
+struct FzLc {
+    double La[3], Lb[3], V, W[6];
+};
+__device__ __forceinline__ void fz_mass_geometry(const FastDerivs& f, double m0p, FzLc& z) {
+    z.V = fma(m0p, f.d2, z.V);
+    const double md3 = m0p * f.d3;
+    z.W[0] = fma(md3, f.X00, z.W[0]);
+    z.W[1] = fma(md3, f.X11, z.W[1]);
+    z.W[2] = fma(md3, f.X22, z.W[2]);
+    z.W[3] = fma(md3, f.X01, z.W[3]);
+    z.W[4] = fma(md3, f.X02, z.W[4]);
+    z.W[5] = fma(md3, f.X12, z.W[5]);
+}
+__device__ __forceinline__ void fz_finish_lc(const FzLc& z, const double c_oct[10], double Lc[3]) {
+    // sum_p m_p U_k(d_p) is U_k with d2 -> V, d3 -> 1, X_ab -> W_ab
+    FastDerivs w;
+    w.d2 = z.V;
+    w.d3 = 1.0;
+    w.X00 = z.W[0];
+    w.X11 = z.W[1];
+    w.X22 = z.W[2];
+    w.X01 = z.W[3];
+    w.X02 = z.W[4];
+    w.X12 = z.W[5];
+    double neg_c[10];
+#pragma unroll
+    for (int o = 0; o < 10; ++o) neg_c[o] = -c_oct[o];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) Lc[a] = z.La[a] + z.Lb[a];
+    fast_upper_correction(w, neg_c, Lc);
+}
+
+// One far pair of the fused form into the FP32 sums and the L_c parts.
+__device__ __forceinline__ void fz_far_pair(const double2* pb, const float4* pa, double Pc0, double Pc1, double Pc2,
+                                            float accf[20], float* ext, double L[3], FzLc& z) {
+    const double2 q0 = pb[0], q1 = pb[SUB_YZ];
+    double op[10];
+#pragma unroll
+    for (int o = 0; o < 5; ++o) {
+        const double2 v = pb[(2 + o) * SUB_YZ];
+        op[2 * o] = v.x;
+        op[2 * o + 1] = v.y;
+    }
+    const float4 f0 = pa[0], f1 = pa[SUB_YZ], f2 = pa[2 * SUB_YZ], f3 = pa[3 * SUB_YZ];
+    const double dX[3] = {Pc0 - q0.x, Pc1 - q0.y, Pc2 - q1.x};
+    FastDerivs f;
+    float dXf[3], rsf;
+    fz_geometry(dX, dXf, f, &rsf);
+    fz_upper(f, op, L);
+    fz_mass_geometry(f, q1.y, z);
+    fz_contract(dXf, rsf, (float)q1.y, f0, f1, f2, f3, accf, ext);
+}
+
+template <int CHUNK>
+__device__ void fz_tile(const float4* sf, const double2* sb, const unsigned* s_ent, int x0, int p, const Tables& t,
+                        uint32_t monomask, double inv_dx, const OutPtr& out) {
+    const WsLane l = ws_lane();
+    const int lane_b = l.i * WB_XS + l.j * WB_ROW + l.k;
+    const int lane_f = l.i * FZ_XS + l.j * FZ_ROW + l.k;
+    const int own_b = p * WB_CLS + WB_XS + WB_ROW + 1 + lane_b;
+    const double2 o0 = sb[own_b], o1 = sb[own_b + SUB_YZ];
+    const double Pc0 = o0.x, Pc1 = o0.y, Pc2 = o1.x;
+    FzLc z;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) z.La[a] = z.Lb[a] = 0.0;
+    z.V = 0.0;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) z.W[k] = 0.0;
+    double acc[20];
+    float accf[20], ext = 0.0f;
+#pragma unroll
+    for (int q = 0; q < 20; ++q) {
+        acc[q] = 0.0;
+        accf[q] = 0.0f;
+    }
+    const int n = t.count[p], nfar = t.count_far[p];
+    const unsigned* ent = s_ent + p * MAX_ENTRIES;
+#pragma unroll 1
+    for (int e0 = 0; e0 < nfar; e0 += CHUNK) {
+        const int e1 = min(e0 + CHUNK, nfar);
+        int e = e0;
+#pragma unroll 1
+        for (; e + 1 < e1; e += 2) {
+            const unsigned ea = ent[e], eb = ent[e + 1];
+            fz_far_pair(sb + (ea & 0xffffu) + lane_b, sf + (ea >> 16) + lane_f, Pc0, Pc1, Pc2, accf, &ext, z.La, z);
+            fz_far_pair(sb + (eb & 0xffffu) + lane_b, sf + (eb >> 16) + lane_f, Pc0, Pc1, Pc2, accf, &ext, z.Lb, z);
+        }
+        if (e < e1) {
+            const unsigned ea = ent[e];
+            fz_far_pair(sb + (ea & 0xffffu) + lane_b, sf + (ea >> 16) + lane_f, Pc0, Pc1, Pc2, accf, &ext, z.La, z);
+        }
+        accf[0] += ext;
+        ext = 0.0f;
+#pragma unroll
+        for (int q = 0; q < 20; ++q) {
+            acc[q] += (double)accf[q];
+            accf[q] = 0.0f;
+        }
+    }
+    const int cx = x0 + ((p >> 2) & 1) + 2 * l.i, cy = ((p >> 1) & 1) + 2 * l.j, cz = (p & 1) + 2 * l.k;
+    if (monomask) {
+        // monopole-only offsets: only leaf-neighbour partners contribute (as masses)
+        const int4* gent = t.entries_ws + p * MAX_ENTRIES;
+#pragma unroll 1
+        for (int e = nfar; e < n; ++e) {
+            const int4 en = __ldg(gent + e);
+            const int ax = cx + entry_sx(en.z), ay = cy + entry_sy(en.z), az = cz + entry_sz(en.z);
+            if (!((monomask >> raw_dir(ax, ay, az)) & 1u)) continue;
+            const double2 q0 = sb[en.y + lane_b], q1 = sb[en.y + lane_b + SUB_YZ];
+            const double dX[3] = {Pc0 - q0.x, Pc1 - q0.y, Pc2 - q1.x};
+            FastDerivs f;
+            float dXf[3], rsf;
+            fz_geometry(dX, dXf, f, &rsf);
+            // a leaf partner carries no octupole: only the mass-weighted part
+            fz_mass_geometry(f, q1.y, z);
+            const float r2invf = rsf * rsf;
+            const float d1 = rsf * r2invf;
+            const float d2 = -3.0f * d1 * r2invf;
+            const float d3 = -5.0f * d2 * r2invf;
+            float D[20];
+            d_tensor<float>(dXf, -rsf, d1, d2, d3, D);
+            const float m0 = (float)q1.y;
+#pragma unroll
+            for (int q = 0; q < 20; ++q) accf[q] = fmaf(m0, D[q], accf[q]);
+        }
+#pragma unroll
+        for (int q = 0; q < 20; ++q) acc[q] += (double)accf[q];
+    }
+    // the target's part of L_c: O_c / m_c against the mass-weighted geometry
+    const double inv_m0 = 1.0 / o1.y;
+    double c_oct[10];
+#pragma unroll
+    for (int o = 0; o < 5; ++o) {
+        const double2 v = sb[own_b + (2 + o) * SUB_YZ];
+        c_oct[2 * o] = v.x * inv_m0;
+        c_oct[2 * o + 1] = v.y * inv_m0;
+    }
+    double corr[3];
+    fz_finish_lc(z, c_oct, corr);
+    // back to physical units: L_(n) = L'_(n) dx^-(n+1), L_c = L_c' dx^-2
+    const double s1 = inv_dx, s2 = s1 * inv_dx, s3 = s2 * inv_dx, s4 = s3 * inv_dx;
+    const int cf = cx * 64 + cy * 8 + cz;
+#pragma unroll
+    for (int q = 0; q < 20; ++q) out.L[q * out.stride + cf] = acc[q] * (q == 0 ? s1 : q < 4 ? s2 : q < 10 ? s3 : s4);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) out.Lc[a * out.stride + cf] = corr[a] * s2;
+}
+
+// RHO multipole tiles in the fused FP32-split form: persistent over the same
+// tile counter as m2l_batch_kernel, 256 threads (one target cell each), one
+// CTA per SM. Root items run the fast FP64 form in 16 units of 32 cells
+// (8 lanes per cell).
+template <int CHUNK>
+__global__ void __launch_bounds__(FZ_THREADS, 1) m2l_split_fz_kernel(BatchArgs a) {
+    extern __shared__ __align__(16) unsigned char fz_dyn[];
+    float4* sf = reinterpret_cast<float4*>(fz_dyn);
+    double2* sb = reinterpret_cast<double2*>(fz_dyn + FZ_A_BYTES);
+    unsigned* s_ent = reinterpret_cast<unsigned*>(fz_dyn + FZ_A_BYTES + WS_B_BYTES);
+    __shared__ ItemInfo it;
+    __shared__ int tile;
+    const int nroot = a.wl.counts[WL_ROOT], nm2l = a.wl.counts[WL_M2L];
+    const int total = ROOT_UNITS_FAST * nroot + 2 * nm2l;
+    const int warp = threadIdx.x >> 5;
+    // far-first partner deltas of the 8 parity classes (double2 delta in the low
+    // 16 bits, float4 delta in the high 16), resident for the whole launch
+    for (int e = threadIdx.x; e < 8 * MAX_ENTRIES; e += blockDim.x) {
+        const int4 en = a.t.entries_ws[e];
+        s_ent[e] = (unsigned)en.y | ((unsigned)en.w << 16);
+    }
+    for (;;) {
+        if (threadIdx.x == 0) tile = atomicAdd(a.wl.counts + WL_M2L_NEXT, 1);
+        __syncthreads();
+        const int t = tile;
+        if (t >= total) break;
+        const int item_idx = (t < ROOT_UNITS_FAST * nroot) ? a.wl.root[t / ROOT_UNITS_FAST]
+                                                            : a.wl.m2l[(t - ROOT_UNITS_FAST * nroot) >> 1];
+        load_item(a, item_idx, it);
+        const int x0 = TILE_X * (t & 1);
+        const size_t sub = (size_t)it.subgrid;
+        OutPtr out{a.L + sub * 20 * NCELL, a.Lc + sub * 3 * NCELL, NCELL, true};
+        if (it.kind == OTFMM_KIND_M2L_ROOT) {
+            double* sm = reinterpret_cast<double*>(fz_dyn);
+            for (int r = threadIdx.x; r < NCELL; r += blockDim.x)
+                for (int q = 0; q < NCOMP; ++q)
+                    sm[q * NCELL + r] = (q < 20) ? a.M[(sub * 20 + q) * NCELL + r] * stage_scale<PREC_FAST>(q)
+                                                 : a.com[(sub * 3 + (q - 20)) * NCELL + r];
+            __syncthreads();
+            root_unit_fast<true, FZ_THREADS / 32>(sm, t % ROOT_UNITS_FAST, a.t, out);
+        } else {
+            const double inv_dx = 1.0 / it.dx;
+            stage_region_fz(sf, sb, it, x0, inv_dx, a.M, a.com, a.mon);
+            __syncthreads();
+            fz_tile<CHUNK>(sf, sb, s_ent, x0, warp, a.t, it.leafmask, inv_dx, out);
+        }
+        __syncthreads();   // shared memory and `it` are reused by the next tile
+    }
+}
+
 }   // namespace otfmm

@@ -245,7 +245,7 @@ struct otfmm_context {
     double* d_soa_scratch = nullptr;   // host-buffer path staging
     int* d_lists = nullptr;            // batched work lists (grown on demand)
     int list_capacity = 0;
-    otfmm_tuning tuning = {OTFMM_SPLIT_WARP_SPECIALISED, 16, 32, 4, OTFMM_P2P_BOX, OTFMM_P2M_LANES};
+    otfmm_tuning tuning = {OTFMM_SPLIT_FUSED, 16, 32, 4, OTFMM_P2P_BOX, OTFMM_P2M_LANES};
     // otfmm_batch_host: device copies of the pool, work list and outputs, a
     // pinned host copy of the reordered work list, two copy streams and events
     struct HostPath {
@@ -305,6 +305,7 @@ int ensure_attributes(int device) {
     rc = rc ? rc : set_smem(m2l_batch_kernel<PREC_FAST, false>, bytes);
     rc = rc ? rc : set_smem(m2l_batch_kernel<PREC_SPLIT, true>, S_SMEM_DOUBLES * (int)sizeof(double));
     rc = rc ? rc : set_smem(m2l_batch_kernel<PREC_SPLIT, false>, S_SMEM_DOUBLES * (int)sizeof(double));
+    rc = rc ? rc : set_smem(m2l_split_fz_kernel<16>, FZ_SMEM_BYTES);
     rc = rc ? rc : set_smem(m2l_split_ws_kernel<16, false, true>, WS_SMEM_BYTES);
     rc = rc ? rc : set_smem(m2l_split_ws_kernel<8, false, true>, WS_SMEM_BYTES);
     rc = rc ? rc : set_smem(m2l_split_ws_kernel<16, true, true>, WS_SMEM_BYTES);
@@ -494,7 +495,8 @@ int otfmm_create(int device, double theta, otfmm_context** out) {
                     entries_split[p * MAX_ENTRIES + k] = int4{row + (qz >> 1), en.y, 2 * row + S_FOFF + (qz >> 1), 0};
                     entries_ws[p * MAX_ENTRIES + k] =
                         int4{cls * WA_CLS + (qx >> 1) * WA_XS + (qy >> 1) * WA_ROW + (qz >> 1),
-                             cls * WB_CLS + (qx >> 1) * WB_XS + (qy >> 1) * WB_ROW + (qz >> 1), en.y, 0};
+                             cls * WB_CLS + (qx >> 1) * WB_XS + (qy >> 1) * WB_ROW + (qz >> 1), en.y,
+                             cls * FZ_CLS + (qx >> 1) * FZ_XS + (qy >> 1) * FZ_ROW + (qz >> 1)};
                     entries_fast[p * MAX_ENTRIES + k++] = en;
                 }
                 if (pass == 0 && far) ++ctx->counts_far[p];
@@ -973,7 +975,7 @@ namespace {
 
 int check_tuning(const otfmm_tuning& t) {
     if (t.split_m2l_form != OTFMM_SPLIT_WARP_SPECIALISED && t.split_m2l_form != OTFMM_SPLIT_SINGLE_ROLE &&
-        t.split_m2l_form != OTFMM_SPLIT_WARP_SPECIALISED_PACKED)
+        t.split_m2l_form != OTFMM_SPLIT_WARP_SPECIALISED_PACKED && t.split_m2l_form != OTFMM_SPLIT_FUSED)
         return fail(OTFMM_ERR_INVALID, "unknown split M2L form");
     if (t.split_m2l_chunk != 8 && t.split_m2l_chunk != 16) return fail(OTFMM_ERR_INVALID, "split M2L chunk must be 8 or 16");
     if (t.split_p2p_chunk != 16 && t.split_p2p_chunk != 32) return fail(OTFMM_ERR_INVALID, "split P2P chunk must be 16 or 32");
@@ -1066,7 +1068,11 @@ int enqueue_batch(otfmm_context* ctx, const double* pool_M, const double* pool_c
     } else {
         if (precision == OTFMM_FP32_SPLIT) {
             const size_t sbytes = S_SMEM_DOUBLES * sizeof(double);
-            if (rho && tu.split_m2l_form != OTFMM_SPLIT_SINGLE_ROLE) {
+            if (rho && tu.split_m2l_form == OTFMM_SPLIT_FUSED) {
+                // promotes every 16 partners whatever the chunk field (every 32 measured
+                // up to 1.4e-6 force error on the uniform batch)
+                m2l_split_fz_kernel<16><<<tiles_grid, FZ_THREADS, FZ_SMEM_BYTES, s>>>(a);
+            } else if (rho && tu.split_m2l_form != OTFMM_SPLIT_SINGLE_ROLE) {
                 const bool packed = (tu.split_m2l_form == OTFMM_SPLIT_WARP_SPECIALISED_PACKED);
                 if (tu.split_m2l_chunk == 8) {
                     if (packed) m2l_split_ws_kernel<8, true, true><<<tiles_grid, WS_THREADS, WS_SMEM_BYTES, s>>>(a);
@@ -1593,12 +1599,13 @@ int otfmm_autotune(otfmm_context* ctx, const double* pool_M, const double* pool_
     otfmm_tuning best = ctx->tuning;
     float tbest = 0.f;
     rc = time_of(best, tbest);
-    const int forms[3] = {OTFMM_SPLIT_WARP_SPECIALISED_PACKED, OTFMM_SPLIT_WARP_SPECIALISED, OTFMM_SPLIT_SINGLE_ROLE};
+    const int forms[4] = {OTFMM_SPLIT_WARP_SPECIALISED_PACKED, OTFMM_SPLIT_WARP_SPECIALISED, OTFMM_SPLIT_SINGLE_ROLE,
+                          OTFMM_SPLIT_FUSED};
     const int m2l_chunks[2] = {8, 16}, p2p_chunks[2] = {16, 32}, lanes[3] = {4, 8, 16};
     const int p2p_forms[2] = {OTFMM_P2P_BOX, OTFMM_P2P_STENCIL}, p2m_forms[2] = {OTFMM_P2M_LANES, OTFMM_P2M_COARSE};
     const bool split = (precision == OTFMM_FP32_SPLIT), fast = (precision != OTFMM_FP64_EXACT);
     for (int dim = 0; dim < 6 && rc == OTFMM_OK; ++dim) {
-        const int nvar = (dim == 3 || dim == 0) ? 3 : 2;
+        const int nvar = dim == 0 ? 4 : dim == 3 ? 3 : 2;
         if ((dim < 3 && !split) || (dim >= 3 && !fast)) continue;
         for (int v = 0; v < nvar && rc == OTFMM_OK; ++v) {
             otfmm_tuning tu = best;

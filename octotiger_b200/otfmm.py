@@ -33,8 +33,8 @@ EXPORTED = ["otfmm_create", "otfmm_destroy", "otfmm_stencil_info", "otfmm_m2l_so
 
 _lib = None
 
-SPLIT_WARP_SPECIALISED, SPLIT_SINGLE_ROLE, SPLIT_WARP_SPECIALISED_PACKED = 0, 1, 2
-SPLIT_FORMS = {0: "warp_specialised", 1: "single_role", 2: "warp_specialised_packed"}
+SPLIT_WARP_SPECIALISED, SPLIT_SINGLE_ROLE, SPLIT_WARP_SPECIALISED_PACKED, SPLIT_FUSED = 0, 1, 2, 3
+SPLIT_FORMS = {0: "warp_specialised", 1: "single_role", 2: "warp_specialised_packed", 3: "fused"}
 P2P_FORMS = {0: "box", 1: "stencil"}
 P2M_FORMS = {0: "coarse", 1: "lanes"}
 
@@ -366,6 +366,29 @@ class BatchSolver:
         d = torch.device("cuda", ctx.device)
         self.L = torch.zeros((pool.n, 20, NCELL), dtype=torch.float64, device=d)
         self.Lc = torch.zeros((pool.n, 3, NCELL), dtype=torch.float64, device=d)
+
+    @classmethod
+    def from_device(cls, ctx: Context, dev: DevicePool, items: np.ndarray) -> "BatchSolver":
+        """A solve over records already resident on the context's device (for
+        example a rank's shard after its halo exchange), with no host copy."""
+        torch = _require_cuda()
+        n = int(dev.n)
+        if tuple(dev.M.shape) != (n, 20, NCELL) or tuple(dev.com.shape) != (n, 3, NCELL) or \
+                tuple(dev.mon.shape) != (n, NCELL) or tuple(dev.is_leaf.shape) != (n,):
+            raise ValueError("device pool arrays have inconsistent shapes")
+        if dev.M.dtype != torch.float64 or dev.is_leaf.dtype != torch.uint8:
+            raise ValueError("device pool: float64 records and uint8 leaf flags expected")
+        self = cls.__new__(cls)
+        self.ctx = ctx
+        self.dev = DevicePool(M=dev.M.contiguous(), com=dev.com.contiguous(), mon=dev.mon.contiguous(),
+                              is_leaf=dev.is_leaf.contiguous(), n=n)
+        self.items_host = order_work_list(items)
+        self.items = upload_work_list(self.items_host, n, ctx.device)
+        self.n_items = len(items)
+        d = torch.device("cuda", ctx.device)
+        self.L = torch.zeros((n, 20, NCELL), dtype=torch.float64, device=d)
+        self.Lc = torch.zeros((n, 3, NCELL), dtype=torch.float64, device=d)
+        return self
 
     def run(self, gsolve_type=RHO, precision=FP64, stream=None) -> None:
         self.ctx.batch(self.dev, self.items, self.n_items, self.L, self.Lc, gsolve_type, precision, stream)

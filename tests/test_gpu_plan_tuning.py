@@ -58,7 +58,11 @@ def test_plan_replays_batch(ctx, precision, solve):
     plan.close()
 
 
-VARIANTS = list(itertools.product([0, 1, 2], [8, 16], [16, 32], [4, 8, 16]))
+# (split M2L form, M2L chunk, P2P chunk, P2M lanes): the warp-specialised,
+# single-role and packed forms with chunks 8 / 16, the fused form with 16
+VARIANTS = (list(itertools.product([0, 1, 2], [8, 16], [16, 32], [4, 8, 16]))
+            + list(itertools.product([3], [16], [16, 32], [4, 8])))
+ALLOWED = list(itertools.product([0, 1, 2, 3], [8, 16], [16, 32], [4, 8, 16]))
 P2P_FORMS = (0, 1)   # OTFMM_P2P_BOX, OTFMM_P2P_STENCIL
 P2M_FORMS = (0, 1)   # OTFMM_P2M_COARSE, OTFMM_P2M_LANES
 
@@ -118,7 +122,7 @@ def test_autotune_keeps_an_allowed_variant(ctx, oracle):
     try:
         s = BatchSolver(ctx, b.pool, b.items)
         t = s.autotune(RHO, "fp32_split", repeats=2)
-        assert (t.split_m2l_form, t.split_m2l_chunk, t.split_p2p_chunk, t.p2m_lanes) in VARIANTS
+        assert (t.split_m2l_form, t.split_m2l_chunk, t.split_p2p_chunk, t.p2m_lanes) in ALLOWED
         assert t.p2p_form in P2P_FORMS and t.p2m_form in P2M_FORMS
         got = ctx.get_tuning()
         assert got.as_dict() == t.as_dict()
@@ -133,7 +137,7 @@ def test_autotune_keeps_an_allowed_variant(ctx, oracle):
 def test_invalid_variants_rejected(ctx):
     from octotiger_b200.otfmm import OtfmmError, Tuning
     keep = ctx.get_tuning()
-    for bad in (Tuning(3, 16, 32, 16), Tuning(0, 12, 32, 16), Tuning(0, 16, 8, 16), Tuning(0, 16, 32, 3),
+    for bad in (Tuning(4, 16, 32, 16), Tuning(0, 12, 32, 16), Tuning(0, 16, 8, 16), Tuning(0, 16, 32, 3),
                 Tuning(0, 16, 32, 16, 2), Tuning(0, 16, 32, 16, 0, 2)):
         with pytest.raises(OtfmmError):
             ctx.set_tuning(bad)

@@ -1,6 +1,8 @@
 """Multi-rank sharding of a work list, on the CPU with gloo ranks (world sizes 2 and 3):
 partition coverage and balance, halo exchange of remote neighbour records, and
-a sharded solve (oracle as the per-rank compute) equal to the global one."""
+a sharded solve (shard.sharded_problem per rank, the oracle as the per-rank
+compute) equal to the global one; records pack and unpack losslessly; a work
+list with two items for one subgrid is refused."""
 from __future__ import annotations
 
 import os
@@ -56,15 +58,8 @@ def _worker(rank, world, port, result_path):
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     try:
         b = _small_amr()
-        parts = shard.partition(b.items, b.levels, b.positions, world)
-        owner = np.full(b.pool.n, -1)
-        for r, p in enumerate(parts):
-            owner[b.items["subgrid"][p]] = r
-        mine = parts[rank]
-        own_ids = np.sort(b.items["subgrid"][mine])
-        owned = shard.SubgridPool(M=b.pool.M[own_ids].copy(), com=b.pool.com[own_ids].copy(),
-                                  mon=b.pool.mon[own_ids].copy(), is_leaf=b.pool.is_leaf[own_ids].copy())
-        local = shard.exchange(b.items[mine], own_ids, owned, rank, world, lambda g: int(owner[g]), dist)
+        # the function bench.py --sharded runs per rank (there with NCCL and a CUDA device)
+        local = shard.sharded_problem(b, rank, world, dist)
         # every record the rank reads equals the global one
         for li, g in enumerate(local.global_ids):
             assert np.array_equal(local.pool.M[li], b.pool.M[g])
@@ -98,3 +93,24 @@ def test_sharded_solve_equals_global(tmp_path, world):
             np.testing.assert_array_equal(L, Lg[g])
             np.testing.assert_array_equal(Lc, Lcg[g])
     assert seen == set(int(s) for s in b.items["subgrid"])
+
+
+def test_records_round_trip():
+    import torch
+    b = _small_amr()
+    idx = [0, 3, 5]
+    t = shard.pack_records(b.pool.M[idx], b.pool.com[idx], b.pool.mon[idx], b.pool.is_leaf[idx])
+    assert t.shape == (3, shard.RECORD)
+    M, com, mon, leaf = shard.unpack_records(t)
+    assert np.array_equal(M.numpy(), b.pool.M[idx]) and np.array_equal(com.numpy(), b.pool.com[idx])
+    assert np.array_equal(mon.numpy(), b.pool.mon[idx]) and np.array_equal(leaf.numpy(), b.pool.is_leaf[idx])
+    # the device path packs torch tensors the same way
+    tt = shard.pack_records(*(torch.from_numpy(getattr(b.pool, k)[idx]) for k in ("M", "com", "mon", "is_leaf")))
+    assert torch.equal(tt, t)
+
+
+def test_partition_refuses_split_subgrid():
+    b = _small_amr()
+    items = np.concatenate([b.items, b.items[:1]])
+    with pytest.raises(ValueError):
+        shard.partition(items, b.levels, b.positions, 2)
