@@ -398,6 +398,34 @@ def gpu_arm(args) -> None:
         e2e_ms = float(t.item())
     e2e_value = world * counts["total"] * args.steps / (e2e_ms * 1e-3)
 
+    # end to end through the reference's own interfaces: the C++ drop-in adapter
+    # (include/otfmm_octotiger.hpp) called once per node from all host threads,
+    # as node_server::compute_fmm calls multipole_kernel_interface /
+    # monopole_kernel_interface, with AoS inputs; concurrent calls aggregated
+    # into batched solves (otfmm_aggregator). Wall time of a whole pass.
+    e2e_adapter = None
+    if not args.no_adapter:
+        from octotiger_b200.otfmm import adapter_pass
+        nthr = os.cpu_count() or 8
+        La, Lca, sec = adapter_pass(ctx, batch.pool, batch.items, solve, args.precision, aggregate=True,
+                                    threads=nthr, max_subgrids=4096, max_items=2048, passes=4)
+        leaf_items = batch.items["kind"] == 2
+        sub_m = batch.items["subgrid"][~leaf_items]
+        sub_l = batch.items["subgrid"][leaf_items]
+        adapter_matches = bool(np.array_equal(La[sub_m], Ld.numpy()[sub_m]) and
+                               np.array_equal(La[sub_l, :4], Ld.numpy()[sub_l, :4]))
+        _, _, sec1 = adapter_pass(ctx, batch.pool, batch.items, solve, args.precision, aggregate=False,
+                                  threads=nthr, passes=1)
+        t_agg = float(np.median(sec[1:]))
+        e2e_adapter = {"value": counts["total"] / t_agg, "unit": UNIT, "s_per_pass": t_agg,
+                       "host_threads": nthr, "passes_timed": len(sec) - 1,
+                       "what": "every node's multipole_kernel_interface / monopole_kernel_interface call through the "
+                               "C++ drop-in adapter from all host threads at once, AoS inputs, calls aggregated into "
+                               "batched solves (wall time of a pass, first call to last return)",
+                       "matches_device_solve": adapter_matches,
+                       "per_call_value": counts["total"] / float(sec1[0]), "per_call_s_per_pass": float(sec1[0]),
+                       "per_call_what": "the same calls without aggregation: one host-buffer kernel call per node"}
+
     # a whole gravity solve where the workload is a full octree (upward M2M,
     # the interaction solve replayed from its graph, downward L2L with the
     # leaves' potential and acceleration), device time per solve
@@ -492,6 +520,7 @@ def gpu_arm(args) -> None:
         "accuracy_vs_fp64_exact": accuracy,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "matches_device_solve": e2e_matches},
+        "e2e_adapter": e2e_adapter,
         "gpu_launches": 4 * args.steps,
         "roofline": roof,
         "clocks": clk.summary(),
@@ -607,6 +636,7 @@ def main() -> None:
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-per-subgrid", action="store_true", help="skip the per-subgrid FP64 comparison")
+    ap.add_argument("--no-adapter", action="store_true", help="skip the end-to-end leg through the C++ adapter")
     ap.add_argument("--sharded", action="store_true",
                     help="partition one solve over the ranks (strong scaling) instead of one replica per rank")
     args = ap.parse_args()

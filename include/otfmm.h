@@ -335,6 +335,46 @@ int otfmm_downward(otfmm_context* ctx, const double* pool_com, const uint8_t* po
 long long otfmm_count_pairs(const otfmm_context* ctx, const uint8_t* is_leaf, int32_t n_subgrids,
                             const otfmm_work_item* items, int32_t n_items, long long per_class[4]);
 
+/* Aggregation of per-node calls (no single counterpart in the reference, whose
+ * node_server::compute_fmm calls the interaction interfaces once per node from
+ * many threads at once, src/node_server.cpp:717-722; its Kokkos backend fuses
+ * concurrent monopole calls, octotiger/monopole_interactions/kernel/
+ * kokkos_kernel.hpp:1357-1405, and its CUDA backend spreads callers over a
+ * stream pool, src/multipole_interactions/legacy/
+ * cuda_multipole_interaction_interface.cpp:64-70). Concurrent calls of every
+ * kind join one batched solve (otfmm_batch_host on the aggregator's own stream):
+ *   1. otfmm_aggregator_reserve(n records: own subgrid first, then neighbours):
+ *      slots[i] is record i's pool slot in the open batch; fill[i] the parts
+ *      (OTFMM_AGG_* bits of need[i]) this caller must write - a record whose
+ *      non-zero key is already in the batch needs none (key = an address that
+ *      identifies the data, the same for a node's own call and for the
+ *      payloads that alias it; 0 = never shared). Blocks while both batch
+ *      buffers are busy.
+ *   2. otfmm_aggregator_record: host pointers to a slot's pinned storage
+ *      (M[20][512], com[3][512], mon[512]); write the parts of fill[i].
+ *   3. otfmm_aggregator_submit: the call's work item (subgrid and neighbour
+ *      fields are slots, -1 = empty); blocks until its batch has run, then
+ *      writes L (20 x 512 for multipole items, 4 x 512 for leaves, SoA) and,
+ *      when L_c is not NULL, L_c (3 x 512).
+ * A batch runs when it is full and all its reserved calls have submitted, or
+ * when it has been idle for idle_us with no call between reserve and submit;
+ * one waiting caller runs it. All calls of an aggregator share its solve type
+ * and precision. Thread-safe; no context-wide lock is held while callers copy
+ * their data. Destroy only with no call in flight. */
+#define OTFMM_AGG_M 1
+#define OTFMM_AGG_COM 2
+#define OTFMM_AGG_MON 4
+typedef struct otfmm_aggregator otfmm_aggregator;
+int otfmm_aggregator_create(otfmm_context* ctx, int32_t max_subgrids, int32_t max_items, int32_t idle_us,
+                            int gsolve_type, int precision, otfmm_aggregator** out);
+int otfmm_aggregator_destroy(otfmm_aggregator* agg);
+int otfmm_aggregator_reserve(otfmm_aggregator* agg, int32_t n, const uint64_t* keys, const uint8_t* is_leaf,
+                             const uint8_t* need, int32_t* slots, uint8_t* fill, int64_t* ticket);
+int otfmm_aggregator_record(otfmm_aggregator* agg, int64_t ticket, int32_t slot, double** M, double** com,
+                            double** mon);
+int otfmm_aggregator_submit(otfmm_aggregator* agg, int64_t ticket, const otfmm_work_item* item, double* L,
+                            double* L_c);
+
 /* Checks a device-side error flag written by the last otfmm_batch on `stream`
  * without synchronizing the whole device: returns OTFMM_OK or OTFMM_ERR_DEVICE. */
 int otfmm_batch_status(otfmm_context* ctx, void* stream);

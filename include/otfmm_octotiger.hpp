@@ -39,6 +39,7 @@
 #include <array>
 #include <cstddef>
 #include <cstdio>
+#include <cstdint>
 #include <cstdlib>
 #include <iostream>
 #include <memory>
@@ -410,6 +411,171 @@ int monopole_kernel_interface(otfmm_context* ctx, const std::vector<double>& mon
     if (!grid) return OTFMM_ERR_INVALID;
     return monopole_kernel_impl(ctx, monopoles, com_ptr, neighbors, type, dx, grid->get_L(), grid->get_L_c(),
                                 contains_multipole_neighbor, precision, grid);
+}
+
+// ---------------------------------------------------------------- aggregated calls
+// The same two interfaces on an otfmm_aggregator (otfmm.h): the call's records
+// (its own subgrid, then its neighbours' payloads) go into the open batch's
+// pinned pool slots - a payload that aliases data already in the batch (same
+// address) is not copied again - and the call waits for the batched solve its
+// work item joined. Output semantics as above. `type` must be the aggregator's
+// solve type; the precision is the aggregator's.
+template <class T>
+inline uint64_t data_key(const T* p) {
+    return static_cast<uint64_t>(reinterpret_cast<std::uintptr_t>(p));
+}
+
+// One aggregated call: own record (M + com for a refined node, masses + com for
+// a leaf) and the 26 neighbour payloads; L (ncomp x 512) and L_c (3 x 512) SoA out.
+template <class Multipole, class SpaceVector, class Neighbor, class GridPtr>
+int aggregated_call(otfmm_aggregator* agg, int kind, const std::vector<Multipole>* own_M,
+                    const std::vector<double>* own_mon, const SpaceVector* own_com,
+                    const std::vector<Neighbor>& neighbors, double dx, const std::array<double, 3>& xbase,
+                    const GridPtr& grid, double* L, double* Lc) {
+    uint64_t keys[27];
+    uint8_t leaf[27], need[27], fill[27];
+    int32_t slots[27];
+    int dir_of[27];
+    const bool own_leaf = (kind == OTFMM_KIND_LEAF);
+    keys[0] = own_leaf ? data_key(own_mon->data()) : data_key(own_M->data());
+    leaf[0] = own_leaf ? 1 : 0;
+    need[0] = own_leaf ? (OTFMM_AGG_MON | OTFMM_AGG_COM) : (OTFMM_AGG_M | OTFMM_AGG_COM);
+    dir_of[0] = -1;
+    int n = 1;
+    if (kind != OTFMM_KIND_M2L_ROOT) {
+        for (int d = 0; d < 26; ++d) {
+            const Neighbor& nb = neighbors[d];
+            if (nb.is_monopole) {
+                if (!nb.data.m) continue;
+                keys[n] = nb.data.m->size() == NCELL ? data_key(nb.data.m->data()) : 0;
+                leaf[n] = 1;
+                need[n] = OTFMM_AGG_MON;
+            } else {
+                if (!nb.data.M) continue;
+                const bool full = nb.data.M->size() == NCELL && nb.data.x && nb.data.x->size() == NCELL;
+                keys[n] = full ? data_key(nb.data.M->data()) : 0;
+                leaf[n] = 0;
+                need[n] = OTFMM_AGG_M | OTFMM_AGG_COM;
+            }
+            dir_of[n++] = d;
+        }
+    }
+    int64_t ticket = 0;
+    int rc = otfmm_aggregator_reserve(agg, n, keys, leaf, need, slots, fill, &ticket);
+    if (rc != OTFMM_OK) return rc;
+    otfmm_work_item item{};
+    item.subgrid = slots[0];
+    item.kind = kind;
+    item.dx = dx;
+    for (int a = 0; a < 3; ++a) item.xbase[a] = xbase[a];
+    for (int d = 0; d < 26; ++d) item.neighbors[d] = -1;
+    for (int i = 0; i < n && rc == OTFMM_OK; ++i) {
+        if (i > 0) item.neighbors[dir_of[i]] = slots[i];
+        if (!fill[i]) continue;
+        double *M, *com, *mon;
+        rc = otfmm_aggregator_record(agg, ticket, slots[i], &M, &com, &mon);
+        if (rc != OTFMM_OK) break;
+        if (i == 0) {
+            for (int u = 0; u < NCELL; ++u) {
+                if (fill[0] & OTFMM_AGG_M)
+                    for (int c = 0; c < 20; ++c) M[c * NCELL + u] = (*own_M)[u][c];
+                if (fill[0] & OTFMM_AGG_COM)
+                    for (int c = 0; c < 3; ++c) com[c * NCELL + u] = own_com[u][c];
+                if (fill[0] & OTFMM_AGG_MON) mon[u] = (*own_mon)[u];
+            }
+            continue;
+        }
+        const int d = dir_of[i];
+        const Neighbor& nb = neighbors[d];
+        if (keys[i] != 0) {   // full-size payload
+            for (int u = 0; u < NCELL; ++u) {
+                if (fill[i] & OTFMM_AGG_MON) mon[u] = (*nb.data.m)[u];
+                if (fill[i] & OTFMM_AGG_M)
+                    for (int c = 0; c < 20; ++c) M[c * NCELL + u] = (*nb.data.M)[u][c];
+                if (fill[i] & OTFMM_AGG_COM)
+                    for (int c = 0; c < 3; ++c) com[c * NCELL + u] = (*nb.data.x)[u][c];
+            }
+            continue;
+        }
+        // compressed payload (get_ilist_n_bnd order): zeros, then the listed cells
+        std::fill(M, M + 20 * NCELL, 0.0);
+        std::fill(com, com + 3 * NCELL, 0.0);
+        std::fill(mon, mon + NCELL, 0.0);
+        if (nb.is_monopole) {
+            const auto& m = *nb.data.m;
+            rc = expand_compressed(grid, d, m.size(), [&](size_t k, int x, int y, int z) {
+                mon[flat_inner(x, y, z)] = m[k];
+            });
+        } else {
+            const auto& nM = *nb.data.M;
+            const size_t cnt = nb.data.x ? std::min(nM.size(), nb.data.x->size()) : 0;
+            rc = expand_compressed(grid, d, cnt, [&](size_t k, int x, int y, int z) {
+                const int u = flat_inner(x, y, z);
+                for (int c = 0; c < 20; ++c) M[c * NCELL + u] = nM[k][c];
+                for (int c = 0; c < 3; ++c) com[c * NCELL + u] = (*nb.data.x)[k][c];
+            });
+        }
+    }
+    if (rc != OTFMM_OK) {
+        // release the reservation so the batch can run without this call
+        item.subgrid = -1;
+        otfmm_aggregator_submit(agg, ticket, &item, L, nullptr);
+        return rc;
+    }
+    return otfmm_aggregator_submit(agg, ticket, &item, L, Lc);
+}
+
+// multipole_kernel_interface on an aggregator, the reference's argument list
+// (multipole_kernel_interface.hpp:18-22).
+template <class Multipole, class SpaceVector, class Neighbor, class GridPtr>
+int multipole_kernel_interface(otfmm_aggregator* agg, const std::vector<double>& /*monopoles*/,
+                               const std::vector<Multipole>& M_ptr,
+                               const std::vector<std::shared_ptr<std::vector<SpaceVector>>>& com_ptr,
+                               const std::vector<Neighbor>& neighbors, int type, double dx,
+                               const std::array<bool, 26>& /*is_direction_empty*/, std::array<double, 3> xbase,
+                               const GridPtr& grid, bool use_root_stencil) {
+    if (!agg || !grid || M_ptr.size() != NCELL || com_ptr.empty() || !com_ptr[0]) return OTFMM_ERR_INVALID;
+    std::vector<double> L(20 * NCELL), Lc(3 * NCELL);
+    const int kind = use_root_stencil ? OTFMM_KIND_M2L_ROOT : OTFMM_KIND_M2L;
+    const int rc = aggregated_call(agg, kind, &M_ptr, static_cast<const std::vector<double>*>(nullptr),
+                                   com_ptr[0]->data(), neighbors, dx, xbase, grid, L.data(), Lc.data());
+    if (rc != OTFMM_OK) return rc;
+    auto& gL = grid->get_L();
+    for (int c = 0; c < 20; ++c)
+        for (int u = 0; u < NCELL; ++u) gL[u][c] += L[c * NCELL + u];
+    if (type == OTFMM_RHO) {
+        auto& gLc = grid->get_L_c();
+        for (int c = 0; c < 3; ++c)
+            for (int u = 0; u < NCELL; ++u) gLc[u][c] = Lc[c * NCELL + u];
+    }
+    return OTFMM_OK;
+}
+
+// monopole_kernel_interface on an aggregator, the reference's argument list
+// (monopole_kernel_interface.hpp:19-23): L[0..3] += P2P (+ P2M); L_c = the
+// P2M correction when a neighbour is refined (RHO).
+template <class SpaceVector, class Neighbor, class GridPtr>
+int monopole_kernel_interface(otfmm_aggregator* agg, const std::vector<double>& monopoles,
+                              const std::vector<std::shared_ptr<std::vector<SpaceVector>>>& com_ptr,
+                              const std::vector<Neighbor>& neighbors, int type, double dx,
+                              const std::array<bool, 26>& /*is_direction_empty*/, const GridPtr& grid,
+                              bool contains_multipole_neighbor) {
+    if (!agg || !grid || monopoles.size() != NCELL || com_ptr.empty() || !com_ptr[0]) return OTFMM_ERR_INVALID;
+    std::vector<double> L(4 * NCELL), Lc(3 * NCELL);
+    using Multipole = std::array<double, 20>;
+    const std::array<double, 3> xbase{0.0, 0.0, 0.0};   // leaves use integer offsets only
+    const int rc = aggregated_call(agg, OTFMM_KIND_LEAF, static_cast<const std::vector<Multipole>*>(nullptr),
+                                   &monopoles, com_ptr[0]->data(), neighbors, dx, xbase, grid, L.data(), Lc.data());
+    if (rc != OTFMM_OK) return rc;
+    auto& gL = grid->get_L();
+    for (int c = 0; c < 4; ++c)
+        for (int u = 0; u < NCELL; ++u) gL[u][c] += L[c * NCELL + u];
+    if (contains_multipole_neighbor && type == OTFMM_RHO) {
+        auto& gLc = grid->get_L_c();
+        for (int c = 0; c < 3; ++c)
+            for (int u = 0; u < NCELL; ++u) gLc[u][c] = Lc[c * NCELL + u];
+    }
+    return OTFMM_OK;
 }
 
 }   // namespace otfmm_octotiger

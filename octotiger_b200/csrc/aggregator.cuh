@@ -1,0 +1,287 @@
+// Aggregation of concurrent per-node interaction calls into batched solves
+// (host side of libotfmm.so; included once by otfmm.cu after the context).
+//
+// node_server::compute_fmm calls the reference's interaction interfaces once
+// per node, from many HPX worker threads at once (src/node_server.cpp:717-722).
+// The reference's Kokkos backend fuses concurrent monopole calls into one
+// launch (monopole_kernel_agg, octotiger/monopole_interactions/kernel/
+// kokkos_kernel.hpp:1357-1405) and its CUDA backend spreads callers over a
+// per-GPU stream pool (src/multipole_interactions/legacy/
+// cuda_multipole_interaction_interface.cpp:64-70). Here every kind of call
+// (multipole, root, monopole with P2M) joins one open batch:
+//   * otfmm_aggregator_reserve gives the call pool slots for its own subgrid and
+//     its neighbours' records in pinned host memory; a record whose key (the
+//     address of the caller's data, the same for a node and for the payloads
+//     that alias it) is already in the batch is not copied again;
+//   * the caller writes the parts it was asked to fill, without any lock;
+//   * otfmm_aggregator_submit adds its work item and waits for its batch;
+//   * a batch runs (otfmm_batch_host on the aggregator's own stream) once it is
+//     full and every reserved call has submitted, or once it has been idle for
+//     `idle_us` with no call between reserve and submit; one of the waiting
+//     callers runs it, the others sleep on a condition variable;
+//   * two batch buffers: one collects while the other runs.
+#pragma once
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+struct otfmm_aggregator {
+    enum State { FREE, OPEN, CLOSED, RUNNING, DONE };
+    struct Out {
+        double* L;
+        double* Lc;
+        int slot;
+        int kind;
+    };
+    struct Batch {
+        State state = FREE;
+        long long epoch = 0;
+        int n_sub = 0, pending = 0, waiting = 0, rc = OTFMM_OK;
+        std::string msg;
+        std::unordered_map<uint64_t, int> keys;
+        std::vector<uint8_t> claimed;   // per slot: parts some caller fills (OTFMM_AGG_*)
+        std::vector<otfmm_work_item> staged;
+        std::vector<Out> outs;
+        std::chrono::steady_clock::time_point last;
+        double *M = nullptr, *com = nullptr, *mon = nullptr, *L = nullptr, *Lc = nullptr;
+        uint8_t* is_leaf = nullptr;
+        otfmm_work_item* items = nullptr;
+    };
+    otfmm_context* ctx = nullptr;
+    int gsolve = OTFMM_RHO, precision = OTFMM_FP64, cap_sub = 0, cap_items = 0;
+    std::chrono::microseconds idle{200};
+    cudaStream_t stream = nullptr;
+    std::mutex mu;       // batch states
+    std::mutex run_mu;   // one batch on the GPU at a time (the context's host-path buffers)
+    std::condition_variable cv;
+    Batch b[2];
+    long long epochs = 0;
+};
+
+namespace {
+
+void agg_free_buffers(otfmm_aggregator::Batch& b) {
+    cudaFreeHost(b.M);
+    cudaFreeHost(b.com);
+    cudaFreeHost(b.mon);
+    cudaFreeHost(b.L);
+    cudaFreeHost(b.Lc);
+    cudaFreeHost(b.is_leaf);
+    cudaFreeHost(b.items);
+}
+
+// Runs batch `k` (the caller holds no lock; the batch is RUNNING).
+void agg_run(otfmm_aggregator* a, otfmm_aggregator::Batch& b) {
+    // multipole items first, as order_work_list does: the long tiles start first
+    std::stable_partition(b.staged.begin(), b.staged.end(),
+                          [](const otfmm_work_item& w) { return w.kind != OTFMM_KIND_LEAF; });
+    std::copy(b.staged.begin(), b.staged.end(), b.items);
+    std::lock_guard<std::mutex> run(a->run_mu);
+    int rc = otfmm_batch_host(a->ctx, b.M, b.com, b.mon, b.is_leaf, b.n_sub, b.items, (int32_t)b.staged.size(), b.L,
+                              b.Lc, a->gsolve, a->precision, a->stream);
+    if (rc == OTFMM_OK) rc = otfmm_batch_status(a->ctx, a->stream);   // synchronises the stream
+    b.rc = rc;
+    if (rc != OTFMM_OK) b.msg = otfmm_last_error();
+}
+
+}   // namespace
+
+extern "C" {
+
+int otfmm_aggregator_create(otfmm_context* ctx, int32_t max_subgrids, int32_t max_items, int32_t idle_us,
+                            int gsolve_type, int precision, otfmm_aggregator** out) {
+    if (!ctx || !out) return fail(OTFMM_ERR_INVALID, "NULL argument");
+    *out = nullptr;
+    if (max_subgrids < 27 || max_items < 1 || idle_us < 0)
+        return fail(OTFMM_ERR_INVALID, "aggregator: max_subgrids >= 27, max_items >= 1, idle_us >= 0");
+    if (gsolve_type != OTFMM_RHO && gsolve_type != OTFMM_DRHODT) return fail(OTFMM_ERR_INVALID, "bad gsolve_type");
+    int rc = check_precision(precision);
+    if (rc) return rc;
+    DeviceGuard g(ctx->device);
+    auto* a = new otfmm_aggregator;
+    a->ctx = ctx;
+    a->gsolve = gsolve_type;
+    a->precision = precision;
+    a->cap_sub = max_subgrids;
+    a->cap_items = max_items;
+    a->idle = std::chrono::microseconds(idle_us);
+    cudaError_t e = cudaStreamCreateWithFlags(&a->stream, cudaStreamNonBlocking);
+    const size_t n = (size_t)max_subgrids;
+    for (int k = 0; k < 2 && e == cudaSuccess; ++k) {
+        otfmm_aggregator::Batch& b = a->b[k];
+        if ((e = cudaHostAlloc((void**)&b.M, sizeof(double) * n * 20 * NCELL, cudaHostAllocDefault)) != cudaSuccess ||
+            (e = cudaHostAlloc((void**)&b.com, sizeof(double) * n * 3 * NCELL, cudaHostAllocDefault)) != cudaSuccess ||
+            (e = cudaHostAlloc((void**)&b.mon, sizeof(double) * n * NCELL, cudaHostAllocDefault)) != cudaSuccess ||
+            (e = cudaHostAlloc((void**)&b.L, sizeof(double) * n * 20 * NCELL, cudaHostAllocDefault)) != cudaSuccess ||
+            (e = cudaHostAlloc((void**)&b.Lc, sizeof(double) * n * 3 * NCELL, cudaHostAllocDefault)) != cudaSuccess ||
+            (e = cudaHostAlloc((void**)&b.is_leaf, n, cudaHostAllocDefault)) != cudaSuccess ||
+            (e = cudaHostAlloc((void**)&b.items, sizeof(otfmm_work_item) * (size_t)max_items, cudaHostAllocDefault)) !=
+                cudaSuccess)
+            break;
+        b.claimed.reserve(n);
+    }
+    if (e != cudaSuccess) {
+        for (auto& b : a->b) agg_free_buffers(b);
+        if (a->stream) cudaStreamDestroy(a->stream);
+        delete a;
+        return cuda_fail(e, "aggregator buffers");
+    }
+    *out = a;
+    return OTFMM_OK;
+}
+
+int otfmm_aggregator_destroy(otfmm_aggregator* a) {
+    if (!a) return OTFMM_OK;
+    {
+        std::lock_guard<std::mutex> lock(a->mu);
+        for (auto& b : a->b)
+            if (b.state != otfmm_aggregator::FREE && (b.pending > 0 || b.waiting > 0))
+                return fail(OTFMM_ERR_INVALID, "aggregator destroyed with calls in flight");
+    }
+    DeviceGuard g(a->ctx->device);
+    cudaStreamSynchronize(a->stream);
+    for (auto& b : a->b) agg_free_buffers(b);
+    cudaStreamDestroy(a->stream);
+    delete a;
+    return OTFMM_OK;
+}
+
+int otfmm_aggregator_reserve(otfmm_aggregator* a, int32_t n, const uint64_t* keys, const uint8_t* is_leaf,
+                             const uint8_t* need, int32_t* slots, uint8_t* fill, int64_t* ticket) {
+    if (!a || !keys || !is_leaf || !need || !slots || !fill || !ticket) return fail(OTFMM_ERR_INVALID, "NULL argument");
+    if (n < 1 || n > 27 || n > a->cap_sub) return fail(OTFMM_ERR_INVALID, "a call reserves 1..27 records");
+    std::unique_lock<std::mutex> lock(a->mu);
+    for (;;) {
+        int k = -1;
+        for (int i = 0; i < 2 && k < 0; ++i)
+            if (a->b[i].state == otfmm_aggregator::OPEN) k = i;
+        for (int i = 0; i < 2 && k < 0; ++i)
+            if (a->b[i].state == otfmm_aggregator::FREE) {
+                otfmm_aggregator::Batch& nb = a->b[i];
+                nb.state = otfmm_aggregator::OPEN;
+                nb.epoch = ++a->epochs;
+                nb.n_sub = nb.pending = nb.waiting = 0;
+                nb.rc = OTFMM_OK;
+                nb.msg.clear();
+                nb.keys.clear();
+                nb.claimed.clear();
+                nb.staged.clear();
+                nb.outs.clear();
+                nb.last = std::chrono::steady_clock::now();
+                k = i;
+            }
+        if (k < 0) {   // both buffers busy: wait for one to come free
+            a->cv.wait(lock);
+            continue;
+        }
+        otfmm_aggregator::Batch& b = a->b[k];
+        int fresh = 0;
+        for (int i = 0; i < n; ++i) {
+            bool dup = false;
+            for (int j = 0; j < i && !dup; ++j) dup = keys[i] != 0 && keys[j] == keys[i];
+            if (!dup && (keys[i] == 0 || !b.keys.count(keys[i]))) ++fresh;
+        }
+        if (b.n_sub + fresh > a->cap_sub || (int)b.staged.size() + b.pending + 1 > a->cap_items) {
+            // full: no more calls join it; it runs once its reserved calls have submitted
+            b.state = otfmm_aggregator::CLOSED;
+            if (b.pending == 0 && b.staged.empty()) b.state = otfmm_aggregator::FREE;
+            a->cv.notify_all();
+            continue;
+        }
+        for (int i = 0; i < n; ++i) {
+            int s = -1;
+            if (keys[i] != 0) {
+                auto it = b.keys.find(keys[i]);
+                if (it != b.keys.end()) s = it->second;
+            }
+            if (s < 0) {
+                s = b.n_sub++;
+                b.claimed.push_back(0);
+                b.is_leaf[s] = is_leaf[i] ? 1 : 0;
+                if (keys[i] != 0) b.keys.emplace(keys[i], s);
+            } else if ((b.is_leaf[s] != 0) != (is_leaf[i] != 0)) {
+                return fail(OTFMM_ERR_INVALID, "a record key is used for a leaf and for a refined subgrid");
+            }
+            slots[i] = s;
+            fill[i] = (uint8_t)(need[i] & ~b.claimed[s]);
+            b.claimed[s] |= need[i];
+        }
+        ++b.pending;
+        b.last = std::chrono::steady_clock::now();
+        *ticket = (int64_t)((b.epoch << 1) | k);
+        return OTFMM_OK;
+    }
+}
+
+int otfmm_aggregator_record(otfmm_aggregator* a, int64_t ticket, int32_t slot, double** M, double** com,
+                            double** mon) {
+    if (!a || !M || !com || !mon) return fail(OTFMM_ERR_INVALID, "NULL argument");
+    std::lock_guard<std::mutex> lock(a->mu);
+    otfmm_aggregator::Batch& b = a->b[ticket & 1];
+    if (b.epoch != (ticket >> 1) || b.state == otfmm_aggregator::FREE || slot < 0 || slot >= b.n_sub)
+        return fail(OTFMM_ERR_INVALID, "stale ticket or slot out of range");
+    *M = b.M + (size_t)slot * 20 * NCELL;
+    *com = b.com + (size_t)slot * 3 * NCELL;
+    *mon = b.mon + (size_t)slot * NCELL;
+    return OTFMM_OK;
+}
+
+int otfmm_aggregator_submit(otfmm_aggregator* a, int64_t ticket, const otfmm_work_item* item, double* L,
+                            double* L_c) {
+    if (!a || !item || !L) return fail(OTFMM_ERR_INVALID, "NULL argument");
+    std::unique_lock<std::mutex> lock(a->mu);
+    otfmm_aggregator::Batch& b = a->b[ticket & 1];
+    if (b.epoch != (ticket >> 1) || (b.state != otfmm_aggregator::OPEN && b.state != otfmm_aggregator::CLOSED))
+        return fail(OTFMM_ERR_INVALID, "stale ticket");
+    bool ok = item->subgrid >= 0 && item->subgrid < b.n_sub && item->kind >= 0 && item->kind <= 2;
+    for (int d = 0; d < 26; ++d) ok = ok && item->neighbors[d] >= -1 && item->neighbors[d] < b.n_sub;
+    --b.pending;
+    b.last = std::chrono::steady_clock::now();
+    if (!ok) {
+        a->cv.notify_all();
+        return fail(OTFMM_ERR_INVALID, "work item refers to slots outside its batch");
+    }
+    b.staged.push_back(*item);
+    b.outs.push_back({L, L_c, item->subgrid, item->kind});
+    const size_t my = b.outs.size() - 1;
+    ++b.waiting;
+    a->cv.notify_all();
+    for (;;) {
+        if (b.state == otfmm_aggregator::DONE) break;
+        const bool idle = b.state == otfmm_aggregator::OPEN && std::chrono::steady_clock::now() - b.last >= a->idle;
+        if ((b.state == otfmm_aggregator::CLOSED || idle) && b.pending == 0) {
+            b.state = otfmm_aggregator::RUNNING;
+            lock.unlock();
+            agg_run(a, b);
+            lock.lock();
+            b.state = otfmm_aggregator::DONE;
+            a->cv.notify_all();
+            break;
+        }
+        a->cv.wait_for(lock, a->idle);
+    }
+    const int rc = b.rc;
+    const std::string msg = b.msg;
+    const otfmm_aggregator::Out o = b.outs[my];
+    lock.unlock();
+    if (rc == OTFMM_OK) {
+        // multipole items: L (20 x 512) and L_c (3 x 512); leaves: L0..L3 and L_c
+        const int ncomp = (o.kind == OTFMM_KIND_LEAF) ? 4 : 20;
+        std::copy(b.L + (size_t)o.slot * 20 * NCELL, b.L + ((size_t)o.slot * 20 + ncomp) * NCELL, o.L);
+        if (o.Lc) std::copy(b.Lc + (size_t)o.slot * 3 * NCELL, b.Lc + ((size_t)o.slot + 1) * 3 * NCELL, o.Lc);
+    }
+    lock.lock();
+    if (--b.waiting == 0) {
+        b.state = otfmm_aggregator::FREE;
+        a->cv.notify_all();
+    }
+    lock.unlock();
+    return rc == OTFMM_OK ? OTFMM_OK : fail(rc, msg);
+}
+
+}   // extern "C"

@@ -1770,3 +1770,5 @@ int otfmm_measure_fma_peaks(int device, double* fp64_tflops, double* fp32_tflops
 }
 
 }   // extern "C"
+
+#include "aggregator.cuh"

@@ -246,3 +246,40 @@ class RefMath(_Common):
                                 _ptr(Lc), int(nthreads))
         _check(rc, "ref_batch")
         return L, Lc
+
+
+REF_GPU_LIB = REF_DIR / "libotfmm_ref_gpu.so"
+
+
+class RefGpu:
+    """The reference's own CUDA interaction kernels (oracle/build_ref_gpu.sh),
+    run on device buffers in the reference's SoA layout: a comparator for the
+    GPU tests and the timing script, never part of the library."""
+
+    def __init__(self, theta: float = 0.5, path: Path = REF_GPU_LIB):
+        if not Path(path).exists():
+            raise FileNotFoundError("reference GPU build missing (run oracle/build_ref_gpu.sh)")
+        self.lib = ctypes.CDLL(str(path))
+        vp, dp, i = ctypes.c_void_p, ctypes.c_double, ctypes.c_int
+        self.lib.refgpu_init.argtypes = [dp]
+        self.lib.refgpu_m2l.argtypes = [vp, vp, vp, vp, vp, vp, dp, i, vp]
+        self.lib.refgpu_p2p.argtypes = [vp, vp, vp, dp, dp, vp]
+        self.lib.refgpu_m2l_scratch_doubles.restype = ctypes.c_size_t
+        self.lib.refgpu_p2p_scratch_doubles.restype = ctypes.c_size_t
+        self.theta = float(theta)
+        _check(self.lib.refgpu_init(self.theta), "refgpu_init")
+
+    def m2l_scratch(self) -> int:
+        return int(self.lib.refgpu_m2l_scratch_doubles())
+
+    def p2p_scratch(self) -> int:
+        return int(self.lib.refgpu_p2p_scratch_doubles())
+
+    def m2l(self, mon, com, M, scratch, L, Lc, rho=True, stream=0):
+        """Device pointers (ints) or torch tensors; asynchronous on `stream`."""
+        p = [t if isinstance(t, int) else t.data_ptr() for t in (mon, com, M, scratch, L, Lc)]
+        _check(self.lib.refgpu_m2l(*p, self.theta, int(rho), stream), "refgpu_m2l")
+
+    def p2p(self, mon, scratch, L4, dx, stream=0):
+        p = [t if isinstance(t, int) else t.data_ptr() for t in (mon, scratch, L4)]
+        _check(self.lib.refgpu_p2p(*p, self.theta, float(dx), stream), "refgpu_p2p")

@@ -14,6 +14,7 @@ ROOT = Path(__file__).resolve().parents[1]
 def test_compressed_payload_staging(tmp_path):
     exe = tmp_path / "staging_test"
     subprocess.run(["g++", "-std=c++17", "-O2", "-Wall", "-Werror", "-I", str(ROOT / "include"),
+                    "-I", str(ROOT / "octotiger_b200" / "csrc"),
                     str(ROOT / "tests" / "cpp" / "staging_test.cpp"), "-o", str(exe)], check=True)
     r = subprocess.run([str(exe)], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr

@@ -21,7 +21,8 @@ ROOT = Path(__file__).resolve().parents[1]
 def adapter_bin(tmp_path_factory):
     out = tmp_path_factory.mktemp("adapter") / "adapter_test"
     lib = ROOT / "octotiger_b200"
-    cmd = ["g++", "-std=c++17", "-O2", "-I", str(ROOT / "include"), str(ROOT / "tests" / "cpp" / "adapter_test.cpp"),
+    cmd = ["g++", "-std=c++17", "-O2", "-I", str(ROOT / "include"), "-I", str(ROOT / "octotiger_b200" / "csrc"),
+           str(ROOT / "tests" / "cpp" / "adapter_test.cpp"),
            "-L", str(lib), "-lotfmm", f"-Wl,-rpath,{lib}", "-o", str(out)]
     subprocess.run(cmd, check=True)
     return out
