@@ -100,8 +100,8 @@ int otfmm_aggregator_create(otfmm_context* ctx, int32_t max_subgrids, int32_t ma
     if (max_subgrids < 27 || max_items < 1 || idle_us < 0)
         return fail(OTFMM_ERR_INVALID, "aggregator: max_subgrids >= 27, max_items >= 1, idle_us >= 0");
     if (gsolve_type != OTFMM_RHO && gsolve_type != OTFMM_DRHODT) return fail(OTFMM_ERR_INVALID, "bad gsolve_type");
-    int rc = check_precision(precision);
-    if (rc) return rc;
+    if (precision != OTFMM_FP64_EXACT && precision != OTFMM_FP64 && precision != OTFMM_FP32_SPLIT)
+        return fail(OTFMM_ERR_INVALID, "unknown precision");
     DeviceGuard g(ctx->device);
     auto* a = new otfmm_aggregator;
     a->ctx = ctx;

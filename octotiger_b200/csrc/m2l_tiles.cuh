@@ -1232,18 +1232,20 @@ __device__ __forceinline__ void fz_finish_lc(const FzLc& z, const double c_oct[1
     fast_upper_correction(w, neg_c, Lc);
 }
 
-// One far pair of the fused form into the FP32 sums and the L_c parts.
+// One far pair of the fused form into the FP32 sums and the L_c parts; CS is
+// the component stride of the staged layout (float4 / double2 units).
+template <int CS = SUB_YZ>
 __device__ __forceinline__ void fz_far_pair(const double2* pb, const float4* pa, double Pc0, double Pc1, double Pc2,
                                             float accf[20], float* ext, double L[3], FzLc& z) {
-    const double2 q0 = pb[0], q1 = pb[SUB_YZ];
+    const double2 q0 = pb[0], q1 = pb[CS];
     double op[10];
 #pragma unroll
     for (int o = 0; o < 5; ++o) {
-        const double2 v = pb[(2 + o) * SUB_YZ];
+        const double2 v = pb[(2 + o) * CS];
         op[2 * o] = v.x;
         op[2 * o + 1] = v.y;
     }
-    const float4 f0 = pa[0], f1 = pa[SUB_YZ], f2 = pa[2 * SUB_YZ], f3 = pa[3 * SUB_YZ];
+    const float4 f0 = pa[0], f1 = pa[CS], f2 = pa[2 * CS], f3 = pa[3 * CS];
     const double dX[3] = {Pc0 - q0.x, Pc1 - q0.y, Pc2 - q1.x};
     FastDerivs f;
     float dXf[3], rsf;
@@ -1251,6 +1253,28 @@ __device__ __forceinline__ void fz_far_pair(const double2* pb, const float4* pa,
     fz_upper(f, op, L);
     fz_mass_geometry(f, q1.y, z);
     fz_contract(dXf, rsf, (float)q1.y, f0, f1, f2, f3, accf, ext);
+}
+
+// A partner with mass only (a leaf neighbour's cell on a monopole-only
+// offset): FP32 mass contraction and the mass-weighted L_c geometry (a leaf
+// partner carries no octupole). cs = component stride of the double2 rows.
+__device__ __forceinline__ void fz_mass_pair(const double2* pb, int cs, double Pc0, double Pc1, double Pc2,
+                                             float accf[20], FzLc& z) {
+    const double2 q0 = pb[0], q1 = pb[cs];
+    const double dX[3] = {Pc0 - q0.x, Pc1 - q0.y, Pc2 - q1.x};
+    FastDerivs f;
+    float dXf[3], rsf;
+    fz_geometry(dX, dXf, f, &rsf);
+    fz_mass_geometry(f, q1.y, z);
+    const float r2invf = rsf * rsf;
+    const float d1 = rsf * r2invf;
+    const float d2 = -3.0f * d1 * r2invf;
+    const float d3 = -5.0f * d2 * r2invf;
+    float D[20];
+    d_tensor<float>(dXf, -rsf, d1, d2, d3, D);
+    const float m0 = (float)q1.y;
+#pragma unroll
+    for (int q = 0; q < 20; ++q) accf[q] = fmaf(m0, D[q], accf[q]);
 }
 
 template <int CHUNK>
@@ -1281,6 +1305,14 @@ __device__ void fz_tile(const float4* sf, const double2* sb, const unsigned* s_e
     for (int e0 = 0; e0 < nfar; e0 += CHUNK) {
         const int e1 = min(e0 + CHUNK, nfar);
         int e = e0;
+        // three pairs in flight (La, Lb, La: the L_c chains of consecutive pairs interleave)
+#pragma unroll 1
+        for (; e + 2 < e1; e += 3) {
+            const unsigned ea = ent[e], eb = ent[e + 1], ec = ent[e + 2];
+            fz_far_pair(sb + (ea & 0xffffu) + lane_b, sf + (ea >> 16) + lane_f, Pc0, Pc1, Pc2, accf, &ext, z.La, z);
+            fz_far_pair(sb + (eb & 0xffffu) + lane_b, sf + (eb >> 16) + lane_f, Pc0, Pc1, Pc2, accf, &ext, z.Lb, z);
+            fz_far_pair(sb + (ec & 0xffffu) + lane_b, sf + (ec >> 16) + lane_f, Pc0, Pc1, Pc2, accf, &ext, z.La, z);
+        }
 #pragma unroll 1
         for (; e + 1 < e1; e += 2) {
             const unsigned ea = ent[e], eb = ent[e + 1];
@@ -1308,22 +1340,7 @@ __device__ void fz_tile(const float4* sf, const double2* sb, const unsigned* s_e
             const int4 en = __ldg(gent + e);
             const int ax = cx + entry_sx(en.z), ay = cy + entry_sy(en.z), az = cz + entry_sz(en.z);
             if (!((monomask >> raw_dir(ax, ay, az)) & 1u)) continue;
-            const double2 q0 = sb[en.y + lane_b], q1 = sb[en.y + lane_b + SUB_YZ];
-            const double dX[3] = {Pc0 - q0.x, Pc1 - q0.y, Pc2 - q1.x};
-            FastDerivs f;
-            float dXf[3], rsf;
-            fz_geometry(dX, dXf, f, &rsf);
-            // a leaf partner carries no octupole: only the mass-weighted part
-            fz_mass_geometry(f, q1.y, z);
-            const float r2invf = rsf * rsf;
-            const float d1 = rsf * r2invf;
-            const float d2 = -3.0f * d1 * r2invf;
-            const float d3 = -5.0f * d2 * r2invf;
-            float D[20];
-            d_tensor<float>(dXf, -rsf, d1, d2, d3, D);
-            const float m0 = (float)q1.y;
-#pragma unroll
-            for (int q = 0; q < 20; ++q) accf[q] = fmaf(m0, D[q], accf[q]);
+            fz_mass_pair(sb + en.y + lane_b, SUB_YZ, Pc0, Pc1, Pc2, accf, z);
         }
 #pragma unroll
         for (int q = 0; q < 20; ++q) acc[q] += (double)accf[q];

@@ -327,6 +327,7 @@ int ensure_attributes(int device) {
     rc = rc ? rc : set_smem(m2l_r2_kernel<PREC_EXACT, false>, PL_SMEM_BYTES);
     rc = rc ? rc : set_smem(m2l_r2_kernel<PREC_FAST, true>, PL_SMEM_BYTES);
     rc = rc ? rc : set_smem(m2l_r2_kernel<PREC_FAST, false>, PL_SMEM_BYTES);
+    rc = rc ? rc : set_smem(m2l_r2_split_kernel, R2S_SMEM_ALLOC);
     rc = rc ? rc : set_smem(p2p_r2_kernel<PREC_EXACT>, R2_SMEM_BYTES);
     rc = rc ? rc : set_smem(p2p_r2_kernel<PREC_FAST>, R2_SMEM_BYTES);
     rc = rc ? rc : set_smem(p2m_coarse_kernel<true>, PC_SMEM_BYTES);
@@ -1023,7 +1024,9 @@ int enqueue_batch(otfmm_context* ctx, const double* pool_M, const double* pool_c
     mark(1);
     const dim3 tiles_grid(sms), p2p_grid(P2P_CTAS_PER_SM * sms), p2m_grid(std::min(n_items, 8 * sms));
     if (ctx->reach > 1) {
-        // theta < 0.5: partners from global memory; the split precision runs the fast FP64 form
+        // theta < 0.5: partner planes streamed through shared memory; the split
+        // precision runs the fused split tiles for the RHO solve and the fast
+        // FP64 form elsewhere (d(rho)/dt tiles, P2P, P2M)
         const size_t rbytes = PL_SMEM_BYTES;
         const dim3 leaf_grid(std::min(n_items, 8 * sms));
         if (precision == OTFMM_FP64_EXACT) {
@@ -1035,7 +1038,8 @@ int enqueue_batch(otfmm_context* ctx, const double* pool_M, const double* pool_c
             if (rho) p2m_batch_kernel<PREC_EXACT, true><<<p2m_grid, P_THREADS, 0, s>>>(a);
             else p2m_batch_kernel<PREC_EXACT, false><<<p2m_grid, P_THREADS, 0, s>>>(a);
         } else {
-            if (rho) m2l_r2_kernel<PREC_FAST, true><<<4 * sms, THREADS, rbytes, s>>>(a);
+            if (rho && precision == OTFMM_FP32_SPLIT) m2l_r2_split_kernel<<<sms, THREADS, R2S_SMEM_ALLOC, s>>>(a);
+            else if (rho) m2l_r2_kernel<PREC_FAST, true><<<4 * sms, THREADS, rbytes, s>>>(a);
             else m2l_r2_kernel<PREC_FAST, false><<<4 * sms, THREADS, rbytes, s>>>(a);
             mark(2);
             p2p_r2_kernel<PREC_FAST><<<leaf_grid, 256, R2_SMEM_BYTES, s>>>(a);

@@ -161,6 +161,179 @@ __global__ void __launch_bounds__(THREADS, 1) m2l_r2_kernel(BatchArgs a) {
     }
 }
 
+// The RHO multipole tiles of theta < 0.5 in the fused FP32-split form
+// (m2l_split_fz_kernel's arithmetic on m2l_r2_kernel's plane streaming): the
+// 12 partner x-planes of a tile are staged one after the other, per (y, z)
+// parity class in rows of 12 (8 cells + 4 pad, so a quarter-warp (k, two j)
+// reads distinct 16-byte slots): FP32 float4 (Q0..Q3) (Q4,Q5,-O0,-O1)
+// (-O2..-O5) (-O6..-O9) and FP64 double2 (Px,Py) (Pz,m0) (O0,O1) .. (O8,O9),
+// everything in units of dx. Each thread serves one target cell and, for its
+// pairs in the plane, builds the FP32 tensor and contraction and the FP64
+// correction L_c in one instruction stream (promoted to FP64 every 16 pairs).
+// Root tiles run the fast FP64 form.
+constexpr int R2S_COMP = 8 * PL_RS;                 // 96 cells of one (y, z) parity class
+constexpr int R2S_F_CLS = 4 * R2S_COMP;             // float4 per class
+constexpr int R2S_D_CLS = 7 * R2S_COMP;             // double2 per class
+constexpr int R2S_F_BYTES = 4 * R2S_F_CLS * 16;     // 24,576
+constexpr int R2S_SMEM_BYTES = R2S_F_BYTES + 4 * R2S_D_CLS * 16;   // 24,576 + 43,008 = 67,584
+constexpr int R2S_SMEM_ALLOC = R2S_SMEM_BYTES > ROOT_SMEM_DOUBLES * 8 ? R2S_SMEM_BYTES : ROOT_SMEM_DOUBLES * 8;
+static_assert(PL_RS % 8 == 4, "rows of 12 sixteen-byte slots: quarter-warps (k, two j) conflict-free");
+
+__global__ void __launch_bounds__(THREADS, 1) m2l_r2_split_kernel(BatchArgs a) {
+    extern __shared__ __align__(16) unsigned char r2s_dyn[];
+    float4* sf = reinterpret_cast<float4*>(r2s_dyn);
+    double2* sb = reinterpret_cast<double2*>(r2s_dyn + R2S_F_BYTES);
+    __shared__ ItemInfo it;
+    __shared__ int tile;
+    constexpr int RU = ROOT_UNITS_FAST;
+    const int nroot = a.wl.counts[WL_ROOT], nm2l = a.wl.counts[WL_M2L];
+    const int total = RU * nroot + 2 * nm2l;
+    for (;;) {
+        if (threadIdx.x == 0) tile = atomicAdd(a.wl.counts + WL_M2L_NEXT, 1);
+        __syncthreads();
+        const int t = tile;
+        if (t >= total) break;
+        const int item_idx = (t < RU * nroot) ? a.wl.root[t / RU] : a.wl.m2l[(t - RU * nroot) >> 1];
+        load_item(a, item_idx, it);
+        const int x0 = TILE_X * (t & 1);
+        const size_t sub = (size_t)it.subgrid;
+        OutPtr out{a.L + sub * 20 * NCELL, a.Lc + sub * 3 * NCELL, NCELL, true};
+        if (it.kind == OTFMM_KIND_M2L_ROOT) {
+            double* sm = reinterpret_cast<double*>(r2s_dyn);
+            for (int r = threadIdx.x; r < NCELL; r += blockDim.x)
+                for (int q = 0; q < NCOMP; ++q)
+                    sm[q * NCELL + r] = (q < 20) ? a.M[(sub * 20 + q) * NCELL + r] * stage_scale<PREC_FAST>(q)
+                                                 : a.com[(sub * 3 + (q - 20)) * NCELL + r];
+            __syncthreads();
+            root_unit_fast<true, THREADS / 32>(sm, t % RU, a.t, out);
+            __syncthreads();   // shared memory and `it` are reused by the next tile
+            continue;
+        }
+        const uint32_t monomask = it.leafmask;
+        const CellMap c = cell_map(x0);
+        const int cu = c.cx * 64 + c.cy * 8 + c.cz;
+        const int lane_off = c.j * PL_RS + c.k;
+        const double inv_dx = 1.0 / it.dx, inv2 = inv_dx * inv_dx, inv3 = inv2 * inv_dx;
+        const double Pc0 = (a.com[(sub * 3 + 0) * NCELL + cu] - it.xbase[0]) * inv_dx;
+        const double Pc1 = (a.com[(sub * 3 + 1) * NCELL + cu] - it.xbase[1]) * inv_dx;
+        const double Pc2 = (a.com[(sub * 3 + 2) * NCELL + cu] - it.xbase[2]) * inv_dx;
+        FzLc z;
+#pragma unroll
+        for (int q = 0; q < 3; ++q) z.La[q] = z.Lb[q] = 0.0;
+        z.V = 0.0;
+#pragma unroll
+        for (int q = 0; q < 6; ++q) z.W[q] = 0.0;
+        double acc[20];
+        float accf[20], ext = 0.0f;
+#pragma unroll
+        for (int q = 0; q < 20; ++q) {
+            acc[q] = 0.0;
+            accf[q] = 0.0f;
+        }
+        int in_chunk = 0;
+        const int2* ent = a.t.entries_r2 + c.p * MAX_ENTRIES_R2;
+        const int* sxs = a.t.r2_sx_start + c.p * 12;
+        for (int plane = x0 - 4; plane <= x0 + 7; ++plane) {
+            __syncthreads();   // the previous plane is consumed
+            {
+                // stage plane `plane`: one cell per thread, in units of dx
+                const int r = threadIdx.x;
+                const int ax = plane, ay = (r >> 4) - 4, az = (r & 15) - 4;
+                const int raw = raw_dir(ax, ay, az);
+                const int src = (raw == 13) ? it.subgrid : it.nb[raw < 13 ? raw : raw - 1];
+                const int u = (ax & 7) * 64 + (ay & 7) * 8 + (az & 7);
+                double m0 = 0.0, q[6], o[10], P[3];
+#pragma unroll
+                for (int k = 0; k < 6; ++k) q[k] = 0.0;
+#pragma unroll
+                for (int k = 0; k < 10; ++k) o[k] = 0.0;
+                if (src < 0) {
+                    // empty direction: zero moments at the cell's own centre
+                    P[0] = ax;
+                    P[1] = ay;
+                    P[2] = az;
+                } else if ((it.leafmask >> raw) & 1u) {
+                    m0 = a.mon[(size_t)src * NCELL + u];
+                    const int ip[3] = {ax + INX, ay + INX, az + INX};
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        const double cc = __dsub_rn(__dadd_rn(__dmul_rn((double)ip[k], it.dx), it.xbase[k]),
+                                                    __dmul_rn((double)INX, it.dx));
+                        P[k] = (cc - it.xbase[k]) * inv_dx;
+                    }
+                } else {
+                    const double* Ms = a.M + (size_t)src * 20 * NCELL + u;
+                    m0 = Ms[0];
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) q[k] = Ms[(4 + k) * NCELL] * ((factor_of(4 + k) / 2.0) * inv2);
+#pragma unroll
+                    for (int k = 0; k < 10; ++k) o[k] = Ms[(10 + k) * NCELL] * ((factor_of(10 + k) / 6.0) * inv3);
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) P[k] = (a.com[((size_t)src * 3 + k) * NCELL + u] - it.xbase[k]) * inv_dx;
+                }
+                const int cls = ((ay & 1) << 1) | (az & 1);
+                const int cell = ((ay + 4) >> 1) * PL_RS + ((az + 4) >> 1);
+                float4* fa = sf + cls * R2S_F_CLS + cell;
+                double2* da = sb + cls * R2S_D_CLS + cell;
+                fa[0] = make_float4((float)q[0], (float)q[1], (float)q[2], (float)q[3]);
+                fa[R2S_COMP] = make_float4((float)q[4], (float)q[5], (float)-o[0], (float)-o[1]);
+                fa[2 * R2S_COMP] = make_float4((float)-o[2], (float)-o[3], (float)-o[4], (float)-o[5]);
+                fa[3 * R2S_COMP] = make_float4((float)-o[6], (float)-o[7], (float)-o[8], (float)-o[9]);
+                da[0] = make_double2(P[0], P[1]);
+                da[R2S_COMP] = make_double2(P[2], m0);
+#pragma unroll
+                for (int k = 0; k < 5; ++k) da[(2 + k) * R2S_COMP] = make_double2(o[2 * k], o[2 * k + 1]);
+            }
+            __syncthreads();
+            const int sx = plane - c.cx;
+            if (sx < -SMAX || sx > SMAX) continue;
+            const int e1 = sxs[sx + SMAX + 1];
+#pragma unroll 1
+            for (int e = sxs[sx + SMAX]; e < e1; ++e) {
+                const int2 en = __ldg(ent + e);
+                // en.x addresses the FP64 plane layout of m2l_r2_kernel: class and cell
+                const int cls = en.x / PL_CLS, cell = en.x - cls * PL_CLS + lane_off;
+                const double2* pb = sb + cls * R2S_D_CLS + cell;
+                if (entry_flags(en.y) & F_FAR) {
+                    fz_far_pair<R2S_COMP>(pb, sf + cls * R2S_F_CLS + cell, Pc0, Pc1, Pc2, accf, &ext, z.La, z);
+                } else {
+                    // monopole-only offsets: only leaf partners carry mass
+                    const int ay = c.cy + entry_sy(en.y), az = c.cz + entry_sz(en.y);
+                    if (!((monomask >> raw_dir(plane, ay, az)) & 1u)) continue;
+                    fz_mass_pair(pb, R2S_COMP, Pc0, Pc1, Pc2, accf, z);
+                }
+                if (++in_chunk == 16) {
+                    in_chunk = 0;
+                    accf[0] += ext;
+                    ext = 0.0f;
+#pragma unroll
+                    for (int q = 0; q < 20; ++q) {
+                        acc[q] += (double)accf[q];
+                        accf[q] = 0.0f;
+                    }
+                }
+            }
+        }
+        accf[0] += ext;
+#pragma unroll
+        for (int q = 0; q < 20; ++q) acc[q] += (double)accf[q];
+        // the target's part of L_c: O_c / m_c against the mass-weighted geometry
+        const double inv_m0 = 1.0 / a.M[(sub * 20) * NCELL + cu];
+        double c_oct[10];
+#pragma unroll
+        for (int k = 0; k < 10; ++k)
+            c_oct[k] = a.M[(sub * 20 + 10 + k) * NCELL + cu] * ((factor_of(10 + k) / 6.0) * inv3) * inv_m0;
+        double corr[3];
+        fz_finish_lc(z, c_oct, corr);
+        const double s1 = inv_dx, s2 = s1 * inv_dx, s3 = s2 * inv_dx, s4 = s3 * inv_dx;
+#pragma unroll
+        for (int q = 0; q < 20; ++q) out.L[q * out.stride + cu] = acc[q] * (q == 0 ? s1 : q < 4 ? s2 : q < 10 ? s3 : s4);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) out.Lc[q * out.stride + cu] = corr[q] * s2;
+        __syncthreads();   // shared memory and `it` are reused by the next tile
+    }
+}
+
 // P2P of leaves: one CTA (512 threads) per leaf, grid stride. The leaf's
 // 18^3 mass halo (padding 5) is staged in shared memory first, refined and
 // empty neighbours as zero mass (monopole update_input,

@@ -100,14 +100,16 @@ def main(names):
         t_ref = timed(lambda: fan(reference_calls))
         t_lib = timed(lambda: fan(library_calls))
         # the reference kernels' multipole results against the library's exact
-        # batched form on the same items (bit-identical expected)
+        # batched form on the same items (equal to rounding: the reference sums
+        # per stencil-column block, then the blocks)
         fan(reference_calls)
         torch.cuda.synchronize()
         ref_L = plain.m_L.cpu().numpy().reshape(len(plain.mpole), 20, -1)[:, :, :512]
         solver = BatchSolver(ctx, b.pool, items)
         solver.run(RHO, "fp64_exact")
         Le, _ = solver.results()
-        same = bool(np.array_equal(ref_L, Le[items["subgrid"][plain.mpole]]))
+        exp = Le[items["subgrid"][plain.mpole]]
+        err = float((np.abs(ref_L - exp).max(axis=(0, 2)) / np.abs(exp).max(axis=(0, 2))).max())
         batched = {}
         for prec in ("fp64", "fp32_split"):
             batched[prec] = timed(lambda: solver.run(RHO, prec))
@@ -116,7 +118,7 @@ def main(names):
             "reference_gpu_per_node": {"ms": t_ref, "value": pairs / (t_ref * 1e-3)},
             "library_fp64_per_node": {"ms": t_lib, "value": pairs / (t_lib * 1e-3)},
             "library_batched": {p: {"ms": t, "value": pairs / (t * 1e-3)} for p, t in batched.items()},
-            "reference_m2l_equals_library_exact": same,
+            "reference_m2l_max_scaled_diff_vs_library_exact": err,
             "note": "root items and P2M calls left out of every figure; batched solves run the same items "
                     "(their P2M included)"}), flush=True)
         del plain, solver

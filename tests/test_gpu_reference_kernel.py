@@ -2,8 +2,12 @@
 oracle/build_ref_gpu.sh with --fmad=false; test infrastructure, never part of
 the library) against the oracle on the same staged SoA buffers: the
 multipole kernel (RHO and d(rho)/dt, with leaf and empty neighbours) and the
-P2P kernel. This pins the comparator that tests/reference_gpu_timing.py times
-beside the library's kernels."""
+P2P kernel. These kernels sum per stencil-column block and then add the 121
+(M2L) or 11 (P2P) block partials in block order, a different summation order
+from the reference's CPU sweep the oracle restates, so they agree to rounding
+(1e-12 per component relative to its largest magnitude), not bit for bit. This
+pins the comparator that tests/reference_gpu_timing.py times beside the
+library's kernels."""
 from __future__ import annotations
 
 import numpy as np
@@ -27,6 +31,11 @@ def _cells(a, ncomp):
     return np.asarray(a).reshape(ncomp, -1)[:, :NCELL]
 
 
+def _close(got, ref, tol=1e-12):
+    scale = np.abs(ref).max(axis=1)
+    assert (np.abs(got - ref).max(axis=1) <= tol * scale).all(), np.abs(got - ref).max(axis=1) / scale
+
+
 @pytest.mark.parametrize("rho", [True, False])
 @pytest.mark.parametrize("case", ["refined", "mixed"])
 def test_reference_m2l_kernel_matches_oracle(refgpu, oracle, rho, case):
@@ -42,9 +51,9 @@ def test_reference_m2l_kernel_matches_oracle(refgpu, oracle, rho, case):
     Lc = torch.zeros(3 * COMPONENT_LENGTH_UNPADDED, dtype=torch.float64, device=d)
     refgpu.m2l(tm, tc, tM, scratch, L, Lc, rho=rho)
     torch.cuda.synchronize()
-    np.testing.assert_array_equal(_cells(L.cpu().numpy(), 20), _cells(Lo, 20))
+    _close(_cells(L.cpu().numpy(), 20), _cells(Lo, 20))
     if rho:
-        np.testing.assert_array_equal(_cells(Lc.cpu().numpy(), 3), _cells(Lco, 3))
+        _close(_cells(Lc.cpu().numpy(), 3), _cells(Lco, 3))
 
 
 def test_reference_p2p_kernel_matches_oracle(refgpu, oracle):
@@ -58,4 +67,4 @@ def test_reference_p2p_kernel_matches_oracle(refgpu, oracle):
     L4 = torch.zeros(4 * COMPONENT_LENGTH_UNPADDED, dtype=torch.float64, device=d)
     refgpu.p2p(torch.from_numpy(mon).to(d), scratch, L4, dx)
     torch.cuda.synchronize()
-    np.testing.assert_array_equal(_cells(L4.cpu().numpy(), 4), _cells(L4o, 4))
+    _close(_cells(L4.cpu().numpy(), 4), _cells(L4o, 4))
