@@ -496,6 +496,14 @@ def gpu_arm(args) -> None:
             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of the same kernel "
                               "on this workload (tuned variant)" if traffic else traffic_note,
             "fp64_peak_tflops": fp64_peak, "fp32_peak_tflops": fp32_peak}
+    # ncu-free pipe evidence: SM cycles per multipole pair of the tile kernel at
+    # the SM clock sampled during the timed region (an FP64 M2L pair needs ~250
+    # FP64-pipe instructions = ~3.9 cycles per pair and SM at 64 FP64 lanes)
+    clk_summary = clk.summary()
+    n_sms = torch.cuda.get_device_properties(local).multi_processor_count
+    if clk_summary.get("sm_mhz") and counts["m2l"]:
+        roof["tile_sm_cycles_per_pair"] = (kernel_ms["m2l"] * 1e-3 * clk_summary["sm_mhz"] * 1e6 * n_sms
+                                           / counts["m2l"])
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -523,7 +531,7 @@ def gpu_arm(args) -> None:
         "e2e_adapter": e2e_adapter,
         "gpu_launches": 4 * args.steps,
         "roofline": roof,
-        "clocks": clk.summary(),
+        "clocks": clk_summary,
         "step_ms": [round(x, 4) for x in per],
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
