@@ -353,14 +353,19 @@ long long otfmm_count_pairs(const otfmm_context* ctx, const uint8_t* is_leaf, in
  *   2. otfmm_aggregator_record: host pointers to a slot's pinned storage
  *      (M[20][512], com[3][512], mon[512]); write the parts of fill[i].
  *   3. otfmm_aggregator_submit: the call's work item (subgrid and neighbour
- *      fields are slots, -1 = empty); blocks until its batch has run, then
- *      writes L (20 x 512 for multipole items, 4 x 512 for leaves, SoA) and,
- *      when L_c is not NULL, L_c (3 x 512).
+ *      fields are slots, -1 = empty) and its output buffers; returns at once.
+ *      Every reserved call must be submitted (a bad item withdraws the call
+ *      and returns OTFMM_ERR_INVALID).
+ *   4. otfmm_aggregator_wait(ticket): blocks until the call's batch has run;
+ *      then L holds 20 x 512 (multipole items) or 4 x 512 (leaves) values and
+ *      L_c, when not NULL, 3 x 512 (SoA). A caller may have many calls
+ *      submitted before it waits (as HPX tasks do).
  * A batch runs when it is full and all its reserved calls have submitted, or
  * when it has been idle for idle_us with no call between reserve and submit;
- * one waiting caller runs it. All calls of an aggregator share its solve type
- * and precision. Thread-safe; no context-wide lock is held while callers copy
- * their data. Destroy only with no call in flight. */
+ * a caller in otfmm_aggregator_wait (or in a reserve that finds both batch
+ * buffers busy) runs it. All calls of an aggregator share its solve type and
+ * precision. Thread-safe; no context-wide lock is held while callers copy their
+ * data. Destroy only with no call in flight. */
 #define OTFMM_AGG_M 1
 #define OTFMM_AGG_COM 2
 #define OTFMM_AGG_MON 4
@@ -374,6 +379,7 @@ int otfmm_aggregator_record(otfmm_aggregator* agg, int64_t ticket, int32_t slot,
                             double** mon);
 int otfmm_aggregator_submit(otfmm_aggregator* agg, int64_t ticket, const otfmm_work_item* item, double* L,
                             double* L_c);
+int otfmm_aggregator_wait(otfmm_aggregator* agg, int64_t ticket);
 
 /* Checks a device-side error flag written by the last otfmm_batch on `stream`
  * without synchronizing the whole device: returns OTFMM_OK or OTFMM_ERR_DEVICE. */

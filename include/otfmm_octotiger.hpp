@@ -417,21 +417,35 @@ int monopole_kernel_interface(otfmm_context* ctx, const std::vector<double>& mon
 // The same two interfaces on an otfmm_aggregator (otfmm.h): the call's records
 // (its own subgrid, then its neighbours' payloads) go into the open batch's
 // pinned pool slots - a payload that aliases data already in the batch (same
-// address) is not copied again - and the call waits for the batched solve its
-// work item joined. Output semantics as above. `type` must be the aggregator's
-// solve type; the precision is the aggregator's.
+// address) is not copied again - and its work item joins the batched solve.
+// Each interface comes as a pair: *_submit returns as soon as the call is in
+// its batch (many calls of a thread may be in flight, as HPX tasks are), and
+// finish() waits for the call's batch and updates the grid exactly as the
+// per-call overloads do; the plain overloads do both. `type` must be the
+// aggregator's solve type; the precision is the aggregator's.
 template <class T>
 inline uint64_t data_key(const T* p) {
     return static_cast<uint64_t>(reinterpret_cast<std::uintptr_t>(p));
 }
 
-// One aggregated call: own record (M + com for a refined node, masses + com for
-// a leaf) and the 26 neighbour payloads; L (ncomp x 512) and L_c (3 x 512) SoA out.
+// A submitted call: its ticket, its result buffers and where they go.
+template <class GridPtr>
+struct AggregatedCall {
+    otfmm_aggregator* agg = nullptr;
+    int64_t ticket = 0;
+    int ncomp = 20;          // L components the call's kind writes (20 multipole, 4 monopole)
+    bool write_lc = false;   // L_c = result (RHO multipole; RHO monopole with a refined neighbour)
+    GridPtr grid{};
+    std::vector<double> L, Lc;
+};
+
+// Reserves, fills and submits one call: own record (M + com for a refined node,
+// masses + com for a leaf) and the 26 neighbour payloads.
 template <class Multipole, class SpaceVector, class Neighbor, class GridPtr>
-int aggregated_call(otfmm_aggregator* agg, int kind, const std::vector<Multipole>* own_M,
-                    const std::vector<double>* own_mon, const SpaceVector* own_com,
-                    const std::vector<Neighbor>& neighbors, double dx, const std::array<double, 3>& xbase,
-                    const GridPtr& grid, double* L, double* Lc) {
+int aggregated_submit(otfmm_aggregator* agg, int kind, const std::vector<Multipole>* own_M,
+                      const std::vector<double>* own_mon, const SpaceVector* own_com,
+                      const std::vector<Neighbor>& neighbors, double dx, const std::array<double, 3>& xbase,
+                      const GridPtr& grid, AggregatedCall<GridPtr>& call) {
     uint64_t keys[27];
     uint8_t leaf[27], need[27], fill[27];
     int32_t slots[27];
@@ -516,66 +530,101 @@ int aggregated_call(otfmm_aggregator* agg, int kind, const std::vector<Multipole
             });
         }
     }
+    call.agg = agg;
+    call.ticket = ticket;
+    call.grid = grid;
+    call.L.assign((size_t)call.ncomp * NCELL, 0.0);
+    call.Lc.assign(3 * NCELL, 0.0);
     if (rc != OTFMM_OK) {
-        // release the reservation so the batch can run without this call
+        // withdraw the reservation so that the batch can run without this call
         item.subgrid = -1;
-        otfmm_aggregator_submit(agg, ticket, &item, L, nullptr);
+        otfmm_aggregator_submit(agg, ticket, &item, call.L.data(), nullptr);
+        call.agg = nullptr;
         return rc;
     }
-    return otfmm_aggregator_submit(agg, ticket, &item, L, Lc);
+    rc = otfmm_aggregator_submit(agg, ticket, &item, call.L.data(), call.Lc.data());
+    if (rc != OTFMM_OK) call.agg = nullptr;
+    return rc;
 }
 
-// multipole_kernel_interface on an aggregator, the reference's argument list
-// (multipole_kernel_interface.hpp:18-22).
-template <class Multipole, class SpaceVector, class Neighbor, class GridPtr>
-int multipole_kernel_interface(otfmm_aggregator* agg, const std::vector<double>& /*monopoles*/,
-                               const std::vector<Multipole>& M_ptr,
-                               const std::vector<std::shared_ptr<std::vector<SpaceVector>>>& com_ptr,
-                               const std::vector<Neighbor>& neighbors, int type, double dx,
-                               const std::array<bool, 26>& /*is_direction_empty*/, std::array<double, 3> xbase,
-                               const GridPtr& grid, bool use_root_stencil) {
-    if (!agg || !grid || M_ptr.size() != NCELL || com_ptr.empty() || !com_ptr[0]) return OTFMM_ERR_INVALID;
-    std::vector<double> L(20 * NCELL), Lc(3 * NCELL);
-    const int kind = use_root_stencil ? OTFMM_KIND_M2L_ROOT : OTFMM_KIND_M2L;
-    const int rc = aggregated_call(agg, kind, &M_ptr, static_cast<const std::vector<double>*>(nullptr),
-                                   com_ptr[0]->data(), neighbors, dx, xbase, grid, L.data(), Lc.data());
+// Waits for a submitted call's batch, then updates the grid: L += result,
+// L_c = result where the reference sets it.
+template <class GridPtr>
+int finish(AggregatedCall<GridPtr>& call) {
+    if (!call.agg) return OTFMM_ERR_INVALID;
+    const int rc = otfmm_aggregator_wait(call.agg, call.ticket);
+    call.agg = nullptr;
     if (rc != OTFMM_OK) return rc;
-    auto& gL = grid->get_L();
-    for (int c = 0; c < 20; ++c)
-        for (int u = 0; u < NCELL; ++u) gL[u][c] += L[c * NCELL + u];
-    if (type == OTFMM_RHO) {
-        auto& gLc = grid->get_L_c();
+    auto& gL = call.grid->get_L();
+    for (int c = 0; c < call.ncomp; ++c)
+        for (int u = 0; u < NCELL; ++u) gL[u][c] += call.L[c * NCELL + u];
+    if (call.write_lc) {
+        auto& gLc = call.grid->get_L_c();
         for (int c = 0; c < 3; ++c)
-            for (int u = 0; u < NCELL; ++u) gLc[u][c] = Lc[c * NCELL + u];
+            for (int u = 0; u < NCELL; ++u) gLc[u][c] = call.Lc[c * NCELL + u];
     }
     return OTFMM_OK;
 }
 
+// multipole_kernel_interface on an aggregator, the reference's argument list
+// (multipole_kernel_interface.hpp:18-22): submit now, finish() later.
+template <class Multipole, class SpaceVector, class Neighbor, class GridPtr>
+int multipole_kernel_interface_submit(otfmm_aggregator* agg, const std::vector<double>& /*monopoles*/,
+                                      const std::vector<Multipole>& M_ptr,
+                                      const std::vector<std::shared_ptr<std::vector<SpaceVector>>>& com_ptr,
+                                      const std::vector<Neighbor>& neighbors, int type, double dx,
+                                      const std::array<bool, 26>& /*is_direction_empty*/,
+                                      std::array<double, 3> xbase, const GridPtr& grid, bool use_root_stencil,
+                                      AggregatedCall<GridPtr>& call) {
+    if (!agg || !grid || M_ptr.size() != NCELL || com_ptr.empty() || !com_ptr[0]) return OTFMM_ERR_INVALID;
+    call.ncomp = 20;
+    call.write_lc = (type == OTFMM_RHO);
+    const int kind = use_root_stencil ? OTFMM_KIND_M2L_ROOT : OTFMM_KIND_M2L;
+    return aggregated_submit(agg, kind, &M_ptr, static_cast<const std::vector<double>*>(nullptr),
+                             com_ptr[0]->data(), neighbors, dx, xbase, grid, call);
+}
+
+template <class Multipole, class SpaceVector, class Neighbor, class GridPtr>
+int multipole_kernel_interface(otfmm_aggregator* agg, const std::vector<double>& monopoles,
+                               const std::vector<Multipole>& M_ptr,
+                               const std::vector<std::shared_ptr<std::vector<SpaceVector>>>& com_ptr,
+                               const std::vector<Neighbor>& neighbors, int type, double dx,
+                               const std::array<bool, 26>& is_direction_empty, std::array<double, 3> xbase,
+                               const GridPtr& grid, bool use_root_stencil) {
+    AggregatedCall<GridPtr> call;
+    const int rc = multipole_kernel_interface_submit(agg, monopoles, M_ptr, com_ptr, neighbors, type, dx,
+                                                     is_direction_empty, xbase, grid, use_root_stencil, call);
+    return rc != OTFMM_OK ? rc : finish(call);
+}
+
 // monopole_kernel_interface on an aggregator, the reference's argument list
-// (monopole_kernel_interface.hpp:19-23): L[0..3] += P2P (+ P2M); L_c = the
-// P2M correction when a neighbour is refined (RHO).
+// (monopole_kernel_interface.hpp:19-23): L[0..3] += P2P (+ P2M); L_c = the P2M
+// correction when a neighbour is refined (RHO).
+template <class SpaceVector, class Neighbor, class GridPtr>
+int monopole_kernel_interface_submit(otfmm_aggregator* agg, const std::vector<double>& monopoles,
+                                     const std::vector<std::shared_ptr<std::vector<SpaceVector>>>& com_ptr,
+                                     const std::vector<Neighbor>& neighbors, int type, double dx,
+                                     const std::array<bool, 26>& /*is_direction_empty*/, const GridPtr& grid,
+                                     bool contains_multipole_neighbor, AggregatedCall<GridPtr>& call) {
+    if (!agg || !grid || monopoles.size() != NCELL || com_ptr.empty() || !com_ptr[0]) return OTFMM_ERR_INVALID;
+    call.ncomp = 4;
+    call.write_lc = contains_multipole_neighbor && type == OTFMM_RHO;
+    using Multipole = std::array<double, 20>;
+    const std::array<double, 3> xbase{0.0, 0.0, 0.0};   // leaves use integer offsets only
+    return aggregated_submit(agg, OTFMM_KIND_LEAF, static_cast<const std::vector<Multipole>*>(nullptr), &monopoles,
+                             com_ptr[0]->data(), neighbors, dx, xbase, grid, call);
+}
+
 template <class SpaceVector, class Neighbor, class GridPtr>
 int monopole_kernel_interface(otfmm_aggregator* agg, const std::vector<double>& monopoles,
                               const std::vector<std::shared_ptr<std::vector<SpaceVector>>>& com_ptr,
                               const std::vector<Neighbor>& neighbors, int type, double dx,
-                              const std::array<bool, 26>& /*is_direction_empty*/, const GridPtr& grid,
+                              const std::array<bool, 26>& is_direction_empty, const GridPtr& grid,
                               bool contains_multipole_neighbor) {
-    if (!agg || !grid || monopoles.size() != NCELL || com_ptr.empty() || !com_ptr[0]) return OTFMM_ERR_INVALID;
-    std::vector<double> L(4 * NCELL), Lc(3 * NCELL);
-    using Multipole = std::array<double, 20>;
-    const std::array<double, 3> xbase{0.0, 0.0, 0.0};   // leaves use integer offsets only
-    const int rc = aggregated_call(agg, OTFMM_KIND_LEAF, static_cast<const std::vector<Multipole>*>(nullptr),
-                                   &monopoles, com_ptr[0]->data(), neighbors, dx, xbase, grid, L.data(), Lc.data());
-    if (rc != OTFMM_OK) return rc;
-    auto& gL = grid->get_L();
-    for (int c = 0; c < 4; ++c)
-        for (int u = 0; u < NCELL; ++u) gL[u][c] += L[c * NCELL + u];
-    if (contains_multipole_neighbor && type == OTFMM_RHO) {
-        auto& gLc = grid->get_L_c();
-        for (int c = 0; c < 3; ++c)
-            for (int u = 0; u < NCELL; ++u) gLc[u][c] = Lc[c * NCELL + u];
-    }
-    return OTFMM_OK;
+    AggregatedCall<GridPtr> call;
+    const int rc = monopole_kernel_interface_submit(agg, monopoles, com_ptr, neighbors, type, dx, is_direction_empty,
+                                                    grid, contains_multipole_neighbor, call);
+    return rc != OTFMM_OK ? rc : finish(call);
 }
 
 }   // namespace otfmm_octotiger

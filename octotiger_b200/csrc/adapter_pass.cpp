@@ -18,6 +18,8 @@
 
 namespace {
 
+constexpr int CALLS_IN_FLIGHT = 64;   // aggregated calls a worker thread submits before it waits
+
 struct Node {
     std::shared_ptr<std::vector<multipole>> M;
     std::shared_ptr<std::vector<space_vector>> com;
@@ -33,8 +35,9 @@ extern "C" {
  * are host arrays in the library's batch layout; they are converted to the
  * reference's AoS node data once, outside the timed passes. mode 1: the
  * aggregated interfaces (an otfmm_aggregator of max_subgrids / max_items /
- * idle_us); mode 0: the per-call interfaces on the context (one host-buffer
- * call per node). seconds[p] = wall time of pass p (all threads, first call to
+ * idle_us; each thread submits 64 calls, then finishes them, as HPX tasks leave
+ * many calls in flight per worker thread); mode 0: the per-call interfaces on
+ * the context (one blocking host-buffer call per node). seconds[p] = wall time of pass p (all threads, first call to
  * last return). After the last pass L_out[n][20][512] / Lc_out[n][3][512]
  * hold the grids of the work items' subgrids (zero elsewhere). Returns the
  * first non-zero status of any call. */
@@ -94,7 +97,44 @@ int otfmm_adapter_pass(otfmm_context* ctx, int32_t n_sub, const double* M, const
             for (auto& l : gr.L_c) l = space_vector{};
         }
         std::atomic<int> next{0};
+        auto note = [&](int rc) {
+            if (rc != OTFMM_OK) {
+                int expect = OTFMM_OK;
+                first_rc.compare_exchange_strong(expect, rc);
+            }
+        };
+        // aggregated: a thread takes CALLS_IN_FLIGHT nodes at a time, submits all
+        // their calls, then finishes them (HPX tasks leave many calls in flight
+        // per worker thread); per-call: one blocking call after the other
+        auto agg_worker = [&]() {
+            std::vector<otfmm_octotiger::AggregatedCall<grid*>> calls(CALLS_IN_FLIGHT);
+            std::vector<int> ok(CALLS_IN_FLIGHT);
+            for (;;) {
+                const int i0 = next.fetch_add(CALLS_IN_FLIGHT);
+                if (i0 >= n_items) return;
+                const int i1 = std::min(n_items, i0 + CALLS_IN_FLIGHT);
+                for (int i = i0; i < i1; ++i) {
+                    const otfmm_work_item& w = items[i];
+                    const Node& nd = nodes[w.subgrid];
+                    const std::array<double, 3> xb{w.xbase[0], w.xbase[1], w.xbase[2]};
+                    int rc;
+                    if (w.kind == OTFMM_KIND_LEAF)
+                        rc = otfmm_octotiger::monopole_kernel_interface_submit(agg, *nd.mon, com_ptrs[i], nbs[i],
+                                                                               gsolve_type, w.dx, empty, &grids[i],
+                                                                               has_refined[i] != 0, calls[i - i0]);
+                    else
+                        rc = otfmm_octotiger::multipole_kernel_interface_submit(
+                            agg, *nd.mon, *nd.M, com_ptrs[i], nbs[i], gsolve_type, w.dx, empty, xb, &grids[i],
+                            w.kind == OTFMM_KIND_M2L_ROOT, calls[i - i0]);
+                    note(rc);
+                    ok[i - i0] = rc == OTFMM_OK;
+                }
+                for (int i = i0; i < i1; ++i)
+                    if (ok[i - i0]) note(otfmm_octotiger::finish(calls[i - i0]));
+            }
+        };
         auto worker = [&]() {
+            if (agg) return agg_worker();
             for (;;) {
                 const int i = next.fetch_add(1);
                 if (i >= n_items) return;
@@ -104,23 +144,15 @@ int otfmm_adapter_pass(otfmm_context* ctx, int32_t n_sub, const double* M, const
                 const std::array<double, 3> xb{w.xbase[0], w.xbase[1], w.xbase[2]};
                 int rc;
                 if (w.kind == OTFMM_KIND_LEAF) {
-                    rc = agg ? otfmm_octotiger::monopole_kernel_interface(agg, *nd.mon, com_ptrs[i], nbs[i], gsolve_type,
-                                                                          w.dx, empty, gp, has_refined[i] != 0)
-                             : otfmm_octotiger::monopole_kernel_interface(ctx, *nd.mon, com_ptrs[i], nbs[i],
-                                                                          gsolve_type, w.dx, empty, gp,
-                                                                          has_refined[i] != 0, precision);
+                    rc = otfmm_octotiger::monopole_kernel_interface(ctx, *nd.mon, com_ptrs[i], nbs[i], gsolve_type,
+                                                                    w.dx, empty, gp, has_refined[i] != 0, precision);
                 } else {
                     const bool root = w.kind == OTFMM_KIND_M2L_ROOT;
-                    rc = agg ? otfmm_octotiger::multipole_kernel_interface(agg, *nd.mon, *nd.M, com_ptrs[i], nbs[i],
-                                                                           gsolve_type, w.dx, empty, xb, gp, root)
-                             : otfmm_octotiger::multipole_kernel_interface(ctx, *nd.mon, *nd.M, com_ptrs[i], nbs[i],
-                                                                           gsolve_type, w.dx, empty, xb, gp, root,
-                                                                           precision);
+                    rc = otfmm_octotiger::multipole_kernel_interface(ctx, *nd.mon, *nd.M, com_ptrs[i], nbs[i],
+                                                                     gsolve_type, w.dx, empty, xb, gp, root,
+                                                                     precision);
                 }
-                if (rc != OTFMM_OK) {
-                    int expect = OTFMM_OK;
-                    first_rc.compare_exchange_strong(expect, rc);
-                }
+                note(rc);
             }
         };
         const auto t0 = std::chrono::steady_clock::now();

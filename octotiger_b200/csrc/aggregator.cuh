@@ -14,11 +14,14 @@
 //     address of the caller's data, the same for a node and for the payloads
 //     that alias it) is already in the batch is not copied again;
 //   * the caller writes the parts it was asked to fill, without any lock;
-//   * otfmm_aggregator_submit adds its work item and waits for its batch;
+//   * otfmm_aggregator_submit adds its work item and returns at once;
+//     otfmm_aggregator_wait blocks until the call's batch has run (so a caller
+//     can have many calls in flight, as HPX tasks do);
 //   * a batch runs (otfmm_batch_host on the aggregator's own stream) once it is
 //     full and every reserved call has submitted, or once it has been idle for
-//     `idle_us` with no call between reserve and submit; one of the waiting
-//     callers runs it, the others sleep on a condition variable;
+//     `idle_us` with no call between reserve and submit; a waiting caller runs
+//     it and copies every call's results to the caller's buffers, the others
+//     sleep on a condition variable;
 //   * two batch buffers: one collects while the other runs.
 #pragma once
 
@@ -31,7 +34,7 @@
 #include <vector>
 
 struct otfmm_aggregator {
-    enum State { FREE, OPEN, CLOSED, RUNNING, DONE };
+    enum State { FREE, OPEN, CLOSED, RUNNING };
     struct Out {
         double* L;
         double* Lc;
@@ -40,9 +43,8 @@ struct otfmm_aggregator {
     };
     struct Batch {
         State state = FREE;
-        long long epoch = 0;
-        int n_sub = 0, pending = 0, waiting = 0, rc = OTFMM_OK;
-        std::string msg;
+        long long epoch = 0, done_epoch = 0;   // the batch collecting now / the last one that ran
+        int n_sub = 0, pending = 0;
         std::unordered_map<uint64_t, int> keys;
         std::vector<uint8_t> claimed;   // per slot: parts some caller fills (OTFMM_AGG_*)
         std::vector<otfmm_work_item> staged;
@@ -61,6 +63,7 @@ struct otfmm_aggregator {
     std::condition_variable cv;
     Batch b[2];
     long long epochs = 0;
+    std::unordered_map<long long, std::pair<int, std::string>> failed;   // epoch -> status of a failed run
 };
 
 namespace {
@@ -75,18 +78,51 @@ void agg_free_buffers(otfmm_aggregator::Batch& b) {
     cudaFreeHost(b.items);
 }
 
-// Runs batch `k` (the caller holds no lock; the batch is RUNNING).
-void agg_run(otfmm_aggregator* a, otfmm_aggregator::Batch& b) {
+// Runs a batch (the caller holds no lock; the batch is RUNNING) and copies
+// every call's results to its buffers: multipole items L (20 x 512) and L_c
+// (3 x 512), leaves L0..L3 and L_c (L_c only where the caller asked for it).
+int agg_run(otfmm_aggregator* a, otfmm_aggregator::Batch& b, std::string& msg) {
     // multipole items first, as order_work_list does: the long tiles start first
-    std::stable_partition(b.staged.begin(), b.staged.end(),
+    std::vector<otfmm_work_item> items(b.staged);
+    std::stable_partition(items.begin(), items.end(),
                           [](const otfmm_work_item& w) { return w.kind != OTFMM_KIND_LEAF; });
-    std::copy(b.staged.begin(), b.staged.end(), b.items);
+    std::copy(items.begin(), items.end(), b.items);
     std::lock_guard<std::mutex> run(a->run_mu);
-    int rc = otfmm_batch_host(a->ctx, b.M, b.com, b.mon, b.is_leaf, b.n_sub, b.items, (int32_t)b.staged.size(), b.L,
+    int rc = otfmm_batch_host(a->ctx, b.M, b.com, b.mon, b.is_leaf, b.n_sub, b.items, (int32_t)items.size(), b.L,
                               b.Lc, a->gsolve, a->precision, a->stream);
     if (rc == OTFMM_OK) rc = otfmm_batch_status(a->ctx, a->stream);   // synchronises the stream
-    b.rc = rc;
-    if (rc != OTFMM_OK) b.msg = otfmm_last_error();
+    if (rc != OTFMM_OK) {
+        msg = otfmm_last_error();
+        return rc;
+    }
+    for (const otfmm_aggregator::Out& o : b.outs) {
+        const int ncomp = (o.kind == OTFMM_KIND_LEAF) ? 4 : 20;
+        std::copy(b.L + (size_t)o.slot * 20 * NCELL, b.L + ((size_t)o.slot * 20 + ncomp) * NCELL, o.L);
+        if (o.Lc) std::copy(b.Lc + (size_t)o.slot * 3 * NCELL, b.Lc + ((size_t)o.slot + 1) * 3 * NCELL, o.Lc);
+    }
+    return OTFMM_OK;
+}
+
+// Runs buffer k if it can run now (full, or idle with no call between
+// reserve and submit); called with the lock held, returns with it held.
+// True if it ran.
+bool agg_try_run(otfmm_aggregator* a, int k, std::unique_lock<std::mutex>& lock) {
+    otfmm_aggregator::Batch& b = a->b[k];
+    const bool idle = b.state == otfmm_aggregator::OPEN && std::chrono::steady_clock::now() - b.last >= a->idle;
+    if (!((b.state == otfmm_aggregator::CLOSED || idle) && b.pending == 0)) return false;
+    const long long e = b.epoch;
+    b.state = otfmm_aggregator::RUNNING;
+    lock.unlock();
+    std::string msg;
+    const int rc = b.staged.empty() ? OTFMM_OK : agg_run(a, b, msg);
+    lock.lock();
+    if (rc != OTFMM_OK) a->failed[e] = {rc, msg};
+    b.done_epoch = e;
+    b.staged.clear();
+    b.outs.clear();
+    b.state = otfmm_aggregator::FREE;
+    a->cv.notify_all();
+    return true;
 }
 
 }   // namespace
@@ -140,7 +176,7 @@ int otfmm_aggregator_destroy(otfmm_aggregator* a) {
     {
         std::lock_guard<std::mutex> lock(a->mu);
         for (auto& b : a->b)
-            if (b.state != otfmm_aggregator::FREE && (b.pending > 0 || b.waiting > 0))
+            if (b.state != otfmm_aggregator::FREE && (b.pending > 0 || !b.staged.empty()))
                 return fail(OTFMM_ERR_INVALID, "aggregator destroyed with calls in flight");
     }
     DeviceGuard g(a->ctx->device);
@@ -165,9 +201,7 @@ int otfmm_aggregator_reserve(otfmm_aggregator* a, int32_t n, const uint64_t* key
                 otfmm_aggregator::Batch& nb = a->b[i];
                 nb.state = otfmm_aggregator::OPEN;
                 nb.epoch = ++a->epochs;
-                nb.n_sub = nb.pending = nb.waiting = 0;
-                nb.rc = OTFMM_OK;
-                nb.msg.clear();
+                nb.n_sub = nb.pending = 0;
                 nb.keys.clear();
                 nb.claimed.clear();
                 nb.staged.clear();
@@ -175,8 +209,10 @@ int otfmm_aggregator_reserve(otfmm_aggregator* a, int32_t n, const uint64_t* key
                 nb.last = std::chrono::steady_clock::now();
                 k = i;
             }
-        if (k < 0) {   // both buffers busy: wait for one to come free
-            a->cv.wait(lock);
+        if (k < 0) {
+            // both buffers busy: run one that can run (its callers may not be
+            // waiting yet), else wait for one to come free
+            if (!agg_try_run(a, 0, lock) && !agg_try_run(a, 1, lock)) a->cv.wait_for(lock, a->idle);
             continue;
         }
         otfmm_aggregator::Batch& b = a->b[k];
@@ -233,55 +269,38 @@ int otfmm_aggregator_record(otfmm_aggregator* a, int64_t ticket, int32_t slot, d
 
 int otfmm_aggregator_submit(otfmm_aggregator* a, int64_t ticket, const otfmm_work_item* item, double* L,
                             double* L_c) {
-    if (!a || !item || !L) return fail(OTFMM_ERR_INVALID, "NULL argument");
-    std::unique_lock<std::mutex> lock(a->mu);
+    if (!a || !item) return fail(OTFMM_ERR_INVALID, "NULL argument");
+    std::lock_guard<std::mutex> lock(a->mu);
     otfmm_aggregator::Batch& b = a->b[ticket & 1];
     if (b.epoch != (ticket >> 1) || (b.state != otfmm_aggregator::OPEN && b.state != otfmm_aggregator::CLOSED))
         return fail(OTFMM_ERR_INVALID, "stale ticket");
-    bool ok = item->subgrid >= 0 && item->subgrid < b.n_sub && item->kind >= 0 && item->kind <= 2;
+    bool ok = L != nullptr && item->subgrid >= 0 && item->subgrid < b.n_sub && item->kind >= 0 && item->kind <= 2;
     for (int d = 0; d < 26; ++d) ok = ok && item->neighbors[d] >= -1 && item->neighbors[d] < b.n_sub;
-    --b.pending;
+    --b.pending;   // the reservation ends either way, so the batch can run without this call
     b.last = std::chrono::steady_clock::now();
-    if (!ok) {
-        a->cv.notify_all();
-        return fail(OTFMM_ERR_INVALID, "work item refers to slots outside its batch");
-    }
+    a->cv.notify_all();
+    if (!ok) return fail(OTFMM_ERR_INVALID, "work item refers to slots outside its batch (call withdrawn)");
     b.staged.push_back(*item);
     b.outs.push_back({L, L_c, item->subgrid, item->kind});
-    const size_t my = b.outs.size() - 1;
-    ++b.waiting;
-    a->cv.notify_all();
+    return OTFMM_OK;
+}
+
+int otfmm_aggregator_wait(otfmm_aggregator* a, int64_t ticket) {
+    if (!a) return fail(OTFMM_ERR_INVALID, "NULL argument");
+    const long long e = ticket >> 1;
+    std::unique_lock<std::mutex> lock(a->mu);
+    otfmm_aggregator::Batch& b = a->b[ticket & 1];
     for (;;) {
-        if (b.state == otfmm_aggregator::DONE) break;
-        const bool idle = b.state == otfmm_aggregator::OPEN && std::chrono::steady_clock::now() - b.last >= a->idle;
-        if ((b.state == otfmm_aggregator::CLOSED || idle) && b.pending == 0) {
-            b.state = otfmm_aggregator::RUNNING;
-            lock.unlock();
-            agg_run(a, b);
-            lock.lock();
-            b.state = otfmm_aggregator::DONE;
-            a->cv.notify_all();
-            break;
-        }
+        if (b.done_epoch >= e) break;
+        if (b.epoch != e) return fail(OTFMM_ERR_INVALID, "unknown ticket");
+        if (agg_try_run(a, (int)(ticket & 1), lock)) continue;
         a->cv.wait_for(lock, a->idle);
     }
-    const int rc = b.rc;
-    const std::string msg = b.msg;
-    const otfmm_aggregator::Out o = b.outs[my];
+    auto it = a->failed.find(e);
+    if (it == a->failed.end()) return OTFMM_OK;
+    const auto f = it->second;
     lock.unlock();
-    if (rc == OTFMM_OK) {
-        // multipole items: L (20 x 512) and L_c (3 x 512); leaves: L0..L3 and L_c
-        const int ncomp = (o.kind == OTFMM_KIND_LEAF) ? 4 : 20;
-        std::copy(b.L + (size_t)o.slot * 20 * NCELL, b.L + ((size_t)o.slot * 20 + ncomp) * NCELL, o.L);
-        if (o.Lc) std::copy(b.Lc + (size_t)o.slot * 3 * NCELL, b.Lc + ((size_t)o.slot + 1) * 3 * NCELL, o.Lc);
-    }
-    lock.lock();
-    if (--b.waiting == 0) {
-        b.state = otfmm_aggregator::FREE;
-        a->cv.notify_all();
-    }
-    lock.unlock();
-    return rc == OTFMM_OK ? OTFMM_OK : fail(rc, msg);
+    return fail(f.first, f.second);
 }
 
 }   // extern "C"
