@@ -48,10 +48,10 @@ L2_FLUSH_BYTES = 256 << 20
 
 # DRAM bytes (read + write) of one launch of the multipole-tile kernel, from
 # ncu captures (dram__bytes_read.sum + dram__bytes_write.sum) of this command
-# on a B200; the algorithmic bytes are the pool read once plus L and L_c written
-# (uniform level 3: 50.3 MB + 48.2 MB).
-PROFILED_TRAFFIC = {("uniform_level3", "fp32_split"): 61.0e6, ("uniform_level3", "fp64"): 57.9e6,
-                    ("amr_polytrope_l6", "fp32_split"): 78.6e6, ("amr_polytrope_l6", "fp64"): 77.4e6}
+# on a B200 (the fused split tiles, the FP64 tiles); the algorithmic bytes are
+# the pool read once plus L and L_c written (uniform level 3: 50.3 MB + 48.2 MB).
+PROFILED_TRAFFIC = {("uniform_level3", "fp32_split"): 48.6e6, ("uniform_level3", "fp64"): 57.9e6,
+                    ("amr_polytrope_l6", "fp32_split"): 65.7e6, ("amr_polytrope_l6", "fp64"): 77.4e6}
 
 
 WORKLOADS = ("uniform_level3", "amr_polytrope", "amr_binary", "single_subgrid")
