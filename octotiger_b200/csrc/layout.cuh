@@ -117,6 +117,7 @@ struct Tables {
                                 // stencil order of the coarse cell's first cell
     const int16_t* pc_slot;     // [27][64]: slot of coarse cell C among direction r's units, -1 if none
     const int* pc_parts;        // [27]: parts each unit's partner lists of direction r are cut in
+    const float4* r2_four_f;    // r2_four rounded to FP32 (the split P2P of theta < 0.5)
 };
 
 __device__ __forceinline__ int entry_sx(int y) { return (y & 15) - 8; }

@@ -219,6 +219,7 @@ struct otfmm_context {
     int2* d_entries_r2 = nullptr;   // stencil-order entries, MAX_ENTRIES_R2 per class (any reach)
     int* d_r2_sx_start = nullptr;
     double4* d_r2_four = nullptr;
+    float4* d_r2_four_f = nullptr;
     int p2m_groups_max = 0;   // cells with partners summed over the 26 directions
     double4* d_p2p_four = nullptr;
     double4* d_p2p_box = nullptr;    // [8][216] per-parity box constants
@@ -244,6 +245,7 @@ struct otfmm_context {
     int* d_err = nullptr;
     double* d_soa_scratch = nullptr;   // host-buffer path staging
     int* d_lists = nullptr;            // batched work lists (grown on demand)
+    long long lists_gen = 0;           // times d_lists was reallocated (a host plan binds one generation)
     int list_capacity = 0;
     otfmm_tuning tuning = {OTFMM_SPLIT_FUSED, 16, 32, 4, OTFMM_P2P_BOX, OTFMM_P2M_LANES};
     // otfmm_batch_host: device copies of the pool, work list and outputs, a
@@ -265,7 +267,7 @@ struct otfmm_context {
                       d_entries_ws, d_four,  d_phase,        d_p2m_start,     d_p2m_list,    d_p2m_perm_start,
                       d_p2m_perm,   d_p2m_slot,     d_p2p_four,      d_entries_r2,  d_r2_sx_start, d_r2_four,
                       d_p2p_box,    d_p2p_cube,     d_pc_unit_start, d_pc_coarse,  d_pc_range,    d_pc_list,
-                      d_pc_slot,    d_pc_parts}; }
+                      d_pc_slot,    d_pc_parts,     d_r2_four_f}; }
 };
 
 namespace {
@@ -603,7 +605,13 @@ int otfmm_create(int device, double theta, otfmm_context** out) {
     if (pc_list.empty()) pc_list.assign(1, 0);
     DeviceGuard g(device);
     cudaError_t e;
-    if ((e = cudaMalloc(&ctx->d_r2_four, sizeof(double4) * r2_four.size())) != cudaSuccess ||
+    std::vector<float4> r2_four_f(r2_four.size());
+    for (size_t q = 0; q < r2_four.size(); ++q)
+        r2_four_f[q] = float4{(float)r2_four[q].x, (float)r2_four[q].y, (float)r2_four[q].z, (float)r2_four[q].w};
+    if ((e = cudaMalloc(&ctx->d_r2_four_f, sizeof(float4) * r2_four_f.size())) != cudaSuccess ||
+        (e = cudaMemcpy(ctx->d_r2_four_f, r2_four_f.data(), sizeof(float4) * r2_four_f.size(),
+                        cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMalloc(&ctx->d_r2_four, sizeof(double4) * r2_four.size())) != cudaSuccess ||
         (e = cudaMemcpy(ctx->d_r2_four, r2_four.data(), sizeof(double4) * r2_four.size(),
                         cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMalloc(&ctx->d_r2_sx_start, sizeof(int) * r2_sx_start.size())) != cudaSuccess ||
@@ -732,6 +740,7 @@ int otfmm_destroy(otfmm_context* ctx) {
     cudaFree(ctx->d_entries_r2);
     cudaFree(ctx->d_r2_sx_start);
     cudaFree(ctx->d_r2_four);
+    cudaFree(ctx->d_r2_four_f);
     {
         auto& hp = ctx->hp;
         if (hp.ready) {
@@ -1025,8 +1034,8 @@ int enqueue_batch(otfmm_context* ctx, const double* pool_M, const double* pool_c
     const dim3 tiles_grid(sms), p2p_grid(P2P_CTAS_PER_SM * sms), p2m_grid(std::min(n_items, 8 * sms));
     if (ctx->reach > 1) {
         // theta < 0.5: partner planes streamed through shared memory; the split
-        // precision runs the fused split tiles for the RHO solve and the fast
-        // FP64 form elsewhere (d(rho)/dt tiles, P2P, P2M)
+        // precision runs the fused split tiles for the RHO solve, the FP32 P2P,
+        // and the fast FP64 form for the d(rho)/dt tiles and P2M
         const size_t rbytes = PL_SMEM_BYTES;
         const dim3 leaf_grid(std::min(n_items, 8 * sms));
         if (precision == OTFMM_FP64_EXACT) {
@@ -1042,7 +1051,10 @@ int enqueue_batch(otfmm_context* ctx, const double* pool_M, const double* pool_c
             else if (rho) m2l_r2_kernel<PREC_FAST, true><<<4 * sms, THREADS, rbytes, s>>>(a);
             else m2l_r2_kernel<PREC_FAST, false><<<4 * sms, THREADS, rbytes, s>>>(a);
             mark(2);
-            p2p_r2_kernel<PREC_FAST><<<leaf_grid, 256, R2_SMEM_BYTES, s>>>(a);
+            if (precision == OTFMM_FP32_SPLIT)
+                p2p_r2_split_kernel<<<leaf_grid, 256, R2_SMEM_BYTES / 2, s>>>(a);
+            else
+                p2p_r2_kernel<PREC_FAST><<<leaf_grid, 256, R2_SMEM_BYTES, s>>>(a);
             mark(3);
             if (rho) p2m_batch_kernel<PREC_FAST, true><<<p2m_grid, P_THREADS, 0, s>>>(a);
             else p2m_batch_kernel<PREC_FAST, false><<<p2m_grid, P_THREADS, 0, s>>>(a);
@@ -1148,6 +1160,7 @@ int ensure_list_capacity(otfmm_context* ctx, int32_t n_items, cudaStream_t s) {
     cudaFree(ctx->d_lists);
     ctx->d_lists = nullptr;
     const int cap = std::max(n_items, 2 * ctx->list_capacity);
+    ++ctx->lists_gen;   // before the allocation: a failed regrowth also invalidates host plans
     OT_CUDA(cudaMalloc(&ctx->d_lists, sizeof(int) * (4 * (size_t)cap + WL_COUNTERS)));
     ctx->list_capacity = cap;
     return OTFMM_OK;
@@ -1163,7 +1176,7 @@ struct otfmm_plan {
     int* err = nullptr;
     bool host = false;      // captured otfmm_batch_host: uses the context's host-path buffers
     long long host_gen = 0; // ... as the captured call left them
-    int* host_lists = nullptr;   // ... and its work-list storage (regrown by a larger solve)
+    long long host_lists_gen = 0;   // ... and its work-list storage's generation (regrown by a larger solve)
 };
 
 extern "C" {
@@ -1530,14 +1543,14 @@ int otfmm_plan_create_host(otfmm_context* ctx, const double* pool_M, const doubl
         return fail(rc, msg);
     }
     plan->host_gen = ctx->hp.gen;
-    plan->host_lists = ctx->d_lists;
+    plan->host_lists_gen = ctx->lists_gen;
     *out = plan;
     return OTFMM_OK;
 }
 
 int otfmm_plan_launch(otfmm_plan* plan, void* stream) {
     if (!plan || !plan->exec) return fail(OTFMM_ERR_INVALID, "NULL plan");
-    if (plan->host && (plan->host_gen != plan->ctx->hp.gen || plan->host_lists != plan->ctx->d_lists))
+    if (plan->host && (plan->host_gen != plan->ctx->hp.gen || plan->host_lists_gen != plan->ctx->lists_gen))
         return fail(OTFMM_ERR_INVALID, "the context's host-path buffers or work lists changed since the plan was made");
     DeviceGuard g(plan->ctx->device);
     OT_CUDA(cudaGraphLaunch(plan->exec, (cudaStream_t)stream));

@@ -420,6 +420,78 @@ __global__ void __launch_bounds__(256) p2p_r2_kernel(BatchArgs a) {
     }
 }
 
+// P2P of leaves at theta < 0.5 in the FP32-split form: the layout and walk of
+// p2p_r2_kernel with the masses staged in FP32 already divided by dx (exact for
+// dx = 2^-k), the monopole constants in FP32 and the four products of a
+// (partner, cell) as two packed FMAs; the FP32 sums are promoted to FP64 every
+// R2_SPLIT_CHUNK partners.
+constexpr int R2_SPLIT_CHUNK = 32;
+__global__ void __launch_bounds__(256) p2p_r2_split_kernel(BatchArgs a) {
+    extern __shared__ float pmf[];
+    __shared__ ItemInfo it;
+    const int p = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i = lane >> 4, j = (lane >> 2) & 3, k = lane & 3;
+    const int cy = ((p >> 1) & 1) + 2 * j, cz = (p & 1) + 2 * k;
+    const int cxa = ((p >> 2) & 1) + 2 * i, cxb = cxa + 4;
+    const int own_a = (cxa + R2_PAD) * R2_PLANE + (cy + R2_PAD) * R2_ROW + (cz + R2_PAD);
+    constexpr int OFF_B = 4 * R2_PLANE;
+    const int n = a.t.count[p];
+    const int2* ent = a.t.entries_r2 + p * MAX_ENTRIES_R2;
+    const float4* four = a.t.r2_four_f + p * MAX_ENTRIES_R2;
+    const int nleaf = a.wl.counts[WL_LEAF];
+    for (int kk = blockIdx.x; kk < nleaf; kk += gridDim.x) {
+        __syncthreads();   // `it` and the halo are reused
+        load_item(a, a.wl.leaf[kk], it);
+        const double dc0 = 1.0 / it.dx;
+        for (int r = threadIdx.x; r < R2_REG * R2_REG * R2_REG; r += blockDim.x) {
+            const int ax = r / (R2_REG * R2_REG) - R2_PAD, ay = (r / R2_REG) % R2_REG - R2_PAD,
+                      az = r % R2_REG - R2_PAD;
+            const int raw = raw_dir(ax, ay, az);
+            const int src = (raw == 13) ? it.subgrid : it.nb[raw < 13 ? raw : raw - 1];
+            double m = 0.0;
+            if (raw == 13 || ((it.leafmask >> raw) & 1u))
+                m = a.mon[(size_t)src * NCELL + (ax & 7) * 64 + (ay & 7) * 8 + (az & 7)];
+            pmf[(ax + R2_PAD) * R2_PLANE + (ay + R2_PAD) * R2_ROW + (az + R2_PAD)] = (float)(m * dc0);
+        }
+        __syncthreads();
+        double ga[4] = {0.0, 0.0, 0.0, 0.0}, gb[4] = {0.0, 0.0, 0.0, 0.0};
+        float2 a01 = make_float2(0.f, 0.f), a23 = a01, b01 = a01, b23 = a01;
+        for (int e0 = 0; e0 < n; e0 += R2_SPLIT_CHUNK) {
+            const int e1 = min(e0 + R2_SPLIT_CHUNK, n);
+#pragma unroll 4
+            for (int e = e0; e < e1; ++e) {
+                const int y = __ldg(&ent[e].y);
+                const float4 f = __ldg(four + e);
+                const int d = own_a + entry_sx(y) * R2_PLANE + entry_sy(y) * R2_ROW + entry_sz(y);
+                const float ma = pmf[d], mb = pmf[d + OFF_B];
+                a01 = __ffma2_rn(make_float2(f.x, f.y), make_float2(ma, ma), a01);
+                a23 = __ffma2_rn(make_float2(f.z, f.w), make_float2(ma, ma), a23);
+                b01 = __ffma2_rn(make_float2(f.x, f.y), make_float2(mb, mb), b01);
+                b23 = __ffma2_rn(make_float2(f.z, f.w), make_float2(mb, mb), b23);
+            }
+            ga[0] += (double)a01.x;
+            ga[1] += (double)a01.y;
+            ga[2] += (double)a23.x;
+            ga[3] += (double)a23.y;
+            gb[0] += (double)b01.x;
+            gb[1] += (double)b01.y;
+            gb[2] += (double)b23.x;
+            gb[3] += (double)b23.y;
+            a01 = a23 = b01 = b23 = make_float2(0.f, 0.f);
+        }
+        const double dc1 = -dc0;
+        double* L = a.L + (size_t)it.subgrid * 20 * NCELL;
+        const int cfa = cxa * 64 + cy * 8 + cz, cfb = cxb * 64 + cy * 8 + cz;
+        L[cfa] = ga[0];
+        L[cfb] = gb[0];
+#pragma unroll
+        for (int c = 1; c < 4; ++c) {
+            L[c * NCELL + cfa] = ga[c] * dc1;
+            L[c * NCELL + cfb] = gb[c] * dc1;
+        }
+    }
+}
+
 // Per-subgrid multipole sweep on the reference's SoA buffers (two tiles of
 // 4 x 8 x 8 cells): phase-one partners take mon + M0 and the higher moments,
 // monopole-only partners the mass alone (kokkos_kernel.hpp:241-283).

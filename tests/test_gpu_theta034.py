@@ -1,8 +1,8 @@
 """Opening angle below 0.5 (theta = 0.34, coarse reach 2, the reference's
 production setting of its rotating-star runs): the plane-streaming kernels
 against the oracle. Exact form bit-identical, fast form within 1e-12; the
-FP32-split form (fused split tiles in the RHO solve, the fast FP64 form for
-d(rho)/dt, P2P and P2M) within 1e-6 on the potential and force, 1e-5 on
+FP32-split form (fused split tiles in the RHO solve, FP32 P2P, the fast FP64
+form for the d(rho)/dt tiles and P2M) within 1e-6 on the potential and force, 1e-5 on
 L4..L19 and 1e-10 on L_c, also on the full-size AMR polytrope."""
 from __future__ import annotations
 
