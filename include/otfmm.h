@@ -206,6 +206,7 @@ int otfmm_batch(otfmm_context* ctx, const double* pool_M, const double* pool_com
 #define OTFMM_P2P_STENCIL 1 /* leaf P2P in stencil order, two cells per thread */
 #define OTFMM_P2M_COARSE 0  /* fast-form P2M: one lane per cell, the 8 cells of a coarse cell share partner loads */
 #define OTFMM_P2M_LANES 1   /* fast-form P2M: p2m_lanes lanes share one cell's partners */
+#define OTFMM_P2M_OCTANT 2  /* P2M by leaf octant, partner slabs in shared memory (the split precision contracts in FP32) */
 typedef struct otfmm_tuning {
     int32_t split_m2l_form;  /* one of the OTFMM_SPLIT_* forms above */
     int32_t split_m2l_chunk; /* FP32 partial sums of the warp-specialised tiles promoted every 8 or 16 partners
@@ -213,7 +214,8 @@ typedef struct otfmm_tuning {
     int32_t split_p2p_chunk; /* FP32 P2P partial sums promoted every 16 or 32 partners (box form: every 18 or 36) */
     int32_t p2m_lanes;       /* fast-form P2M: at most 4, 8 or 16 lanes share one cell's entries */
     int32_t p2p_form;        /* OTFMM_P2P_BOX or OTFMM_P2P_STENCIL (fast and split forms, theta >= 0.5) */
-    int32_t p2m_form;        /* OTFMM_P2M_COARSE or OTFMM_P2M_LANES (fast and split forms, theta >= 0.5) */
+    int32_t p2m_form;        /* OTFMM_P2M_COARSE, OTFMM_P2M_LANES or OTFMM_P2M_OCTANT (fast and split forms,
+                              * theta >= 0.5) */
 } otfmm_tuning;
 
 /* One otfmm_batch with CUDA events between its launches: kernel_ms receives the
@@ -225,7 +227,7 @@ int otfmm_batch_profile(otfmm_context* ctx, const double* pool_M, const double* 
                         int32_t n_items, double* L, double* L_c, int gsolve_type, int precision, float kernel_ms[4],
                         void* stream);
 
-/* The context's current variants (defaults: fused, 16, 32, 4, box, lanes). */
+/* The context's current variants (defaults: fused, 16, 32, 4, box, octant). */
 int otfmm_get_tuning(const otfmm_context* ctx, otfmm_tuning* out);
 int otfmm_set_tuning(otfmm_context* ctx, const otfmm_tuning* t);
 

@@ -169,15 +169,26 @@ enum : int {
     WL_P2M_NEXT = 4,
     WL_ROOT = 5,
     WL_LEAF_NEXT = 6,
-    WL_COUNTERS = 8
+    WL_P2M_UNITS = 7,        // P2M octant units listed from the front of p2m_units
+    WL_P2M_UNITS_BACK = 8,   // ... and from its back
+    WL_COUNTERS = 10
 };
 struct WorkLists {
-    int* m2l;      // refined, non-root items
-    int* root;     // level-0 items
-    int* leaf;     // leaf items
-    int* p2m;      // leaf items with a refined neighbour
-    int* counts;   // WL_* counters
+    int* m2l;        // refined, non-root items
+    int* root;       // level-0 items
+    int* leaf;       // leaf items
+    int* p2m;        // leaf items with a refined neighbour
+    int* counts;     // WL_* counters
+    int* p2m_units;  // P2M octant units (item << 3 | octant), unit_cap entries
+    int unit_cap;
 };
+// Work-list storage (ints) for a capacity of cap items: four item lists, the
+// counters, 8 P2M octant units per item.
+constexpr size_t work_list_ints(size_t cap) { return 12 * cap + WL_COUNTERS; }
+__host__ __device__ inline WorkLists work_lists(int* base, size_t cap) {
+    return WorkLists{base, base + cap, base + 2 * cap, base + 3 * cap, base + 4 * cap, base + 4 * cap + WL_COUNTERS,
+                     (int)(8 * cap)};
+}
 
 struct BatchArgs {
     const double* M;
@@ -202,33 +213,97 @@ __device__ __forceinline__ bool item_valid(const BatchArgs& a, const otfmm_work_
     return !b;
 }
 
-// One thread per work item: validates it (a malformed item raises the error
-// flag and is dropped before anything reads with its fields) and appends it
-// to the list of its kind.
-__global__ void classify_kernel(BatchArgs a) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.n_items) return;
-    const otfmm_work_item& w = a.items[i];
-    if (!item_valid(a, w)) {
-        atomicOr(a.err, 1);
-        return;
-    }
-    if (w.kind == OTFMM_KIND_M2L) {
-        a.wl.m2l[atomicAdd(a.wl.counts + WL_M2L, 1)] = i;
-    } else if (w.kind == OTFMM_KIND_M2L_ROOT) {
-        a.wl.root[atomicAdd(a.wl.counts + WL_ROOT, 1)] = i;
-    } else {
-        a.wl.leaf[atomicAdd(a.wl.counts + WL_LEAF, 1)] = i;
-        bool refined_nb = false;
-        for (int d = 0; d < 26; ++d) refined_nb |= (w.neighbors[d] >= 0 && !a.is_leaf[w.neighbors[d]]);
-        if (refined_nb) a.wl.p2m[atomicAdd(a.wl.counts + WL_P2M, 1)] = i;
-    }
-}
-
 // Raw-direction bit mask (bit 13, the centre, left out) of 26 per-direction flags.
 __device__ __forceinline__ uint32_t raw_bits(uint32_t dirbits) {
     return (dirbits & 0x1fffu) | ((dirbits >> 13) << 14);
 }
+
+// Raw directions (bit r, centre excluded) facing octant o = sx + 2 sy + 4 sz
+// of a subgrid (4x4x4 cells): every offset component is 0 or points out of
+// the octant's side.
+__host__ __device__ constexpr uint32_t octant_dirs(int o) {
+    uint32_t m = 0;
+    for (int r = 0; r < 27; ++r) {
+        const int d[3] = {r % 3 - 1, (r / 3) % 3 - 1, r / 9 - 1};
+        bool ok = (r != 13);
+        for (int c = 0; c < 3; ++c) {
+            const int s = (o >> c) & 1;
+            ok = ok && (d[c] == 0 || d[c] == 2 * s - 1);
+        }
+        if (ok) m |= 1u << r;
+    }
+    return m;
+}
+__constant__ uint32_t c_octant_dirs[8] = {octant_dirs(0), octant_dirs(1), octant_dirs(2), octant_dirs(3),
+                                          octant_dirs(4), octant_dirs(5), octant_dirs(6), octant_dirs(7)};
+// Raw directions across a face (one non-zero offset component).
+constexpr uint32_t FACE_DIRS = (1u << 4) | (1u << 10) | (1u << 12) | (1u << 14) | (1u << 16) | (1u << 22);
+
+// Reserves n slots of a list for each lane of a full warp with one atomic
+// (lanes in order): returns the lane's first slot.
+__device__ __forceinline__ int warp_reserve(int* counter, int n) {
+    const int lane = threadIdx.x & 31;
+    int incl = n;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    int base = 0;
+    if (lane == 31 && incl > 0) base = atomicAdd(counter, incl);
+    return __shfl_sync(0xffffffffu, base, 31) + incl - n;
+}
+
+// One thread per work item (blocks of whole warps): validates it (a malformed
+// item raises the error flag and is dropped before anything reads with its
+// fields) and appends it to the list of its kind, one atomic per warp and
+// list. A leaf with refined neighbours also goes to the P2M list, with its
+// P2M octant units (unit = item << 3 | octant, item < 2^27): the octants
+// facing a refined neighbour across a face from the front of p2m_units, the
+// others from its back (the P2M kernel takes the front ones first).
+__global__ void classify_kernel(BatchArgs a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int kind = -1;
+    uint32_t refmask = 0;
+    if (i < a.n_items) {
+        const otfmm_work_item& w = a.items[i];
+        if (!item_valid(a, w)) {
+            atomicOr(a.err, 1);
+        } else {
+            kind = w.kind;
+            if (kind == OTFMM_KIND_LEAF) {
+                uint32_t refined = 0;
+                for (int d = 0; d < 26; ++d)
+                    if (w.neighbors[d] >= 0 && !a.is_leaf[w.neighbors[d]]) refined |= 1u << d;
+                refmask = raw_bits(refined);
+            }
+        }
+    }
+    const int s_m2l = warp_reserve(a.wl.counts + WL_M2L, kind == OTFMM_KIND_M2L);
+    const int s_root = warp_reserve(a.wl.counts + WL_ROOT, kind == OTFMM_KIND_M2L_ROOT);
+    const int s_leaf = warp_reserve(a.wl.counts + WL_LEAF, kind == OTFMM_KIND_LEAF);
+    const int s_p2m = warp_reserve(a.wl.counts + WL_P2M, refmask != 0);
+    if (kind == OTFMM_KIND_M2L) a.wl.m2l[s_m2l] = i;
+    if (kind == OTFMM_KIND_M2L_ROOT) a.wl.root[s_root] = i;
+    if (kind == OTFMM_KIND_LEAF) a.wl.leaf[s_leaf] = i;
+    if (refmask) a.wl.p2m[s_p2m] = i;
+    uint32_t front = 0, back = 0;
+#pragma unroll
+    for (int o = 0; o < 8; ++o) {
+        const uint32_t m = refmask & c_octant_dirs[o];
+        if (m & FACE_DIRS) front |= 1u << o;
+        else if (m) back |= 1u << o;
+    }
+    int sf = warp_reserve(a.wl.counts + WL_P2M_UNITS, __popc(front));
+    int sb = warp_reserve(a.wl.counts + WL_P2M_UNITS_BACK, __popc(back));
+#pragma unroll
+    for (int o = 0; o < 8; ++o) {
+        const int unit = (int)(((unsigned)i << 3) | (unsigned)o);
+        if ((front >> o) & 1u) a.wl.p2m_units[sf++] = unit;
+        if ((back >> o) & 1u) a.wl.p2m_units[a.wl.unit_cap - 1 - sb++] = unit;
+    }
+}
+
 
 // Copies an item (already validated by classify_kernel) into shared memory:
 // the first warp, one lane per direction, with the leaf / neighbour masks.

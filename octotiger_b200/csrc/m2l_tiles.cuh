@@ -1151,7 +1151,10 @@ __device__ __forceinline__ void fz_geometry(const double dX[3], float dXf[3], Fa
     f.X01 = dX[0] * dX[1];
     f.X02 = dX[0] * dX[2];
     f.X12 = dX[1] * dX[2];
-    const double r2 = fmax(f.X00 + f.X11 + f.X22, 1.0e-20);
+    // no FP64 clamp: the seed comes from the clamped FP32 r2, so the Newton
+    // step stays finite at r2 = 0, and below r2 = 1e-20 a clamp would move rs
+    // by less than 1e-14 of its value
+    const double r2 = f.X00 + f.X11 + f.X22;
     const double y = (double)*rsf;
     const double rs = y * fma(-0.5 * r2 * y, y, 1.5);
     const double r2inv = rs * rs;

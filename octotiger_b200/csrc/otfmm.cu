@@ -36,6 +36,7 @@
 #include "layout.cuh"
 #include "leaf_kernels.cuh"
 #include "m2l_tiles.cuh"
+#include "p2m_octant.cuh"
 #include "pair_math.cuh"
 #include "reach2_kernels.cuh"
 #include "soa_kernels.cuh"
@@ -247,7 +248,7 @@ struct otfmm_context {
     int* d_lists = nullptr;            // batched work lists (grown on demand)
     long long lists_gen = 0;           // times d_lists was reallocated (a host plan binds one generation)
     int list_capacity = 0;
-    otfmm_tuning tuning = {OTFMM_SPLIT_FUSED, 16, 32, 4, OTFMM_P2P_BOX, OTFMM_P2M_LANES};
+    otfmm_tuning tuning = {OTFMM_SPLIT_FUSED, 16, 32, 4, OTFMM_P2P_BOX, OTFMM_P2M_OCTANT};
     // otfmm_batch_host: device copies of the pool, work list and outputs, a
     // pinned host copy of the reordered work list, two copy streams and events
     struct HostPath {
@@ -334,6 +335,10 @@ int ensure_attributes(int device) {
     rc = rc ? rc : set_smem(p2p_r2_kernel<PREC_FAST>, R2_SMEM_BYTES);
     rc = rc ? rc : set_smem(p2m_coarse_kernel<true>, PC_SMEM_BYTES);
     rc = rc ? rc : set_smem(p2m_coarse_kernel<false>, PC_SMEM_BYTES);
+    rc = rc ? rc : set_smem(p2m_octant_kernel<PREC_SPLIT, true>, PO_SMEM_BYTES);
+    rc = rc ? rc : set_smem(p2m_octant_kernel<PREC_SPLIT, false>, PO_SMEM_BYTES);
+    rc = rc ? rc : set_smem(p2m_octant_kernel<PREC_FAST, true>, PO_SMEM_BYTES);
+    rc = rc ? rc : set_smem(p2m_octant_kernel<PREC_FAST, false>, PO_SMEM_BYTES);
     rc = rc ? rc : set_smem(p2m_fast_kernel<true>, 7 * 8 * 6 * NCELL);
     rc = rc ? rc : set_smem(p2m_fast_kernel<false>, 7 * 8 * 6 * NCELL);
     rc = rc ? rc : set_smem(soa_m2l_kernel<PREC_EXACT, true, false>, bytes);
@@ -991,7 +996,8 @@ int check_tuning(const otfmm_tuning& t) {
     if (t.split_p2p_chunk != 16 && t.split_p2p_chunk != 32) return fail(OTFMM_ERR_INVALID, "split P2P chunk must be 16 or 32");
     if (t.p2m_lanes != 4 && t.p2m_lanes != 8 && t.p2m_lanes != 16) return fail(OTFMM_ERR_INVALID, "P2M lanes must be 4, 8 or 16");
     if (t.p2p_form != OTFMM_P2P_BOX && t.p2p_form != OTFMM_P2P_STENCIL) return fail(OTFMM_ERR_INVALID, "unknown P2P form");
-    if (t.p2m_form != OTFMM_P2M_COARSE && t.p2m_form != OTFMM_P2M_LANES) return fail(OTFMM_ERR_INVALID, "unknown P2M form");
+    if (t.p2m_form != OTFMM_P2M_COARSE && t.p2m_form != OTFMM_P2M_LANES && t.p2m_form != OTFMM_P2M_OCTANT)
+        return fail(OTFMM_ERR_INVALID, "unknown P2M form");
     return OTFMM_OK;
 }
 
@@ -1000,7 +1006,8 @@ int check_batch_args(otfmm_context* ctx, const double* pool_M, const double* poo
                      double* L, double* L_c, int gsolve_type, int precision) {
     if (!ctx || !pool_M || !pool_com || !pool_mon || !pool_is_leaf || !items || !L || !L_c)
         return fail(OTFMM_ERR_INVALID, "NULL argument");
-    if (n_subgrids <= 0 || n_items < 0 || n_items > (1 << 29)) return fail(OTFMM_ERR_INVALID, "bad sizes");
+    // at most 2^27 items: 8 P2M octant units per item stay below 2^30 list entries
+    if (n_subgrids <= 0 || n_items < 0 || n_items > (1 << 27)) return fail(OTFMM_ERR_INVALID, "bad sizes");
     if (gsolve_type != OTFMM_RHO && gsolve_type != OTFMM_DRHODT) return fail(OTFMM_ERR_INVALID, "bad gsolve_type");
     return check_precision(precision, true);
 }
@@ -1017,7 +1024,7 @@ int enqueue_batch(otfmm_context* ctx, const double* pool_M, const double* pool_c
     auto mark = [&](int i) {
         if (marks) cudaEventRecord(marks[i], s);
     };
-    WorkLists wl{lists, lists + cap, lists + 2 * (size_t)cap, lists + 3 * (size_t)cap, lists + 4 * (size_t)cap};
+    const WorkLists wl = work_lists(lists, (size_t)cap);
     if (reset_err) OT_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
     OT_CUDA(cudaMemsetAsync(wl.counts, 0, sizeof(int) * WL_COUNTERS, s));
     BatchArgs a{pool_M, pool_com, pool_mon, pool_is_leaf, n_subgrids, items, n_items, L, L_c, ctx->tables(),
@@ -1133,7 +1140,16 @@ int enqueue_batch(otfmm_context* ctx, const double* pool_M, const double* pool_c
             }
         }
         mark(3);
-        if (tu.p2m_form == OTFMM_P2M_COARSE && ctx->pc_ok) {
+        if (tu.p2m_form == OTFMM_P2M_OCTANT && ctx->pc_ok) {
+            const dim3 grid(2 * sms);   // persistent: two CTAs per SM take the units
+            if (precision == OTFMM_FP32_SPLIT) {
+                if (rho) p2m_octant_kernel<PREC_SPLIT, true><<<grid, PO_THREADS, PO_SMEM_BYTES, ls>>>(a);
+                else p2m_octant_kernel<PREC_SPLIT, false><<<grid, PO_THREADS, PO_SMEM_BYTES, ls>>>(a);
+            } else {
+                if (rho) p2m_octant_kernel<PREC_FAST, true><<<grid, PO_THREADS, PO_SMEM_BYTES, ls>>>(a);
+                else p2m_octant_kernel<PREC_FAST, false><<<grid, PO_THREADS, PO_SMEM_BYTES, ls>>>(a);
+            }
+        } else if (tu.p2m_form == OTFMM_P2M_COARSE && ctx->pc_ok) {
             if (rho) p2m_coarse_kernel<true><<<p2m_grid, PC_THREADS, PC_SMEM_BYTES, ls>>>(a);
             else p2m_coarse_kernel<false><<<p2m_grid, PC_THREADS, PC_SMEM_BYTES, ls>>>(a);
         } else {
@@ -1161,7 +1177,7 @@ int ensure_list_capacity(otfmm_context* ctx, int32_t n_items, cudaStream_t s) {
     ctx->d_lists = nullptr;
     const int cap = std::max(n_items, 2 * ctx->list_capacity);
     ++ctx->lists_gen;   // before the allocation: a failed regrowth also invalidates host plans
-    OT_CUDA(cudaMalloc(&ctx->d_lists, sizeof(int) * (4 * (size_t)cap + WL_COUNTERS)));
+    OT_CUDA(cudaMalloc(&ctx->d_lists, sizeof(int) * work_list_ints((size_t)cap)));
     ctx->list_capacity = cap;
     return OTFMM_OK;
 }
@@ -1471,7 +1487,7 @@ int otfmm_plan_create(otfmm_context* ctx, const double* pool_M, const double* po
     plan->ctx = ctx;
     cudaStream_t cs = nullptr;
     cudaError_t e;
-    if ((e = cudaMalloc(&plan->lists, sizeof(int) * (4 * (size_t)n_items + WL_COUNTERS))) != cudaSuccess ||
+    if ((e = cudaMalloc(&plan->lists, sizeof(int) * work_list_ints((size_t)n_items))) != cudaSuccess ||
         (e = cudaMalloc(&plan->err, sizeof(int))) != cudaSuccess ||
         (e = cudaMemset(plan->err, 0, sizeof(int))) != cudaSuccess ||
         (e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking)) != cudaSuccess ||
@@ -1619,10 +1635,10 @@ int otfmm_autotune(otfmm_context* ctx, const double* pool_M, const double* pool_
     const int forms[4] = {OTFMM_SPLIT_WARP_SPECIALISED_PACKED, OTFMM_SPLIT_WARP_SPECIALISED, OTFMM_SPLIT_SINGLE_ROLE,
                           OTFMM_SPLIT_FUSED};
     const int m2l_chunks[2] = {8, 16}, p2p_chunks[2] = {16, 32}, lanes[3] = {4, 8, 16};
-    const int p2p_forms[2] = {OTFMM_P2P_BOX, OTFMM_P2P_STENCIL}, p2m_forms[2] = {OTFMM_P2M_LANES, OTFMM_P2M_COARSE};
+    const int p2p_forms[2] = {OTFMM_P2P_BOX, OTFMM_P2P_STENCIL}, p2m_forms[3] = {OTFMM_P2M_LANES, OTFMM_P2M_COARSE, OTFMM_P2M_OCTANT};
     const bool split = (precision == OTFMM_FP32_SPLIT), fast = (precision != OTFMM_FP64_EXACT);
     for (int dim = 0; dim < 6 && rc == OTFMM_OK; ++dim) {
-        const int nvar = dim == 0 ? 4 : dim == 3 ? 3 : 2;
+        const int nvar = dim == 0 ? 4 : (dim == 3 || dim == 5) ? 3 : 2;
         if ((dim < 3 && !split) || (dim >= 3 && !fast)) continue;
         for (int v = 0; v < nvar && rc == OTFMM_OK; ++v) {
             otfmm_tuning tu = best;

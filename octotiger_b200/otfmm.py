@@ -36,7 +36,7 @@ _lib = None
 SPLIT_WARP_SPECIALISED, SPLIT_SINGLE_ROLE, SPLIT_WARP_SPECIALISED_PACKED, SPLIT_FUSED = 0, 1, 2, 3
 SPLIT_FORMS = {0: "warp_specialised", 1: "single_role", 2: "warp_specialised_packed", 3: "fused"}
 P2P_FORMS = {0: "box", 1: "stencil"}
-P2M_FORMS = {0: "coarse", 1: "lanes"}
+P2M_FORMS = {0: "coarse", 1: "lanes", 2: "octant"}
 
 
 class Tuning(ctypes.Structure):

@@ -64,7 +64,7 @@ VARIANTS = (list(itertools.product([0, 1, 2], [8, 16], [16, 32], [4, 8, 16]))
             + list(itertools.product([3], [16], [16, 32], [4, 8])))
 ALLOWED = list(itertools.product([0, 1, 2, 3], [8, 16], [16, 32], [4, 8, 16]))
 P2P_FORMS = (0, 1)   # OTFMM_P2P_BOX, OTFMM_P2P_STENCIL
-P2M_FORMS = (0, 1)   # OTFMM_P2M_COARSE, OTFMM_P2M_LANES
+P2M_FORMS = (0, 1, 2)   # OTFMM_P2M_COARSE, OTFMM_P2M_LANES, OTFMM_P2M_OCTANT
 
 
 @pytest.mark.parametrize("form,m2l_chunk,p2p_chunk,lanes", VARIANTS)
@@ -115,6 +115,40 @@ def test_leaf_forms_within_tolerance(oracle, solve, theta, p2p_form, p2m_form, p
         c.close()
 
 
+@pytest.mark.parametrize("solve", [RHO, DRHODT])
+@pytest.mark.parametrize("case", ["all_refined", "mixed"])
+@pytest.mark.parametrize("precision", ["fp64", "fp32_split"])
+def test_p2m_octant_form_against_oracle(oracle, solve, case, precision):
+    """The octant P2M on a leaf whose 26 neighbours are all refined (every
+    octant has its 3 faces, 3 edges and corner: the largest slab set), and on
+    a leaf with leaf and empty neighbours mixed in; against the oracle and
+    against the lane form."""
+    from octotiger_b200.otfmm import BatchSolver, Context, Tuning
+    b = (syn.single_subgrid(seed=95, leaf_centre=True) if case == "all_refined"
+         else syn.single_subgrid(seed=96, leaf_centre=True, leaf_dirs=(0, 4, 12, 21), empty_dirs=(7, 25)))
+    Lo, Lco = oracle.batch(0.5, b.pool, b.items, rho=(solve == RHO))
+    c = Context(0, 0.5)
+    try:
+        got = {}
+        for form in (1, 2):
+            c.set_tuning(Tuning(3, 16, 32, 4, 0, form))
+            s = BatchSolver(c, b.pool, b.items)
+            s.run(solve, precision)
+            got[form] = s.results()
+        L, Lc = got[2]
+        e = scaled(L, Lo)
+        if precision == "fp64":
+            assert e.max() <= 1e-12 and scaled(Lc, Lco).max() <= 1e-12, e
+            assert scaled(L, got[1][0]).max() <= 1e-13
+        else:
+            assert e[:4].max() <= 1e-6, e
+            assert scaled(Lc, Lco).max() <= 1e-10
+        sub = int(b.items[0]["subgrid"])
+        assert np.isfinite(L[sub, :4]).all() and (np.abs(L[sub, :4]) > 0).all()
+    finally:
+        c.close()
+
+
 def test_autotune_keeps_an_allowed_variant(ctx, oracle):
     from octotiger_b200.otfmm import BatchSolver
     b = amr_small()
@@ -138,7 +172,7 @@ def test_invalid_variants_rejected(ctx):
     from octotiger_b200.otfmm import OtfmmError, Tuning
     keep = ctx.get_tuning()
     for bad in (Tuning(4, 16, 32, 16), Tuning(0, 12, 32, 16), Tuning(0, 16, 8, 16), Tuning(0, 16, 32, 3),
-                Tuning(0, 16, 32, 16, 2), Tuning(0, 16, 32, 16, 0, 2)):
+                Tuning(0, 16, 32, 16, 2), Tuning(0, 16, 32, 16, 0, 3)):
         with pytest.raises(OtfmmError):
             ctx.set_tuning(bad)
     assert ctx.get_tuning().as_dict() == keep.as_dict()
