@@ -25,6 +25,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -234,6 +235,10 @@ struct otfmm_context {
     int* d_pc_parts = nullptr;
     int pc_units = 0;                // units over all 26 directions
     bool pc_ok = false;              // the 8 cells of every coarse cell share their partners
+    bool po_ok = false;              // pc_ok, and every octant's partner sub-slabs fit PO_CELLS
+    int4* d_po_box = nullptr;        // P2M octant tables (reach 1)
+    int2* d_po_range = nullptr;
+    uint16_t* d_po_list = nullptr;
     int box_grid[6] = {};            // resident CTAs of the box P2P kernels (all SMs)
     // leaf kernels of a batched solve run on `aux`, forked after the
     // classification and joined before the solve ends, so that they fill the
@@ -268,7 +273,7 @@ struct otfmm_context {
                       d_entries_ws, d_four,  d_phase,        d_p2m_start,     d_p2m_list,    d_p2m_perm_start,
                       d_p2m_perm,   d_p2m_slot,     d_p2p_four,      d_entries_r2,  d_r2_sx_start, d_r2_four,
                       d_p2p_box,    d_p2p_cube,     d_pc_unit_start, d_pc_coarse,  d_pc_range,    d_pc_list,
-                      d_pc_slot,    d_pc_parts,     d_r2_four_f}; }
+                      d_pc_slot,    d_pc_parts,     d_r2_four_f,     d_po_box,     d_po_range,    d_po_list}; }
 };
 
 namespace {
@@ -606,6 +611,55 @@ int otfmm_create(int device, double theta, otfmm_context** out) {
         pc_parts[r] = std::max(1, (longest + PC_PART - 1) / PC_PART);
         if ((pc_unit_start[r + 1] - pc_unit_start[r]) * pc_parts[r] > PC_ROUND_ITEMS) ctx->pc_ok = false;
     }
+    // P2M by octant (reach 1): per (direction r, octant o) the box of the
+    // neighbour's cells that the octant's coarse cells have as partners (its
+    // sub-slab: x, y, z of the low corner and the cell count; then the extents),
+    // per (r, coarse cell C) those partners as indices into the sub-slab, in the
+    // stencil order of C's first cell
+    std::vector<int4> po_box(2 * 27 * 8, int4{0, 0, 0, 0});
+    std::vector<int2> po_range(27 * 64, int2{0, 0});
+    std::vector<uint16_t> po_list;
+    ctx->po_ok = ctx->pc_ok;
+    for (int o = 0; o < 8 && ctx->po_ok; ++o) {
+        int cells = 0;
+        for (int r = 0; r < 27; ++r) {
+            if (r == 13) continue;
+            int lo[3] = {8, 8, 8}, hi[3] = {-1, -1, -1};
+            auto first_cell = [&](int w) {
+                const int Cx = 2 * (o & 1) + (w & 1), Cy = 2 * ((o >> 1) & 1) + ((w >> 1) & 1),
+                          Cz = 2 * ((o >> 2) & 1) + (w >> 2);
+                return std::array<int, 2>{Cx * 16 + Cy * 4 + Cz, (2 * Cx) * 64 + (2 * Cy) * 8 + 2 * Cz};
+            };
+            for (int w = 0; w < 8; ++w) {
+                const int cu = first_cell(w)[1];
+                for (int q = p2m_start[cu * 28 + r]; q < p2m_start[cu * 28 + r + 1]; ++q) {
+                    const int u = p2m_list[q], c3[3] = {u >> 6, (u >> 3) & 7, u & 7};
+                    for (int d = 0; d < 3; ++d) {
+                        lo[d] = std::min(lo[d], c3[d]);
+                        hi[d] = std::max(hi[d], c3[d]);
+                    }
+                }
+            }
+            if (hi[0] < 0) continue;
+            if (!((octant_dirs(o) >> r) & 1u)) ctx->po_ok = false;   // a partner outside the octant's directions
+            const int n[3] = {hi[0] - lo[0] + 1, hi[1] - lo[1] + 1, hi[2] - lo[2] + 1};
+            po_box[(r * 8 + o) * 2] = int4{lo[0], lo[1], lo[2], n[0] * n[1] * n[2]};
+            po_box[(r * 8 + o) * 2 + 1] = int4{n[0], n[1], n[2], 0};
+            cells += n[0] * n[1] * n[2];
+            for (int w = 0; w < 8; ++w) {
+                const auto fc = first_cell(w);
+                po_range[r * 64 + fc[0]].x = (int)po_list.size();
+                for (int q = p2m_start[fc[1] * 28 + r]; q < p2m_start[fc[1] * 28 + r + 1]; ++q) {
+                    const int u = p2m_list[q];
+                    po_list.push_back(
+                        (uint16_t)((((u >> 6) - lo[0]) * n[1] + (((u >> 3) & 7) - lo[1])) * n[2] + ((u & 7) - lo[2])));
+                }
+                po_range[r * 64 + fc[0]].y = (int)po_list.size();
+            }
+        }
+        if (cells > PO_CELLS) ctx->po_ok = false;
+    }
+    if (po_list.empty()) po_list.assign(1, 0);
     if (pc_coarse.empty()) pc_coarse.assign(4, -1);
     if (pc_list.empty()) pc_list.assign(1, 0);
     DeviceGuard g(device);
@@ -639,6 +693,15 @@ int otfmm_create(int device, double theta, otfmm_context** out) {
                         cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMalloc(&ctx->d_pc_list, sizeof(uint16_t) * pc_list.size())) != cudaSuccess ||
         (e = cudaMemcpy(ctx->d_pc_list, pc_list.data(), sizeof(uint16_t) * pc_list.size(),
+                        cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMalloc(&ctx->d_po_box, sizeof(int4) * po_box.size())) != cudaSuccess ||
+        (e = cudaMemcpy(ctx->d_po_box, po_box.data(), sizeof(int4) * po_box.size(), cudaMemcpyHostToDevice)) !=
+            cudaSuccess ||
+        (e = cudaMalloc(&ctx->d_po_range, sizeof(int2) * po_range.size())) != cudaSuccess ||
+        (e = cudaMemcpy(ctx->d_po_range, po_range.data(), sizeof(int2) * po_range.size(), cudaMemcpyHostToDevice)) !=
+            cudaSuccess ||
+        (e = cudaMalloc(&ctx->d_po_list, sizeof(uint16_t) * po_list.size())) != cudaSuccess ||
+        (e = cudaMemcpy(ctx->d_po_list, po_list.data(), sizeof(uint16_t) * po_list.size(),
                         cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMalloc(&ctx->d_pc_parts, sizeof(int) * pc_parts.size())) != cudaSuccess ||
         (e = cudaMemcpy(ctx->d_pc_parts, pc_parts.data(), sizeof(int) * pc_parts.size(),
@@ -735,6 +798,9 @@ int otfmm_destroy(otfmm_context* ctx) {
     cudaFree(ctx->d_pc_list);
     cudaFree(ctx->d_pc_slot);
     cudaFree(ctx->d_pc_parts);
+    cudaFree(ctx->d_po_box);
+    cudaFree(ctx->d_po_range);
+    cudaFree(ctx->d_po_list);
     if (ctx->aux) {
         cudaStreamSynchronize(ctx->aux);
         cudaStreamDestroy(ctx->aux);
@@ -1140,8 +1206,8 @@ int enqueue_batch(otfmm_context* ctx, const double* pool_M, const double* pool_c
             }
         }
         mark(3);
-        if (tu.p2m_form == OTFMM_P2M_OCTANT && ctx->pc_ok) {
-            const dim3 grid(2 * sms);   // persistent: two CTAs per SM take the units
+        if (tu.p2m_form == OTFMM_P2M_OCTANT && ctx->po_ok) {
+            const dim3 grid(PO_CTAS_PER_SM * sms);   // persistent: the resident CTAs take the units
             if (precision == OTFMM_FP32_SPLIT) {
                 if (rho) p2m_octant_kernel<PREC_SPLIT, true><<<grid, PO_THREADS, PO_SMEM_BYTES, ls>>>(a);
                 else p2m_octant_kernel<PREC_SPLIT, false><<<grid, PO_THREADS, PO_SMEM_BYTES, ls>>>(a);

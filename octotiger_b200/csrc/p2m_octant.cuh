@@ -23,24 +23,27 @@ namespace otfmm {
 // face first). Every target cell belongs to exactly one unit, which forms its
 // whole P2M sum, so no partial crosses units and the result does not depend
 // on the schedule.
-//   * the slabs (pc_slab_shape) of the octant's refined directions are staged
-//     once, in units of dx from the leaf's origin, with the fast form's
-//     factors folded into the moments;
-//   * warp w takes coarse cell w of the octant; lane = 8 f + c: cell c of the
-//     coarse cell (whose 8 cells share one partner list per direction) and
-//     partner stride f (partners f, f + 4, ... of each list), so the 8 lanes
-//     of a cell group read one partner together and a warp has no divergence;
+//   * the partner sub-slabs (Tables::po_box: the part of a refined
+//     neighbour's 2-cell slab that the octant's cells reach) of the octant's
+//     refined directions are staged once, in units of dx from the leaf's
+//     origin, with the fast form's factors folded into the moments;
+//   * the octant's coarse cells with partners go to the 4 warps in turn;
+//     lane = 8 f + c: cell c of the coarse cell (whose 8 cells share one
+//     partner list per direction) and partner stride f (partners f, f + 4, ...
+//     of each list), so the 8 lanes of a cell read one partner together and a
+//     warp has no divergence;
 //   * directions in raw order, partners in list order; the four strides are
 //     added by a fixed butterfly; the unit adds the sum to the P2P result in L
-//     and writes L_c.
+//     and writes L_c of its cells with partners.
+// 128-thread CTAs, four per SM (shared memory and 124 registers allow four).
 // Split form: FP32 sums promoted to FP64 after each direction (at most 18
 // partners in FP32).
-constexpr int PO_THREADS = 256;
-constexpr int PO_CELLS = 3 * 128 + 3 * 32 + 8;   // slabs of 3 faces, 3 edges and a corner
+constexpr int PO_THREADS = 128;
+constexpr int PO_CTAS_PER_SM = 4;
+constexpr int PO_CELLS = 296;                    // sub-slabs of 3 faces (2x6x6), 3 edges (2x2x6), a corner
 constexpr int PO_ROW_BYTES = 192;                // staged bytes of one slab cell
-constexpr int PO_SMEM_BYTES = PO_CELLS * PO_ROW_BYTES;   // 93696
-static_assert(2 * (PO_SMEM_BYTES + 1024 + 512) <= 233472, "two CTAs per SM");
-static_assert((PO_CELLS * 16) % 16 == 0, "row blocks stay 16-byte aligned");
+constexpr int PO_SMEM_BYTES = PO_CELLS * PO_ROW_BYTES;   // 56832
+static_assert(PO_CTAS_PER_SM * (PO_SMEM_BYTES + 1024 + 256) <= 233472, "four CTAs per SM");
 
 // FP32-split pair: target at X (units of dx, FP64), partner slab cell v.
 // Rows: sf = (Q0..Q3), (Q4, Q5, -O0, -O1), (-O2..-O5), (-O6..-O9), (m, -D0, -D1, -D2)
@@ -139,21 +142,22 @@ __device__ __forceinline__ void p2m_fast_pair(const double X[3], const double2* 
 }
 
 template <int PREC, bool RHO>
-__global__ void __launch_bounds__(PO_THREADS, 2) p2m_octant_kernel(BatchArgs a) {
+__global__ void __launch_bounds__(PO_THREADS, PO_CTAS_PER_SM) p2m_octant_kernel(BatchArgs a) {
     extern __shared__ __align__(16) unsigned char po_dyn[];
     constexpr bool SPLIT = (PREC == PREC_SPLIT);
     // split: 5 float4 rows, then 7 double2 rows; fast: 12 double2 rows
     float4* sf = reinterpret_cast<float4*>(po_dyn);
     double2* sd = reinterpret_cast<double2*>(po_dyn + (SPLIT ? 5 * PO_CELLS * 16 : 0));
     __shared__ ItemInfo it;
-    __shared__ int s_unit, s_nr;
+    __shared__ int s_unit, s_nr, s_ncc;
     __shared__ int8_t s_rdir[8];          // the octant's refined directions, in raw order
-    __shared__ int s_rcell[9];            // their first slab cell
+    __shared__ int s_rcell[9];            // their first staged cell
+    __shared__ int8_t s_cc[8];            // the octant's coarse cells with partners there
     const int n_front = a.wl.counts[WL_P2M_UNITS], total = n_front + a.wl.counts[WL_P2M_UNITS_BACK];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int f = lane >> 3, ci = lane & 7;
     for (;;) {
-        __syncthreads();   // `it`, the direction table and the slabs are reused
+        __syncthreads();   // `it`, the direction tables and the slabs are reused
         if (threadIdx.x == 0) s_unit = atomicAdd(a.wl.counts + WL_P2M_NEXT, 1);
         __syncthreads();
         const int u = s_unit;
@@ -166,28 +170,37 @@ __global__ void __launch_bounds__(PO_THREADS, 2) p2m_octant_kernel(BatchArgs a) 
             int n = 0, cells = 0;
             for (int r = 0; r < 27; ++r) {
                 if (!((m >> r) & 1u)) continue;
-                int lo[3], sz[3];
-                pc_slab_shape(r, lo, sz);
                 s_rdir[n] = (int8_t)r;
                 s_rcell[n] = cells;
-                cells += sz[0] * sz[1] * sz[2];
+                cells += __ldg(a.t.po_box + (r * 8 + oct) * 2).w;
                 ++n;
             }
             s_rcell[n] = cells;
             s_nr = n;
+            int ncc = 0;
+            for (int w = 0; w < 8; ++w) {
+                const int C = (2 * (oct & 1) + (w & 1)) * 16 + (2 * ((oct >> 1) & 1) + ((w >> 1) & 1)) * 4 +
+                              2 * ((oct >> 2) & 1) + (w >> 2);
+                bool any = false;
+                for (int k = 0; k < n; ++k) {
+                    const int2 be = __ldg(a.t.po_range + s_rdir[k] * 64 + C);
+                    any |= be.y > be.x;
+                }
+                if (any) s_cc[ncc++] = (int8_t)C;
+            }
+            s_ncc = ncc;
         }
         __syncthreads();
         const int nr = s_nr;
         const size_t sub = (size_t)it.subgrid;
         const double inv_dx = 1.0 / it.dx, inv2 = inv_dx * inv_dx, inv3 = inv2 * inv_dx;
-        // stage the slabs (scaled, in units of dx from the leaf's origin)
+        // stage the sub-slabs (scaled, in units of dx from the leaf's origin)
         for (int t = threadIdx.x; t < s_rcell[nr]; t += blockDim.x) {
             int k = 0;
             while (s_rcell[k + 1] <= t) ++k;
             const int r = s_rdir[k], idx = t - s_rcell[k];
-            int lo[3], sz[3];
-            pc_slab_shape(r, lo, sz);
-            const int x = lo[0] + idx / (sz[1] * sz[2]), y = lo[1] + (idx / sz[2]) % sz[1], z = lo[2] + idx % sz[2];
+            const int4 lo = __ldg(a.t.po_box + (r * 8 + oct) * 2), n = __ldg(a.t.po_box + (r * 8 + oct) * 2 + 1);
+            const int x = lo.x + idx / (n.y * n.z), y = lo.y + (idx / n.z) % n.y, z = lo.z + idx % n.z;
             const int uc = x * 64 + y * 8 + z;
             const size_t nb = (size_t)it.nb[r < 13 ? r : r - 1];
             const double* Ms = a.M + nb * 20 * NCELL + uc;
@@ -229,52 +242,52 @@ __global__ void __launch_bounds__(PO_THREADS, 2) p2m_octant_kernel(BatchArgs a) 
             }
         }
         __syncthreads();
-        // warp w: coarse cell w of the octant; lane: cell ci, partner stride f
-        const int Cx = 2 * (oct & 1) + (warp & 1), Cy = 2 * ((oct >> 1) & 1) + ((warp >> 1) & 1),
-                  Cz = 2 * ((oct >> 2) & 1) + (warp >> 2);
-        const int C = Cx * 16 + Cy * 4 + Cz;
-        const int cu = (2 * Cx + (ci & 1)) * 64 + (2 * Cy + ((ci >> 1) & 1)) * 8 + (2 * Cz + (ci >> 2));
-        double X[3];
+        for (int j = warp; j < s_ncc; j += PO_THREADS / 32) {
+            const int C = s_cc[j];
+            const int cu = (2 * (C >> 4) + (ci & 1)) * 64 + (2 * ((C >> 2) & 3) + ((ci >> 1) & 1)) * 8 +
+                           (2 * (C & 3) + (ci >> 2));
+            double X[3];
 #pragma unroll
-        for (int c = 0; c < 3; ++c) X[c] = (__ldg(a.com + (sub * 3 + c) * NCELL + cu) - it.xbase[c]) * inv_dx;
-        double acc[4] = {0.0, 0.0, 0.0, 0.0}, corr[3] = {0.0, 0.0, 0.0};
-        for (int k = 0; k < nr; ++k) {
-            const int r = s_rdir[k];
-            const int2 be = __ldg(a.t.pc_range + r * 64 + C);
-            if (SPLIT) {
-                const float4* sfk = sf + s_rcell[k];
-                const double2* sdk = sd + s_rcell[k];
-                float2 a0 = make_float2(0.0f, 0.0f);
-                float a13[3] = {0.0f, 0.0f, 0.0f};
+            for (int c = 0; c < 3; ++c) X[c] = (__ldg(a.com + (sub * 3 + c) * NCELL + cu) - it.xbase[c]) * inv_dx;
+            double acc[4] = {0.0, 0.0, 0.0, 0.0}, corr[3] = {0.0, 0.0, 0.0};
+            for (int k = 0; k < nr; ++k) {
+                const int2 be = __ldg(a.t.po_range + s_rdir[k] * 64 + C);
+                if (SPLIT) {
+                    const float4* sfk = sf + s_rcell[k];
+                    const double2* sdk = sd + s_rcell[k];
+                    float2 a0 = make_float2(0.0f, 0.0f);
+                    float a13[3] = {0.0f, 0.0f, 0.0f};
 #pragma unroll 2
-                for (int q = be.x + f; q < be.y; q += 4)
-                    p2m_split_pair<RHO>(X, sfk, sdk, __ldg(a.t.pc_list + q), a0, a13, corr);
-                acc[0] += (double)a0.x + (double)a0.y;
+                    for (int q = be.x + f; q < be.y; q += 4)
+                        p2m_split_pair<RHO>(X, sfk, sdk, __ldg(a.t.po_list + q), a0, a13, corr);
+                    acc[0] += (double)a0.x + (double)a0.y;
 #pragma unroll
-                for (int c = 0; c < 3; ++c) acc[1 + c] += (double)a13[c];
-            } else {
-                const double2* sdk = sd + s_rcell[k];
+                    for (int c = 0; c < 3; ++c) acc[1 + c] += (double)a13[c];
+                } else {
+                    const double2* sdk = sd + s_rcell[k];
 #pragma unroll 2
-                for (int q = be.x + f; q < be.y; q += 4) p2m_fast_pair<RHO>(X, sdk, __ldg(a.t.pc_list + q), acc, corr);
+                    for (int q = be.x + f; q < be.y; q += 4)
+                        p2m_fast_pair<RHO>(X, sdk, __ldg(a.t.po_list + q), acc, corr);
+                }
             }
-        }
-        // the four partner strides of a cell, in a fixed order
+            // the four partner strides of a cell, in a fixed order
 #pragma unroll
-        for (int o = 8; o <= 16; o <<= 1) {
+            for (int o = 8; o <= 16; o <<= 1) {
 #pragma unroll
-            for (int q = 0; q < 4; ++q) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+                for (int q = 0; q < 4; ++q) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
 #pragma unroll
-            for (int q = 0; q < 3; ++q) corr[q] += __shfl_xor_sync(0xffffffffu, corr[q], o);
-        }
-        if (f == 0) {
-            // back to physical units: L0 dx^-1, L1..L3 dx^-2, L_c dx^-2
-            double* L = a.L + sub * 20 * NCELL + cu;
-            double* Lc = a.Lc + sub * 3 * NCELL + cu;
-            L[0] += acc[0] * inv_dx;
+                for (int q = 0; q < 3; ++q) corr[q] += __shfl_xor_sync(0xffffffffu, corr[q], o);
+            }
+            if (f == 0) {
+                // back to physical units: L0 dx^-1, L1..L3 dx^-2, L_c dx^-2
+                double* L = a.L + sub * 20 * NCELL + cu;
+                double* Lc = a.Lc + sub * 3 * NCELL + cu;
+                L[0] += acc[0] * inv_dx;
 #pragma unroll
-            for (int q = 1; q < 4; ++q) L[q * NCELL] += acc[q] * inv2;
+                for (int q = 1; q < 4; ++q) L[q * NCELL] += acc[q] * inv2;
 #pragma unroll
-            for (int q = 0; q < 3; ++q) Lc[q * NCELL] = RHO ? corr[q] * inv2 : 0.0;
+                for (int q = 0; q < 3; ++q) Lc[q * NCELL] = RHO ? corr[q] * inv2 : 0.0;
+            }
         }
     }
 }

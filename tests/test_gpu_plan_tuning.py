@@ -145,6 +145,8 @@ def test_p2m_octant_form_against_oracle(oracle, solve, case, precision):
             assert scaled(Lc, Lco).max() <= 1e-10
         sub = int(b.items[0]["subgrid"])
         assert np.isfinite(L[sub, :4]).all() and (np.abs(L[sub, :4]) > 0).all()
+        # the octant kernel ran (a fallback to the lane form would give its bits)
+        assert not np.array_equal(L, got[1][0])
     finally:
         c.close()
 
