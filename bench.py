@@ -53,6 +53,18 @@ L2_FLUSH_BYTES = 256 << 20
 PROFILED_TRAFFIC = {("uniform_level3", "fp32_split"): 48.6e6, ("uniform_level3", "fp64"): 57.9e6,
                     ("amr_polytrope_l6", "fp32_split"): 65.7e6, ("amr_polytrope_l6", "fp64"): 77.4e6}
 
+# Pipe utilisation of one launch of the multipole-tile kernel from ncu --set
+# full captures of this command on a B200 (percent of peak while the SMs are
+# active), reported beside the nominal-FLOP fraction: the fused split tiles on
+# the uniform and AMR batches, the FP64 tiles on the uniform batch.
+PROFILED_PIPES = {
+    ("uniform_level3", "fp32_split"): {"issue_active": 53.5, "fp64_pipe": 41.6, "fma_pipe": 26.0, "xu_pipe": 15.8,
+                                       "warps_per_sm": 8.0},
+    ("amr_polytrope_l6", "fp32_split"): {"issue_active": 51.6, "fp64_pipe": 40.8, "fma_pipe": 25.7, "xu_pipe": 15.8,
+                                         "warps_per_sm": 8.0},
+    ("uniform_level3", "fp64"): {"issue_active": 40.8, "fp64_pipe": 62.1},
+}
+
 
 WORKLOADS = ("uniform_level3", "amr_polytrope", "amr_binary", "single_subgrid")
 
@@ -498,6 +510,12 @@ def gpu_arm(args) -> None:
             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of the same kernel "
                               "on this workload (tuned variant)" if traffic else traffic_note,
             "fp64_peak_tflops": fp64_peak, "fp32_peak_tflops": fp32_peak}
+    pipes = PROFILED_PIPES.get((batch.name, args.precision))
+    roof["ncu_pipes_pct"] = dict(pipes, source="ncu --set full, one launch of the same kernel on this workload "
+                                              "(sm__pipe_*_cycles_active, smsp__issue_active)") if pipes else None
+    if not pipes:
+        roof["ncu_pipes_note"] = (f"no ncu capture of the {args.precision} tile kernel on the {batch.name} workload "
+                                  "is recorded in PROFILED_PIPES")
     # ncu-free pipe evidence: SM cycles per multipole pair of the tile kernel at
     # the SM clock sampled during the timed region (an FP64 M2L pair needs ~250
     # FP64-pipe instructions = ~3.9 cycles per pair and SM at 64 FP64 lanes)

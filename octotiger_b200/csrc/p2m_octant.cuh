@@ -141,6 +141,67 @@ __device__ __forceinline__ void p2m_fast_pair(const double X[3], const double2* 
     fast_p2m_pair<RHO>(X, Y, mp, L, Lc);
 }
 
+// One staged sub-slab cell: scaled moments and the centre of mass in units
+// of dx from the leaf's origin.
+struct SlabCell {
+    double m0, q[6], o[10], dp[3], P[3];
+};
+
+// Loads staged cell t of the unit (directions dirs, first cells cell0).
+template <bool RHO>
+__device__ __forceinline__ SlabCell load_slab_cell(const BatchArgs& a, const ItemInfo& it, int oct,
+                                                   const int8_t* dirs, const int* cell0, int t, double inv_dx,
+                                                   double inv2, double inv3) {
+    int k = 0;
+    while (cell0[k + 1] <= t) ++k;
+    const int r = dirs[k], idx = t - cell0[k];
+    const int4 lo = __ldg(a.t.po_box + (r * 8 + oct) * 2), n = __ldg(a.t.po_box + (r * 8 + oct) * 2 + 1);
+    const int x = lo.x + idx / (n.y * n.z), y = lo.y + (idx / n.z) % n.y, z = lo.z + idx % n.z;
+    const int uc = x * 64 + y * 8 + z;
+    const size_t nb = (size_t)it.nb[r < 13 ? r : r - 1];
+    const double* Ms = a.M + nb * 20 * NCELL + uc;
+    SlabCell c;
+    c.m0 = __ldg(Ms);
+#pragma unroll
+    for (int k2 = 0; k2 < 6; ++k2) c.q[k2] = __ldg(Ms + (4 + k2) * NCELL) * ((factor_of(4 + k2) / 2.0) * inv2);
+#pragma unroll
+    for (int k2 = 0; k2 < 10; ++k2) c.o[k2] = __ldg(Ms + (10 + k2) * NCELL) * ((factor_of(10 + k2) / 6.0) * inv3);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) c.dp[d] = RHO ? 0.0 : __ldg(Ms + (1 + d) * NCELL) * inv_dx;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) c.P[d] = (__ldg(a.com + (nb * 3 + d) * NCELL + uc) - it.xbase[d]) * inv_dx;
+    return c;
+}
+
+// Writes staged cell t in the split rows (sf, sd) or the fast rows (sd).
+template <bool SPLIT, bool RHO>
+__device__ __forceinline__ void store_slab_cell(float4* sf, double2* sd, int t, const SlabCell& c) {
+    if (SPLIT) {
+        sf[t] = make_float4((float)c.q[0], (float)c.q[1], (float)c.q[2], (float)c.q[3]);
+        sf[PO_CELLS + t] = make_float4((float)c.q[4], (float)c.q[5], (float)-c.o[0], (float)-c.o[1]);
+        sf[2 * PO_CELLS + t] = make_float4((float)-c.o[2], (float)-c.o[3], (float)-c.o[4], (float)-c.o[5]);
+        sf[3 * PO_CELLS + t] = make_float4((float)-c.o[6], (float)-c.o[7], (float)-c.o[8], (float)-c.o[9]);
+        sf[4 * PO_CELLS + t] = make_float4((float)c.m0, (float)-c.dp[0], (float)-c.dp[1], (float)-c.dp[2]);
+        sd[t] = make_double2(c.P[0], c.P[1]);
+        sd[PO_CELLS + t] = make_double2(c.P[2], 0.0);
+        if (RHO) {
+#pragma unroll
+            for (int k = 0; k < 5; ++k) sd[(2 + k) * PO_CELLS + t] = make_double2(c.o[2 * k], c.o[2 * k + 1]);
+        }
+    } else {
+        sd[t] = make_double2(c.P[0], c.P[1]);
+        sd[PO_CELLS + t] = make_double2(c.P[2], c.m0);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) sd[(2 + k) * PO_CELLS + t] = make_double2(c.q[2 * k], c.q[2 * k + 1]);
+#pragma unroll
+        for (int k = 0; k < 5; ++k) sd[(5 + k) * PO_CELLS + t] = make_double2(c.o[2 * k], c.o[2 * k + 1]);
+        if (!RHO) {
+            sd[10 * PO_CELLS + t] = make_double2(c.dp[0], c.dp[1]);
+            sd[11 * PO_CELLS + t] = make_double2(c.dp[2], 0.0);
+        }
+    }
+}
+
 template <int PREC, bool RHO>
 __global__ void __launch_bounds__(PO_THREADS, PO_CTAS_PER_SM) p2m_octant_kernel(BatchArgs a) {
     extern __shared__ __align__(16) unsigned char po_dyn[];
@@ -165,82 +226,51 @@ __global__ void __launch_bounds__(PO_THREADS, PO_CTAS_PER_SM) p2m_octant_kernel(
         const int unit = (u < n_front) ? a.wl.p2m_units[u] : a.wl.p2m_units[a.wl.unit_cap - 1 - (u - n_front)];
         const int oct = unit & 7;
         load_item(a, (int)((unsigned)unit >> 3), it);
-        if (threadIdx.x == 0) {
+        if (warp == 0) {
+            // lane l < n: the l-th refined direction facing the octant (raw
+            // order) and where its sub-slab starts
             const uint32_t m = it.nbmask & ~it.leafmask & c_octant_dirs[oct];
-            int n = 0, cells = 0;
-            for (int r = 0; r < 27; ++r) {
-                if (!((m >> r) & 1u)) continue;
-                s_rdir[n] = (int8_t)r;
-                s_rcell[n] = cells;
-                cells += __ldg(a.t.po_box + (r * 8 + oct) * 2).w;
-                ++n;
+            const int n = __popc(m);
+            int r = 0, incl = 0;
+            if (lane < n) {
+                r = (int)__fns(m, 0, lane + 1);
+                incl = __ldg(a.t.po_box + (r * 8 + oct) * 2).w;
             }
-            s_rcell[n] = cells;
-            s_nr = n;
-            int ncc = 0;
-            for (int w = 0; w < 8; ++w) {
-                const int C = (2 * (oct & 1) + (w & 1)) * 16 + (2 * ((oct >> 1) & 1) + ((w >> 1) & 1)) * 4 +
-                              2 * ((oct >> 2) & 1) + (w >> 2);
-                bool any = false;
-                for (int k = 0; k < n; ++k) {
-                    const int2 be = __ldg(a.t.po_range + s_rdir[k] * 64 + C);
+#pragma unroll
+            for (int o = 1; o < 8; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            if (lane < n) {
+                s_rdir[lane] = (int8_t)r;
+                s_rcell[lane + 1] = incl;
+            }
+            // lane w < 8: coarse cell w of the octant, if it has partners there
+            const int C = (2 * (oct & 1) + (lane & 1)) * 16 + (2 * ((oct >> 1) & 1) + ((lane >> 1) & 1)) * 4 +
+                          2 * ((oct >> 2) & 1) + ((lane >> 2) & 1);
+            bool any = false;
+            for (int k = 0; k < n; ++k) {
+                const int rk = __shfl_sync(0xffffffffu, r, k);
+                if (lane < 8) {
+                    const int2 be = __ldg(a.t.po_range + rk * 64 + C);
                     any |= be.y > be.x;
                 }
-                if (any) s_cc[ncc++] = (int8_t)C;
             }
-            s_ncc = ncc;
+            const unsigned act = __ballot_sync(0xffffffffu, lane < 8 && any);
+            if (lane < 8 && any) s_cc[__popc(act & ((1u << lane) - 1u))] = (int8_t)C;
+            if (lane == 0) {
+                s_rcell[0] = 0;
+                s_nr = n;
+                s_ncc = __popc(act);
+            }
         }
         __syncthreads();
         const int nr = s_nr;
         const size_t sub = (size_t)it.subgrid;
         const double inv_dx = 1.0 / it.dx, inv2 = inv_dx * inv_dx, inv3 = inv2 * inv_dx;
         // stage the sub-slabs (scaled, in units of dx from the leaf's origin)
-        for (int t = threadIdx.x; t < s_rcell[nr]; t += blockDim.x) {
-            int k = 0;
-            while (s_rcell[k + 1] <= t) ++k;
-            const int r = s_rdir[k], idx = t - s_rcell[k];
-            const int4 lo = __ldg(a.t.po_box + (r * 8 + oct) * 2), n = __ldg(a.t.po_box + (r * 8 + oct) * 2 + 1);
-            const int x = lo.x + idx / (n.y * n.z), y = lo.y + (idx / n.z) % n.y, z = lo.z + idx % n.z;
-            const int uc = x * 64 + y * 8 + z;
-            const size_t nb = (size_t)it.nb[r < 13 ? r : r - 1];
-            const double* Ms = a.M + nb * 20 * NCELL + uc;
-            double q[6], o[10], dp[3] = {0.0, 0.0, 0.0}, P[3];
-            const double m0 = __ldg(Ms);
-#pragma unroll
-            for (int k2 = 0; k2 < 6; ++k2) q[k2] = __ldg(Ms + (4 + k2) * NCELL) * ((factor_of(4 + k2) / 2.0) * inv2);
-#pragma unroll
-            for (int k2 = 0; k2 < 10; ++k2) o[k2] = __ldg(Ms + (10 + k2) * NCELL) * ((factor_of(10 + k2) / 6.0) * inv3);
-            if (!RHO) {
-#pragma unroll
-                for (int c = 0; c < 3; ++c) dp[c] = __ldg(Ms + (1 + c) * NCELL) * inv_dx;
-            }
-#pragma unroll
-            for (int c = 0; c < 3; ++c) P[c] = (__ldg(a.com + (nb * 3 + c) * NCELL + uc) - it.xbase[c]) * inv_dx;
-            if (SPLIT) {
-                sf[t] = make_float4((float)q[0], (float)q[1], (float)q[2], (float)q[3]);
-                sf[PO_CELLS + t] = make_float4((float)q[4], (float)q[5], (float)-o[0], (float)-o[1]);
-                sf[2 * PO_CELLS + t] = make_float4((float)-o[2], (float)-o[3], (float)-o[4], (float)-o[5]);
-                sf[3 * PO_CELLS + t] = make_float4((float)-o[6], (float)-o[7], (float)-o[8], (float)-o[9]);
-                sf[4 * PO_CELLS + t] = make_float4((float)m0, (float)-dp[0], (float)-dp[1], (float)-dp[2]);
-                sd[t] = make_double2(P[0], P[1]);
-                sd[PO_CELLS + t] = make_double2(P[2], 0.0);
-                if (RHO) {
-#pragma unroll
-                    for (int k2 = 0; k2 < 5; ++k2) sd[(2 + k2) * PO_CELLS + t] = make_double2(o[2 * k2], o[2 * k2 + 1]);
-                }
-            } else {
-                sd[t] = make_double2(P[0], P[1]);
-                sd[PO_CELLS + t] = make_double2(P[2], m0);
-#pragma unroll
-                for (int k2 = 0; k2 < 3; ++k2) sd[(2 + k2) * PO_CELLS + t] = make_double2(q[2 * k2], q[2 * k2 + 1]);
-#pragma unroll
-                for (int k2 = 0; k2 < 5; ++k2) sd[(5 + k2) * PO_CELLS + t] = make_double2(o[2 * k2], o[2 * k2 + 1]);
-                if (!RHO) {
-                    sd[10 * PO_CELLS + t] = make_double2(dp[0], dp[1]);
-                    sd[11 * PO_CELLS + t] = make_double2(dp[2], 0.0);
-                }
-            }
-        }
+        for (int t = threadIdx.x; t < s_rcell[nr]; t += PO_THREADS)
+            store_slab_cell<SPLIT, RHO>(sf, sd, t, load_slab_cell<RHO>(a, it, oct, s_rdir, s_rcell, t, inv_dx, inv2, inv3));
         __syncthreads();
         for (int j = warp; j < s_ncc; j += PO_THREADS / 32) {
             const int C = s_cc[j];
