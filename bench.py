@@ -369,11 +369,18 @@ def gpu_arm(args) -> None:
     # call writes every result but leaves the leaves' L4..L19 (no kernel writes them)
     L_pin = torch.zeros(solver.L.shape, dtype=torch.float64).pin_memory()
     Lc_pin = torch.zeros(solver.Lc.shape, dtype=torch.float64).pin_memory()
-    # bytes the call uploads: the moments of refined subgrids, the masses of the pool
-    # chunks holding leaves (all of it unless no subgrid is a leaf), every centre of mass
+    # bytes the call uploads from page-locked buffers: the moments of refined
+    # subgrids, the masses of the pool chunks holding leaves (all of it unless no
+    # subgrid is a leaf), the centres of mass of refined subgrids and of leaves
+    # with a refined neighbour, the leaf and centre-of-mass flags, the work list
     n_ref = int((batch.pool.is_leaf == 0).sum())
     mon_bytes = pin["mon"].numel() * 8 if n_ref < batch.pool.n else 0
-    h2d = (n_ref * 20 * 512 * 8 + mon_bytes + sum(pin[k].numel() * pin[k].element_size() for k in ("com", "is_leaf"))
+    needs_com = batch.pool.is_leaf == 0
+    for w in batch.items:
+        nb = w["neighbors"][w["neighbors"] >= 0]
+        if w["kind"] == 2 and (batch.pool.is_leaf[nb] == 0).any():
+            needs_com[w["subgrid"]] = True
+    h2d = (n_ref * 20 * 512 * 8 + mon_bytes + int(needs_com.sum()) * 3 * 512 * 8 + 2 * batch.pool.n
            + items_pin.numel())
     n_leaf = int((batch.pool.is_leaf == 1).sum())
     d2h = L_pin.numel() * 8 - n_leaf * 16 * 512 * 8 + Lc_pin.numel() * 8

@@ -275,10 +275,15 @@ int otfmm_plan_destroy(otfmm_plan* plan);
  * subgrids, which no kernel writes (the reference's monopole kernels output
  * L[0..3] and L_c) and which are left as the caller set them. The pool is uploaded in
  * chunks of consecutive subgrids (the moments of refined subgrids, the masses
- * of chunks with leaves and every centre of mass: what the kernels read); each work item runs once the records it
+ * of chunks with leaves and the centres of mass: what the kernels read); each work item runs once the records it
  * reads have arrived and each output range is copied back once final, on two
  * copy streams, so uploads, kernels and downloads overlap when neighbours have
- * nearby pool indices. Device copies live in the context (grown on demand).
+ * nearby pool indices. When pool_M, pool_com, L and L_c are page-locked host
+ * memory mapped into the device's address space (cudaHostAlloc /
+ * cudaMallocHost, 16-byte aligned) the scattered records move by one SM-copy
+ * launch per chunk instead of one DMA copy per run of subgrids, and only the
+ * centres of mass of refined subgrids and of leaves with a refined neighbour
+ * are uploaded; other buffers take the copy engines. Device copies live in the context (grown on demand).
  * Asynchronous: the outputs are valid once `stream` has completed; a later
  * call waits for the earlier call's uploads. Calls of one context share its
  * device copies: consecutive calls on the same stream run in order, calls on

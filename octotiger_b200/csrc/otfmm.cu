@@ -36,6 +36,7 @@
 #include "../../include/otfmm.h"
 #include "layout.cuh"
 #include "leaf_kernels.cuh"
+#include "host_copies.cuh"
 #include "m2l_tiles.cuh"
 #include "p2m_octant.cuh"
 #include "pair_math.cuh"
@@ -260,6 +261,8 @@ struct otfmm_context {
         int n_sub = 0, n_items = 0;
         double *M = nullptr, *com = nullptr, *mon = nullptr, *L = nullptr, *Lc = nullptr;
         uint8_t* is_leaf = nullptr;
+        uint8_t* needs_com = nullptr;          // [n_sub] the subgrid's centres of mass are read
+        uint8_t* needs_com_pinned = nullptr;
         otfmm_work_item* items = nullptr;
         otfmm_work_item* items_pinned = nullptr;
         cudaStream_t h2d = nullptr, d2h = nullptr;
@@ -827,6 +830,8 @@ int otfmm_destroy(otfmm_context* ctx) {
         cudaFree(hp.L);
         cudaFree(hp.Lc);
         cudaFree(hp.is_leaf);
+        cudaFree(hp.needs_com);
+        cudaFreeHost(hp.needs_com_pinned);
         cudaFree(hp.items);
         cudaFreeHost(hp.items_pinned);
     }
@@ -1356,6 +1361,32 @@ int otfmm_batch_profile(otfmm_context* ctx, const double* pool_M, const double* 
     return OTFMM_OK;
 }
 
+// The device address of host buffer [p, p + bytes) when its first and last
+// bytes are page-locked host memory mapped into the device's address space at
+// one offset (a cudaHostAlloc / cudaMallocHost / mapped cudaHostRegister
+// buffer) and it starts on a 16-byte boundary; nullptr otherwise (pageable
+// memory, for one: the SM copies are then not used).
+const void* mapped_host(const void* p, size_t bytes) {
+    if (!p || bytes == 0 || (reinterpret_cast<uintptr_t>(p) & 15u)) return nullptr;
+    cudaPointerAttributes a0, a1;
+    if (cudaPointerGetAttributes(&a0, p) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    const void* q = static_cast<const char*>(p) + bytes - 1;
+    if (cudaPointerGetAttributes(&a1, q) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    if (a0.type != cudaMemoryTypeHost || a1.type != cudaMemoryTypeHost || !a0.devicePointer || !a1.devicePointer)
+        return nullptr;
+    if (static_cast<const char*>(a1.devicePointer) - static_cast<const char*>(a0.devicePointer) !=
+        static_cast<ptrdiff_t>(bytes - 1))
+        return nullptr;
+    if (reinterpret_cast<uintptr_t>(a0.devicePointer) & 15u) return nullptr;
+    return a0.devicePointer;
+}
+
 int otfmm_batch_host(otfmm_context* ctx, const double* pool_M, const double* pool_com, const double* pool_mon,
                      const uint8_t* pool_is_leaf, int32_t n_subgrids, const otfmm_work_item* items, int32_t n_items,
                      double* L, double* L_c, int gsolve_type, int precision, void* stream) {
@@ -1397,8 +1428,10 @@ int otfmm_batch_host(otfmm_context* ctx, const double* pool_M, const double* poo
         cudaFree(hp.L);
         cudaFree(hp.Lc);
         cudaFree(hp.is_leaf);
+        cudaFree(hp.needs_com);
+        cudaFreeHost(hp.needs_com_pinned);
         hp.M = hp.com = hp.mon = hp.L = hp.Lc = nullptr;
-        hp.is_leaf = nullptr;
+        hp.is_leaf = hp.needs_com = hp.needs_com_pinned = nullptr;
         hp.n_sub = 0;
         const size_t n = (size_t)n_subgrids;
         OT_CUDA(cudaMalloc(&hp.M, sizeof(double) * 20 * NCELL * n));
@@ -1407,6 +1440,8 @@ int otfmm_batch_host(otfmm_context* ctx, const double* pool_M, const double* poo
         OT_CUDA(cudaMalloc(&hp.L, sizeof(double) * 20 * NCELL * n));
         OT_CUDA(cudaMalloc(&hp.Lc, sizeof(double) * 3 * NCELL * n));
         OT_CUDA(cudaMalloc(&hp.is_leaf, n));
+        OT_CUDA(cudaMalloc(&hp.needs_com, n));
+        OT_CUDA(cudaMallocHost(&hp.needs_com_pinned, n));
         hp.n_sub = n_subgrids;
     }
     if (n_items > hp.n_items) {
@@ -1453,10 +1488,33 @@ int otfmm_batch_host(otfmm_context* ctx, const double* pool_M, const double* poo
     }
     for (int k = 1; k < K; ++k) need[k] = std::max(need[k], need[k - 1]);   // copy out in pool order
     const size_t cell = NCELL * sizeof(double);
+    // page-locked, mapped host buffers: the scattered records (moments of the
+    // refined subgrids, outputs) move by one SM-copy launch per chunk on the
+    // copy streams instead of one DMA copy per run of subgrids
+    const size_t nsub = (size_t)n_subgrids;
+    const double* M_dev = static_cast<const double*>(mapped_host(pool_M, 20 * cell * nsub));
+    const double* com_dev = static_cast<const double*>(mapped_host(pool_com, 3 * cell * nsub));
+    double* L_dev = static_cast<double*>(const_cast<void*>(mapped_host(L, 20 * cell * nsub)));
+    double* Lc_dev = static_cast<double*>(const_cast<void*>(mapped_host(L_c, 3 * cell * nsub)));
+    const bool sm_in = (M_dev != nullptr && com_dev != nullptr), sm_out = (L_dev != nullptr && Lc_dev != nullptr);
+    if (sm_in) {
+        // the centres of mass the kernels read: those of refined subgrids and of
+        // leaves with a refined neighbour (P2M targets); a leaf enters every
+        // other interaction as masses at its cell centres
+        for (size_t i = 0; i < nsub; ++i) hp.needs_com_pinned[i] = pool_is_leaf[i] ? 0 : 1;
+        for (int i = 0; i < n_items; ++i) {
+            const otfmm_work_item& w = items[i];
+            if (w.kind != OTFMM_KIND_LEAF) continue;
+            for (int d = 0; d < 26; ++d)
+                if (w.neighbors[d] >= 0 && !pool_is_leaf[w.neighbors[d]]) hp.needs_com_pinned[w.subgrid] = 1;
+        }
+    }
     OT_CUDA(cudaEventRecord(ev_start, s));
     OT_CUDA(cudaStreamWaitEvent(hp.h2d, ev_start, 0));
     OT_CUDA(cudaStreamWaitEvent(hp.d2h, ev_start, 0));
     OT_CUDA(cudaMemcpyAsync(hp.is_leaf, pool_is_leaf, (size_t)n_subgrids, cudaMemcpyHostToDevice, hp.h2d));
+    if (sm_in)
+        OT_CUDA(cudaMemcpyAsync(hp.needs_com, hp.needs_com_pinned, nsub, cudaMemcpyHostToDevice, hp.h2d));
     OT_CUDA(cudaMemcpyAsync(hp.items, hp.items_pinned, sizeof(otfmm_work_item) * (size_t)n_items,
                             cudaMemcpyHostToDevice, hp.h2d));
     for (int k = 0; k < K; ++k) {
@@ -1465,22 +1523,28 @@ int otfmm_batch_host(otfmm_context* ctx, const double* pool_M, const double* poo
         // of a chunk with leaves (one copy): the kernels read nothing else (a leaf
         // enters as masses at its cell centres, a refined subgrid as moments)
         bool any_leaf = false;
-        for (size_t i = a; i < a + n;) {
-            if (pool_is_leaf[i]) {
-                any_leaf = true;
-                ++i;
-                continue;
+        for (size_t i = a; i < a + n; ++i) any_leaf |= pool_is_leaf[i] != 0;
+        if (sm_in) {
+            gather_pool_kernel<<<(unsigned)n, HC_THREADS, 0, hp.h2d>>>(M_dev, com_dev, hp.M, hp.com, hp.is_leaf,
+                                                                       hp.needs_com, (int)a);
+        } else {
+            for (size_t i = a; i < a + n;) {
+                if (pool_is_leaf[i]) {
+                    ++i;
+                    continue;
+                }
+                size_t j = i + 1;
+                while (j < a + n && !pool_is_leaf[j]) ++j;
+                OT_CUDA(cudaMemcpyAsync(hp.M + i * 20 * NCELL, pool_M + i * 20 * NCELL, (j - i) * 20 * cell,
+                                        cudaMemcpyHostToDevice, hp.h2d));
+                i = j;
             }
-            size_t j = i + 1;
-            while (j < a + n && !pool_is_leaf[j]) ++j;
-            OT_CUDA(cudaMemcpyAsync(hp.M + i * 20 * NCELL, pool_M + i * 20 * NCELL, (j - i) * 20 * cell,
-                                    cudaMemcpyHostToDevice, hp.h2d));
-            i = j;
         }
         if (any_leaf)
             OT_CUDA(cudaMemcpyAsync(hp.mon + a * NCELL, pool_mon + a * NCELL, n * cell, cudaMemcpyHostToDevice, hp.h2d));
-        OT_CUDA(cudaMemcpyAsync(hp.com + a * 3 * NCELL, pool_com + a * 3 * NCELL, n * 3 * cell,
-                                cudaMemcpyHostToDevice, hp.h2d));
+        if (!sm_in)
+            OT_CUDA(cudaMemcpyAsync(hp.com + a * 3 * NCELL, pool_com + a * 3 * NCELL, n * 3 * cell,
+                                    cudaMemcpyHostToDevice, hp.h2d));
         OT_CUDA(cudaEventRecord(ev_h2d[k], hp.h2d));
     }
     OT_CUDA(cudaEventRecord(ev_items, hp.h2d));
@@ -1504,6 +1568,12 @@ int otfmm_batch_host(otfmm_context* ctx, const double* pool_M, const double* poo
         const size_t a = bnd[k], n = bnd[k + 1] - bnd[k];
         // L of refined subgrids whole; of leaves the monopole kernels' L0..L3
         // (their L4..L19 stay as the caller set them), runs of consecutive ones
+        if (sm_out) {
+            scatter_outputs_kernel<<<(unsigned)n, HC_THREADS, 0, hp.d2h>>>(hp.L, hp.Lc, L_dev, Lc_dev, hp.is_leaf,
+                                                                           (int)a);
+            OT_CUDA(cudaEventRecord(ev_d2h[k], hp.d2h));
+            continue;
+        }
         for (size_t i = a; i < a + n;) {
             const uint8_t leaf = pool_is_leaf[i];
             size_t j = i + 1;
@@ -1522,6 +1592,7 @@ int otfmm_batch_host(otfmm_context* ctx, const double* pool_M, const double* poo
     }
     OT_CUDA(cudaEventRecord(ev_done, hp.d2h));
     OT_CUDA(cudaStreamWaitEvent(s, ev_done, 0));
+    OT_CUDA(cudaGetLastError());
     return OTFMM_OK;
 }
 

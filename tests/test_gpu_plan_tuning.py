@@ -195,11 +195,14 @@ def test_batch_profile_times_each_kernel_and_matches_batch(ctx):
 
 
 @pytest.mark.parametrize("precision", ["fp64_exact", "fp32_split"])
-@pytest.mark.parametrize("pinned", [False, True])
+@pytest.mark.parametrize("pinned", [False, True, "inputs"])
 def test_batch_host_matches_device_batch(ctx, precision, pinned):
     """otfmm_batch_host (chunked uploads, kernels and downloads) gives the
     device batch's results, zeros where the solve writes nothing, and leaves
-    L[4..19] of leaf subgrids (no kernel writes them) as the caller set them."""
+    L[4..19] of leaf subgrids (no kernel writes them) as the caller set them:
+    with pageable buffers (copy engines), page-locked ones (the SMs move the
+    moments in and the outputs out) and page-locked inputs with pageable
+    outputs."""
     import torch
     from octotiger_b200.otfmm import BatchSolver, order_work_list
     b = amr_small()
@@ -208,14 +211,17 @@ def test_batch_host_matches_device_batch(ctx, precision, pinned):
     L0, Lc0 = s.results()
     n = b.pool.n
     items = order_work_list(b.items)
-    if pinned:
+    if pinned:   # True or "inputs"
         arrs = {k: torch.from_numpy(getattr(b.pool, k)).pin_memory() for k in ("M", "com", "mon", "is_leaf")}
         it = torch.from_numpy(items.view(np.uint8).reshape(-1).copy()).pin_memory()
-        L = torch.full((n, 20, 512), np.nan, dtype=torch.float64).pin_memory()
-        Lc = torch.full((n, 3, 512), np.nan, dtype=torch.float64).pin_memory()
     else:
         arrs = {k: np.ascontiguousarray(getattr(b.pool, k)) for k in ("M", "com", "mon", "is_leaf")}
         it = items
+    pinned = pinned is True
+    if pinned:
+        L = torch.full((n, 20, 512), np.nan, dtype=torch.float64).pin_memory()
+        Lc = torch.full((n, 3, 512), np.nan, dtype=torch.float64).pin_memory()
+    else:
         L = np.full((n, 20, 512), np.nan)
         Lc = np.full((n, 3, 512), np.nan)
     for _ in range(2):   # the second call reuses the context's buffers
