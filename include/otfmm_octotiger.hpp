@@ -439,6 +439,16 @@ struct AggregatedCall {
     std::vector<double> L, Lc;
 };
 
+// Rows c = 0..K-1 (row stride NCELL) of a pool record from the cells' AoS
+// values src[u][c], 8 cells at a time, so that every block writes whole cache
+// lines of each row (about twice as fast as a cell-by-cell transpose).
+template <int K, class AoS>
+inline void aos_to_soa(double* dst, const AoS& src) {
+    for (int u0 = 0; u0 < NCELL; u0 += 8)
+        for (int c = 0; c < K; ++c)
+            for (int u = u0; u < u0 + 8; ++u) dst[c * NCELL + u] = src[u][c];
+}
+
 // Reserves, fills and submits one call: own record (M + com for a refined node,
 // masses + com for a leaf) and the 26 neighbour payloads.
 template <class Multipole, class SpaceVector, class Neighbor, class GridPtr>
@@ -490,25 +500,17 @@ int aggregated_submit(otfmm_aggregator* agg, int kind, const std::vector<Multipo
         rc = otfmm_aggregator_record(agg, ticket, slots[i], &M, &com, &mon);
         if (rc != OTFMM_OK) break;
         if (i == 0) {
-            for (int u = 0; u < NCELL; ++u) {
-                if (fill[0] & OTFMM_AGG_M)
-                    for (int c = 0; c < 20; ++c) M[c * NCELL + u] = (*own_M)[u][c];
-                if (fill[0] & OTFMM_AGG_COM)
-                    for (int c = 0; c < 3; ++c) com[c * NCELL + u] = own_com[u][c];
-                if (fill[0] & OTFMM_AGG_MON) mon[u] = (*own_mon)[u];
-            }
+            if (fill[0] & OTFMM_AGG_M) aos_to_soa<20>(M, *own_M);
+            if (fill[0] & OTFMM_AGG_COM) aos_to_soa<3>(com, own_com);
+            if (fill[0] & OTFMM_AGG_MON) std::copy(own_mon->begin(), own_mon->begin() + NCELL, mon);
             continue;
         }
         const int d = dir_of[i];
         const Neighbor& nb = neighbors[d];
         if (keys[i] != 0) {   // full-size payload
-            for (int u = 0; u < NCELL; ++u) {
-                if (fill[i] & OTFMM_AGG_MON) mon[u] = (*nb.data.m)[u];
-                if (fill[i] & OTFMM_AGG_M)
-                    for (int c = 0; c < 20; ++c) M[c * NCELL + u] = (*nb.data.M)[u][c];
-                if (fill[i] & OTFMM_AGG_COM)
-                    for (int c = 0; c < 3; ++c) com[c * NCELL + u] = (*nb.data.x)[u][c];
-            }
+            if (fill[i] & OTFMM_AGG_MON) std::copy(nb.data.m->begin(), nb.data.m->begin() + NCELL, mon);
+            if (fill[i] & OTFMM_AGG_M) aos_to_soa<20>(M, *nb.data.M);
+            if (fill[i] & OTFMM_AGG_COM) aos_to_soa<3>(com, *nb.data.x);
             continue;
         }
         // compressed payload (get_ilist_n_bnd order): zeros, then the listed cells
@@ -556,12 +558,14 @@ int finish(AggregatedCall<GridPtr>& call) {
     call.agg = nullptr;
     if (rc != OTFMM_OK) return rc;
     auto& gL = call.grid->get_L();
-    for (int c = 0; c < call.ncomp; ++c)
-        for (int u = 0; u < NCELL; ++u) gL[u][c] += call.L[c * NCELL + u];
+    for (int u0 = 0; u0 < NCELL; u0 += 8)
+        for (int c = 0; c < call.ncomp; ++c)
+            for (int u = u0; u < u0 + 8; ++u) gL[u][c] += call.L[c * NCELL + u];
     if (call.write_lc) {
         auto& gLc = call.grid->get_L_c();
-        for (int c = 0; c < 3; ++c)
-            for (int u = 0; u < NCELL; ++u) gLc[u][c] = call.Lc[c * NCELL + u];
+        for (int u0 = 0; u0 < NCELL; u0 += 8)
+            for (int c = 0; c < 3; ++c)
+                for (int u = u0; u < u0 + 8; ++u) gLc[u][c] = call.Lc[c * NCELL + u];
     }
     return OTFMM_OK;
 }
