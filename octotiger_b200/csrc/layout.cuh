@@ -118,6 +118,7 @@ struct Tables {
     const int16_t* pc_slot;     // [27][64]: slot of coarse cell C among direction r's units, -1 if none
     const int* pc_parts;        // [27]: parts each unit's partner lists of direction r are cut in
     const float4* r2_four_f;    // r2_four rounded to FP32 (the split P2P of theta < 0.5)
+    const int* r2_p2p_delta;    // [8][MAX_ENTRIES_R2]: offset of each entries_r2 partner in the reach-2 P2P halo
     // P2M by octant (reach 1)
     const int4* po_box;         // [27][8][2]: sub-slab of direction r for octant o: (low x, y, z, cells), (extents)
     const int2* po_range;       // [27][64]: partner range in po_list of coarse cell C in direction r

@@ -223,6 +223,7 @@ struct otfmm_context {
     int* d_r2_sx_start = nullptr;
     double4* d_r2_four = nullptr;
     float4* d_r2_four_f = nullptr;
+    int* d_r2_p2p_delta = nullptr;
     int p2m_groups_max = 0;   // cells with partners summed over the 26 directions
     double4* d_p2p_four = nullptr;
     double4* d_p2p_box = nullptr;    // [8][216] per-parity box constants
@@ -276,7 +277,7 @@ struct otfmm_context {
                       d_entries_ws, d_four,  d_phase,        d_p2m_start,     d_p2m_list,    d_p2m_perm_start,
                       d_p2m_perm,   d_p2m_slot,     d_p2p_four,      d_entries_r2,  d_r2_sx_start, d_r2_four,
                       d_p2p_box,    d_p2p_cube,     d_pc_unit_start, d_pc_coarse,  d_pc_range,    d_pc_list,
-                      d_pc_slot,    d_pc_parts,     d_r2_four_f,     d_po_box,     d_po_range,    d_po_list}; }
+                      d_pc_slot,    d_pc_parts,     d_r2_four_f,     d_r2_p2p_delta, d_po_box,   d_po_range,    d_po_list}; }
 };
 
 namespace {
@@ -670,7 +671,20 @@ int otfmm_create(int device, double theta, otfmm_context** out) {
     std::vector<float4> r2_four_f(r2_four.size());
     for (size_t q = 0; q < r2_four.size(); ++q)
         r2_four_f[q] = float4{(float)r2_four[q].x, (float)r2_four[q].y, (float)r2_four[q].z, (float)r2_four[q].w};
-    if ((e = cudaMalloc(&ctx->d_r2_four_f, sizeof(float4) * r2_four_f.size())) != cudaSuccess ||
+    // position of every long-list partner in the parity-split FP32 halo of the
+    // reach-2 split P2P, relative to the lane's own sub-lattice position
+    std::vector<int> r2_p2p_delta(8 * (size_t)MAX_ENTRIES_R2, 0);
+    for (int p = 0; p < 8; ++p)
+        for (int e2 = 0; e2 < ctx->counts[p]; ++e2) {
+            const int y = entries_r2[p * (size_t)MAX_ENTRIES_R2 + e2].y;
+            r2_p2p_delta[p * (size_t)MAX_ENTRIES_R2 + e2] =
+                r2f_index(((p >> 2) & 1) + (y & 15) - 8 + R2_PAD, ((p >> 1) & 1) + ((y >> 4) & 15) - 8 + R2_PAD,
+                          (p & 1) + ((y >> 8) & 15) - 8 + R2_PAD);
+        }
+    if ((e = cudaMalloc(&ctx->d_r2_p2p_delta, sizeof(int) * r2_p2p_delta.size())) != cudaSuccess ||
+        (e = cudaMemcpy(ctx->d_r2_p2p_delta, r2_p2p_delta.data(), sizeof(int) * r2_p2p_delta.size(),
+                        cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMalloc(&ctx->d_r2_four_f, sizeof(float4) * r2_four_f.size())) != cudaSuccess ||
         (e = cudaMemcpy(ctx->d_r2_four_f, r2_four_f.data(), sizeof(float4) * r2_four_f.size(),
                         cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMalloc(&ctx->d_r2_four, sizeof(double4) * r2_four.size())) != cudaSuccess ||
@@ -815,6 +829,7 @@ int otfmm_destroy(otfmm_context* ctx) {
     cudaFree(ctx->d_r2_sx_start);
     cudaFree(ctx->d_r2_four);
     cudaFree(ctx->d_r2_four_f);
+    cudaFree(ctx->d_r2_p2p_delta);
     {
         auto& hp = ctx->hp;
         if (hp.ready) {
@@ -1130,7 +1145,7 @@ int enqueue_batch(otfmm_context* ctx, const double* pool_M, const double* pool_c
             else m2l_r2_kernel<PREC_FAST, false><<<4 * sms, THREADS, rbytes, s>>>(a);
             mark(2);
             if (precision == OTFMM_FP32_SPLIT)
-                p2p_r2_split_kernel<<<leaf_grid, 256, R2_SMEM_BYTES / 2, s>>>(a);
+                p2p_r2_split_kernel<<<leaf_grid, 256, R2F_SMEM_BYTES, s>>>(a);
             else
                 p2p_r2_kernel<PREC_FAST><<<leaf_grid, 256, R2_SMEM_BYTES, s>>>(a);
             mark(3);

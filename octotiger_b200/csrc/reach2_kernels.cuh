@@ -426,6 +426,30 @@ __global__ void __launch_bounds__(256) p2p_r2_kernel(BatchArgs a) {
 // (partner, cell) as two packed FMAs; the FP32 sums are promoted to FP64 every
 // R2_SPLIT_CHUNK partners.
 constexpr int R2_SPLIT_CHUNK = 32;
+// Its FP32 halo is split by parity into 9^3 sub-lattices (rows of 12, planes
+// of 112 floats): the 32 lanes of a warp (one parity class, cells two apart)
+// then read 32 distinct banks (the unsplit layout gave up to 4-way conflicts).
+constexpr int R2F_RS = 12, R2F_XS = 112, R2F_CLS = 9 * R2F_XS;
+constexpr int R2F_SMEM_BYTES = 8 * R2F_CLS * 4;   // 32,256
+// Position of halo cell (rx, ry, rz) = absolute coordinates + R2_PAD, each in [0, 17].
+__host__ __device__ constexpr int r2f_index(int rx, int ry, int rz) {
+    return (((rx & 1) << 2) | ((ry & 1) << 1) | (rz & 1)) * R2F_CLS + (rx >> 1) * R2F_XS + (ry >> 1) * R2F_RS +
+           (rz >> 1);
+}
+constexpr bool r2f_conflict_free() {
+    bool seen[32] = {};
+    for (int i = 0; i < 2; ++i)
+        for (int j = 0; j < 4; ++j)
+            for (int k = 0; k < 4; ++k) {
+                const int b = (i * R2F_XS + j * R2F_RS + k) % 32;
+                if (seen[b]) return false;
+                seen[b] = true;
+            }
+    return true;
+}
+static_assert(r2f_conflict_free(), "a warp's 32 cells fall in 32 distinct banks");
+static_assert(8 * R2F_XS + 8 * R2F_RS + 8 < R2F_CLS, "sub-lattice planes hold 9 x 9 x 9 cells");
+
 __global__ void __launch_bounds__(256) p2p_r2_split_kernel(BatchArgs a) {
     extern __shared__ float pmf[];
     __shared__ ItemInfo it;
@@ -433,11 +457,11 @@ __global__ void __launch_bounds__(256) p2p_r2_split_kernel(BatchArgs a) {
     const int i = lane >> 4, j = (lane >> 2) & 3, k = lane & 3;
     const int cy = ((p >> 1) & 1) + 2 * j, cz = (p & 1) + 2 * k;
     const int cxa = ((p >> 2) & 1) + 2 * i, cxb = cxa + 4;
-    const int own_a = (cxa + R2_PAD) * R2_PLANE + (cy + R2_PAD) * R2_ROW + (cz + R2_PAD);
-    constexpr int OFF_B = 4 * R2_PLANE;
+    const int own_a = i * R2F_XS + j * R2F_RS + k;   // plus the entry's delta: the partner of cell cxa
+    constexpr int OFF_B = 2 * R2F_XS;                // cell cxb = cxa + 4
     const int n = a.t.count[p];
-    const int2* ent = a.t.entries_r2 + p * MAX_ENTRIES_R2;
     const float4* four = a.t.r2_four_f + p * MAX_ENTRIES_R2;
+    const int* delta = a.t.r2_p2p_delta + p * MAX_ENTRIES_R2;
     const int nleaf = a.wl.counts[WL_LEAF];
     for (int kk = blockIdx.x; kk < nleaf; kk += gridDim.x) {
         __syncthreads();   // `it` and the halo are reused
@@ -451,7 +475,7 @@ __global__ void __launch_bounds__(256) p2p_r2_split_kernel(BatchArgs a) {
             double m = 0.0;
             if (raw == 13 || ((it.leafmask >> raw) & 1u))
                 m = a.mon[(size_t)src * NCELL + (ax & 7) * 64 + (ay & 7) * 8 + (az & 7)];
-            pmf[(ax + R2_PAD) * R2_PLANE + (ay + R2_PAD) * R2_ROW + (az + R2_PAD)] = (float)(m * dc0);
+            pmf[r2f_index(ax + R2_PAD, ay + R2_PAD, az + R2_PAD)] = (float)(m * dc0);
         }
         __syncthreads();
         double ga[4] = {0.0, 0.0, 0.0, 0.0}, gb[4] = {0.0, 0.0, 0.0, 0.0};
@@ -460,9 +484,8 @@ __global__ void __launch_bounds__(256) p2p_r2_split_kernel(BatchArgs a) {
             const int e1 = min(e0 + R2_SPLIT_CHUNK, n);
 #pragma unroll 4
             for (int e = e0; e < e1; ++e) {
-                const int y = __ldg(&ent[e].y);
                 const float4 f = __ldg(four + e);
-                const int d = own_a + entry_sx(y) * R2_PLANE + entry_sy(y) * R2_ROW + entry_sz(y);
+                const int d = own_a + __ldg(delta + e);
                 const float ma = pmf[d], mb = pmf[d + OFF_B];
                 a01 = __ffma2_rn(make_float2(f.x, f.y), make_float2(ma, ma), a01);
                 a23 = __ffma2_rn(make_float2(f.z, f.w), make_float2(ma, ma), a23);
