@@ -123,6 +123,8 @@ struct Tables {
     const int4* po_box;         // [27][8][2]: sub-slab of direction r for octant o: (low x, y, z, cells), (extents)
     const int2* po_range;       // [27][64]: partner range in po_list of coarse cell C in direction r
     const uint16_t* po_list;    // partner cells as indices into the sub-slab of (r, octant of C)
+    const int2* entries_r2s;    // entries_r2 with each sx group's full-multipole entries first
+    const int* r2s_far_end;     // [8][11]: end of each sx group's full-multipole entries in entries_r2s
 };
 
 __device__ __forceinline__ int entry_sx(int y) { return (y & 15) - 8; }

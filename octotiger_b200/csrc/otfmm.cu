@@ -221,6 +221,8 @@ struct otfmm_context {
     int16_t* d_p2m_slot = nullptr;
     int2* d_entries_r2 = nullptr;   // stencil-order entries, MAX_ENTRIES_R2 per class (any reach)
     int* d_r2_sx_start = nullptr;
+    int2* d_entries_r2s = nullptr;     // entries_r2 with each sx group's far entries first
+    int* d_r2s_far_end = nullptr;      // [8][11]: end of each sx group's far entries
     double4* d_r2_four = nullptr;
     float4* d_r2_four_f = nullptr;
     int* d_r2_p2p_delta = nullptr;
@@ -277,7 +279,8 @@ struct otfmm_context {
                       d_entries_ws, d_four,  d_phase,        d_p2m_start,     d_p2m_list,    d_p2m_perm_start,
                       d_p2m_perm,   d_p2m_slot,     d_p2p_four,      d_entries_r2,  d_r2_sx_start, d_r2_four,
                       d_p2p_box,    d_p2p_cube,     d_pc_unit_start, d_pc_coarse,  d_pc_range,    d_pc_list,
-                      d_pc_slot,    d_pc_parts,     d_r2_four_f,     d_r2_p2p_delta, d_po_box,   d_po_range,    d_po_list}; }
+                      d_pc_slot,    d_pc_parts,     d_r2_four_f,     d_r2_p2p_delta, d_po_box,   d_po_range,    d_po_list,
+                      d_entries_r2s, d_r2s_far_end}; }
 };
 
 namespace {
@@ -444,6 +447,24 @@ int otfmm_create(int device, double theta, otfmm_context** out) {
         }
         while (sx_prev < SMAX + 1) r2_sx_start[p * 12 + (++sx_prev) + SMAX] = ctx->counts[p];
     }
+    // the same lists with each sx group's full-multipole (far) entries first, for
+    // the split tiles of theta < 0.5 (their far pairs run three at a time), and
+    // where each group's far entries end
+    std::vector<int2> entries_r2s(entries_r2.size(), int2{0, 0});
+    std::vector<int> r2s_far_end(8 * 11, 0);
+    for (int p = 0; p < 8; ++p)
+        for (int g = 0; g < 11; ++g) {
+            const int b = r2_sx_start[p * 12 + g], en_end = r2_sx_start[p * 12 + g + 1];
+            int k = b;
+            for (int pass = 0; pass < 2; ++pass)
+                for (int e = b; e < en_end; ++e) {
+                    const int2 en = entries_r2[p * (size_t)MAX_ENTRIES_R2 + e];
+                    const bool far = (((en.y >> 12) & 3) & F_FAR) != 0;
+                    if (far == (pass == 0)) entries_r2s[p * (size_t)MAX_ENTRIES_R2 + k++] = en;
+                    if (pass == 0 && e + 1 == en_end) r2s_far_end[p * 11 + g] = k;
+                }
+            if (b == en_end) r2s_far_end[p * 11 + g] = b;
+        }
     if (reach <= 1) {
         build_entries(ctx->st, theta, MAX_ENTRIES, entries, ctx->counts, reach);
     } else {
@@ -690,6 +711,12 @@ int otfmm_create(int device, double theta, otfmm_context** out) {
         (e = cudaMalloc(&ctx->d_r2_four, sizeof(double4) * r2_four.size())) != cudaSuccess ||
         (e = cudaMemcpy(ctx->d_r2_four, r2_four.data(), sizeof(double4) * r2_four.size(),
                         cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMalloc(&ctx->d_entries_r2s, sizeof(int2) * entries_r2s.size())) != cudaSuccess ||
+        (e = cudaMemcpy(ctx->d_entries_r2s, entries_r2s.data(), sizeof(int2) * entries_r2s.size(),
+                        cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMalloc(&ctx->d_r2s_far_end, sizeof(int) * r2s_far_end.size())) != cudaSuccess ||
+        (e = cudaMemcpy(ctx->d_r2s_far_end, r2s_far_end.data(), sizeof(int) * r2s_far_end.size(),
+                        cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMalloc(&ctx->d_r2_sx_start, sizeof(int) * r2_sx_start.size())) != cudaSuccess ||
         (e = cudaMemcpy(ctx->d_r2_sx_start, r2_sx_start.data(), sizeof(int) * r2_sx_start.size(),
                         cudaMemcpyHostToDevice)) != cudaSuccess ||
@@ -827,6 +854,8 @@ int otfmm_destroy(otfmm_context* ctx) {
     cudaFree(ctx->d_p2m_slot);
     cudaFree(ctx->d_entries_r2);
     cudaFree(ctx->d_r2_sx_start);
+    cudaFree(ctx->d_entries_r2s);
+    cudaFree(ctx->d_r2s_far_end);
     cudaFree(ctx->d_r2_four);
     cudaFree(ctx->d_r2_four_f);
     cudaFree(ctx->d_r2_p2p_delta);

@@ -231,8 +231,9 @@ __global__ void __launch_bounds__(THREADS, 1) m2l_r2_split_kernel(BatchArgs a) {
             accf[q] = 0.0f;
         }
         int in_chunk = 0;
-        const int2* ent = a.t.entries_r2 + c.p * MAX_ENTRIES_R2;
+        const int2* ent = a.t.entries_r2s + c.p * MAX_ENTRIES_R2;
         const int* sxs = a.t.r2_sx_start + c.p * 12;
+        const int* fend = a.t.r2s_far_end + c.p * 11;
         for (int plane = x0 - 4; plane <= x0 + 7; ++plane) {
             __syncthreads();   // the previous plane is consumed
             {
@@ -287,14 +288,42 @@ __global__ void __launch_bounds__(THREADS, 1) m2l_r2_split_kernel(BatchArgs a) {
             __syncthreads();
             const int sx = plane - c.cx;
             if (sx < -SMAX || sx > SMAX) continue;
-            const int e1 = sxs[sx + SMAX + 1];
+            // the plane's full-multipole partners three at a time (the L_c chains of
+            // consecutive pairs interleave in La / Lb), then the monopole-only ones;
+            // FP32 sums promoted to FP64 every 15 pairs
+            const int eb = sxs[sx + SMAX], ef = fend[sx + SMAX], e1 = sxs[sx + SMAX + 1];
+            int e = eb;
 #pragma unroll 1
-            for (int e = sxs[sx + SMAX]; e < e1; ++e) {
+            for (; e + 2 < ef; e += 3) {
+                const int2 na = __ldg(ent + e), nb = __ldg(ent + e + 1), nc = __ldg(ent + e + 2);
+                const int ca = na.x / PL_CLS, la = na.x - ca * PL_CLS + lane_off;
+                const int cb = nb.x / PL_CLS, lb = nb.x - cb * PL_CLS + lane_off;
+                const int cc = nc.x / PL_CLS, lc = nc.x - cc * PL_CLS + lane_off;
+                fz_far_pair<R2S_COMP>(sb + ca * R2S_D_CLS + la, sf + ca * R2S_F_CLS + la, Pc0, Pc1, Pc2, accf, &ext,
+                                      z.La, z);
+                fz_far_pair<R2S_COMP>(sb + cb * R2S_D_CLS + lb, sf + cb * R2S_F_CLS + lb, Pc0, Pc1, Pc2, accf, &ext,
+                                      z.Lb, z);
+                fz_far_pair<R2S_COMP>(sb + cc * R2S_D_CLS + lc, sf + cc * R2S_F_CLS + lc, Pc0, Pc1, Pc2, accf, &ext,
+                                      z.La, z);
+                in_chunk += 3;
+                if (in_chunk >= 15) {
+                    in_chunk = 0;
+                    accf[0] += ext;
+                    ext = 0.0f;
+#pragma unroll
+                    for (int q = 0; q < 20; ++q) {
+                        acc[q] += (double)accf[q];
+                        accf[q] = 0.0f;
+                    }
+                }
+            }
+#pragma unroll 1
+            for (; e < e1; ++e) {
                 const int2 en = __ldg(ent + e);
                 // en.x addresses the FP64 plane layout of m2l_r2_kernel: class and cell
                 const int cls = en.x / PL_CLS, cell = en.x - cls * PL_CLS + lane_off;
                 const double2* pb = sb + cls * R2S_D_CLS + cell;
-                if (entry_flags(en.y) & F_FAR) {
+                if (e < ef) {
                     fz_far_pair<R2S_COMP>(pb, sf + cls * R2S_F_CLS + cell, Pc0, Pc1, Pc2, accf, &ext, z.La, z);
                 } else {
                     // monopole-only offsets: only leaf partners carry mass
@@ -302,7 +331,7 @@ __global__ void __launch_bounds__(THREADS, 1) m2l_r2_split_kernel(BatchArgs a) {
                     if (!((monomask >> raw_dir(plane, ay, az)) & 1u)) continue;
                     fz_mass_pair(pb, R2S_COMP, Pc0, Pc1, Pc2, accf, z);
                 }
-                if (++in_chunk == 16) {
+                if (++in_chunk >= 15) {
                     in_chunk = 0;
                     accf[0] += ext;
                     ext = 0.0f;
