@@ -1160,26 +1160,38 @@ int enqueue_batch(otfmm_context* ctx, const double* pool_M, const double* pool_c
         // and the fast FP64 form for the d(rho)/dt tiles and P2M
         const size_t rbytes = PL_SMEM_BYTES;
         const dim3 leaf_grid(std::min(n_items, 8 * sms));
+        // leaf kernels beside the tiles (outside profiling), as at theta >= 0.5
+        const bool fork = (marks == nullptr);
+        cudaStream_t ls = s;
+        if (fork) {
+            OT_CUDA(cudaEventRecord(ctx->ev_fork, s));
+            OT_CUDA(cudaStreamWaitEvent(ctx->aux, ctx->ev_fork, 0));
+            ls = ctx->aux;
+        }
         if (precision == OTFMM_FP64_EXACT) {
             if (rho) m2l_r2_kernel<PREC_EXACT, true><<<4 * sms, THREADS, rbytes, s>>>(a);
             else m2l_r2_kernel<PREC_EXACT, false><<<4 * sms, THREADS, rbytes, s>>>(a);
             mark(2);
-            p2p_r2_kernel<PREC_EXACT><<<leaf_grid, 256, R2_SMEM_BYTES, s>>>(a);
+            p2p_r2_kernel<PREC_EXACT><<<leaf_grid, 256, R2_SMEM_BYTES, ls>>>(a);
             mark(3);
-            if (rho) p2m_batch_kernel<PREC_EXACT, true><<<p2m_grid, P_THREADS, 0, s>>>(a);
-            else p2m_batch_kernel<PREC_EXACT, false><<<p2m_grid, P_THREADS, 0, s>>>(a);
+            if (rho) p2m_batch_kernel<PREC_EXACT, true><<<p2m_grid, P_THREADS, 0, ls>>>(a);
+            else p2m_batch_kernel<PREC_EXACT, false><<<p2m_grid, P_THREADS, 0, ls>>>(a);
         } else {
             if (rho && precision == OTFMM_FP32_SPLIT) m2l_r2_split_kernel<<<sms, THREADS, R2S_SMEM_ALLOC, s>>>(a);
             else if (rho) m2l_r2_kernel<PREC_FAST, true><<<4 * sms, THREADS, rbytes, s>>>(a);
             else m2l_r2_kernel<PREC_FAST, false><<<4 * sms, THREADS, rbytes, s>>>(a);
             mark(2);
             if (precision == OTFMM_FP32_SPLIT)
-                p2p_r2_split_kernel<<<leaf_grid, 256, R2F_SMEM_BYTES, s>>>(a);
+                p2p_r2_split_kernel<<<leaf_grid, 256, R2F_SMEM_BYTES, ls>>>(a);
             else
-                p2p_r2_kernel<PREC_FAST><<<leaf_grid, 256, R2_SMEM_BYTES, s>>>(a);
+                p2p_r2_kernel<PREC_FAST><<<leaf_grid, 256, R2_SMEM_BYTES, ls>>>(a);
             mark(3);
-            if (rho) p2m_batch_kernel<PREC_FAST, true><<<p2m_grid, P_THREADS, 0, s>>>(a);
-            else p2m_batch_kernel<PREC_FAST, false><<<p2m_grid, P_THREADS, 0, s>>>(a);
+            if (rho) p2m_batch_kernel<PREC_FAST, true><<<p2m_grid, P_THREADS, 0, ls>>>(a);
+            else p2m_batch_kernel<PREC_FAST, false><<<p2m_grid, P_THREADS, 0, ls>>>(a);
+        }
+        if (fork) {
+            OT_CUDA(cudaEventRecord(ctx->ev_join, ls));
+            OT_CUDA(cudaStreamWaitEvent(s, ctx->ev_join, 0));
         }
         mark(4);
         OT_CUDA(cudaGetLastError());
