@@ -516,7 +516,7 @@ __global__ void __launch_bounds__(P_THREADS) p2m_batch_kernel(BatchArgs a) {
             for (int q = 0; q < 3; ++q) corr[q] = (P64 == PREC_EXACT && active) ? s_acc[4 + q][cu] : 0.0;
             const int beg = active ? __ldg(a.t.p2m_start + cu * 28 + raw) : 0;
             const int end = active ? __ldg(a.t.p2m_start + cu * 28 + raw + 1) : 0;
-#pragma unroll 1
+#pragma unroll 2
             for (int q = beg + f; q < end; q += F) {
                 const int u = __ldg(a.t.p2m_list + q);
                 double Y[3], mp[20];
