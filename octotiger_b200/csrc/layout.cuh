@@ -80,6 +80,9 @@ static_assert(P_XS >= P_SUB * P_RS && P_RS % 16 == 12 && P_XS % 32 == 16, "P2P r
 // Monopole constants {-1/r, x/r^3, y/r^3, z/r^3} per stencil offset (they do
 // not depend on theta), read warp-uniformly through the constant cache.
 __constant__ double c_four[FULL][4];
+// The same constants rounded to FP32 (the split P2P of theta < 0.5 reads them by
+// stencil index, warp-uniformly).
+__constant__ float4 c_four_f[FULL];
 
 // Entry flags
 constexpr int F_FAR = 1;    // phase-one offset: full multipole partner
@@ -117,8 +120,8 @@ struct Tables {
                                 // stencil order of the coarse cell's first cell
     const int16_t* pc_slot;     // [27][64]: slot of coarse cell C among direction r's units, -1 if none
     const int* pc_parts;        // [27]: parts each unit's partner lists of direction r are cut in
-    const float4* r2_four_f;    // r2_four rounded to FP32 (the split P2P of theta < 0.5)
-    const int* r2_p2p_delta;    // [8][MAX_ENTRIES_R2]: offset of each entries_r2 partner in the reach-2 P2P halo
+    const int* r2_p2p_delta;    // [8][MAX_ENTRIES_R2]: each entries_r2 partner's offset in the split reach-2 P2P
+                                // halo << 11 | its stencil index
     // P2M by octant (reach 1)
     const int4* po_box;         // [27][8][2]: sub-slab of direction r for octant o: (low x, y, z, cells), (extents)
     const int2* po_range;       // [27][64]: partner range in po_list of coarse cell C in direction r

@@ -224,7 +224,6 @@ struct otfmm_context {
     int2* d_entries_r2s = nullptr;     // entries_r2 with each sx group's far entries first
     int* d_r2s_far_end = nullptr;      // [8][11]: end of each sx group's far entries
     double4* d_r2_four = nullptr;
-    float4* d_r2_four_f = nullptr;
     int* d_r2_p2p_delta = nullptr;
     int p2m_groups_max = 0;   // cells with partners summed over the 26 directions
     double4* d_p2p_four = nullptr;
@@ -279,7 +278,7 @@ struct otfmm_context {
                       d_entries_ws, d_four,  d_phase,        d_p2m_start,     d_p2m_list,    d_p2m_perm_start,
                       d_p2m_perm,   d_p2m_slot,     d_p2p_four,      d_entries_r2,  d_r2_sx_start, d_r2_four,
                       d_p2p_box,    d_p2p_cube,     d_pc_unit_start, d_pc_coarse,  d_pc_range,    d_pc_list,
-                      d_pc_slot,    d_pc_parts,     d_r2_four_f,     d_r2_p2p_delta, d_po_box,   d_po_range,    d_po_list,
+                      d_pc_slot,    d_pc_parts,     d_r2_p2p_delta, d_po_box,   d_po_range,    d_po_list,
                       d_entries_r2s, d_r2s_far_end}; }
 };
 
@@ -314,6 +313,7 @@ int ensure_attributes(int device) {
     if (g_attr_set[device]) return OTFMM_OK;
     const int bytes = SMEM_DOUBLES * (int)sizeof(double);
     int rc = OTFMM_OK;
+    rc = rc ? rc : set_smem(p2p_r2_split_kernel, R2F_SMEM_BYTES + 8 * MAX_ENTRIES_R2 * 4);
     rc = rc ? rc : set_smem(m2l_batch_kernel<PREC_EXACT, true>, bytes);
     rc = rc ? rc : set_smem(m2l_batch_kernel<PREC_EXACT, false>, bytes);
     rc = rc ? rc : set_smem(m2l_batch_kernel<PREC_FAST, true>, bytes);
@@ -689,24 +689,23 @@ int otfmm_create(int device, double theta, otfmm_context** out) {
     if (pc_list.empty()) pc_list.assign(1, 0);
     DeviceGuard g(device);
     cudaError_t e;
-    std::vector<float4> r2_four_f(r2_four.size());
-    for (size_t q = 0; q < r2_four.size(); ++q)
-        r2_four_f[q] = float4{(float)r2_four[q].x, (float)r2_four[q].y, (float)r2_four[q].z, (float)r2_four[q].w};
     // position of every long-list partner in the parity-split FP32 halo of the
-    // reach-2 split P2P, relative to the lane's own sub-lattice position
+    // reach-2 split P2P, relative to the lane's own sub-lattice position, with
+    // its stencil index (the constants' index) in the low 11 bits
     std::vector<int> r2_p2p_delta(8 * (size_t)MAX_ENTRIES_R2, 0);
+    std::vector<float4> four_f(FULL);
+    for (int q = 0; q < FULL; ++q)
+        four_f[q] = float4{(float)ctx->st.four[q][0], (float)ctx->st.four[q][1], (float)ctx->st.four[q][2],
+                           (float)ctx->st.four[q][3]};
     for (int p = 0; p < 8; ++p)
         for (int e2 = 0; e2 < ctx->counts[p]; ++e2) {
             const int y = entries_r2[p * (size_t)MAX_ENTRIES_R2 + e2].y;
-            r2_p2p_delta[p * (size_t)MAX_ENTRIES_R2 + e2] =
-                r2f_index(((p >> 2) & 1) + (y & 15) - 8 + R2_PAD, ((p >> 1) & 1) + ((y >> 4) & 15) - 8 + R2_PAD,
-                          (p & 1) + ((y >> 8) & 15) - 8 + R2_PAD);
+            const int d = r2f_index(((p >> 2) & 1) + (y & 15) - 8 + R2_PAD, ((p >> 1) & 1) + ((y >> 4) & 15) - 8 + R2_PAD,
+                                    (p & 1) + ((y >> 8) & 15) - 8 + R2_PAD);
+            r2_p2p_delta[p * (size_t)MAX_ENTRIES_R2 + e2] = (d << 11) | ((y >> 16) & 2047);
         }
     if ((e = cudaMalloc(&ctx->d_r2_p2p_delta, sizeof(int) * r2_p2p_delta.size())) != cudaSuccess ||
         (e = cudaMemcpy(ctx->d_r2_p2p_delta, r2_p2p_delta.data(), sizeof(int) * r2_p2p_delta.size(),
-                        cudaMemcpyHostToDevice)) != cudaSuccess ||
-        (e = cudaMalloc(&ctx->d_r2_four_f, sizeof(float4) * r2_four_f.size())) != cudaSuccess ||
-        (e = cudaMemcpy(ctx->d_r2_four_f, r2_four_f.data(), sizeof(float4) * r2_four_f.size(),
                         cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMalloc(&ctx->d_r2_four, sizeof(double4) * r2_four.size())) != cudaSuccess ||
         (e = cudaMemcpy(ctx->d_r2_four, r2_four.data(), sizeof(double4) * r2_four.size(),
@@ -792,6 +791,7 @@ int otfmm_create(int device, double theta, otfmm_context** out) {
         (e = cudaMemcpy(ctx->d_entries_p2p, entries_p2p.data(), sizeof(int2) * entries_p2p.size(),
                         cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemcpyToSymbol(c_four, ctx->st.four, sizeof(double) * 4 * FULL)) != cudaSuccess ||
+        (e = cudaMemcpyToSymbol(c_four_f, four_f.data(), sizeof(float4) * FULL)) != cudaSuccess ||
         (e = cudaMemcpy(ctx->d_entries_split, entries_split.data(), sizeof(int4) * entries_split.size(),
                         cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemcpy(ctx->d_entries, entries.data(), sizeof(int2) * entries.size(), cudaMemcpyHostToDevice)) !=
@@ -857,7 +857,6 @@ int otfmm_destroy(otfmm_context* ctx) {
     cudaFree(ctx->d_entries_r2s);
     cudaFree(ctx->d_r2s_far_end);
     cudaFree(ctx->d_r2_four);
-    cudaFree(ctx->d_r2_four_f);
     cudaFree(ctx->d_r2_p2p_delta);
     {
         auto& hp = ctx->hp;
@@ -1182,7 +1181,7 @@ int enqueue_batch(otfmm_context* ctx, const double* pool_M, const double* pool_c
             else m2l_r2_kernel<PREC_FAST, false><<<4 * sms, THREADS, rbytes, s>>>(a);
             mark(2);
             if (precision == OTFMM_FP32_SPLIT)
-                p2p_r2_split_kernel<<<leaf_grid, 256, R2F_SMEM_BYTES, ls>>>(a);
+                p2p_r2_split_kernel<<<leaf_grid, 256, r2f_smem_bytes(ctx->counts), ls>>>(a);
             else
                 p2p_r2_kernel<PREC_FAST><<<leaf_grid, 256, R2_SMEM_BYTES, ls>>>(a);
             mark(3);

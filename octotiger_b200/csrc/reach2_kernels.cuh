@@ -478,6 +478,14 @@ constexpr bool r2f_conflict_free() {
 }
 static_assert(r2f_conflict_free(), "a warp's 32 cells fall in 32 distinct banks");
 static_assert(8 * R2F_XS + 8 * R2F_RS + 8 < R2F_CLS, "sub-lattice planes hold 9 x 9 x 9 cells");
+static_assert(8 * R2F_CLS < (1 << 21) && FULL <= 2048, "halo offset and stencil index pack into one int");
+// Dynamic shared memory of the split reach-2 P2P: the halo, then the 8 parity
+// classes' packed partner lists.
+inline int r2f_smem_bytes(const int counts[8]) {
+    int n = 0;
+    for (int p = 0; p < 8; ++p) n += counts[p];
+    return R2F_SMEM_BYTES + 4 * n;
+}
 
 __global__ void __launch_bounds__(256) p2p_r2_split_kernel(BatchArgs a) {
     extern __shared__ float pmf[];
@@ -489,8 +497,21 @@ __global__ void __launch_bounds__(256) p2p_r2_split_kernel(BatchArgs a) {
     const int own_a = i * R2F_XS + j * R2F_RS + k;   // plus the entry's delta: the partner of cell cxa
     constexpr int OFF_B = 2 * R2F_XS;                // cell cxb = cxa + 4
     const int n = a.t.count[p];
-    const float4* four = a.t.r2_four_f + p * MAX_ENTRIES_R2;
-    const int* delta = a.t.r2_p2p_delta + p * MAX_ENTRIES_R2;
+    // the 8 classes' packed partner lists (halo offset << 11 | stencil index),
+    // resident for the whole launch: an entry costs one broadcast shared load
+    // and one uniform constant-cache read
+    int* s_pk = reinterpret_cast<int*>(pmf + 8 * R2F_CLS);
+    int first = 0, total = 0;
+    for (int q = 0; q < 8; ++q) {
+        if (q == p) first = total;
+        total += a.t.count[q];
+    }
+    for (int t = threadIdx.x; t < total; t += blockDim.x) {
+        int q = 0, b = 0;
+        while (t >= b + a.t.count[q]) b += a.t.count[q++];
+        s_pk[t] = __ldg(a.t.r2_p2p_delta + q * MAX_ENTRIES_R2 + (t - b));
+    }
+    const int* pk = s_pk + first;
     const int nleaf = a.wl.counts[WL_LEAF];
     for (int kk = blockIdx.x; kk < nleaf; kk += gridDim.x) {
         __syncthreads();   // `it` and the halo are reused
@@ -513,8 +534,9 @@ __global__ void __launch_bounds__(256) p2p_r2_split_kernel(BatchArgs a) {
             const int e1 = min(e0 + R2_SPLIT_CHUNK, n);
 #pragma unroll 4
             for (int e = e0; e < e1; ++e) {
-                const float4 f = __ldg(four + e);
-                const int d = own_a + __ldg(delta + e);
+                const int w = pk[e];
+                const float4 f = c_four_f[w & 2047];
+                const int d = own_a + (w >> 11);
                 const float ma = pmf[d], mb = pmf[d + OFF_B];
                 a01 = __ffma2_rn(make_float2(f.x, f.y), make_float2(ma, ma), a01);
                 a23 = __ffma2_rn(make_float2(f.z, f.w), make_float2(ma, ma), a23);
