@@ -383,7 +383,9 @@ def gpu_arm(args) -> None:
     h2d = (n_ref * 20 * 512 * 8 + mon_bytes + int(needs_com.sum()) * 3 * 512 * 8 + 2 * batch.pool.n
            + items_pin.numel())
     n_leaf = int((batch.pool.is_leaf == 1).sum())
-    d2h = L_pin.numel() * 8 - n_leaf * 16 * 512 * 8 + Lc_pin.numel() * 8
+    # bytes it downloads: L of refined subgrids, L0..L3 of leaves, L_c where the
+    # solve writes it (refined subgrids, leaves with a refined neighbour)
+    d2h = L_pin.numel() * 8 - n_leaf * 16 * 512 * 8 + int(needs_com.sum()) * 3 * 512 * 8
 
     def e2e_step():
         ctx.batch_host(pin["M"], pin["com"], pin["mon"], pin["is_leaf"], batch.pool.n, items_pin, len(items_h),

@@ -273,7 +273,8 @@ int otfmm_plan_destroy(otfmm_plan* plan);
  * it computes nothing, as node_server::compute_fmm zeroes L / L_c before the
  * reference's kernels (src/node_server.cpp:701-705) - except L[4..19] of leaf
  * subgrids, which no kernel writes (the reference's monopole kernels output
- * L[0..3] and L_c) and which are left as the caller set them. The pool is uploaded in
+ * L[0..3] and L_c), and L_c of leaves without a refined neighbour (which only
+ * the P2M writes), both left as the caller set them. The pool is uploaded in
  * chunks of consecutive subgrids (the moments of refined subgrids, the masses
  * of chunks with leaves and the centres of mass: what the kernels read); each work item runs once the records it
  * reads have arrived and each output range is copied back once final, on two

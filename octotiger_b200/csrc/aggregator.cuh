@@ -95,10 +95,19 @@ int agg_run(otfmm_aggregator* a, otfmm_aggregator::Batch& b, std::string& msg) {
         msg = otfmm_last_error();
         return rc;
     }
+    // leaves with a refined neighbour (the only leaves whose L_c the solve writes)
+    std::vector<uint8_t> p2m_leaf(b.n_sub, 0);
+    for (const otfmm_work_item& w : items) {
+        if (w.kind != OTFMM_KIND_LEAF) continue;
+        for (int d = 0; d < 26; ++d)
+            if (w.neighbors[d] >= 0 && !b.is_leaf[w.neighbors[d]]) p2m_leaf[w.subgrid] = 1;
+    }
     for (const otfmm_aggregator::Out& o : b.outs) {
         const int ncomp = (o.kind == OTFMM_KIND_LEAF) ? 4 : 20;
         std::copy(b.L + (size_t)o.slot * 20 * NCELL, b.L + ((size_t)o.slot * 20 + ncomp) * NCELL, o.L);
-        if (o.Lc) std::copy(b.Lc + (size_t)o.slot * 3 * NCELL, b.Lc + ((size_t)o.slot + 1) * 3 * NCELL, o.Lc);
+        if (!o.Lc) continue;
+        if (o.kind == OTFMM_KIND_LEAF && !p2m_leaf[o.slot]) std::fill(o.Lc, o.Lc + 3 * NCELL, 0.0);
+        else std::copy(b.Lc + (size_t)o.slot * 3 * NCELL, b.Lc + ((size_t)o.slot + 1) * 3 * NCELL, o.Lc);
     }
     return OTFMM_OK;
 }

@@ -57,19 +57,23 @@ __global__ void __launch_bounds__(HC_THREADS) gather_pool_kernel(const double* _
 }
 
 // Download of pool chunk [a, a + n): L[0..19] of a refined subgrid, L[0..3] of
-// a leaf (its L[4..19] are left as the caller set them) and L_c of both, from
-// the device into the mapped host outputs (one CTA per subgrid).
+// a leaf (its L[4..19] are left as the caller set them), and L_c of the
+// subgrids flagged in writes_lc (refined ones, leaves with a refined
+// neighbour; the others' L_c is left as the caller set it), from the device
+// into the mapped host outputs (one CTA per subgrid).
 __global__ void __launch_bounds__(HC_THREADS) scatter_outputs_kernel(const double* __restrict__ dev_L,
                                                                      const double* __restrict__ dev_Lc,
                                                                      double* __restrict__ host_L,
                                                                      double* __restrict__ host_Lc,
-                                                                     const uint8_t* __restrict__ is_leaf, int a) {
+                                                                     const uint8_t* __restrict__ is_leaf,
+                                                                     const uint8_t* __restrict__ writes_lc, int a) {
     const size_t i = (size_t)a + blockIdx.x;
     const int ncomp = is_leaf[i] ? 4 : 20;
     cta_copy(reinterpret_cast<double2*>(host_L + i * 20 * NCELL),
              reinterpret_cast<const double2*>(dev_L + i * 20 * NCELL), ncomp * NCELL / 2);
-    cta_copy(reinterpret_cast<double2*>(host_Lc + i * 3 * NCELL),
-             reinterpret_cast<const double2*>(dev_Lc + i * 3 * NCELL), 3 * NCELL / 2);
+    if (writes_lc[i])
+        cta_copy(reinterpret_cast<double2*>(host_Lc + i * 3 * NCELL),
+                 reinterpret_cast<const double2*>(dev_Lc + i * 3 * NCELL), 3 * NCELL / 2);
 }
 
 }   // namespace otfmm

@@ -1552,24 +1552,23 @@ int otfmm_batch_host(otfmm_context* ctx, const double* pool_M, const double* poo
     double* L_dev = static_cast<double*>(const_cast<void*>(mapped_host(L, 20 * cell * nsub)));
     double* Lc_dev = static_cast<double*>(const_cast<void*>(mapped_host(L_c, 3 * cell * nsub)));
     const bool sm_in = (M_dev != nullptr && com_dev != nullptr), sm_out = (L_dev != nullptr && Lc_dev != nullptr);
-    if (sm_in) {
-        // the centres of mass the kernels read: those of refined subgrids and of
-        // leaves with a refined neighbour (P2M targets); a leaf enters every
-        // other interaction as masses at its cell centres
-        for (size_t i = 0; i < nsub; ++i) hp.needs_com_pinned[i] = pool_is_leaf[i] ? 0 : 1;
-        for (int i = 0; i < n_items; ++i) {
-            const otfmm_work_item& w = items[i];
-            if (w.kind != OTFMM_KIND_LEAF) continue;
-            for (int d = 0; d < 26; ++d)
-                if (w.neighbors[d] >= 0 && !pool_is_leaf[w.neighbors[d]]) hp.needs_com_pinned[w.subgrid] = 1;
-        }
+    // the subgrids whose centres of mass the kernels read and whose L_c they
+    // write: the refined ones and the leaves with a refined neighbour (P2M
+    // targets); a leaf enters every other interaction as masses at its cell
+    // centres, and no kernel writes the L_c of a leaf without a refined
+    // neighbour (the reference's P2P does not either)
+    for (size_t i = 0; i < nsub; ++i) hp.needs_com_pinned[i] = pool_is_leaf[i] ? 0 : 1;
+    for (int i = 0; i < n_items; ++i) {
+        const otfmm_work_item& w = items[i];
+        if (w.kind != OTFMM_KIND_LEAF) continue;
+        for (int d = 0; d < 26; ++d)
+            if (w.neighbors[d] >= 0 && !pool_is_leaf[w.neighbors[d]]) hp.needs_com_pinned[w.subgrid] = 1;
     }
     OT_CUDA(cudaEventRecord(ev_start, s));
     OT_CUDA(cudaStreamWaitEvent(hp.h2d, ev_start, 0));
     OT_CUDA(cudaStreamWaitEvent(hp.d2h, ev_start, 0));
     OT_CUDA(cudaMemcpyAsync(hp.is_leaf, pool_is_leaf, (size_t)n_subgrids, cudaMemcpyHostToDevice, hp.h2d));
-    if (sm_in)
-        OT_CUDA(cudaMemcpyAsync(hp.needs_com, hp.needs_com_pinned, nsub, cudaMemcpyHostToDevice, hp.h2d));
+    OT_CUDA(cudaMemcpyAsync(hp.needs_com, hp.needs_com_pinned, nsub, cudaMemcpyHostToDevice, hp.h2d));
     OT_CUDA(cudaMemcpyAsync(hp.items, hp.items_pinned, sizeof(otfmm_work_item) * (size_t)n_items,
                             cudaMemcpyHostToDevice, hp.h2d));
     for (int k = 0; k < K; ++k) {
@@ -1622,10 +1621,12 @@ int otfmm_batch_host(otfmm_context* ctx, const double* pool_M, const double* poo
         OT_CUDA(cudaStreamWaitEvent(hp.d2h, ev_comp[need[k]], 0));
         const size_t a = bnd[k], n = bnd[k + 1] - bnd[k];
         // L of refined subgrids whole; of leaves the monopole kernels' L0..L3
-        // (their L4..L19 stay as the caller set them), runs of consecutive ones
+        // (their L4..L19 stay as the caller set them); L_c where a kernel writes
+        // it (refined subgrids, leaves with a refined neighbour); runs of
+        // consecutive ones
         if (sm_out) {
             scatter_outputs_kernel<<<(unsigned)n, HC_THREADS, 0, hp.d2h>>>(hp.L, hp.Lc, L_dev, Lc_dev, hp.is_leaf,
-                                                                           (int)a);
+                                                                           hp.needs_com, (int)a);
             OT_CUDA(cudaEventRecord(ev_d2h[k], hp.d2h));
             continue;
         }
@@ -1641,8 +1642,17 @@ int otfmm_batch_host(otfmm_context* ctx, const double* pool_M, const double* poo
                                         cudaMemcpyDeviceToHost, hp.d2h));
             i = j;
         }
-        OT_CUDA(cudaMemcpyAsync(L_c + a * 3 * NCELL, hp.Lc + a * 3 * NCELL, n * 3 * cell, cudaMemcpyDeviceToHost,
-                                hp.d2h));
+        for (size_t i = a; i < a + n;) {
+            if (!hp.needs_com_pinned[i]) {
+                ++i;
+                continue;
+            }
+            size_t j = i + 1;
+            while (j < a + n && hp.needs_com_pinned[j]) ++j;
+            OT_CUDA(cudaMemcpyAsync(L_c + i * 3 * NCELL, hp.Lc + i * 3 * NCELL, (j - i) * 3 * cell,
+                                    cudaMemcpyDeviceToHost, hp.d2h));
+            i = j;
+        }
         OT_CUDA(cudaEventRecord(ev_d2h[k], hp.d2h));
     }
     OT_CUDA(cudaEventRecord(ev_done, hp.d2h));

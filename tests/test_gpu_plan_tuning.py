@@ -194,12 +194,24 @@ def test_batch_profile_times_each_kernel_and_matches_batch(ctx):
     np.testing.assert_array_equal(Lc, Lc0)
 
 
+def _writes_lc(b):
+    """Subgrids whose L_c a solve writes: the refined ones and the leaves with a
+    refined neighbour."""
+    w = b.pool.is_leaf == 0
+    for it in b.items:
+        nb = it["neighbors"][it["neighbors"] >= 0]
+        if it["kind"] == 2 and (b.pool.is_leaf[nb] == 0).any():
+            w[it["subgrid"]] = True
+    return w
+
+
 @pytest.mark.parametrize("precision", ["fp64_exact", "fp32_split"])
 @pytest.mark.parametrize("pinned", [False, True, "inputs"])
 def test_batch_host_matches_device_batch(ctx, precision, pinned):
     """otfmm_batch_host (chunked uploads, kernels and downloads) gives the
     device batch's results, zeros where the solve writes nothing, and leaves
-    L[4..19] of leaf subgrids (no kernel writes them) as the caller set them:
+    L[4..19] of leaf subgrids and L_c of leaves without a refined neighbour (no
+    kernel writes them) as the caller set them:
     with pageable buffers (copy engines), page-locked ones (the SMs move the
     moments in and the outputs out) and page-locked inputs with pageable
     outputs."""
@@ -235,7 +247,9 @@ def test_batch_host_matches_device_batch(ctx, precision, pinned):
         np.testing.assert_array_equal(Lh[~leaf], L0[~leaf])
         np.testing.assert_array_equal(Lh[leaf, :4], L0[leaf, :4])
         assert np.isnan(Lh[leaf, 4:]).all()
-        np.testing.assert_array_equal(Lch, Lc0)
+        writes_lc = _writes_lc(b)
+        np.testing.assert_array_equal(Lch[writes_lc], Lc0[writes_lc])
+        assert np.isnan(Lch[~writes_lc]).all()
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32_split"])
@@ -262,6 +276,7 @@ def test_host_plan_replays_batch_host(ctx, precision):
         L.fill_(np.nan)
         Lc.fill_(np.nan)
         L[torch.from_numpy(leaf)] = 0.0   # the caller zeroes L (leaves' L4..L19 are not written)
+        Lc[torch.from_numpy(~_writes_lc(b))] = 0.0   # and L_c (only P2M writes a leaf's)
         plan.launch()
         torch.cuda.synchronize()
         plan.status()
