@@ -428,8 +428,12 @@ def gpu_arm(args) -> None:
     if not args.no_adapter:
         from octotiger_b200.otfmm import adapter_pass
         nthr = os.cpu_count() or 8
+        # a batch holds up to 8,192 records; every thread keeps up to 512 calls in
+        # flight (an HPX task waiting on its call's future is suspended and its
+        # worker runs other nodes' tasks: a solve's calls can all be in flight)
+        cap = int(min(8192, max(64, batch.pool.n)))
         La, Lca, sec = adapter_pass(ctx, batch.pool, batch.items, solve, args.precision, aggregate=True,
-                                    threads=nthr, max_subgrids=4096, max_items=2048, passes=4)
+                                    threads=nthr, max_subgrids=cap, max_items=cap, passes=4, calls_in_flight=512)
         leaf_items = batch.items["kind"] == 2
         sub_m = batch.items["subgrid"][~leaf_items]
         sub_l = batch.items["subgrid"][leaf_items]
@@ -442,8 +446,10 @@ def gpu_arm(args) -> None:
         e2e_adapter = {"value": counts["total"] / t_agg, "unit": UNIT, "s_per_pass": t_agg,
                        "host_threads": nthr, "passes_timed": len(sec) - 1,
                        "what": "every node's multipole_kernel_interface / monopole_kernel_interface call through the "
-                               "C++ drop-in adapter from all host threads at once, AoS inputs, calls aggregated into "
-                               "batched solves (wall time of a pass, first call to last return)",
+                               "C++ drop-in adapter from all host threads at once (up to 512 calls in flight per "
+                               "thread), AoS inputs, calls aggregated into batched solves of up to %d records, results "
+                               "added into the grids' cells by the batch (wall time of a pass, first call to last "
+                               "return)" % cap,
                        "matches_device_solve": adapter_matches,
                        "per_call_value": counts["total"] / float(sec1[0]), "per_call_s_per_pass": float(sec1[0]),
                        "per_call_what": "the same calls without aggregation: one host-buffer kernel call per node "

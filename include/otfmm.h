@@ -126,11 +126,10 @@ int otfmm_m2l_soa_host(otfmm_context* ctx, const double* mon, const double* M, c
  * pre-sized memory budget, threads that must not trigger the implicit device
  * synchronisation of cudaMalloc/cudaFree, or HPX tasks on a hot path where the
  * reference uses recycled buffers. The first call on a device looks up the
- * array's device address (cudaGetSymbolAddress) and should come before any
- * stream capture. With CUDA's lazy module loading the library's device code,
- * and the array with it, is placed on a device when the library is first used
- * there, so make that first call at set-up time, before the code that must not
- * allocate runs. Larger n_subgrids is rejected (OTFMM_ERR_INVALID). All calls
+ * array's device address (cudaGetSymbolAddress). With CUDA's lazy module
+ * loading the library's device code, and the array with it, is placed on a
+ * device when the library is first used there, so make that first call at
+ * set-up time, before the code that must not allocate runs. Larger n_subgrids is rejected (OTFMM_ERR_INVALID). All calls
  * share the one array: calls that overlap on the GPU would race, so calls
  * from this library are serialised and each waits for its stream before it
  * returns, on error returns too. */
@@ -364,10 +363,16 @@ long long otfmm_count_pairs(const otfmm_context* ctx, const uint8_t* is_leaf, in
  *      fields are slots, -1 = empty) and its output buffers; returns at once.
  *      Every reserved call must be submitted (a bad item withdraws the call
  *      and returns OTFMM_ERR_INVALID).
+ *      otfmm_aggregator_submit_aos instead: the results go into the caller's
+ *      array-of-structures cells when the batch runs, L[u * l_stride + c] +=
+ *      component c of cell u (the reference's L += result) and, when L_c is
+ *      not NULL, L_c[u * lc_stride + c] = component c (L_c = result); no
+ *      intermediate buffer, and the caller leaves those cells alone until its
+ *      wait returns.
  *   4. otfmm_aggregator_wait(ticket): blocks until the call's batch has run;
  *      then L holds 20 x 512 (multipole items) or 4 x 512 (leaves) values and
- *      L_c, when not NULL, 3 x 512 (SoA). A caller may have many calls
- *      submitted before it waits (as HPX tasks do).
+ *      L_c, when not NULL, 3 x 512 (SoA), or the AoS cells are updated. A
+ *      caller may have many calls submitted before it waits (as HPX tasks do).
  * A batch runs when it is full and all its reserved calls have submitted, or
  * when it has been idle for idle_us with no call between reserve and submit;
  * a caller in otfmm_aggregator_wait (or in a reserve that finds both batch
@@ -387,6 +392,11 @@ int otfmm_aggregator_record(otfmm_aggregator* agg, int64_t ticket, int32_t slot,
                             double** mon);
 int otfmm_aggregator_submit(otfmm_aggregator* agg, int64_t ticket, const otfmm_work_item* item, double* L,
                             double* L_c);
+/* l_stride >= the components of the item's kind (20 multipole, 4 leaf),
+ * lc_stride >= 3, in doubles. A leaf without a refined neighbour has no P2M
+ * part: its L_c cells are set to zero, as otfmm_aggregator_submit's L_c. */
+int otfmm_aggregator_submit_aos(otfmm_aggregator* agg, int64_t ticket, const otfmm_work_item* item, double* L,
+                                int32_t l_stride, double* L_c, int32_t lc_stride);
 int otfmm_aggregator_wait(otfmm_aggregator* agg, int64_t ticket);
 
 /* Checks a device-side error flag written by the last otfmm_batch on `stream`

@@ -44,6 +44,7 @@
 #include <iostream>
 #include <memory>
 #include <type_traits>
+#include <utility>
 #include <vector>
 
 #include "otfmm.h"
@@ -435,9 +436,29 @@ struct AggregatedCall {
     int64_t ticket = 0;
     int ncomp = 20;          // L components the call's kind writes (20 multipole, 4 monopole)
     bool write_lc = false;   // L_c = result (RHO multipole; RHO monopole with a refined neighbour)
+    bool in_place = true;    // let the batch write a grid of flat cells itself (set before submitting)
+    bool direct = false;     // the batch writes the grid's cells itself (otfmm_aggregator_submit_aos)
     GridPtr grid{};
-    std::vector<double> L, Lc;
+    std::vector<double> L, Lc;   // SoA results otherwise, applied by finish()
 };
+
+// Cell u's component c of `v` (taylor<4> / space_vector cells) is the double
+// at data() + u * K + c: K doubles per cell, reached through operator[] as
+// plain members. Checked on the element type and on the addresses of cells 0
+// and 1; such a grid gets its results written in place by the batch.
+template <int K, class V>
+inline double* flat_cells(V& v) {
+    using E = typename V::value_type;
+    if constexpr (sizeof(E) == K * sizeof(double) && std::is_standard_layout_v<E> &&
+                  std::is_same_v<decltype(std::declval<E&>()[0]), double&>) {
+        if (v.size() < (size_t)NCELL) return nullptr;
+        double* base = reinterpret_cast<double*>(v.data());
+        const bool flat = &v[0][0] == base && &v[0][K - 1] == base + K - 1 && &v[1][0] == base + K;
+        return flat ? base : nullptr;
+    } else {
+        return nullptr;
+    }
+}
 
 // Rows c = 0..K-1 (row stride NCELL) of a pool record from the cells' AoS
 // values src[u][c], 8 cells at a time, so that every block writes whole cache
@@ -535,28 +556,36 @@ int aggregated_submit(otfmm_aggregator* agg, int kind, const std::vector<Multipo
     call.agg = agg;
     call.ticket = ticket;
     call.grid = grid;
-    call.L.assign((size_t)call.ncomp * NCELL, 0.0);
-    call.Lc.assign(3 * NCELL, 0.0);
     if (rc != OTFMM_OK) {
         // withdraw the reservation so that the batch can run without this call
         item.subgrid = -1;
-        otfmm_aggregator_submit(agg, ticket, &item, call.L.data(), nullptr);
+        otfmm_aggregator_submit(agg, ticket, &item, nullptr, nullptr);
         call.agg = nullptr;
         return rc;
     }
-    rc = otfmm_aggregator_submit(agg, ticket, &item, call.L.data(), call.Lc.data());
+    double* gL = flat_cells<20>(grid->get_L());
+    double* gLc = call.write_lc ? flat_cells<3>(grid->get_L_c()) : nullptr;
+    call.direct = call.in_place && gL && (gLc || !call.write_lc);
+    if (call.direct) {
+        rc = otfmm_aggregator_submit_aos(agg, ticket, &item, gL, 20, gLc, 3);
+    } else {
+        call.L.assign((size_t)call.ncomp * NCELL, 0.0);
+        call.Lc.assign(3 * NCELL, 0.0);
+        rc = otfmm_aggregator_submit(agg, ticket, &item, call.L.data(), call.Lc.data());
+    }
     if (rc != OTFMM_OK) call.agg = nullptr;
     return rc;
 }
 
 // Waits for a submitted call's batch, then updates the grid: L += result,
-// L_c = result where the reference sets it.
+// L_c = result where the reference sets it (a grid of flat cells was updated
+// by the batch already).
 template <class GridPtr>
 int finish(AggregatedCall<GridPtr>& call) {
     if (!call.agg) return OTFMM_ERR_INVALID;
     const int rc = otfmm_aggregator_wait(call.agg, call.ticket);
     call.agg = nullptr;
-    if (rc != OTFMM_OK) return rc;
+    if (rc != OTFMM_OK || call.direct) return rc;
     auto& gL = call.grid->get_L();
     for (int u0 = 0; u0 < NCELL; u0 += 8)
         for (int c = 0; c < call.ncomp; ++c)

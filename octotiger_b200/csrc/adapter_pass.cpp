@@ -18,8 +18,6 @@
 
 namespace {
 
-constexpr int CALLS_IN_FLIGHT = 64;   // aggregated calls a worker thread submits before it waits
-
 struct Node {
     std::shared_ptr<std::vector<multipole>> M;
     std::shared_ptr<std::vector<space_vector>> com;
@@ -35,8 +33,12 @@ extern "C" {
  * are host arrays in the library's batch layout; they are converted to the
  * reference's AoS node data once, outside the timed passes. mode 1: the
  * aggregated interfaces (an otfmm_aggregator of max_subgrids / max_items /
- * idle_us; each thread submits 64 calls, then finishes them, as HPX tasks leave
- * many calls in flight per worker thread); mode 0: the per-call interfaces on
+ * idle_us; each thread submits calls_in_flight calls, then finishes them: an
+ * HPX task that waits on a future is suspended and its worker thread runs
+ * other nodes' tasks, so many calls per thread are in flight), the batch
+ * writing the grids' cells
+ * itself; mode 2: the same with SoA results that finish() adds to the grids on
+ * the caller's thread; mode 0: the per-call interfaces on
  * the context (one blocking host-buffer call per node). seconds[p] = wall time of pass p (all threads, first call to
  * last return). After the last pass L_out[n][20][512] / Lc_out[n][3][512]
  * hold the grids of the work items' subgrids (zero elsewhere). Returns the
@@ -44,9 +46,10 @@ extern "C" {
 int otfmm_adapter_pass(otfmm_context* ctx, int32_t n_sub, const double* M, const double* com, const double* mon,
                        const uint8_t* is_leaf, const otfmm_work_item* items, int32_t n_items, int gsolve_type,
                        int precision, int32_t mode, int32_t threads, int32_t max_subgrids, int32_t max_items,
-                       int32_t idle_us, int32_t passes, double* L_out, double* Lc_out, double* seconds) {
+                       int32_t idle_us, int32_t passes, int32_t calls_in_flight, double* L_out, double* Lc_out,
+                       double* seconds) {
     if (!ctx || !M || !com || !mon || !is_leaf || !items || !L_out || !Lc_out || !seconds || n_sub < 1 ||
-        n_items < 1 || threads < 1 || passes < 1)
+        n_items < 1 || threads < 1 || passes < 1 || mode < 0 || mode > 2 || calls_in_flight < 1)
         return OTFMM_ERR_INVALID;
     for (int i = 0; i < n_items; ++i)
         if (items[i].subgrid < 0 || items[i].subgrid >= n_sub) return OTFMM_ERR_INVALID;
@@ -85,7 +88,7 @@ int otfmm_adapter_pass(otfmm_context* ctx, int32_t n_sub, const double* M, const
         com_ptrs[i] = {nodes[items[i].subgrid].com};
     }
     otfmm_aggregator* agg = nullptr;
-    if (mode == 1) {
+    if (mode == 1 || mode == 2) {
         const int rc = otfmm_aggregator_create(ctx, max_subgrids, max_items, idle_us, gsolve_type, precision, &agg);
         if (rc != OTFMM_OK) return rc;
     }
@@ -103,16 +106,17 @@ int otfmm_adapter_pass(otfmm_context* ctx, int32_t n_sub, const double* M, const
                 first_rc.compare_exchange_strong(expect, rc);
             }
         };
-        // aggregated: a thread takes CALLS_IN_FLIGHT nodes at a time, submits all
-        // their calls, then finishes them (HPX tasks leave many calls in flight
-        // per worker thread); per-call: one blocking call after the other
+        // aggregated: a thread takes calls_in_flight nodes at a time, submits all
+        // their calls, then finishes them; per-call: one blocking call after the
+        // other
         auto agg_worker = [&]() {
-            std::vector<otfmm_octotiger::AggregatedCall<grid*>> calls(CALLS_IN_FLIGHT);
-            std::vector<int> ok(CALLS_IN_FLIGHT);
+            std::vector<otfmm_octotiger::AggregatedCall<grid*>> calls(calls_in_flight);
+            for (auto& c : calls) c.in_place = (mode == 1);
+            std::vector<int> ok(calls_in_flight);
             for (;;) {
-                const int i0 = next.fetch_add(CALLS_IN_FLIGHT);
+                const int i0 = next.fetch_add(calls_in_flight);
                 if (i0 >= n_items) return;
-                const int i1 = std::min(n_items, i0 + CALLS_IN_FLIGHT);
+                const int i1 = std::min(n_items, i0 + calls_in_flight);
                 for (int i = i0; i < i1; ++i) {
                     const otfmm_work_item& w = items[i];
                     const Node& nd = nodes[w.subgrid];

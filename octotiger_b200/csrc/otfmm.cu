@@ -284,11 +284,15 @@ struct otfmm_context {
 
 namespace {
 
+// Makes the context's device current for a call, and with it its primary
+// context on the calling thread: a thread that has never called the runtime
+// reports device 0 with no context bound yet, and then, among others,
+// cudaPointerGetAttributes finds no device pointer for mapped host memory.
 struct DeviceGuard {
     int prev = -1;
     explicit DeviceGuard(int dev) {
         cudaGetDevice(&prev);
-        if (prev != dev) cudaSetDevice(dev);
+        cudaSetDevice(dev);
     }
     ~DeviceGuard() {
         int cur = -1;
@@ -959,9 +963,8 @@ int otfmm_m2l_soa_host(otfmm_context* ctx, const double* mon, const double* M, c
 
 // Host-buffer multipole call that allocates nothing: device staging comes
 // from the static g_noalloc_scratch array. Its device address is looked up
-// once per device (cudaGetSymbolAddress, on the first call on that device,
-// which should therefore come before any stream capture); later calls reuse
-// it. The array is shared by every call: calls are serialised here, each call
+// once per device (cudaGetSymbolAddress, on the first call on that device);
+// later calls reuse it. The array is shared by every call: calls are serialised here, each call
 // clears the output staging it reads back, and each waits for its stream
 // before it returns, on error returns too.
 int otfmm_m2l_soa_host_noalloc(otfmm_context* ctx, int32_t n_subgrids, const double* mon, const double* M,

@@ -5,7 +5,9 @@ threads at once, AoS inputs, neighbour payloads aliasing the neighbours' data
 calls into batched solves; the grids after the pass must equal the oracle:
 bit-identical in the exact FP64 form, within 1e-12 in the fast form. Small
 batch capacities force many batches (full batches close while others run);
-the per-call interfaces on the context give the same results."""
+the per-call interfaces on the context give the same results. The batch
+writes the grids' cells itself (otfmm_aggregator_submit_aos), or, with
+in_place off, finish() adds SoA results on the caller's thread."""
 from __future__ import annotations
 
 import numpy as np
@@ -58,12 +60,15 @@ def scaled(a, ref):
     return np.where(den > 0, num / np.where(den > 0, den, 1), num)
 
 
+@pytest.mark.parametrize("in_place", [True, False])
 @pytest.mark.parametrize("solve", [RHO, DRHODT])
-@pytest.mark.parametrize("max_subgrids,threads", [(64, 8), (4096, 16)])
-def test_aggregated_adapter_exact_matches_oracle(ctx, oracle, tree, solve, max_subgrids, threads):
+@pytest.mark.parametrize("max_subgrids,threads,in_flight", [(64, 8, 64), (4096, 16, 512)])
+def test_aggregated_adapter_exact_matches_oracle(ctx, oracle, tree, solve, max_subgrids, threads, in_flight,
+                                                 in_place):
     from octotiger_b200.otfmm import adapter_pass
     L, Lc, sec = adapter_pass(ctx, tree.pool, tree.items, solve, "fp64_exact", aggregate=True, threads=threads,
-                              max_subgrids=max_subgrids, max_items=max_subgrids // 2, passes=2)
+                              max_subgrids=max_subgrids, max_items=max_subgrids // 2, passes=2, in_place=in_place,
+                              calls_in_flight=in_flight)
     Le, Lce = expected(tree, oracle, solve)
     np.testing.assert_array_equal(L, Le)
     np.testing.assert_array_equal(Lc, Lce)
@@ -101,5 +106,27 @@ def test_aggregator_rejects_bad_arguments(ctx):
     assert lib.otfmm_aggregator_create(ctx.handle, 8, 4, 100, RHO, 1, ctypes.byref(agg)) == -1   # < 27 slots
     assert lib.otfmm_aggregator_create(ctx.handle, 64, 4, 100, 7, 1, ctypes.byref(agg)) == -1    # bad solve type
     assert lib.otfmm_aggregator_create(ctx.handle, 64, 4, 100, RHO, 1, ctypes.byref(agg)) == 0
+    # AoS outputs with strides below a cell's components: the call is withdrawn
+    # (its reservation ends, so the aggregator can be destroyed afterwards)
+    from octotiger_b200.layout import WORK_ITEM_DTYPE
+    lib.otfmm_aggregator_reserve.argtypes = [ctypes.c_void_p, ctypes.c_int32] + [ctypes.c_void_p] * 6
+    lib.otfmm_aggregator_submit_aos.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
+                                                ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32]
+    keys = np.zeros(1, np.uint64)
+    leaf = np.zeros(1, np.uint8)
+    need = np.array([3], np.uint8)   # moments and centres of mass
+    slots = np.zeros(1, np.int32)
+    fill = np.zeros(1, np.uint8)
+    cells = np.zeros(512 * 20)
+    for l_stride, lc_stride in [(10, 3), (20, 2), (0, 3)]:
+        ticket = ctypes.c_int64()
+        assert lib.otfmm_aggregator_reserve(agg, 1, keys.ctypes.data, leaf.ctypes.data, need.ctypes.data,
+                                            slots.ctypes.data, fill.ctypes.data, ctypes.byref(ticket)) == 0
+        item = np.zeros(1, WORK_ITEM_DTYPE)
+        item["subgrid"] = slots[0]
+        item["neighbors"] = -1
+        item["dx"] = 1.0
+        assert lib.otfmm_aggregator_submit_aos(agg, ticket, item.ctypes.data, cells.ctypes.data, l_stride,
+                                               cells.ctypes.data, lc_stride) == -1
     lib.otfmm_aggregator_destroy.argtypes = [ctypes.c_void_p]
     assert lib.otfmm_aggregator_destroy(agg) == 0
