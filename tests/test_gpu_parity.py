@@ -195,6 +195,37 @@ def test_device_rejects_bad_work_item(ctx):
     ctx.batch_status()
 
 
+def test_empty_work_list(ctx, oracle):
+    """No work items: the device and host-buffer batched calls return at once
+    and write nothing; the next non-empty solve is unaffected."""
+    import torch
+    from octotiger_b200.otfmm import DevicePool
+    b = syn.single_subgrid(seed=52)
+    dev = DevicePool.upload(b.pool)
+    raw = torch.from_numpy(b.items.view(np.uint8).reshape(-1).copy()).cuda()
+    L = torch.full((b.pool.n, 20, NCELL), 7.0, dtype=torch.float64, device="cuda")
+    Lc = torch.full((b.pool.n, 3, NCELL), 7.0, dtype=torch.float64, device="cuda")
+    for precision in ("fp64_exact", "fp64", "fp32_split"):
+        ctx.batch(dev, raw, 0, L, Lc, RHO, precision)
+        ctx.batch_status()
+    assert bool((L == 7.0).all()) and bool((Lc == 7.0).all())
+    Lh = np.full((b.pool.n, 20, NCELL), 7.0)
+    Lch = np.full((b.pool.n, 3, NCELL), 7.0)
+    ctx.batch_host(b.pool.M, b.pool.com, b.pool.mon, b.pool.is_leaf, b.pool.n, b.items, 0, Lh, Lch, RHO,
+                   "fp32_split")
+    ctx.batch_status()
+    assert (Lh == 7.0).all() and (Lch == 7.0).all()
+    # the same context then solves the item as usual (bit-identical to the oracle)
+    Lo, Lco = oracle.batch(0.5, b.pool, b.items, rho=True)
+    L.zero_()
+    Lc.zero_()
+    ctx.batch(dev, raw, 1, L, Lc, RHO, "fp64_exact")
+    ctx.batch_status()
+    s = int(b.items[0]["subgrid"])
+    np.testing.assert_array_equal(L.cpu().numpy()[s], Lo[s])
+    np.testing.assert_array_equal(Lc.cpu().numpy()[s], Lco[s])
+
+
 def test_fma_peaks_measurable():
     from octotiger_b200.otfmm import measure_fma_peaks
     f64, f32 = measure_fma_peaks(0)
