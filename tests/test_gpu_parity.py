@@ -272,3 +272,34 @@ def test_library_pair_count_matches_oracle(ctx, oracle, name):
     tot, per = ctx.count_pairs(b.pool.is_leaf, b.items)
     tot_o, per_o = oracle.count_pairs(0.5, b.pool, b.items)
     assert tot == tot_o and list(per) == list(per_o)
+
+
+@pytest.mark.parametrize("theta", [0.7, 1.0])
+@pytest.mark.parametrize("solve", [RHO, DRHODT])
+@pytest.mark.parametrize("name", ["mixed", "amr_small"])
+def test_other_opening_angles(oracle, theta, solve, name):
+    """Opening angles above 0.5 (smaller multipole stencils, larger P2P boxes
+    relative to them): exact form bit-identical, fast form within 1e-12,
+    FP32-split form within its bars, against the oracle at the same theta."""
+    from octotiger_b200.otfmm import BatchSolver, Context
+    b = CASES[name]()
+    Lo, Lco = oracle.batch(theta, b.pool, b.items, rho=(solve == RHO))
+    sel = b.items["subgrid"]
+    c = Context(0, theta)
+    try:
+        s = BatchSolver(c, b.pool, b.items)
+        s.run(solve, "fp64_exact")
+        L, Lc = s.results()
+        np.testing.assert_array_equal(L[sel], Lo[sel])
+        np.testing.assert_array_equal(Lc[sel], Lco[sel])
+        s.run(solve, "fp64")
+        L, Lc = s.results()
+        assert scaled_err(L[sel], Lo[sel]).max() <= FP64_TOL
+        s.run(solve, "fp32_split")
+        L, Lc = s.results()
+        e = scaled_err(L[sel], Lo[sel])
+        assert e[:4].max() <= 1e-6 and e[4:].max() <= 1e-5, e
+        if solve == RHO:
+            assert scaled_err(Lc[sel], Lco[sel]).max() <= 1e-10
+    finally:
+        c.close()
