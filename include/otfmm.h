@@ -369,7 +369,10 @@ long long otfmm_count_pairs(const otfmm_context* ctx, const uint8_t* is_leaf, in
  *      not NULL, L_c[u * lc_stride + c] = component c (L_c = result); no
  *      intermediate buffer, and the caller leaves those cells alone until its
  *      wait returns.
- *   4. otfmm_aggregator_wait(ticket): blocks until the call's batch has run;
+ *   4. otfmm_aggregator_wait(ticket): blocks until the call's batch has run
+ *      (otfmm_aggregator_poll(ticket) instead returns at once: 1 once the
+ *      batch has run, 0 before, so that a task can yield to its scheduler in
+ *      between; a poll that finds the batch ready to run runs it);
  *      then L holds 20 x 512 (multipole items) or 4 x 512 (leaves) values and
  *      L_c, when not NULL, 3 x 512 (SoA), or the AoS cells are updated. A
  *      caller may have many calls submitted before it waits (as HPX tasks do).
@@ -397,6 +400,7 @@ int otfmm_aggregator_submit(otfmm_aggregator* agg, int64_t ticket, const otfmm_w
  * part: its L_c cells are set to zero, as otfmm_aggregator_submit's L_c. */
 int otfmm_aggregator_submit_aos(otfmm_aggregator* agg, int64_t ticket, const otfmm_work_item* item, double* L,
                                 int32_t l_stride, double* L_c, int32_t lc_stride);
+int otfmm_aggregator_poll(otfmm_aggregator* agg, int64_t ticket);
 int otfmm_aggregator_wait(otfmm_aggregator* agg, int64_t ticket);
 
 /* Checks a device-side error flag written by the last otfmm_batch on `stream`

@@ -577,6 +577,16 @@ int aggregated_submit(otfmm_aggregator* agg, int kind, const std::vector<Multipo
     return rc;
 }
 
+// 1 once a submitted call's batch has run (finish() then returns at once), 0
+// before, < 0 on error. Does not wait for other callers; it may run a batch
+// that is ready to run (the batch's solve time). An HPX task polls and yields
+// in between instead of blocking its worker thread in finish().
+template <class GridPtr>
+int ready(const AggregatedCall<GridPtr>& call) {
+    if (!call.agg) return OTFMM_ERR_INVALID;
+    return otfmm_aggregator_poll(call.agg, call.ticket);
+}
+
 // Waits for a submitted call's batch, then updates the grid: L += result,
 // L_c = result where the reference sets it (a grid of flat cells was updated
 // by the batch already).

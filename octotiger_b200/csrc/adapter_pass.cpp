@@ -38,7 +38,9 @@ extern "C" {
  * other nodes' tasks, so many calls per thread are in flight), the batch
  * writing the grids' cells
  * itself; mode 2: the same with SoA results that finish() adds to the grids on
- * the caller's thread; mode 0: the per-call interfaces on
+ * the caller's thread; mode 3: as mode 1, but a thread polls its calls
+ * (otfmm_octotiger::ready) and yields in between instead of blocking in
+ * finish(), as an HPX task would; mode 0: the per-call interfaces on
  * the context (one blocking host-buffer call per node). seconds[p] = wall time of pass p (all threads, first call to
  * last return). After the last pass L_out[n][20][512] / Lc_out[n][3][512]
  * hold the grids of the work items' subgrids (zero elsewhere). Returns the
@@ -49,7 +51,7 @@ int otfmm_adapter_pass(otfmm_context* ctx, int32_t n_sub, const double* M, const
                        int32_t idle_us, int32_t passes, int32_t calls_in_flight, double* L_out, double* Lc_out,
                        double* seconds) {
     if (!ctx || !M || !com || !mon || !is_leaf || !items || !L_out || !Lc_out || !seconds || n_sub < 1 ||
-        n_items < 1 || threads < 1 || passes < 1 || mode < 0 || mode > 2 || calls_in_flight < 1)
+        n_items < 1 || threads < 1 || passes < 1 || mode < 0 || mode > 3 || calls_in_flight < 1)
         return OTFMM_ERR_INVALID;
     for (int i = 0; i < n_items; ++i)
         if (items[i].subgrid < 0 || items[i].subgrid >= n_sub) return OTFMM_ERR_INVALID;
@@ -88,7 +90,7 @@ int otfmm_adapter_pass(otfmm_context* ctx, int32_t n_sub, const double* M, const
         com_ptrs[i] = {nodes[items[i].subgrid].com};
     }
     otfmm_aggregator* agg = nullptr;
-    if (mode == 1 || mode == 2) {
+    if (mode >= 1) {
         const int rc = otfmm_aggregator_create(ctx, max_subgrids, max_items, idle_us, gsolve_type, precision, &agg);
         if (rc != OTFMM_OK) return rc;
     }
@@ -111,7 +113,7 @@ int otfmm_adapter_pass(otfmm_context* ctx, int32_t n_sub, const double* M, const
         // other
         auto agg_worker = [&]() {
             std::vector<otfmm_octotiger::AggregatedCall<grid*>> calls(calls_in_flight);
-            for (auto& c : calls) c.in_place = (mode == 1);
+            for (auto& c : calls) c.in_place = (mode != 2);
             std::vector<int> ok(calls_in_flight);
             for (;;) {
                 const int i0 = next.fetch_add(calls_in_flight);
@@ -132,6 +134,16 @@ int otfmm_adapter_pass(otfmm_context* ctx, int32_t n_sub, const double* M, const
                             w.kind == OTFMM_KIND_M2L_ROOT, calls[i - i0]);
                     note(rc);
                     ok[i - i0] = rc == OTFMM_OK;
+                }
+                if (mode == 3) {
+                    // poll the calls in order, yielding while one is not ready (the
+                    // calls after it are in the same batch or a later one)
+                    for (int i = i0; i < i1; ++i) {
+                        if (!ok[i - i0]) continue;
+                        while (otfmm_octotiger::ready(calls[i - i0]) == 0) std::this_thread::yield();
+                        note(otfmm_octotiger::finish(calls[i - i0]));   // returns at once (or the error)
+                        ok[i - i0] = 0;
+                    }
                 }
                 for (int i = i0; i < i1; ++i)
                     if (ok[i - i0]) note(otfmm_octotiger::finish(calls[i - i0]));

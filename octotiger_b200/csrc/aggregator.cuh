@@ -445,6 +445,23 @@ int otfmm_aggregator_submit_aos(otfmm_aggregator* a, int64_t ticket, const otfmm
     return agg_submit(a, ticket, item, L, l_stride, L_c, L_c ? lc_stride : 0);
 }
 
+int otfmm_aggregator_poll(otfmm_aggregator* a, int64_t ticket) {
+    if (!a) return fail(OTFMM_ERR_INVALID, "NULL argument");
+    const long long e = ticket >> 1;
+    const int k = (int)(ticket & 1);
+    otfmm_aggregator::Batch& b = a->b[k];
+    if (b.done_epoch.load(std::memory_order_acquire) >= e) return 1;
+    // no lock while the batch runs on another thread: pollers spin on this
+    if (b.epoch.load(std::memory_order_relaxed) == e && b.state.load(std::memory_order_relaxed) == otfmm_aggregator::RUNNING)
+        return 0;
+    std::unique_lock<AggLock> lock(a->mu);
+    if (b.done_epoch >= e) return 1;
+    if (b.epoch != e) return fail(OTFMM_ERR_INVALID, "unknown ticket");
+    // a batch that can run now runs on this thread, as in a wait
+    agg_try_run(a, k, lock);
+    return b.done_epoch >= e ? 1 : 0;
+}
+
 int otfmm_aggregator_wait(otfmm_aggregator* a, int64_t ticket) {
     if (!a) return fail(OTFMM_ERR_INVALID, "NULL argument");
     const long long e = ticket >> 1;

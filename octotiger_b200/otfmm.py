@@ -615,7 +615,8 @@ PASS_LIB_PATH = Path(__file__).resolve().parent / "libotfmm_adapter_pass.so"
 
 def adapter_pass(ctx: Context, pool: SubgridPool, items: np.ndarray, gsolve_type=RHO, precision=FP64,
                  aggregate: bool = True, threads: int = 8, max_subgrids: int = 2048, max_items: int = 1024,
-                 idle_us: int = 200, passes: int = 1, in_place: bool = True, calls_in_flight: int = 64):
+                 idle_us: int = 200, passes: int = 1, in_place: bool = True, calls_in_flight: int = 64,
+                 poll: bool = False):
     """One or more passes over a work list through the C++ drop-in adapter,
     driven like node_server::compute_fmm (one call per node from `threads`
     host threads, AoS inputs; libotfmm_adapter_pass.so). aggregate: the
@@ -624,7 +625,9 @@ def adapter_pass(ctx: Context, pool: SubgridPool, items: np.ndarray, gsolve_type
     itself (otfmm_aggregator_submit_aos), else finish() applies SoA results.
     calls_in_flight: aggregated calls a thread submits before it finishes
     them (HPX suspends a task that waits on its future and runs other nodes'
-    tasks, so a solve's calls can all be in flight at once). Returns (L [n,20,512], L_c [n,3,512], seconds per pass)."""
+    tasks, so a solve's calls can all be in flight at once). poll: threads
+    poll their calls (otfmm_octotiger::ready) and yield in between instead of
+    blocking in finish() (results in place). Returns (L [n,20,512], L_c [n,3,512], seconds per pass)."""
     load_library()
     if not PASS_LIB_PATH.exists():
         raise FileNotFoundError(f"{PASS_LIB_PATH} not built: run `python -m octotiger_b200.build`")
@@ -641,7 +644,7 @@ def adapter_pass(ctx: Context, pool: SubgridPool, items: np.ndarray, gsolve_type
     sec = np.zeros(passes)
     _check(lib.otfmm_adapter_pass(ctx.handle, pool.n, M.ctypes.data, com.ctypes.data, mon.ctypes.data,
                                   leaf.ctypes.data, items.ctypes.data, len(items), int(gsolve_type),
-                                  precision_code(precision), (1 if in_place else 2) if aggregate else 0, threads, max_subgrids, max_items,
+                                  precision_code(precision), (3 if poll else 1 if in_place else 2) if aggregate else 0, threads, max_subgrids, max_items,
                                   idle_us, passes, calls_in_flight, L.ctypes.data, Lc.ctypes.data, sec.ctypes.data))
     return L, Lc, sec
 

@@ -75,6 +75,19 @@ def test_aggregated_adapter_exact_matches_oracle(ctx, oracle, tree, solve, max_s
     assert (sec > 0).all()
 
 
+@pytest.mark.parametrize("max_subgrids,in_flight", [(64, 16), (4096, 512)])
+def test_aggregated_adapter_polling(ctx, oracle, tree, max_subgrids, in_flight):
+    """Threads poll their calls (otfmm_octotiger::ready) and yield instead of
+    blocking in finish(); a poll runs a batch that is ready to run."""
+    from octotiger_b200.otfmm import adapter_pass
+    L, Lc, _ = adapter_pass(ctx, tree.pool, tree.items, RHO, "fp64_exact", aggregate=True, threads=8,
+                            max_subgrids=max_subgrids, max_items=max_subgrids // 2, passes=2,
+                            calls_in_flight=in_flight, poll=True)
+    Le, Lce = expected(tree, oracle, RHO)
+    np.testing.assert_array_equal(L, Le)
+    np.testing.assert_array_equal(Lc, Lce)
+
+
 def test_aggregated_adapter_fast_and_split(ctx, oracle, tree):
     from octotiger_b200.otfmm import adapter_pass
     Le, Lce = expected(tree, oracle, RHO)
