@@ -378,8 +378,8 @@ long long otfmm_count_pairs(const otfmm_context* ctx, const uint8_t* is_leaf, in
  *      caller may have many calls submitted before it waits (as HPX tasks do).
  * A batch runs when it is full and all its reserved calls have submitted, or
  * when it has been idle for idle_us with no call between reserve and submit;
- * a caller in otfmm_aggregator_wait (or in a reserve that finds both batch
- * buffers busy) runs it. All calls of an aggregator share its solve type and
+ * a caller in otfmm_aggregator_wait or _poll (or in a reserve that finds both
+ * batch buffers busy) runs it. All calls of an aggregator share its solve type and
  * precision. Thread-safe; no context-wide lock is held while callers copy their
  * data. Destroy only with no call in flight. */
 #define OTFMM_AGG_M 1
