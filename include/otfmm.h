@@ -29,7 +29,10 @@
  *     (multipole_kernel_interface.cpp:107-158); here the caller decides.
  *   - Thread-safe: a context may be used from several host threads; each call
  *     is enqueued on the stream the caller passes (cudaStream_t as void*,
- *     NULL = legacy default stream).
+ *     NULL = the calling thread's default stream: the library is built with
+ *     per-thread default streams, which synchronise with the legacy default
+ *     stream as any blocking stream does, and calls from several threads on
+ *     their own default streams run concurrently).
  *   - Layouts: "SoA" is the reference's per-subgrid kernel layout
  *     (mon[5832], M[20][5851], com[3][5851] over the 18^3 padded halo;
  *     L[20][531], L_c[3][531]); "pool" is M[n][20][512], com[n][3][512],

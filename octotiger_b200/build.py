@@ -62,7 +62,8 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         build_adapter_pass()
         return LIB
     cmd = [_nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
-           "--expt-relaxed-constexpr", "-I", str(ROOT / "include"), "-o", str(LIB) + ".tmp", *map(str, SOURCES)]
+           "--expt-relaxed-constexpr", "--default-stream", "per-thread", "-I", str(ROOT / "include"), "-o",
+           str(LIB) + ".tmp", *map(str, SOURCES)]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     res = subprocess.run(cmd, capture_output=True, text=True)

@@ -31,6 +31,8 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/otfmm.h"
@@ -252,7 +254,9 @@ struct otfmm_context {
     double* d_four = nullptr;
     uint8_t* d_phase = nullptr;
     int* d_err = nullptr;
-    double* d_soa_scratch = nullptr;   // host-buffer path staging
+    // staging of otfmm_m2l_soa_host, one buffer per calling thread, so that
+    // concurrent calls (each on its thread's default stream) do not serialise
+    std::unordered_map<std::thread::id, double*> soa_scratch;
     int* d_lists = nullptr;            // batched work lists (grown on demand)
     long long lists_gen = 0;           // times d_lists was reallocated (a host plan binds one generation)
     int list_capacity = 0;
@@ -886,7 +890,7 @@ int otfmm_destroy(otfmm_context* ctx) {
     cudaFree(ctx->d_four);
     cudaFree(ctx->d_phase);
     cudaFree(ctx->d_err);
-    cudaFree(ctx->d_soa_scratch);
+    for (auto& kv : ctx->soa_scratch) cudaFree(kv.second);
     cudaFree(ctx->d_lists);
     delete ctx;
     return OTFMM_OK;
@@ -941,11 +945,21 @@ int otfmm_m2l_soa(otfmm_context* ctx, const double* mon, const double* M, const 
 int otfmm_m2l_soa_host(otfmm_context* ctx, const double* mon, const double* M, const double* com, double* L,
                        double* L_c, int gsolve_type, int use_root_stencil, int precision) {
     if (!ctx || !M || !com || !L) return fail(OTFMM_ERR_INVALID, "NULL argument");
-    std::lock_guard<std::mutex> lock(ctx->mu);
     DeviceGuard g(ctx->device);
     const size_t n_in = ENTRIES + 20 * (size_t)CL + 3 * (size_t)CL, n_out = 23 * (size_t)CLU;
-    if (!ctx->d_soa_scratch) OT_CUDA(cudaMalloc(&ctx->d_soa_scratch, sizeof(double) * (n_in + n_out)));
-    double* d_mon = ctx->d_soa_scratch;
+    const std::thread::id self = std::this_thread::get_id();
+    double* scratch = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(ctx->mu);
+        auto it = ctx->soa_scratch.find(self);
+        if (it != ctx->soa_scratch.end()) scratch = it->second;
+    }
+    if (!scratch) {
+        OT_CUDA(cudaMalloc(&scratch, sizeof(double) * (n_in + n_out)));
+        std::lock_guard<std::mutex> lock(ctx->mu);
+        ctx->soa_scratch[self] = scratch;
+    }
+    double* d_mon = scratch;
     double* d_M = d_mon + ENTRIES;
     double* d_com = d_M + 20 * CL;
     double* d_L = d_com + 3 * CL;
