@@ -190,6 +190,29 @@ int main() {
         g->ilist_n_bnd[d] = bad;
         if (stage_all(own, own_x, own_m, nbs, g, got) != OTFMM_ERR_INVALID) fail("out-of-band cell accepted");
     }
+    // flat_cells: the grid cells the aggregated calls write in place are K
+    // contiguous doubles reached through operator[]; anything else is refused
+    {
+        std::vector<multipole> L(512);
+        if (oo::flat_cells<20>(L) != &L[0][0]) fail("taylor<4>-like cells not flat");
+        std::vector<space_vector> Lc(512);
+        if (oo::flat_cells<3>(Lc) != &Lc[0][0]) fail("space_vector cells not flat");
+        struct Tagged {
+            double v[20];
+            int tag;
+            double& operator[](int i) { return v[i]; }
+        };
+        std::vector<Tagged> T(512);
+        if (oo::flat_cells<20>(T) != nullptr) fail("cells with another member taken as flat");
+        struct Proxy {
+            std::array<double, 20> v;
+            double operator[](int i) const { return v[i]; }
+        };
+        std::vector<Proxy> P(512);
+        if (oo::flat_cells<20>(P) != nullptr) fail("cells read by value taken as flat");
+        std::vector<multipole> few(100);
+        if (oo::flat_cells<20>(few) != nullptr) fail("fewer than 512 cells taken as flat");
+    }
     std::printf("staging ok\n");
     return 0;
 }

@@ -2,7 +2,8 @@
 compressed neighbour payloads (the cells of grid::get_ilist_n_bnd(dir), as
 grid::get_gravity_boundary packs remote neighbours) expand to the same
 buffers as full-size payloads, left-out cells read as update_input's zeros,
-and malformed lists are rejected (tests/cpp/staging_test.cpp)."""
+and malformed lists are rejected (tests/cpp/staging_test.cpp). Also: which
+grid cell types the aggregated calls write in place (flat_cells)."""
 from __future__ import annotations
 
 import subprocess
