@@ -371,7 +371,8 @@ long long otfmm_count_pairs(const otfmm_context* ctx, const uint8_t* is_leaf, in
  *      component c of cell u (the reference's L += result) and, when L_c is
  *      not NULL, L_c[u * lc_stride + c] = component c (L_c = result); no
  *      intermediate buffer, and the caller leaves those cells alone until its
- *      wait returns.
+ *      wait returns (two calls in flight must not name the same cells: the
+ *      results of one batch are written by several threads).
  *   4. otfmm_aggregator_wait(ticket): blocks until the call's batch has run
  *      (otfmm_aggregator_poll(ticket) instead returns at once: 1 once the
  *      batch has run, 0 before, so that a task can yield to its scheduler in
